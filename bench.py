@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""bench.py -- DA cycles/s of the LBM2D-LETKF forecast-and-assimilate cycle on B200.
+
+Workload (the DA_LETKF OSSE at M=16, 256^2): 16 members resident on one GPU, D2Q9
+BGK + Smagorinsky (Cs 0.1, tau 0.51), forcing as config.h (kf 4, fkf 5.6), IC
+E(k) ~ k^4 exp(-2 (k/4)^2) at rms 0.05 lattice (1.0 physical), ensemble = nature IC
++ 10% random-phase perturbations; observations (u, v, rho) every 4th point
+(4,096 sites) with sigma_u = 0.1 x rms velocity; Gaspari-Cohn R-localisation over
+a 4-cell radius (DA_XYPRUNE=4, LETKF_RLOC_LEN=1, 75 observations per point);
+inflation 1.1; one analysis every 100 steps (DAPRUNE=5 x iiter=20).
+
+One bench "step" = one DA cycle = the LETKF analysis + 100 LBM steps.
+
+  value     cycles/s with the observations already resident on the device
+            (lbl_cycle_async with NULL observation pointers), device time from
+            CUDA events on the engine's stream, max over ranks
+  e2e       the same through the public C ABI with host buffers every cycle:
+            observation fields copied in (compacted into pinned staging, H2D),
+            cycle graph, and the forecast RMSE of the ensemble-mean velocity
+            against the nature run read back (lbl_rmse_uv)
+  roofline  the fused stream-collide kernel (the dominant kernel): 72 B per
+            lattice update (9 float loads + 9 float stores) x M*nx*ny per launch
+            / the average launch time from CUDA events (lbl_profile_step)
+  cpu_baseline  the FP64 OpenMP oracle on this host's cores, bounded sample
+
+`--impl reference` times the reference's path on the host cores.  The reference
+has no CPU implementation (its only backend is CUDA + MPI + cuBLAS/cuSOLVER), so
+its arm is the FP64 OpenMP restatement of the reference's path in oracle/.
+
+Multi-GPU: replicas only (one independent experiment per GPU, no collective on
+the data path); `value` is the cycles of all ranks / the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "lbm2d-letkf_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+NX = 256
+M = 16
+STEPS_PER_CYCLE = 100
+P_OBS = 4
+METRIC = "DA cycles/s"
+UNIT = "cycles/s"
+WORKLOAD = ("DA_LETKF OSSE, M=16 members resident on 1 GPU, 256x256 D2Q9 BGK+Smagorinsky (Cs 0.1, tau 0.51), "
+            "obs (u,v,rho) every 4th point (4096 sites), GC localisation radius 4 cells (75 obs/point), "
+            "inflation 1.1, 100 LBM steps + 1 LETKF analysis per cycle, FP32")
+
+
+def workload_config(lbl, mode="DA_LETKF", n_ens=M):
+    return lbl.config_default(
+        mode, NX, n_ens, da_xyprune=P_OBS, letkf_rloc_len=1, letkf_covinf=1.1, obs_error_u=0.1,
+        obs_error_rho=0.01, daprune=5, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP, ic_amp=1.0,
+        ens_init=lbl.ENS_PERTURBED, ens_perturb=0.1)
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per stream-collide launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "lbm_step_kernel_256x256_M16.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            out, _ = self.proc.communicate(timeout=10)
+            self.lines = [l for l in out.strip().split("\n") if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            p = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(p[0]))
+                mx.append(float(p[1]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, p[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_observations(lbl, n_cycles, seed=2024):
+    """Nature run (member id 0) and its observations at the end of every cycle."""
+    nat = lbl.Ensemble(workload_config(lbl, "NATURE", 1))
+    nat.init(0)
+    rng = np.random.default_rng(seed)
+    obs, truth = [], []
+    nsite = np.ones((NX, NX), bool)
+    nsite[::P_OBS, ::P_OBS] = False
+    for _ in range(n_cycles):
+        nat.update(0, STEPS_PER_CYCLE)
+        r, u, v, _ = nat.get_fields(0)
+        ro = (r + 0.01 * rng.standard_normal(r.shape)).astype(np.float32)
+        uo = (u + 0.1 * rng.standard_normal(u.shape)).astype(np.float32)
+        vo = (v + 0.1 * rng.standard_normal(v.shape)).astype(np.float32)
+        for a in (ro, uo, vo):
+            a[nsite] = np.nan
+        obs.append((ro, uo, vo))
+        truth.append((u.copy(), v.copy()))
+    nat.close()
+    return obs, truth
+
+
+def cpu_baseline_sample(lbl, oracle, obs, threads=None):
+    """Oracle (FP64, OpenMP, this host's cores) on a bounded sample of one cycle:
+    4 LBM steps of the whole 16-member ensemble + the analysis of 16 of the 256 rows,
+    scaled to a full cycle (25x the steps, 16x the rows)."""
+    nthreads = oracle.set_threads(threads or os.cpu_count())
+    o = oracle.Oracle(workload_config(lbl))
+    o.init(0)
+    rng = np.random.default_rng(5)
+    o.step(1, rng.normal(0, 0.84, 4 * 29).astype(np.float32))  # warm caches / page in
+    t0 = time.perf_counter()
+    o.step(4, rng.normal(0, 0.84, 4 * 29 * 4).astype(np.float32))
+    t_steps = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    o.assimilate_rows(*obs, 120, 136)
+    t_ana = time.perf_counter() - t0
+    o.close()
+    cycle = 25 * t_steps + 16 * t_ana
+    return {"value": 1.0 / cycle, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": "4 LBM steps of 16x256^2 + LETKF of 16/256 rows, scaled x25 / x16 to one cycle",
+            "lbm_glups": 4 * M * NX * NX / t_steps / 1e9, "analysis_s_per_cycle": 16 * t_ana}
+
+
+def init_dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return None, 0, 1, int(os.environ.get("LOCAL_RANK", "0"))
+    import datetime
+    import torch
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist, dist.get_rank(), ws, local
+
+
+def reduce_max(dist, x, device):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def run_engine(args, dist, rank, world, device):
+    import lbl
+    import oracle
+    K, W = args.steps, args.warmup
+    obs, truth = make_observations(lbl, W + K + 1)
+    ens = lbl.Ensemble(workload_config(lbl), device=device)
+    ens.init(0)
+    T = STEPS_PER_CYCLE
+    # first cycle has no analysis (t = 0): bring the ensemble to t = 100
+    ens.cycle_async(0, None, None, None, T)
+    ens.sync()
+
+    # ---- value: resident observations --------------------------------------------
+    clk = ClockSampler(device).__enter__()  # sampled from warm-up to the end of the timed region
+    ens.cycle_async(T, *obs[0], T)  # uploads the observations once
+    for c in range(1, W):
+        ens.cycle_async((c + 1) * T, None, None, None, T)
+    ens.sync()
+    barrier(dist)
+    if True:
+        ens.event_record(0)
+        for c in range(K):
+            ens.cycle_async((W + c + 1) * T, None, None, None, T)
+        ens.event_record(1)
+        ms = ens.event_elapsed(0, 1)
+        ens.sync()
+    clk.__exit__(None, None, None)
+    ms_max = reduce_max(dist, ms, device)
+    value = world * K / (ms_max / 1e3)
+    stats = ens.letkf_stats()
+
+    # ---- e2e: host observations in, RMSE out, every cycle -----------------------------
+    e2e_ens = lbl.Ensemble(workload_config(lbl), device=device)
+    e2e_ens.init(0)
+    e2e_ens.cycle_async(0, None, None, None, T)
+    for c in range(W):
+        e2e_ens.cycle_async((c + 1) * T, *obs[c], T)
+        e2e_ens.rmse_uv(*truth[c + 1])
+    e2e_ens.sync()
+    barrier(dist)
+    rmse = []
+    e2e_ens.event_record(0)
+    for c in range(W, W + K):
+        e2e_ens.cycle_async((c + 1) * T, *obs[c], T)
+        rmse.append(e2e_ens.rmse_uv(*truth[c + 1]))
+    e2e_ens.event_record(1)
+    ms_e2e = reduce_max(dist, e2e_ens.event_elapsed(0, 1), device)
+    e2e_value = world * K / (ms_e2e / 1e3)
+    nsites = (NX // P_OBS) ** 2
+    h2d = 3 * nsites * 4 + 2 * NX * NX * 4 + 4 * T
+    d2h = 8
+
+    # ---- roofline of the stream-collide kernel ------------------------------------------
+    ens.profile_step(20)
+    ms_step = ens.profile_step(200)
+    bytes_per_launch = 72.0 * M * NX * NX
+    achieved = bytes_per_launch / (ms_step * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = ncu_traffic()
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded nature run + Gaussian observation noise)",
+        "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "working set 221 MB (f ping-pong 151 MB + forcing 67 MB) > 126 MB L2",
+                   "observations": "value leg reuses the resident observations; e2e uploads them every cycle"},
+        "glups": M * NX * NX * T * K * world / (ms_max / 1e3) / 1e9,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "forecast_rmse_uv_last": rmse[-1] if rmse else None},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "lbm_step_kernel", "ms_per_launch": ms_step,
+                     "algorithmic_bytes_per_launch": bytes_per_launch, "peak_kind": peak_kind},
+        "gpu_launches": K * (T + 3),
+        "letkf": stats,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(lbl, oracle, obs[0])
+    ens.close()
+    e2e_ens.close()
+    return line
+
+
+def run_reference(args, rank, world):
+    """The reference's path on the host cores: FP64 OpenMP restatement (oracle/)."""
+    import lbl
+    import oracle
+    if rank != 0:
+        return None
+    nthreads = oracle.set_threads(os.cpu_count())
+    o = oracle.Oracle(workload_config(lbl))
+    o.init(0)
+    rng = np.random.default_rng(9)
+    obs_nan = np.full((NX, NX), np.nan, np.float32)
+    ro, uo, vo = obs_nan.copy(), obs_nan.copy(), obs_nan.copy()
+    ro[::P_OBS, ::P_OBS] = 1.0 + 0.01 * rng.standard_normal((NX // P_OBS, NX // P_OBS))
+    uo[::P_OBS, ::P_OBS] = rng.standard_normal((NX // P_OBS, NX // P_OBS))
+    vo[::P_OBS, ::P_OBS] = rng.standard_normal((NX // P_OBS, NX // P_OBS))
+
+    def one():
+        t0 = time.perf_counter()
+        o.step(2, rng.normal(0, 0.84, 4 * 29 * 2).astype(np.float32))
+        t1 = time.perf_counter()
+        o.assimilate_rows(ro, uo, vo, 0, 8)
+        t2 = time.perf_counter()
+        return 50 * (t1 - t0) + 32 * (t2 - t1)  # scaled to 100 steps + 256 rows
+
+    for _ in range(args.warmup):
+        one()
+    est = [one() for _ in range(args.steps)]
+    value = len(est) / sum(est)
+    o.close()
+    sample = "2 LBM steps of 16x256^2 + LETKF of 8/256 rows per step, scaled x50 / x32 to one cycle"
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "backend": "FP64 OpenMP CPU restatement of the reference path"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        # the CPU reference arm runs on rank 0 only; other ranks exit without work
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    dist, rank, world, device = init_dist()
+    try:
+        line = run_engine(args, dist, rank, world, device)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,198 @@
+/*
+ * lbl.h -- C ABI of liblbl, the B200-native forecast-and-assimilate engine
+ * (D2Q9 BGK + Smagorinsky lattice Boltzmann ensemble + LETKF analysis).
+ *
+ * One context (lbl_ctx) holds a whole ensemble of M members resident on one GPU
+ * as a batch dimension.  It replaces the reference's one-MPI-rank-per-member
+ * design: the reference's entry points for this path are the C++ functions
+ *
+ *   void update(data&, int t)                                  src/lbm.h:16-29
+ *   void DataAssimilator::assimilate(data&, const mpi&, int t)  src/assimilate.h:54-68
+ *   void output(const data&, util::mpi, int t)                  src/io.h:7, src/io.cu:22
+ *   data::data(int ensemble_id)                                 src/data.h:55, src/data.cu:25-303
+ *
+ * and the run-time knobs are the compile-time macros of src/config.h and
+ * config/makefile.macro.in, which lbl_config mirrors field by field.
+ *
+ * Conventions
+ *   - every function returns int: 0 = LBL_OK, negative = error;
+ *     lbl_last_error(ctx) gives the message of the last failure on that ctx;
+ *   - no C++ exception crosses this boundary;
+ *   - caller buffers are plain host pointers borrowed for the duration of the call;
+ *   - a ctx owns all device memory, its stream and its CUDA graphs; one ctx per
+ *     host thread; calls are synchronous on return unless named *_async.
+ *   - field arrays are float32, nx*ny values, i (x) fastest, like the
+ *     reference's ij(i,j) = i + nx*j (src/config.h:210).  Populations f are
+ *     [q][y][x] per member (src/config.h:212, ijq = ij + nx*ny*q).
+ */
+#ifndef LBL_H_
+#define LBL_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBL_ABI_VERSION 1
+
+/* status codes */
+#define LBL_OK              0
+#define LBL_ERR_ARG        -1   /* bad argument / configuration value          */
+#define LBL_ERR_CUDA       -2   /* CUDA runtime error                          */
+#define LBL_ERR_CURAND     -3   /* cuRAND error                                */
+#define LBL_ERR_IO         -4   /* file could not be read / written            */
+#define LBL_ERR_NAN        -5   /* NaN detected (reference: io.cu:79-83,       */
+                                /*  letkf_solver.h:352-364)                    */
+#define LBL_ERR_STATE      -6   /* call out of order (e.g. update before init) */
+#define LBL_ERR_NOMEM      -7   /* device allocation failed                    */
+#define LBL_ERR_UNSUPPORTED -8  /* configuration not supported by this build   */
+#define LBL_ERR_NOCONV     -9   /* Jacobi eigensolver hit its sweep limit      */
+
+/* run modes: the reference's -DTEST=<mode> (src/config.h:28-108) */
+#define LBL_MODE_NATURE   0
+#define LBL_MODE_OBSERVE  1
+#define LBL_MODE_DA_LETKF 2
+
+/* initial condition kinds */
+#define LBL_IC_REFERENCE  0  /* src/data.cu:53-120: band exp(-(k-kf)^2/5), |k-kf|<=10, max|u| = ic_amp */
+#define LBL_IC_K4EXP      1  /* E(k) ~ k^4 exp(-2 (k/4)^2), rms |u| = ic_amp (physical units)          */
+
+/* initial ensemble kinds */
+#define LBL_ENS_INDEPENDENT 0 /* member k: own random phases, seed = k + ofs + 334 (src/data.cu:31-35) */
+#define LBL_ENS_PERTURBED   1 /* member k: nature IC + independent random-phase field at ens_perturb amplitude */
+
+/* timer selectors for lbl_timer_csv */
+#define LBL_TIMER_MAIN  0    /* io/elapsed_time_rank%d.csv       (src/main.cu:143)  */
+#define LBL_TIMER_LETKF 1    /* io/letkf_elapsed_time_rank%d.csv (src/main.cu:145)  */
+
+typedef struct lbl_config {
+    int32_t abi_version;     /* must be LBL_ABI_VERSION                                   */
+    int32_t mode;            /* LBL_MODE_*                                                */
+    int32_t nx, ny;          /* grid; reference NX = 64*SCALER, square (config.h:88-89)   */
+    int32_t n_ens;           /* M, ensemble members (reference: MPI ranks)                */
+    int32_t iiter;           /* steps per output slot; reference 5*SCALER (config.h:136)  */
+    int32_t ioprune;         /* IOPRUNE (config.h:90-92)                                  */
+    int32_t daprune;         /* DAPRUNE (config.h:55-57)                                  */
+    int32_t da_xyprune;      /* DA_XYPRUNE, observation spacing p (config.h:59-61)        */
+    int32_t letkf_rloc_len;  /* LETKF_RLOC_LEN; 0 = macro undefined (letkf.cu:45-55)      */
+    int32_t iter_main;       /* iiter*2000 in the reference (config.h:144)                */
+    int32_t spinup;          /* spin-up steps; reference 100000*iiter (config.h:139)      */
+    int32_t ic_kind;         /* LBL_IC_*                                                  */
+    int32_t ens_init;        /* LBL_ENS_*                                                 */
+    int32_t compat_stale_v;  /* 1: after an analysis v is not refreshed (letkf.cu:340-355) */
+    int32_t jacobi_max_sweeps; /* reference syevj: 100 (cu_matrix_eigensolver_wrapper.hpp:193) */
+    int32_t write_mat;       /* reserved (LETKF matrix dumps); must be 0                  */
+    int32_t pad0;
+    double letkf_covinf;     /* LETKF_COVINF, multiplicative inflation beta (config.h:48-50) */
+    double obs_error_rho;    /* OBS_ERROR_RHO (config.h:190-202)                          */
+    double obs_error_u;      /* OBS_ERROR_U                                               */
+    double cs;               /* Smagorinsky constant; reference hard-codes 0.2 (lbm.cu:59) */
+    double nu;               /* molecular viscosity; reference 1e-4 (config.h:157)        */
+    double tau;              /* if > 0 overrides nu: nu = (tau-0.5)*c*c*dt/3              */
+    double cfl;              /* 0.05 (config.h:153)                                       */
+    double rho_ref;          /* 1    (config.h:156)                                       */
+    double u_ref;            /* 1    (config.h:182)                                       */
+    double h_ref;            /* 2*pi (config.h:158)                                       */
+    double kf;               /* forcing wavenumber 4 (config.h:161)                       */
+    double fkf;              /* forcing amplitude 5.6 at nx=256 (config.h:171)            */
+    double friction_rate;    /* 5e-4 (config.h:180)                                       */
+    double ic_amp;           /* 0.01 = reference p_amp (data.cu:53)                       */
+    double ens_perturb;      /* amplitude ratio for LBL_ENS_PERTURBED                     */
+    double jacobi_tol;       /* reference syevj: 1e-6 (cu_matrix_eigensolver_wrapper.hpp:192) */
+    uint64_t force_seed;     /* cuRAND MTGP32 seed, 1991 (data.cu:294)                    */
+    uint64_t obs_seed;       /* OBSERVE noise engine seed 334 (io.cu:321)                 */
+} lbl_config;
+
+typedef struct lbl_ctx lbl_ctx;
+
+/* Fill *cfg with the reference's defaults for a run mode at grid nx (= 64*SCALER)
+ * and ensemble size n_ens: config.h with SCALER = nx/64, LES on, FORCE_TURB on.
+ * OBS_ERROR_* have no default in the reference (config.h:195 #error); they are
+ * set to the values of run/jserr:146-147 (rho 0.01, u 0.1). */
+int lbl_config_default(lbl_config* cfg, int mode, int nx, int n_ens);
+
+/* Create a context on CUDA device `device`.  Replaces data(rank+ofs) allocation
+ * plus DataAssimilator(mpi) (main.cu:58-61).  No initial condition yet. */
+int lbl_create(const lbl_config* cfg, int device, lbl_ctx** out);
+int lbl_destroy(lbl_ctx* ctx);
+const char* lbl_last_error(const lbl_ctx* ctx);   /* never NULL */
+const char* lbl_version(void);
+
+/* Initial condition of every member and forcing initialisation.
+ * ens_offset is main.cu's argv[1] (main.cu:42-45): member k uses ensemble id
+ * k + ens_offset (seed +334 in DA_LETKF, data.cu:31-35).
+ * Replaces stdata::init_lbm (data.cu:25-141) and init_force/init_forces
+ * (data.cu:143-237), including the two update_forces calls made at init. */
+int lbl_init(lbl_ctx* ctx, int ens_offset);
+
+/* nsteps LBM steps of every member: update(dat, t0), ..., update(dat, t0+nsteps-1)
+ * (lbm.h:16-29: forcing refresh, pull streaming + macros, Smagorinsky, BGK+force,
+ * swap).  t is accepted for interface parity; the reference ignores it. */
+int lbl_update(lbl_ctx* ctx, int t0, int nsteps);
+int lbl_update_async(lbl_ctx* ctx, int t0, int nsteps);
+
+/* One LETKF analysis at time t, observations given as host arrays (nx*ny each,
+ * NaN off the observation lattice, like io/observed/ens0000/{rho,u,v}_step*.dat).
+ * Replaces DataAssimilator::assimilate -> assimilate_letkf_uv (letkf.cu:120-360),
+ * including its `(t/iiter) % daprune` gate: returns LBL_OK without work off-cycle. */
+int lbl_assimilate(lbl_ctx* ctx, int t, const float* rho_o, const float* u_o, const float* v_o);
+int lbl_assimilate_async(lbl_ctx* ctx, int t, const float* rho_o, const float* u_o, const float* v_o);
+/* Same, reading io/observed/ens0000/{rho,u,v}_step%010d.dat under `io_prefix`
+ * (letkf.cu:197-220). */
+int lbl_assimilate_files(lbl_ctx* ctx, int t, const char* io_prefix);
+
+/* One forecast-and-assimilate cycle: analysis at t (if due) followed by
+ * n_fc forecast steps, launched as one CUDA graph.  NULL observation pointers
+ * reuse the observations already resident on the device from the previous call. */
+int lbl_cycle_async(lbl_ctx* ctx, int t, const float* rho_o, const float* u_o, const float* v_o, int n_fc);
+int lbl_sync(lbl_ctx* ctx);
+
+/* output(dat, mpi, t) (io.cu:22-266): writes the reference's .dat files under
+ * io_prefix for the mode (calc/, nature/, observed/, ensemble statistics).
+ * Gate `t % (iiter*ioprune) == 0` as in the reference. */
+int lbl_output(lbl_ctx* ctx, int t, const char* io_prefix);
+
+/* Field access (parity injection and inspection). */
+int lbl_get_f(lbl_ctx* ctx, int member, float* f /* 9*nx*ny */);
+int lbl_set_f(lbl_ctx* ctx, int member, const float* f);
+int lbl_get_fields(lbl_ctx* ctx, int member, float* rho, float* u, float* v, float* vor);
+int lbl_get_ens_stats(lbl_ctx* ctx, float* u_mean, float* v_mean, float* vor_mean, float* vor_std);
+int lbl_get_force(lbl_ctx* ctx, float* fx, float* fy);
+/* The 4*n_modes normals the forcing of the last step used, the mode table and
+ * the reference's buffer cursor (data.cu:239-350). */
+int lbl_get_force_state(lbl_ctx* ctx, float* randoms /* 4*n_modes */, float* kx, float* ky,
+                        float* amp, int* n_modes, int* i_rand_outdated);
+/* Observations generated by OBSERVE mode at the last output (host copies). */
+int lbl_get_observed(lbl_ctx* ctx, float* rho_o, float* u_o, float* v_o, float* vor_o);
+/* Analysis diagnostics of the last assimilate: max Jacobi sweeps, number of
+ * grid points that hit the sweep limit, NaN flag. */
+int lbl_get_letkf_stats(lbl_ctx* ctx, int* max_sweeps, int* n_noconv, int* nan_flag);
+/* FP64 domain reductions of member `member` (-1 = ensemble mean fields):
+ * kinetic energy, enstrophy, mass (src/data.cu:458-542 inspect()). */
+int lbl_get_diagnostics(lbl_ctx* ctx, int member, double* energy, double* enstrophy, double* mass);
+/* RMSE of the ensemble-mean (u,v) against host truth fields (FP64). */
+int lbl_rmse_uv(lbl_ctx* ctx, const float* u_true, const float* v_true, double* rmse);
+
+/* Profiling: n back-to-back launches of the fused stream-collide kernel on the
+ * context's stream, timed with CUDA events; *ms_per_launch = average per launch.
+ * The state advances by n steps with the last computed force field. */
+int lbl_profile_step(lbl_ctx* ctx, int n, double* ms_per_launch);
+
+/* CUDA events on the context's stream, for device-side timing by callers:
+ * slot in [0, 8).  lbl_event_elapsed waits for slot b and returns ms from a to b. */
+int lbl_event_record(lbl_ctx* ctx, int slot);
+int lbl_event_elapsed(lbl_ctx* ctx, int slot_a, int slot_b, double* ms);
+
+/* Timers: writes the "#tag,sec" CSV (util/timer.hpp:66-72) into buf.
+ * Returns the number of bytes needed (excluding NUL) or a negative status. */
+int lbl_timer_csv(lbl_ctx* ctx, int which, char* buf, size_t cap);
+int lbl_timer_clear(lbl_ctx* ctx, int which);
+/* Host-side tag timer driven by the caller (main.cu's util::timer). */
+int lbl_timer_transit(lbl_ctx* ctx, int which, const char* tag);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBL_H_ */

@@ -1,0 +1,974 @@
+// lbl_api.cu -- the C ABI of liblbl (include/lbl.h): context, initial condition,
+// forcing scheduler, forecast graphs, LETKF analysis, output and accessors.
+//
+// Host arithmetic that the reference performs on the CPU in FP32 (initial
+// condition rescale and feq, data.cu:113-141) is done here in FP32 on the host in
+// the same order, so the initial populations are bit-identical to the reference's.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "lbl_internal.h"
+
+using namespace lbl;
+
+namespace {
+
+#define LBL_CK(call)                                                                            \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                      \
+            return LBL_ERR_CUDA;                                                                \
+        }                                                                                       \
+    } while (0)
+
+#define LBL_CKR(call)                                                                           \
+    do {                                                                                        \
+        curandStatus_t e_ = (call);                                                             \
+        if (e_ != CURAND_STATUS_SUCCESS) {                                                      \
+            ctx->err = std::string(#call) + ": curand status " + std::to_string(int(e_));        \
+            return LBL_ERR_CURAND;                                                              \
+        }                                                                                       \
+    } while (0)
+
+#define LBL_TRY(expr)                     \
+    do {                                  \
+        int rc_ = (expr);                 \
+        if (rc_ != LBL_OK) return rc_;    \
+    } while (0)
+
+constexpr int ex_h(int q) { return (q % 3) - 1; }
+constexpr int ey_h(int q) { return (q / 3) - 1; }
+constexpr float wq_h(int q) {
+    return (ex_h(q) * ex_h(q) + ey_h(q) * ey_h(q)) == 0   ? float(4. / 9.)
+           : (ex_h(q) * ex_h(q) + ey_h(q) * ey_h(q)) == 1 ? float(1. / 9.)
+                                                           : float(1. / 36.);
+}
+
+// feq evaluated on the host in FP32 (lbm.h:31-39), as init_lbm does (data.cu:131-139)
+inline float feq_host(float rho, float u, float v, int q, float c) {
+    const float uc0 = (u * ex_h(q) + v * ey_h(q)) / c;
+    const float uu0 = (u * u + v * v) / (c * c);
+    return rho * wq_h(q) * (float(1.) + float(3.) * uc0 + float(4.5) * uc0 * uc0 - float(1.5) * uu0);
+}
+
+double gaspari_cohn(double d) {  // letkf.cu:104-109
+    if (d <= 0) return 1.0;
+    if (d <= 1) return -d * d * d * d * d / 4. + d * d * d * d / 2. + d * d * d * 5. / 8. - d * d * 5. / 3. + 1;
+    if (d <= 2) return d * d * d * d * d / 12. - d * d * d * d / 2. + d * d * d * 5. / 8. + d * d * 5. / 3. - d * 5 + 4 - 2. / 3. / d;
+    return 0.0;
+}
+
+int fail(lbl_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int set_device(lbl_ctx* ctx) {
+    LBL_CK(cudaSetDevice(ctx->device));
+    return LBL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// configuration
+// ---------------------------------------------------------------------------
+Phys derive_phys(const lbl_config& cfg) {
+    Phys P{};
+    P.nx = cfg.nx; P.ny = cfg.ny; P.M = cfg.n_ens; P.nxy = cfg.nx * cfg.ny;
+    P.c = float(cfg.u_ref) / float(cfg.cfl);                       // config.h:248 (constexpr real)
+    P.dx = float(cfg.h_ref / (cfg.ny - 1));                        // config.h:250
+    P.dt = P.dx / P.c;                                             // config.h:251
+    double nu = cfg.nu;
+    if (cfg.tau > 0) nu = (cfg.tau - 0.5) * double(P.c) * double(P.c) * double(P.dt) / 3.0;
+    P.nu = float(nu);
+    P.cs2 = P.c * P.c / 3;                                         // lbm.h:50
+    P.fr_dt = float(cfg.friction_rate) / P.dt;                     // lbm.h:52 (constexpr real)
+    P.u_ref = float(cfg.u_ref);
+    P.two_dx = 2 * P.dx;
+    P.les_k = cfg.cs * cfg.cs * double(P.dx) * double(P.dx);       // lbm.cu:59-60 (double cs)
+    P.c_d = P.c; P.dt_d = P.dt;
+    P.tau_k = 3.0 / P.c_d / P.c_d / P.dt_d;
+    P.inv_nx = 1.0f / float(cfg.nx);
+    P.inv_ny = 1.0f / float(cfg.ny);
+    return P;
+}
+
+Geo derive_geo(const lbl_config& cfg) {
+    Geo G{};
+    G.p = cfg.da_xyprune;
+    if (cfg.letkf_rloc_len <= 0) {                                 // letkf.cu:45-49
+        G.dloc = G.p - 1;
+        G.nl = G.p == 1 ? 0 : 2;
+        G.off = G.p == 1 ? 0 : 1;
+        G.nox = G.p == 1 ? 1 : 4;
+    } else {                                                       // letkf.cu:50-55
+        G.dloc = double(cfg.letkf_rloc_len) * G.p;
+        G.off = 0;
+        G.nl = cfg.letkf_rloc_len * 2;
+        G.nox = G.nl * 2 + 1;
+    }
+    G.nobs = G.nox * G.nox * 3;                                    // letkf.cu:56
+    G.nsx = cfg.nx / G.p;
+    G.nsy = cfg.ny / G.p;
+    return G;
+}
+
+int validate(const lbl_config& c, std::string& err) {
+    if (c.abi_version != LBL_ABI_VERSION) { err = "abi_version mismatch"; return LBL_ERR_ARG; }
+    if (c.mode < LBL_MODE_NATURE || c.mode > LBL_MODE_DA_LETKF) { err = "unknown mode"; return LBL_ERR_ARG; }
+    if (c.nx < 32 || c.ny < 8 || c.nx > 1024 || c.nx % 32 != 0) {
+        err = "nx must be a multiple of 32 in [32, 1024] and ny >= 8"; return LBL_ERR_ARG;
+    }
+    if (c.n_ens < 1) { err = "n_ens must be >= 1"; return LBL_ERR_ARG; }
+    if (c.iiter < 1 || c.ioprune < 1 || c.daprune < 1) { err = "iiter/ioprune/daprune must be >= 1"; return LBL_ERR_ARG; }
+    if (c.da_xyprune < 1 || c.nx % c.da_xyprune != 0 || c.ny % c.da_xyprune != 0) {
+        err = "DA_XYPRUNE must divide nx and ny (letkf.cu:30 static_assert)"; return LBL_ERR_ARG;
+    }
+    if (c.letkf_rloc_len < 0 || c.letkf_rloc_len > 8) { err = "LETKF_RLOC_LEN out of range [0, 8]"; return LBL_ERR_ARG; }
+    if (!(c.letkf_covinf > 0)) { err = "LETKF_COVINF must be > 0"; return LBL_ERR_ARG; }
+    if (!(c.obs_error_rho > 0) || !(c.obs_error_u > 0)) { err = "OBS_ERROR_RHO/OBS_ERROR_U must be > 0"; return LBL_ERR_ARG; }
+    if (!(c.cfl > 0) || !(c.u_ref > 0) || !(c.h_ref > 0)) { err = "cfl, u_ref, h_ref must be > 0"; return LBL_ERR_ARG; }
+    if (c.tau != 0 && !(c.tau > 0.5)) { err = "tau must be > 0.5 (or 0 to use nu)"; return LBL_ERR_ARG; }
+    if (c.jacobi_max_sweeps < 1 || c.jacobi_max_sweeps > 1000) { err = "jacobi_max_sweeps out of range"; return LBL_ERR_ARG; }
+    if (c.write_mat != 0) { err = "write_mat is not supported by this build"; return LBL_ERR_UNSUPPORTED; }
+    if (c.mode == LBL_MODE_DA_LETKF && !analysis_supported(c.n_ens)) {
+        err = "DA_LETKF supports 2 <= n_ens <= 32 in this build"; return LBL_ERR_UNSUPPORTED;
+    }
+    if (c.mode == LBL_MODE_DA_LETKF && analysis_smem_bytes(c.n_ens, derive_geo(c).nobs) > kAnalysisSmemLimit) {
+        err = "observation window too large for the analysis kernel's shared memory (reduce LETKF_RLOC_LEN)";
+        return LBL_ERR_UNSUPPORTED;
+    }
+    return LBL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// forcing: the reference's cursor over a buffer of 4096*n normals refilled by
+// curandGenerateNormal (data.cu:240-247).  Returns the pool offset of the 4*n
+// normals of this call.
+// ---------------------------------------------------------------------------
+int force_call(lbl_ctx* ctx, int* offset) {
+    const int n4 = 4 * ctx->n_modes;
+    ctx->i_rand_outdated += n4;
+    if (ctx->i_rand_outdated + n4 >= ctx->n_rand_buf) {
+        ctx->rand_block++;
+        const int slot = int(ctx->rand_block % ctx->pool_slots);
+        LBL_CKR(curandGenerateNormal(ctx->gen, ctx->d_pool + size_t(slot) * ctx->n_rand_buf, ctx->n_rand_buf,
+                                     0.0f, 0.84089641525f));
+        ctx->i_rand_outdated = 0;
+    }
+    *offset = int(ctx->rand_block % ctx->pool_slots) * ctx->n_rand_buf + ctx->i_rand_outdated;
+    ctx->last_sched = *offset;
+    return LBL_OK;
+}
+
+// compact the observations at the sites into [u, v, rho][site] (letkf.cu:230-269 gather)
+void compact_obs(const lbl_ctx* ctx, const float* ro, const float* uo, const float* vo, float* dst) {
+    const int ns = ctx->G.nsx * ctx->G.nsy, p = ctx->G.p, nx = ctx->P.nx;
+    for (int sj = 0; sj < ctx->G.nsy; sj++)
+        for (int si = 0; si < ctx->G.nsx; si++) {
+            const int s = si + ctx->G.nsx * sj;
+            const size_t ij = size_t(si) * p + size_t(nx) * sj * p;
+            dst[s] = uo[ij];
+            dst[ns + s] = vo[ij];
+            dst[2 * ns + s] = ro[ij];
+        }
+}
+
+// schedule the forcing of `n` consecutive calls and upload the offsets through
+// one of two pinned staging buffers (an event guards each buffer's reuse)
+int schedule_force(lbl_ctx* ctx, int n) {
+    const int b = ctx->sched_buf;
+    ctx->sched_buf ^= 1;
+    LBL_CK(cudaEventSynchronize(ctx->ev[4 + b]));
+    int* h = ctx->h_sched[b];
+    for (int s = 0; s < n; s++) LBL_TRY(force_call(ctx, &h[s]));
+    LBL_CK(cudaMemcpyAsync(ctx->d_sched, h, sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream));
+    LBL_CK(cudaEventRecord(ctx->ev[4 + b], ctx->stream));
+    return LBL_OK;
+}
+
+// stage the site observations through one of two pinned buffers and upload them
+int upload_obs(lbl_ctx* ctx, const float* ro, const float* uo, const float* vo) {
+    const int b = ctx->yo_buf;
+    ctx->yo_buf ^= 1;
+    LBL_CK(cudaEventSynchronize(ctx->ev[6 + b]));
+    compact_obs(ctx, ro, uo, vo, ctx->h_yo[b]);
+    const size_t ns = size_t(ctx->G.nsx) * ctx->G.nsy;
+    LBL_CK(cudaMemcpyAsync(ctx->d_yo, ctx->h_yo[b], sizeof(float) * 3 * ns, cudaMemcpyHostToDevice, ctx->stream));
+    LBL_CK(cudaEventRecord(ctx->ev[6 + b], ctx->stream));
+    return LBL_OK;
+}
+
+// enqueue: forcing chunk + n LBM steps starting from buffer `cur`; macros are
+// written on the last two steps (the only ones output/lbm2euler can observe).
+void enqueue_steps(lbl_ctx* ctx, int n, int cur, cudaStream_t s) {
+    launch_force_chunk(ctx, n, 0, s);
+    for (int k = 0; k < n; k++) {
+        const int src = (cur + k) & 1, dst = src ^ 1;
+        const bool mac = k >= n - 2;
+        launch_lbm_step(ctx, ctx->f[src], ctx->f[dst], ctx->d_force + size_t(k) * 2 * ctx->P.nxy,
+                        mac ? ctx->mac[dst] : nullptr, s);
+    }
+}
+
+void enqueue_analysis(lbl_ctx* ctx, int cur, cudaStream_t s) {
+    launch_obs_ensemble(ctx, ctx->f[cur], s);
+    launch_analysis(ctx, ctx->f[cur], ctx->f[cur ^ 1], ctx->mac[cur ^ 1], s);
+}
+
+// Build (once) and launch a graph.  kind: 0 = steps, 1 = cycle (analysis + steps).
+int launch_graph(lbl_ctx* ctx, int kind, int n) {
+    const long long key = ((long long)kind << 40) | ((long long)n << 1) | ctx->cur;
+    auto it = ctx->graphs.find(key);
+    if (it == ctx->graphs.end()) {
+        cudaGraph_t g = nullptr;
+        LBL_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int cur = ctx->cur;
+        if (kind == 1) { enqueue_analysis(ctx, cur, ctx->stream); cur ^= 1; }
+        if (n > 0) enqueue_steps(ctx, n, cur, ctx->stream);
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &g);
+        if (le != cudaSuccess || ee != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return fail(ctx, LBL_ERR_CUDA, std::string("graph capture failed: ") +
+                                               cudaGetErrorString(le != cudaSuccess ? le : ee));
+        }
+        cudaGraphExec_t ge;
+        const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) return fail(ctx, LBL_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+        it = ctx->graphs.emplace(key, ge).first;
+    }
+    LBL_CK(cudaGraphLaunch(it->second, ctx->stream));
+    return LBL_OK;
+}
+
+int read_stats(lbl_ctx* ctx) {
+    LBL_CK(cudaMemcpy(ctx->h_stats, ctx->d_stats, sizeof(int) * 3, cudaMemcpyDeviceToHost));
+    if (ctx->h_stats[2]) return fail(ctx, LBL_ERR_NAN, "NaN in the LETKF analysis (letkf_solver.h:352-364 sanity)");
+    return LBL_OK;
+}
+
+bool da_due(const lbl_ctx* ctx, int t) { return ((t / ctx->cfg.iiter) % ctx->cfg.daprune) == 0; }
+
+// initial velocity of one ensemble id on the device, rescaled on the host (FP32)
+int ic_member(lbl_ctx* ctx, int seed, std::vector<float>& u, std::vector<float>& v) {
+    const lbl_config& cfg = ctx->cfg;
+    const int nx = cfg.nx, ny = cfg.ny, nk = nx / 2;
+    std::mt19937 eng(seed);                                      // data.cu:43-45
+    std::uniform_real_distribution<float> dist(-1, 1);
+    std::vector<double> kx, ky, pp, th;
+    const float k0 = float(cfg.kf);
+    for (int kj = 0; kj < nk; kj++)
+        for (int ki = 0; ki < nk; ki++) {
+            const float k = std::sqrt(float(ki * ki + kj * kj));
+            float pk;
+            if (cfg.ic_kind == LBL_IC_REFERENCE) {
+                const float dk = 10, sigma = 5;
+                pk = (k0 - dk <= k && k <= k0 + dk) ? std::exp(-(k - k0) * (k - k0) / sigma) : 0.f;
+            } else {
+                const float s = k / k0;
+                pk = (k > 0 && s * s <= 23.0f) ? std::sqrt(k) * std::exp(-s * s) : 0.f;
+            }
+            const float theta = float(dist(eng) * M_PI);
+            if (pk != 0.f) {
+                kx.push_back(2 * M_PI * ki / nx);
+                ky.push_back(2 * M_PI * kj / ny);
+                pp.push_back(pk);
+                th.push_back(theta);
+            }
+        }
+    const int n = int(kx.size());
+    std::vector<double> tab;
+    tab.insert(tab.end(), kx.begin(), kx.end());
+    tab.insert(tab.end(), ky.begin(), ky.end());
+    tab.insert(tab.end(), pp.begin(), pp.end());
+    tab.insert(tab.end(), th.begin(), th.end());
+    double* d_tab = nullptr;
+    float* d_uv = nullptr;
+    const size_t nxy = size_t(nx) * ny;
+    LBL_CK(cudaMalloc(&d_tab, sizeof(double) * std::max<size_t>(tab.size(), 1)));
+    LBL_CK(cudaMalloc(&d_uv, sizeof(float) * 2 * nxy));
+    LBL_CK(cudaMemcpy(d_tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+    launch_ic_velocity(d_tab, n, nx, ny, d_uv, d_uv + nxy, ctx->stream);
+    LBL_CK(cudaGetLastError());
+    u.resize(nxy); v.resize(nxy);
+    LBL_CK(cudaMemcpyAsync(u.data(), d_uv, sizeof(float) * nxy, cudaMemcpyDeviceToHost, ctx->stream));
+    LBL_CK(cudaMemcpyAsync(v.data(), d_uv + nxy, sizeof(float) * nxy, cudaMemcpyDeviceToHost, ctx->stream));
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(d_tab);
+    cudaFree(d_uv);
+    if (cfg.ic_kind == LBL_IC_REFERENCE) {                       // data.cu:113-120
+        float vmax = float(1e-30 * cfg.u_ref);
+        for (size_t ij = 0; ij < nxy; ij++) vmax = std::max(vmax, std::sqrt(u[ij] * u[ij] + v[ij] * v[ij]));
+        const float s = float(cfg.u_ref) / vmax * float(cfg.ic_amp);
+        for (size_t ij = 0; ij < nxy; ij++) { u[ij] *= s; v[ij] *= s; }
+    } else {
+        double e = 0;
+        for (size_t ij = 0; ij < nxy; ij++) e += double(u[ij]) * u[ij] + double(v[ij]) * v[ij];
+        const float s = float(cfg.ic_amp / std::sqrt(e / double(nxy) + 1e-300));
+        for (size_t ij = 0; ij < nxy; ij++) { u[ij] *= s; v[ij] *= s; }
+    }
+    return LBL_OK;
+}
+
+int build_weight_table(lbl_ctx* ctx) {
+    const Geo& G = ctx->G;
+    const lbl_config& cfg = ctx->cfg;
+    const int np = G.p * G.p;
+    std::vector<int> tab(size_t(4) * np * G.nobs + np, 0);
+    int* cnt = tab.data() + size_t(4) * np * G.nobs;
+    for (int pj = 0; pj < G.p; pj++)
+        for (int pi = 0; pi < G.p; pi++) {
+            const int pat = pi + G.p * pj;
+            int n = 0;
+            for (int b = 0; b < G.nox; b++)
+                for (int a = 0; a < G.nox; a++) {
+                    const int da = a - (G.nl - G.off), db = b - (G.nl - G.off);
+                    const int di = pi - da * G.p, dj = pj - db * G.p;   // i - io, j - jo
+                    const bool valid = !(std::abs(di) > G.nl * G.p || std::abs(dj) > G.nl * G.p);
+                    if (!valid) continue;
+                    double gc = 1.0;
+                    if (G.p > 1) gc = gaspari_cohn(std::sqrt(double(di * di + dj * dj)) / (G.dloc + 1e-6));
+                    for (int var = 0; var < 3; var++) {
+                        const double sig = var == 2 ? cfg.obs_error_rho : cfg.obs_error_u;
+                        const float w = float(gc / (sig * sig));
+                        if (!(w > 0.f)) continue;
+                        int* e = tab.data() + (size_t(pat) * G.nobs + n) * 4;
+                        e[0] = da; e[1] = db; e[2] = var;
+                        std::memcpy(&e[3], &w, sizeof(float));
+                        n++;
+                    }
+                }
+            cnt[pat] = n;
+        }
+    LBL_CK(cudaMalloc(&ctx->d_wtab, sizeof(int) * tab.size()));
+    LBL_CK(cudaMemcpy(ctx->d_wtab, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice));
+    return LBL_OK;
+}
+
+int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
+    ctx->cfg = *cfg;
+    ctx->device = device;
+    LBL_TRY(validate(*cfg, ctx->err));
+    ctx->P = derive_phys(*cfg);
+    ctx->G = derive_geo(*cfg);
+    LBL_TRY(set_device(ctx));
+    LBL_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    const size_t nxy = size_t(ctx->P.nxy), M = size_t(ctx->P.M);
+    for (int b = 0; b < 2; b++) {
+        LBL_CK(cudaMalloc(&ctx->f[b], sizeof(float) * M * kQ * nxy));
+        LBL_CK(cudaMalloc(&ctx->mac[b], sizeof(float) * M * 3 * nxy));
+        LBL_CK(cudaMemset(ctx->mac[b], 0, sizeof(float) * M * 3 * nxy));
+    }
+    // forcing mode table (data.cu:161-237), amplitudes normalised in long double
+    {
+        const float kf = float(cfg->kf), sigma = 1, dk = 2;
+        const int kmax = int(kf + dk);
+        long double asum = 0;
+        int n = 0;
+        for (int y = 0; y < kmax; y++)
+            for (int x = 0; x < kmax; x++) {
+                if (x == 0 && y == 0) continue;
+                const double k = std::sqrt(double(y * y + x * x));
+                if (kf - dk <= k && k <= kf + dk) {
+                    if (n >= kMaxModes) return fail(ctx, LBL_ERR_UNSUPPORTED, "too many forcing modes");
+                    const float a = float(std::exp(-(k - kf) * (k - kf) / sigma));
+                    asum += a;
+                    ctx->h_kx[n] = float(x); ctx->h_ky[n] = float(y); ctx->h_amp[n] = a;
+                    n++;
+                }
+            }
+        if (n == 0) return fail(ctx, LBL_ERR_ARG, "forcing wavenumber band is empty");
+        const float total = float(cfg->fkf * cfg->u_ref / 1.0);
+        for (int i = 0; i < n; i++) ctx->h_amp[i] = float(ctx->h_amp[i] * (total / asum));
+        ctx->n_modes = n;
+        std::vector<float> tab(3 * n);
+        for (int i = 0; i < n; i++) { tab[i] = ctx->h_kx[i]; tab[n + i] = ctx->h_ky[i]; tab[2 * n + i] = ctx->h_amp[i]; }
+        LBL_CK(cudaMalloc(&ctx->d_modes, sizeof(float) * 3 * n));
+        LBL_CK(cudaMemcpy(ctx->d_modes, tab.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice));
+        ctx->n_rand_buf = n * 4096;                                        // data.cu:297
+        LBL_CK(cudaMalloc(&ctx->d_pool, sizeof(float) * ctx->pool_slots * size_t(ctx->n_rand_buf)));
+    }
+    ctx->force_cap = int(std::max<long long>(8, std::min<long long>(1023, (64ll << 20) / (8ll * nxy))));
+    LBL_CK(cudaMalloc(&ctx->d_force, sizeof(float) * 2 * nxy * ctx->force_cap));
+    LBL_CK(cudaMemset(ctx->d_force, 0, sizeof(float) * 2 * nxy * ctx->force_cap));
+    LBL_CK(cudaMalloc(&ctx->d_sched, sizeof(int) * ctx->force_cap));
+    for (int b = 0; b < 2; b++) LBL_CK(cudaMallocHost(&ctx->h_sched[b], sizeof(int) * ctx->force_cap));
+    LBL_CKR(curandCreateGenerator(&ctx->gen, CURAND_RNG_PSEUDO_MTGP32));   // data.cu:293-294
+    LBL_CKR(curandSetPseudoRandomGeneratorSeed(ctx->gen, cfg->force_seed));
+    LBL_CKR(curandSetStream(ctx->gen, ctx->stream));
+    // LETKF buffers
+    if (cfg->mode == LBL_MODE_DA_LETKF) {
+        const size_t ns = size_t(ctx->G.nsx) * ctx->G.nsy;
+        LBL_TRY(build_weight_table(ctx));
+        LBL_CK(cudaMalloc(&ctx->d_yo, sizeof(float) * 3 * ns));
+        for (int b = 0; b < 2; b++) LBL_CK(cudaMallocHost(&ctx->h_yo[b], sizeof(float) * 3 * ns));
+        LBL_CK(cudaMalloc(&ctx->d_dY, sizeof(float) * 3 * ns * M));
+        LBL_CK(cudaMalloc(&ctx->d_dyo, sizeof(float) * 3 * ns));
+    }
+    LBL_CK(cudaMalloc(&ctx->d_stats, sizeof(int) * 4));
+    LBL_CK(cudaMemset(ctx->d_stats, 0, sizeof(int) * 4));
+    LBL_CK(cudaMalloc(&ctx->d_red, sizeof(double) * 8));
+    LBL_CK(cudaMalloc(&ctx->d_tmp, sizeof(float) * 2 * nxy));
+    for (auto& e : ctx->ev) LBL_CK(cudaEventCreate(&e));
+    for (auto& e : ctx->user_ev) LBL_CK(cudaEventCreate(&e));
+    ctx->have_events = true;
+    if (analysis_prepare() != 0) return fail(ctx, LBL_ERR_CUDA, "cudaFuncSetAttribute(analysis_kernel) failed");
+    ctx->timers[LBL_TIMER_MAIN].t0 = wall_time();
+    ctx->timers[LBL_TIMER_LETKF].t0 = wall_time();
+    return LBL_OK;
+}
+
+void destroy_impl(lbl_ctx* ctx) {
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
+    ctx->graphs.clear();
+    if (ctx->gen) curandDestroyGenerator(ctx->gen);
+    for (int b = 0; b < 2; b++) { cudaFree(ctx->f[b]); cudaFree(ctx->mac[b]); }
+    cudaFree(ctx->d_modes); cudaFree(ctx->d_pool); cudaFree(ctx->d_force); cudaFree(ctx->d_sched);
+    cudaFree(ctx->d_wtab); cudaFree(ctx->d_yo); cudaFree(ctx->d_dY); cudaFree(ctx->d_dyo);
+    cudaFree(ctx->d_stats); cudaFree(ctx->d_red); cudaFree(ctx->d_tmp);
+    for (int b = 0; b < 2; b++) {
+        if (ctx->h_yo[b]) cudaFreeHost(ctx->h_yo[b]);
+        if (ctx->h_sched[b]) cudaFreeHost(ctx->h_sched[b]);
+    }
+    if (ctx->have_events) {
+        for (auto& e : ctx->ev) cudaEventDestroy(e);
+        for (auto& e : ctx->user_ev) cudaEventDestroy(e);
+    }
+    if (ctx->obs_engine) obs_engine_free(ctx->obs_engine);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+}
+
+int init_impl(lbl_ctx* ctx, int ens_offset) {
+    const lbl_config& cfg = ctx->cfg;
+    const size_t nxy = size_t(ctx->P.nxy);
+    const int M = ctx->P.M;
+    ctx->ens_offset = ens_offset;
+    ctx->cur = 0;
+    const int add = cfg.mode == LBL_MODE_DA_LETKF ? 334 : 0;       // data.cu:31-35
+    std::vector<float> un, vn;
+    if (cfg.ens_init == LBL_ENS_PERTURBED) LBL_TRY(ic_member(ctx, ens_offset, un, vn));
+    std::vector<float> fh(kQ * nxy), mh(3 * nxy);
+    const float r0 = float(cfg.rho_ref);
+    for (int m = 0; m < M; m++) {
+        std::vector<float> u, v;
+        LBL_TRY(ic_member(ctx, m + ens_offset + add, u, v));
+        if (cfg.ens_init == LBL_ENS_PERTURBED) {
+            const float a = float(cfg.ens_perturb);
+            for (size_t ij = 0; ij < nxy; ij++) { u[ij] = un[ij] + a * u[ij]; v[ij] = vn[ij] + a * v[ij]; }
+        }
+        for (size_t ij = 0; ij < nxy; ij++) {
+            for (int q = 0; q < kQ; q++) fh[q * nxy + ij] = feq_host(r0, u[ij], v[ij], q, ctx->P.c);
+            mh[ij] = r0; mh[nxy + ij] = u[ij]; mh[2 * nxy + ij] = v[ij];
+        }
+        for (int b = 0; b < 2; b++) {  // data_0_ and data_1_ both start from the IC (data.h:55)
+            LBL_CK(cudaMemcpy(ctx->f[b] + size_t(m) * kQ * nxy, fh.data(), sizeof(float) * kQ * nxy,
+                              cudaMemcpyHostToDevice));
+            LBL_CK(cudaMemcpy(ctx->mac[b] + size_t(m) * 3 * nxy, mh.data(), sizeof(float) * 3 * nxy,
+                              cudaMemcpyHostToDevice));
+        }
+    }
+    // forcing: cursor starts "outdated", two update_forces calls at init (data.cu:236, :158)
+    ctx->i_rand_outdated = ctx->n_rand_buf;
+    ctx->rand_block = -1;
+    LBL_TRY(schedule_force(ctx, 2));
+    launch_force_chunk(ctx, 2, 0, ctx->stream);
+    LBL_CK(cudaGetLastError());
+    ctx->last_force_slot = 1;
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    ctx->initialised = true;
+    return LBL_OK;
+}
+
+int update_impl(lbl_ctx* ctx, int nsteps, bool sync) {
+    if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_update before lbl_init");
+    if (nsteps < 0) return fail(ctx, LBL_ERR_ARG, "nsteps < 0");
+    int left = nsteps;
+    while (left > 0) {
+        // each chunk writes macros on its last two steps, so whatever the chunking,
+        // the last two steps of the call leave rho,u,v in both buffers
+        const int n = std::min(left, ctx->force_cap);
+        LBL_TRY(schedule_force(ctx, n));
+        LBL_TRY(launch_graph(ctx, 0, n));
+        ctx->cur ^= (n & 1);
+        ctx->last_force_slot = n - 1;
+        left -= n;
+    }
+    if (sync) LBL_CK(cudaStreamSynchronize(ctx->stream));
+    return LBL_OK;
+}
+
+int assimilate_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const float* vo, bool sync) {
+    if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate before lbl_init");
+    if (ctx->cfg.mode != LBL_MODE_DA_LETKF) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate needs mode DA_LETKF");
+    TimerMap& tm = ctx->timers[LBL_TIMER_LETKF];
+    timer_transit(tm, "_ignored");                                  // letkf.cu:121
+    if (!da_due(ctx, t)) return LBL_OK;                             // letkf.cu:122-123
+    if (!ro || !uo || !vo) return fail(ctx, LBL_ERR_ARG, "null observation pointer");
+    LBL_CK(cudaMemsetAsync(ctx->d_stats, 0, sizeof(int) * 3, ctx->stream));
+    const double h0 = wall_time();
+    LBL_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    LBL_TRY(upload_obs(ctx, ro, uo, vo));
+    const double h1 = wall_time();
+    LBL_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    launch_obs_ensemble(ctx, ctx->f[ctx->cur], ctx->stream);
+    LBL_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    launch_analysis(ctx, ctx->f[ctx->cur], ctx->f[ctx->cur ^ 1], ctx->mac[ctx->cur ^ 1], ctx->stream);
+    LBL_CK(cudaGetLastError());
+    LBL_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    ctx->cur ^= 1;                                                   // dat.swap(), letkf.cu:357
+    if (sync) {
+        LBL_CK(cudaEventSynchronize(ctx->ev[3]));
+        // stage tags of letkf.cu:133-336.  The member transposes and MPI exchanges of
+        // the reference are index maps inside the kernels here, and update_xk /
+        // lbm2euler are fused into the analysis kernel, so those tags stay at 0.
+        float ms_h2d = 0, ms_obs = 0, ms_ana = 0;
+        cudaEventElapsedTime(&ms_h2d, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&ms_obs, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&ms_ana, ctx->ev[2], ctx->ev[3]);
+        timer_add(tm, "load_obs", (h1 - h0) + 1e-3 * ms_h2d);
+        timer_add(tm, "pack_yk", 1e-3 * ms_obs);
+        timer_add(tm, "solve", 1e-3 * ms_ana);
+        for (const char* tag : {"pack_xk", "mpi_yk", "set_yo", "mpi_xk", "solve_comm_ovlp", "mpi_barrier",
+                                "mpi_xsol", "update_xk", "lbm2euler"})
+            timer_add(tm, tag, 0.0);
+        timer_transit(tm, "_ignored");
+        LBL_TRY(read_stats(ctx));
+    }
+    return LBL_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* lbl_version(void) { return "liblbl 0.1 (sm_100a)"; }
+
+const char* lbl_last_error(const lbl_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int lbl_config_default(lbl_config* c, int mode, int nx, int n_ens) {
+    if (!c) return LBL_ERR_ARG;
+    std::memset(c, 0, sizeof(*c));
+    const int scaler = nx / 64;
+    c->abi_version = LBL_ABI_VERSION;
+    c->mode = mode;
+    c->nx = nx; c->ny = nx;                  // config.h:133-134
+    c->n_ens = n_ens;
+    c->iiter = 5 * (scaler > 0 ? scaler : 1); // config.h:136
+    c->ioprune = 10;                         // config.h:91
+    c->daprune = 10;                         // config.h:56
+    c->da_xyprune = 1;                       // config.h:60
+    c->letkf_rloc_len = 0;
+    c->iter_main = c->iiter * 2000;          // config.h:144
+    c->spinup = 100000 * c->iiter;           // config.h:139
+    c->ic_kind = LBL_IC_REFERENCE;
+    c->ens_init = LBL_ENS_INDEPENDENT;
+    c->compat_stale_v = 1;
+    c->jacobi_max_sweeps = 100;
+    c->letkf_covinf = 1.0;                   // config.h:49
+    c->obs_error_rho = 0.01;                 // run/jserr:146-147
+    c->obs_error_u = 0.1;
+    c->cs = 0.2;                             // lbm.cu:59
+    c->nu = 1e-4;                            // config.h:157
+    c->tau = 0;
+    c->cfl = 0.05;                           // config.h:153
+    c->rho_ref = 1;
+    c->u_ref = 1;
+    c->h_ref = 2 * M_PI;
+    c->kf = 4;                               // config.h:161
+    c->fkf = 5.6;                            // config.h:171
+    c->friction_rate = 5e-4;                 // config.h:180
+    c->ic_amp = 0.01;                        // data.cu:53
+    c->ens_perturb = 0.1;
+    c->jacobi_tol = 1e-6;                    // cu_matrix_eigensolver_wrapper.hpp:192
+    c->force_seed = 1991;                    // data.cu:294
+    c->obs_seed = 334;                       // io.cu:321
+    return LBL_OK;
+}
+
+int lbl_create(const lbl_config* cfg, int device, lbl_ctx** out) {
+    if (!cfg || !out) return LBL_ERR_ARG;
+    *out = nullptr;
+    lbl_ctx* ctx = new (std::nothrow) lbl_ctx();
+    if (!ctx) return LBL_ERR_NOMEM;
+    const int rc = create_impl(cfg, device, ctx);
+    *out = ctx;  // returned even on failure so lbl_last_error can explain; caller destroys
+    return rc;
+}
+
+int lbl_destroy(lbl_ctx* ctx) {
+    if (!ctx) return LBL_OK;
+    destroy_impl(ctx);
+    delete ctx;
+    return LBL_OK;
+}
+
+int lbl_init(lbl_ctx* ctx, int ens_offset) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    return init_impl(ctx, ens_offset);
+}
+
+int lbl_update(lbl_ctx* ctx, int t0, int nsteps) {
+    (void)t0;
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    return update_impl(ctx, nsteps, true);
+}
+
+int lbl_update_async(lbl_ctx* ctx, int t0, int nsteps) {
+    (void)t0;
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    return update_impl(ctx, nsteps, false);
+}
+
+int lbl_sync(lbl_ctx* ctx) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->cfg.mode == LBL_MODE_DA_LETKF) LBL_TRY(read_stats(ctx));
+    return LBL_OK;
+}
+
+int lbl_assimilate(lbl_ctx* ctx, int t, const float* ro, const float* uo, const float* vo) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    return assimilate_impl(ctx, t, ro, uo, vo, true);
+}
+
+int lbl_assimilate_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, const float* vo) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    return assimilate_impl(ctx, t, ro, uo, vo, false);
+}
+
+int lbl_assimilate_files(lbl_ctx* ctx, int t, const char* io_prefix) {
+    if (!ctx || !io_prefix) return LBL_ERR_ARG;
+    if (ctx->cfg.mode != LBL_MODE_DA_LETKF) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate needs mode DA_LETKF");
+    if (!da_due(ctx, t)) { timer_transit(ctx->timers[LBL_TIMER_LETKF], "_ignored"); return LBL_OK; }
+    const size_t nxy = size_t(ctx->P.nxy);
+    std::vector<float> ro(nxy), uo(nxy), vo(nxy);
+    const std::string step = to_string_aligned(t / ctx->cfg.iiter, 10);
+    const std::string dir = std::string(io_prefix) + "/observed/ens0000/";
+    LBL_TRY(read_dat(dir + "rho_step" + step + ".dat", ro.data(), nxy, ctx->err));
+    LBL_TRY(read_dat(dir + "u_step" + step + ".dat", uo.data(), nxy, ctx->err));
+    LBL_TRY(read_dat(dir + "v_step" + step + ".dat", vo.data(), nxy, ctx->err));
+    return lbl_assimilate(ctx, t, ro.data(), uo.data(), vo.data());
+}
+
+int lbl_cycle_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, const float* vo, int n_fc) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_cycle_async before lbl_init");
+    if (n_fc < 0 || n_fc > ctx->force_cap) return fail(ctx, LBL_ERR_ARG, "n_fc out of range for one graph");
+    const bool due = ctx->cfg.mode == LBL_MODE_DA_LETKF && t > 0 && da_due(ctx, t);
+    if (due && ro && uo && vo) LBL_TRY(upload_obs(ctx, ro, uo, vo));  // NULL: resident observations
+    if (n_fc > 0) LBL_TRY(schedule_force(ctx, n_fc));
+    LBL_TRY(launch_graph(ctx, due ? 1 : 0, n_fc));
+    if (due) ctx->cur ^= 1;
+    ctx->cur ^= (n_fc & 1);
+    if (n_fc > 0) ctx->last_force_slot = n_fc - 1;
+    return LBL_OK;
+}
+
+int lbl_output(lbl_ctx* ctx, int t, const char* io_prefix) {
+    if (!ctx || !io_prefix) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    const lbl_config& cfg = ctx->cfg;
+    if (t % (cfg.iiter * cfg.ioprune) != 0) return LBL_OK;          // io.cu:23
+    const int nx = cfg.nx, ny = cfg.ny, M = cfg.n_ens;
+    const size_t nxy = size_t(nx) * ny;
+    const std::string pre(io_prefix);
+    const std::string step = "_step" + to_string_aligned(t / cfg.iiter, 10) + ".dat";
+    std::vector<float> mh(size_t(M) * 3 * nxy);
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    LBL_CK(cudaMemcpy(mh.data(), ctx->mac[ctx->cur], sizeof(float) * mh.size(), cudaMemcpyDeviceToHost));
+    std::vector<float> vor(size_t(M) * nxy);
+    for (int m = 0; m < M; m++) {
+        const float* u = mh.data() + (size_t(m) * 3 + 1) * nxy;
+        const float* v = mh.data() + (size_t(m) * 3 + 2) * nxy;
+        vorticity_host(nx, ny, ctx->P.dx, u, v, vor.data() + size_t(m) * nxy);
+        for (size_t ij = 0; ij < nxy; ij++)
+            if (std::isnan(vor[size_t(m) * nxy + ij])) return fail(ctx, LBL_ERR_NAN, "nan value detected");  // io.cu:79-83
+    }
+    auto dname = [&](const std::string& kind, int id) { return pre + "/" + kind + "/ens" + to_string_aligned(id, 4); };
+    if (cfg.mode == LBL_MODE_DA_LETKF) {                            // ENSEMBLE_STAT (io.cu:88-139)
+        std::vector<float> um(nxy, 0.f), vm(nxy, 0.f), wm(nxy, 0.f), w2(nxy, 0.f), ws(nxy, 0.f);
+        if (M > 1) {
+            const float iv = float(1) / M;
+            for (int m = 0; m < M; m++)
+                for (size_t ij = 0; ij < nxy; ij++) {
+                    wm[ij] += vor[size_t(m) * nxy + ij];
+                    um[ij] += mh[(size_t(m) * 3 + 1) * nxy + ij];
+                    vm[ij] += mh[(size_t(m) * 3 + 2) * nxy + ij];
+                    const float a = vor[size_t(m) * nxy + ij];
+                    w2[ij] += iv * (a * a);
+                }
+            for (size_t ij = 0; ij < nxy; ij++) {
+                wm[ij] *= iv; um[ij] *= iv; vm[ij] *= iv;
+                ws[ij] = std::sqrt(w2[ij] - wm[ij] * wm[ij]);
+            }
+        }
+        if (mkdir_p(pre + "/calc") != 0) return fail(ctx, LBL_ERR_IO, "could not create " + pre + "/calc");
+        LBL_TRY(write_dat(pre + "/calc/ens_mean_u" + step, um.data(), nxy, ctx->err));
+        LBL_TRY(write_dat(pre + "/calc/ens_mean_v" + step, vm.data(), nxy, ctx->err));
+        LBL_TRY(write_dat(pre + "/calc/ens_vor_mean" + step, wm.data(), nxy, ctx->err));
+        LBL_TRY(write_dat(pre + "/calc/ens_vor_std" + step, ws.data(), nxy, ctx->err));
+    }
+    for (int m = 0; m < M; m++) {
+        const int id = m + ctx->ens_offset;
+        const float* r = mh.data() + (size_t(m) * 3 + 0) * nxy;
+        const float* u = mh.data() + (size_t(m) * 3 + 1) * nxy;
+        const float* v = mh.data() + (size_t(m) * 3 + 2) * nxy;
+        const float* w = vor.data() + size_t(m) * nxy;
+        if (cfg.mode != LBL_MODE_OBSERVE) {                          // io.cu:151-157
+            const std::string d = dname("calc", id);
+            if (mkdir_p(d) != 0) return fail(ctx, LBL_ERR_IO, "could not create " + d);
+            LBL_TRY(write_dat(d + "/vor" + step, w, nxy, ctx->err));
+            LBL_TRY(write_dat(d + "/rho" + step, r, nxy, ctx->err));
+            LBL_TRY(write_dat(d + "/u" + step, u, nxy, ctx->err));
+            LBL_TRY(write_dat(d + "/v" + step, v, nxy, ctx->err));
+        }
+        if (cfg.mode == LBL_MODE_OBSERVE && id == 0) {               // io.cu:160-246
+            if (!ctx->obs_engine) ctx->obs_engine = obs_engine_new(uint32_t(cfg.obs_seed + id));
+            for (auto& a : ctx->h_obs) a.resize(nxy);
+            observe_host(ctx->obs_engine, nx, ny, cfg.da_xyprune, float(cfg.obs_error_rho), float(cfg.obs_error_u),
+                         r, u, v, ctx->h_obs[0].data(), ctx->h_obs[1].data(), ctx->h_obs[2].data(),
+                         ctx->h_obs[3].data(), ctx->P.dx);
+            const std::string d = dname("observed", id);
+            if (mkdir_p(d) != 0) return fail(ctx, LBL_ERR_IO, "could not create " + d);
+            LBL_TRY(write_dat(d + "/rho" + step, ctx->h_obs[0].data(), nxy, ctx->err));
+            LBL_TRY(write_dat(d + "/u" + step, ctx->h_obs[1].data(), nxy, ctx->err));
+            LBL_TRY(write_dat(d + "/v" + step, ctx->h_obs[2].data(), nxy, ctx->err));
+            LBL_TRY(write_dat(d + "/vor" + step, ctx->h_obs[3].data(), nxy, ctx->err));
+        }
+        if ((cfg.mode == LBL_MODE_NATURE || cfg.mode == LBL_MODE_OBSERVE) && id == 0) {  // io.cu:248-258
+            const std::string d = dname("nature", id);
+            if (mkdir_p(d) != 0) return fail(ctx, LBL_ERR_IO, "could not create " + d);
+            LBL_TRY(write_dat(d + "/rho" + step, r, nxy, ctx->err));
+            LBL_TRY(write_dat(d + "/u" + step, u, nxy, ctx->err));
+            LBL_TRY(write_dat(d + "/v" + step, v, nxy, ctx->err));
+            LBL_TRY(write_dat(d + "/vor" + step, w, nxy, ctx->err));
+        }
+    }
+    return LBL_OK;
+}
+
+int lbl_get_f(lbl_ctx* ctx, int member, float* f) {
+    if (!ctx || !f || member < 0 || member >= ctx->P.M) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    const size_t n = size_t(kQ) * ctx->P.nxy;
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    LBL_CK(cudaMemcpy(f, ctx->f[ctx->cur] + member * n, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    return LBL_OK;
+}
+
+int lbl_set_f(lbl_ctx* ctx, int member, const float* f) {
+    if (!ctx || !f || member < 0 || member >= ctx->P.M) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    const size_t n = size_t(kQ) * ctx->P.nxy;
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    LBL_CK(cudaMemcpy(ctx->f[ctx->cur] + member * n, f, sizeof(float) * n, cudaMemcpyHostToDevice));
+    launch_macros(ctx, ctx->f[ctx->cur], ctx->mac[ctx->cur], ctx->stream);
+    LBL_CK(cudaGetLastError());
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    return LBL_OK;
+}
+
+int lbl_get_fields(lbl_ctx* ctx, int member, float* rho, float* u, float* v, float* vor) {
+    if (!ctx || member < 0 || member >= ctx->P.M) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    const size_t nxy = size_t(ctx->P.nxy);
+    std::vector<float> h(3 * nxy);
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    LBL_CK(cudaMemcpy(h.data(), ctx->mac[ctx->cur] + size_t(member) * 3 * nxy, sizeof(float) * 3 * nxy,
+                      cudaMemcpyDeviceToHost));
+    if (rho) std::memcpy(rho, h.data(), sizeof(float) * nxy);
+    if (u) std::memcpy(u, h.data() + nxy, sizeof(float) * nxy);
+    if (v) std::memcpy(v, h.data() + 2 * nxy, sizeof(float) * nxy);
+    if (vor) vorticity_host(ctx->P.nx, ctx->P.ny, ctx->P.dx, h.data() + nxy, h.data() + 2 * nxy, vor);
+    return LBL_OK;
+}
+
+int lbl_get_ens_stats(lbl_ctx* ctx, float* u_mean, float* v_mean, float* vor_mean, float* vor_std) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    const int M = ctx->P.M;
+    const size_t nxy = size_t(ctx->P.nxy);
+    std::vector<float> mh(size_t(M) * 3 * nxy), w(nxy);
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    LBL_CK(cudaMemcpy(mh.data(), ctx->mac[ctx->cur], sizeof(float) * mh.size(), cudaMemcpyDeviceToHost));
+    std::vector<float> um(nxy, 0.f), vm(nxy, 0.f), wm(nxy, 0.f), w2(nxy, 0.f);
+    const float iv = float(1) / M;
+    for (int m = 0; m < M; m++) {
+        const float* u = mh.data() + (size_t(m) * 3 + 1) * nxy;
+        const float* v = mh.data() + (size_t(m) * 3 + 2) * nxy;
+        vorticity_host(ctx->P.nx, ctx->P.ny, ctx->P.dx, u, v, w.data());
+        for (size_t ij = 0; ij < nxy; ij++) {
+            um[ij] += u[ij]; vm[ij] += v[ij]; wm[ij] += w[ij]; w2[ij] += iv * (w[ij] * w[ij]);
+        }
+    }
+    for (size_t ij = 0; ij < nxy; ij++) {
+        um[ij] *= iv; vm[ij] *= iv; wm[ij] *= iv;
+        if (u_mean) u_mean[ij] = um[ij];
+        if (v_mean) v_mean[ij] = vm[ij];
+        if (vor_mean) vor_mean[ij] = wm[ij];
+        if (vor_std) vor_std[ij] = std::sqrt(w2[ij] - wm[ij] * wm[ij]);
+    }
+    return LBL_OK;
+}
+
+int lbl_get_force(lbl_ctx* ctx, float* fx, float* fy) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    const size_t nxy = size_t(ctx->P.nxy);
+    const float* F = ctx->d_force + size_t(ctx->last_force_slot) * 2 * nxy;
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    if (fx) LBL_CK(cudaMemcpy(fx, F, sizeof(float) * nxy, cudaMemcpyDeviceToHost));
+    if (fy) LBL_CK(cudaMemcpy(fy, F + nxy, sizeof(float) * nxy, cudaMemcpyDeviceToHost));
+    return LBL_OK;
+}
+
+int lbl_get_force_state(lbl_ctx* ctx, float* randoms, float* kx, float* ky, float* amp, int* n_modes,
+                        int* i_rand_outdated) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    const int n = ctx->n_modes;
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    if (randoms)
+        LBL_CK(cudaMemcpy(randoms, ctx->d_pool + ctx->last_sched, sizeof(float) * 4 * n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++) {
+        if (kx) kx[i] = ctx->h_kx[i];
+        if (ky) ky[i] = ctx->h_ky[i];
+        if (amp) amp[i] = ctx->h_amp[i];
+    }
+    if (n_modes) *n_modes = n;
+    if (i_rand_outdated) *i_rand_outdated = ctx->i_rand_outdated;
+    return LBL_OK;
+}
+
+int lbl_get_observed(lbl_ctx* ctx, float* rho_o, float* u_o, float* v_o, float* vor_o) {
+    if (!ctx) return LBL_ERR_ARG;
+    if (ctx->h_obs[0].empty()) return fail(ctx, LBL_ERR_STATE, "no observation generated yet (OBSERVE output)");
+    const size_t n = sizeof(float) * ctx->P.nxy;
+    if (rho_o) std::memcpy(rho_o, ctx->h_obs[0].data(), n);
+    if (u_o) std::memcpy(u_o, ctx->h_obs[1].data(), n);
+    if (v_o) std::memcpy(v_o, ctx->h_obs[2].data(), n);
+    if (vor_o) std::memcpy(vor_o, ctx->h_obs[3].data(), n);
+    return LBL_OK;
+}
+
+int lbl_get_letkf_stats(lbl_ctx* ctx, int* max_sweeps, int* n_noconv, int* nan_flag) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    LBL_CK(cudaMemcpy(ctx->h_stats, ctx->d_stats, sizeof(int) * 3, cudaMemcpyDeviceToHost));
+    if (max_sweeps) *max_sweeps = ctx->h_stats[0];
+    if (n_noconv) *n_noconv = ctx->h_stats[1];
+    if (nan_flag) *nan_flag = ctx->h_stats[2];
+    return LBL_OK;
+}
+
+int lbl_get_diagnostics(lbl_ctx* ctx, int member, double* energy, double* enstrophy, double* mass) {
+    if (!ctx || member < -1 || member >= ctx->P.M) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    launch_diag(ctx, ctx->mac[ctx->cur], member, ctx->d_red, ctx->stream);
+    LBL_CK(cudaGetLastError());
+    double h[3];
+    LBL_CK(cudaMemcpyAsync(h, ctx->d_red, sizeof(double) * 3, cudaMemcpyDeviceToHost, ctx->stream));
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    const double n = double(ctx->P.nxy);
+    if (energy) *energy = h[0] / n;
+    if (enstrophy) *enstrophy = h[1] / n;
+    if (mass) *mass = h[2] / n;
+    return LBL_OK;
+}
+
+int lbl_rmse_uv(lbl_ctx* ctx, const float* u_true, const float* v_true, double* rmse) {
+    if (!ctx || !u_true || !v_true || !rmse) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    const size_t nxy = size_t(ctx->P.nxy);
+    LBL_CK(cudaMemcpyAsync(ctx->d_tmp, u_true, sizeof(float) * nxy, cudaMemcpyHostToDevice, ctx->stream));
+    LBL_CK(cudaMemcpyAsync(ctx->d_tmp + nxy, v_true, sizeof(float) * nxy, cudaMemcpyHostToDevice, ctx->stream));
+    launch_rmse(ctx, ctx->mac[ctx->cur], ctx->d_tmp, ctx->d_tmp + nxy, ctx->d_red, ctx->stream);
+    LBL_CK(cudaGetLastError());
+    double h = 0;
+    LBL_CK(cudaMemcpyAsync(&h, ctx->d_red, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    *rmse = std::sqrt(h / double(nxy));
+    return LBL_OK;
+}
+
+int lbl_profile_step(lbl_ctx* ctx, int n, double* ms_per_launch) {
+    if (!ctx || n < 1 || !ms_per_launch) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_profile_step before lbl_init");
+    const float* force = ctx->d_force + size_t(ctx->last_force_slot) * 2 * ctx->P.nxy;
+    LBL_CK(cudaEventRecord(ctx->ev[8], ctx->stream));
+    for (int k = 0; k < n; k++) {
+        launch_lbm_step(ctx, ctx->f[ctx->cur], ctx->f[ctx->cur ^ 1], force, nullptr, ctx->stream);
+        ctx->cur ^= 1;
+    }
+    LBL_CK(cudaGetLastError());
+    LBL_CK(cudaEventRecord(ctx->ev[9], ctx->stream));
+    LBL_CK(cudaEventSynchronize(ctx->ev[9]));
+    float ms = 0;
+    LBL_CK(cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]));
+    *ms_per_launch = double(ms) / n;
+    return LBL_OK;
+}
+
+int lbl_event_record(lbl_ctx* ctx, int slot) {
+    if (!ctx || slot < 0 || slot >= 8) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    LBL_CK(cudaEventRecord(ctx->user_ev[slot], ctx->stream));
+    return LBL_OK;
+}
+
+int lbl_event_elapsed(lbl_ctx* ctx, int a, int b, double* ms) {
+    if (!ctx || a < 0 || a >= 8 || b < 0 || b >= 8 || !ms) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    LBL_CK(cudaEventSynchronize(ctx->user_ev[b]));
+    float v = 0;
+    LBL_CK(cudaEventElapsedTime(&v, ctx->user_ev[a], ctx->user_ev[b]));
+    *ms = v;
+    return LBL_OK;
+}
+
+int lbl_timer_csv(lbl_ctx* ctx, int which, char* buf, size_t cap) {
+    if (!ctx || which < 0 || which > 1) return LBL_ERR_ARG;
+    const std::string s = timer_csv(ctx->timers[which]);
+    if (buf && cap > 0) {
+        const size_t n = std::min(cap - 1, s.size());
+        std::memcpy(buf, s.data(), n);
+        buf[n] = 0;
+    }
+    return int(s.size());
+}
+
+int lbl_timer_clear(lbl_ctx* ctx, int which) {
+    if (!ctx || which < 0 || which > 1) return LBL_ERR_ARG;
+    ctx->timers[which].map.clear();
+    return LBL_OK;
+}
+
+int lbl_timer_transit(lbl_ctx* ctx, int which, const char* tag) {
+    if (!ctx || !tag || which < 0 || which > 1) return LBL_ERR_ARG;
+    timer_transit(ctx->timers[which], tag);
+    return LBL_OK;
+}
+
+}  // extern "C"

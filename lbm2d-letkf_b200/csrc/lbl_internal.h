@@ -1,0 +1,158 @@
+// lbl_internal.h -- device-side data structures and kernel launchers shared by the
+// liblbl translation units.  Not part of the public ABI (see include/lbl.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <curand.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/lbl.h"
+
+namespace lbl {
+
+constexpr int kQ = 9;
+constexpr int kMaxModes = 128;     // forcing modes (29 at kf=4)
+constexpr int kMaxNobs = 3 * 33 * 33;  // observation window slots (RLOC_LEN <= 8)
+constexpr int kMaxMemberLanes = 32;    // register-resident analysis kernel handles M <= 32
+
+// Physical constants derived once per context, in the precision the reference
+// evaluates them in (config.h:248-254 are constexpr `real` = float).
+struct Phys {
+    int nx, ny, M;
+    int nxy;                 // nx*ny
+    float c;                 // u_ref/cfl
+    float dx, dt;            // h_ref/(ny-1), dx/c
+    float nu;                // molecular viscosity (float, config::nu)
+    float cs2;               // c*c/3 (lbm.h:50)
+    float fr_dt;             // friction_rate/dt (lbm.h:52, constexpr real)
+    float u_ref;
+    float two_dx;            // 2*dx (lbm.cu:44-47)
+    double les_k;            // cs*cs*dx*dx evaluated in double like lbm.cu:59-60
+    double tau_k;            // 3/c/c/dt chain, applied as ((3*nu)/c)/c)/dt in double
+    double c_d, dt_d;        // c, dt widened to double for the tau chain
+    float inv_nx, inv_ny;    // 1/nx, 1/ny for the forcing coordinates
+};
+
+// LETKF geometry (letkf.cu:29-56)
+struct Geo {
+    int p;        // DA_XYPRUNE
+    int nl;       // n_obs_local
+    int off;      // obs_offset
+    int nox;      // n_obs_x
+    int nobs;     // 3*nox*nox
+    double dloc;  // d_local (GC length)
+    int nsx, nsy; // observation sites per row / column (nx/p, ny/p)
+};
+
+struct TimerMap {
+    std::map<std::string, double> map;
+    std::string cur = "_uninitialized";
+    double t0 = 0;
+};
+
+}  // namespace lbl
+
+struct lbl_ctx {
+    lbl_config cfg{};
+    lbl::Phys P{};
+    lbl::Geo G{};
+    int device = 0;
+    int ens_offset = 0;
+    bool initialised = false;
+    std::string err;
+    cudaStream_t stream = nullptr;
+
+    // ensemble state, double buffered like data::d()/dn() (data.h:45-64)
+    float* f[2] = {nullptr, nullptr};    // [M][9][ny][nx]
+    float* mac[2] = {nullptr, nullptr};  // [M][3][ny][nx]  rho, u, v (post-stream macros)
+    int cur = 0;                         // index of d()
+
+    // forcing (data.cu:161-350)
+    int n_modes = 0;
+    float h_kx[lbl::kMaxModes], h_ky[lbl::kMaxModes], h_amp[lbl::kMaxModes];
+    float* d_modes = nullptr;            // [3][n_modes]
+    curandGenerator_t gen = nullptr;
+    int n_rand_buf = 0;                  // 4096 * n_modes
+    int i_rand_outdated = 0;             // cursor of data.cu:240-247
+    long long rand_block = -1;           // index of the normal block currently in use
+    int pool_slots = 4;
+    float* d_pool = nullptr;             // [pool_slots][n_rand_buf]
+    int force_cap = 0;                   // steps the force buffer holds
+    float* d_force = nullptr;            // [force_cap][2][ny][nx]
+    int* d_sched = nullptr;              // [force_cap] offsets into d_pool
+    int* h_sched[2] = {nullptr, nullptr};  // pinned staging, alternating
+    int sched_buf = 0;
+    int last_sched = 0;                  // pool offset used by the last step's forcing
+    int last_force_slot = 0;             // force-buffer slot of the last step
+
+    // LETKF
+    int* d_wtab = nullptr;               // int4 [p*p][nobs] window entries + int [p*p] counts
+    float* d_yo = nullptr;               // [3][nsites] observations at sites (u, v, rho)
+    float* h_yo[2] = {nullptr, nullptr}; // pinned staging of the above, alternating
+    int yo_buf = 0;
+    float* d_dY = nullptr;               // [3][nsites][M] H(x)-mean at sites
+    float* d_dyo = nullptr;              // [3][nsites] yo - mean
+    int* d_stats = nullptr;              // [0] max sweeps, [1] non-converged points, [2] NaN flag
+    int h_stats[3] = {0, 0, 0};
+
+    // diagnostics scratch
+    double* d_red = nullptr;             // reduction scratch (8 doubles)
+    float* d_tmp = nullptr;              // nxy*2 floats (truth fields)
+
+    // OBSERVE noise engine state lives host side (io.cu:321 function-static engine)
+    void* obs_engine = nullptr;          // std::mt19937*
+    std::vector<float> h_obs[4];         // last generated observed rho, u, v, vor
+
+    // CUDA graphs keyed by (kind, n, parity)
+    std::map<long long, cudaGraphExec_t> graphs;
+
+    // timers
+    lbl::TimerMap timers[2];
+    cudaEvent_t ev[16] = {};             // 0-3 stage timing, 4-5 sched staging, 6-7 obs staging, 8-9 profile
+    cudaEvent_t user_ev[8] = {};         // lbl_event_record slots
+    bool have_events = false;
+};
+
+namespace lbl {
+
+// ---- kernels (lbm_kernels.cu, compiled with the reference's -use_fast_math) ----
+void launch_ic_velocity(const double* modes /*[4][n]*/, int n_modes, int nx, int ny,
+                        float* u, float* v, cudaStream_t s);
+void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s);
+void launch_lbm_step(const lbl_ctx* c, const float* fin, float* fout, const float* force,
+                     float* mac_out, cudaStream_t s);
+void launch_macros(const lbl_ctx* c, const float* f, float* mac, cudaStream_t s);
+
+// ---- kernels (letkf_kernels.cu) ----
+void launch_obs_ensemble(const lbl_ctx* c, const float* f, cudaStream_t s);
+void launch_analysis(const lbl_ctx* c, const float* fin, float* fout, float* mac_out, cudaStream_t s);
+int analysis_supported(int M);
+size_t analysis_smem_bytes(int M, int nobs);
+constexpr size_t kAnalysisSmemLimit = 200 * 1024;
+int analysis_prepare();
+
+// ---- kernels (diag_kernels.cu) ----
+void launch_diag(const lbl_ctx* c, const float* mac, int member, double* red, cudaStream_t s);
+void launch_rmse(const lbl_ctx* c, const float* mac, const float* ut, const float* vt, double* red,
+                 cudaStream_t s);
+
+// ---- host helpers (host_io.cpp) ----
+std::string to_string_aligned(int t, int digits);
+int write_dat(const std::string& fname, const float* p, size_t n, std::string& err);
+int read_dat(const std::string& fname, float* p, size_t n, std::string& err);
+int mkdir_p(const std::string& path);
+void vorticity_host(int nx, int ny, float dx, const float* u, const float* v, float* vor);
+void* obs_engine_new(uint32_t seed);
+void obs_engine_free(void* e);
+void observe_host(void* engine, int nx, int ny, int p, float er, float eu, const float* r, const float* u,
+                  const float* v, float* ro, float* uo, float* vo, float* voro, float dx);
+double wall_time();
+void timer_transit(TimerMap& t, const std::string& tag);
+void timer_add(TimerMap& t, const std::string& tag, double sec);
+std::string timer_csv(const TimerMap& t);
+
+}  // namespace lbl

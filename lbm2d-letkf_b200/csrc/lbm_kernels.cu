@@ -1,0 +1,310 @@
+// lbm_kernels.cu -- D2Q9 BGK + Smagorinsky forecast kernels for sm_100a.
+//
+// This translation unit is compiled with -use_fast_math, like the reference
+// (config/makefile.compiler.in:42), so that the forcing sin/cos, the Smagorinsky
+// sqrt and the float divisions take the same hardware paths as the reference's
+// kernels.  Expressions are written in the reference's evaluation order
+// (float / double promotions included) for the same reason.
+//
+// Kernels
+//   ic_velocity_kernel  stream-function initial velocity (data.cu:76-110)
+//   force_chunk_kernel  Watanabe-97 random forcing for a chunk of steps (data.cu:317-348)
+//   lbm_step_kernel     fused pull streaming + macros + Smagorinsky + BGK + force
+//                       (lbm.cu:24-160, lbm.h:31-109, lbm_collision_srt.h:8-16)
+//   macros_kernel       rho,u,v moments of f (lbm.h:72-109)
+#include <cmath>
+
+#include "lbl_internal.h"
+
+namespace lbl {
+namespace {
+
+__host__ __device__ constexpr int ex_q(int q) { return (q % 3) - 1; }  // config.h:257
+__host__ __device__ constexpr int ey_q(int q) { return (q / 3) - 1; }  // config.h:258
+__host__ __device__ constexpr float w_q(int q) {                       // config.h:260-263
+    return (ex_q(q) * ex_q(q) + ey_q(q) * ey_q(q)) == 0   ? float(4. / 9.)
+           : (ex_q(q) * ex_q(q) + ey_q(q) * ey_q(q)) == 1 ? float(1. / 9.)
+                                                           : float(1. / 36.);
+}
+
+// feq (lbm.h:31-39)
+__device__ __forceinline__ float feq(float rho, float u, float v, int q, float c) {
+    const float uc0 = (u * ex_q(q) + v * ey_q(q)) / c;
+    const float uu0 = (u * u + v * v) / (c * c);
+    return rho * w_q(q) * (float(1.) + float(3.) * uc0 + float(4.5) * uc0 * uc0 - float(1.5) * uu0);
+}
+
+// rf / uf / vf (lbm.h:72-109; VELOCITY_FORCE_CORRECTION and ICLBM are off)
+__device__ __forceinline__ float rf(const float (&f)[kQ]) {
+    float ret = 0;
+#pragma unroll
+    for (int q = 0; q < kQ; q++) ret += f[q];
+    return ret;
+}
+__device__ __forceinline__ float uf(const float (&f)[kQ], float rho, float c) {
+    float ret = 0;
+#pragma unroll
+    for (int q = 0; q < kQ; q++) ret += f[q] * c * ex_q(q);
+    ret /= rho;
+    return ret;
+}
+__device__ __forceinline__ float vf(const float (&f)[kQ], float rho, float c) {
+    float ret = 0;
+#pragma unroll
+    for (int q = 0; q < kQ; q++) ret += f[q] * c * ey_q(q);
+    ret /= rho;
+    return ret;
+}
+
+// force_acc (lbm.h:41-70; first-order term only, FORCE_SECOND_ORDER off)
+__device__ __forceinline__ float force_acc(float fx_, float fy_, int q, float rho, float u, float v,
+                                           const Phys& P) {
+    const float cx = P.u_ref * ex_q(q);
+    const float cy = P.u_ref * ey_q(q);
+    const float wq = w_q(q);
+    const float fx = (fx_ - P.fr_dt * u) * P.dt;
+    const float fy = (fy_ - P.fr_dt * v) * P.dt;
+    const float f1 = (cx * fx + cy * fy) / P.cs2;
+    float ret = f1;
+    ret *= wq * rho;
+    return ret;
+}
+
+// ---------------------------------------------------------------------------
+// initial velocity from the stream-function modes (data.cu:76-110).  The sum is
+// accumulated in a float that receives each FP64 term, exactly like `real utmp`.
+// ---------------------------------------------------------------------------
+__global__ void ic_velocity_kernel(const double* __restrict__ modes, int n, int nx, int ny,
+                                   float* __restrict__ u, float* __restrict__ v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= nx || j >= ny) return;
+    const double* kxa = modes;
+    const double* kya = modes + n;
+    const double* pa = modes + 2 * n;
+    const double* tha = modes + 3 * n;
+    float utmp = 0, vtmp = 0;
+    for (int k = 0; k < n; k++) {
+        const double kx = kxa[k], ky = kya[k];
+        const float p = float(pa[k]), th = float(tha[k]);
+        const double cs = cos(kx * i + ky * j + th);
+        utmp += p * ky * cs;
+        vtmp += p * -kx * cs;
+    }
+    u[i + nx * j] = utmp;
+    v[i + nx * j] = vtmp;
+}
+
+// ---------------------------------------------------------------------------
+// Watanabe-97 forcing for `nsteps` consecutive steps (data.cu:317-348).  The
+// field does not depend on the member, so it is computed once per step for the
+// whole ensemble.  sched[s] is the offset, in the normal pool, of the 4*n normals
+// that step s uses (the reference's force_theta_d[i_rand_outdated]).
+// ---------------------------------------------------------------------------
+__global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __restrict__ sched,
+                                   const float* __restrict__ modes, int n, float* __restrict__ force,
+                                   int slot0, int cap, Phys P) {
+    extern __shared__ float s_mode[];  // kx[n], ky[n], amp[n], r[4n]
+    const int s = blockIdx.y;
+    const float* rnd = pool + sched[s];
+    for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) s_mode[k] = modes[k];
+    for (int k = threadIdx.x; k < 4 * n; k += blockDim.x) s_mode[3 * n + k] = rnd[k];
+    __syncthreads();
+    const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= P.nxy) return;
+    const int nx = P.nx, ny = P.ny;
+    const int i = ij % nx, j = ij / nx;
+    const float x = float(i - nx / 2) * P.inv_nx;
+    const float y = float(j - ny / 2) * P.inv_ny;
+    const float* force_kx = s_mode;
+    const float* force_ky = s_mode + n;
+    const float* force_amp = s_mode + 2 * n;
+    const float* force_rand = s_mode + 3 * n;
+    float f_x = 0;
+    float f_y = 0;
+    for (int k = 0; k < n; k++) {
+        const float kx = force_kx[k];
+        const float ky = force_ky[k];
+        const float theta = 2 * M_PI * (kx * x + ky * y);
+        const float sine = sin(theta);
+        const float cosi = cos(theta);
+        const float r[4] = {force_rand[k + 0 * n], force_rand[k + 1 * n], force_rand[k + 2 * n],
+                            force_rand[k + 3 * n]};
+        const float amp = force_amp[k];
+        f_x += amp * 2 * M_PI * ky * ((r[0] * kx + r[1] * ky) * sine + (r[2] * kx + r[3] * ky) * cosi);
+        f_y += amp * 2 * M_PI * (-kx) * ((r[0] * kx + r[1] * ky) * sine + (r[2] * kx + r[3] * ky) * cosi);
+    }
+    float* F = force + size_t((slot0 + s) % cap) * 2 * P.nxy;
+    F[ij] = f_x;
+    F[P.nxy + ij] = f_y;
+}
+
+// ---------------------------------------------------------------------------
+// Fused LBM step.  One CTA = one member x one strip of TY rows, one thread per
+// column x.  Each thread marches up its column: it pulls row jj+1 (prefetched one
+// row ahead), computes that row's post-stream macros, shares u,v through a 3-row
+// shared-memory ring for the x+-1 neighbours, and finalises row jj (Smagorinsky
+// from the post-stream u,v stencil, BGK toward feq, Guo-less first-order force
+// with friction) straight from registers.  Rows j0-1 and j1 are pulled as halo so
+// that the whole step is one pass over f: 72 B/cell of compulsory traffic in FP32.
+// ---------------------------------------------------------------------------
+template <bool WRITE_MAC>
+__global__ void __launch_bounds__(1024) lbm_step_kernel(const float* __restrict__ fin, float* __restrict__ fout,
+                                                        const float* __restrict__ force,
+                                                        float* __restrict__ mac, Phys P, int TY) {
+    extern __shared__ float s_uv[];  // [3][2][nx]
+    const int nx = P.nx, ny = P.ny, nxy = P.nxy;
+    const int x = threadIdx.x;
+    const int m = blockIdx.y;
+    const int j0 = blockIdx.x * TY;
+    const int j1 = min(j0 + TY, ny);
+    const float* __restrict__ fm = fin + size_t(m) * kQ * nxy;
+    float* __restrict__ fo = fout + size_t(m) * kQ * nxy;
+    const int xm = (x == 0) ? nx - 1 : x - 1;
+    const int xp = (x == nx - 1) ? 0 : x + 1;
+    const float* __restrict__ Fx = force;
+    const float* __restrict__ Fy = force + nxy;
+
+    // pull streaming: fc[q] = f[(i-ex, j-ey)] periodic (lbm.cu:82-87)
+    auto pull = [&](int jj, float (&fc)[kQ]) {
+        const int r0 = (jj + ny) % ny;
+        const int rm = (jj - 1 + ny) % ny;  // source row for ey = +1
+        const int rp = (jj + 1) % ny;       // source row for ey = -1
+#pragma unroll
+        for (int q = 0; q < kQ; q++) {
+            const int col = ex_q(q) == -1 ? xp : (ex_q(q) == 0 ? x : xm);
+            const int row = ey_q(q) == -1 ? rp : (ey_q(q) == 0 ? r0 : rm);
+            fc[q] = __ldg(fm + size_t(q) * nxy + row * nx + col);
+        }
+    };
+    auto slot = [&](int row) { return ((row - j0 + 1) % 3) * 2 * nx; };
+
+    float fA[kQ], fB[kQ], fC[kQ];
+    float rA, uA, vA, rB, uB, vB, uM, vM;
+    {  // halo row below the strip: only its u,v (own column) are needed
+        float t[kQ];
+        pull(j0 - 1, t);
+        const float r = rf(t);
+        uM = uf(t, r, P.c);
+        vM = vf(t, r, P.c);
+    }
+    pull(j0, fA);
+    rA = rf(fA);
+    uA = uf(fA, rA, P.c);
+    vA = vf(fA, rA, P.c);
+    s_uv[slot(j0) + x] = uA;
+    s_uv[slot(j0) + nx + x] = vA;
+    pull(j0 + 1, fB);
+
+    for (int jc = j0; jc < j1; jc++) {
+        if (jc + 2 <= j1) pull(jc + 2, fC);  // prefetch the row after next
+        rB = rf(fB);
+        uB = uf(fB, rB, P.c);
+        vB = vf(fB, rB, P.c);
+        s_uv[slot(jc + 1) + x] = uB;
+        s_uv[slot(jc + 1) + nx + x] = vB;
+        __syncthreads();
+
+        // Smagorinsky eddy viscosity from the post-stream velocity (lbm.cu:42-60)
+        const float* su = s_uv + slot(jc);
+        const float ue = su[xp], uw = su[xm], ve = su[nx + xp], vw = su[nx + xm];
+        const float ux = (ue - uw) / P.two_dx;
+        const float uy = (uB - uM) / P.two_dx;
+        const float vx = (ve - vw) / P.two_dx;
+        const float vy = (vB - vM) / P.two_dx;
+        const float s00 = ux;
+        const float s01 = float(.5) * (uy + vx);
+        const float s10 = s01;
+        const float s11 = vy;
+        const float ss = sqrt(2 * (s00 * s00 + s01 * s10 + s10 * s01 + s11 * s11));
+        const float nus = float(P.les_k * double(ss));
+
+        // relaxation (lbm.cu:132-139): tau in double from the float viscosity
+        const float nu = P.nu + nus;
+        const float c = P.c, dt = P.dt;
+        const float tau = 0.5 + 3. * nu / c / c / dt;
+        const float omega = 1. / tau;
+
+        // BGK (lbm_collision_srt.h:8-16) + force (lbm.cu:142-147)
+        const int ij = jc * nx + x;
+        const float fxc = Fx[ij], fyc = Fy[ij];
+#pragma unroll
+        for (int q = 0; q < kQ; q++) {
+            const float feqq = feq(rA, uA, vA, q, P.c);
+            const float fneq = fA[q] - feqq;
+            fA[q] -= omega * fneq;
+        }
+#pragma unroll
+        for (int q = 0; q < kQ; q++) fA[q] += force_acc(fxc, fyc, q, rA, uA, vA, P);
+#pragma unroll
+        for (int q = 0; q < kQ; q++) fo[size_t(q) * nxy + ij] = fA[q];
+        if (WRITE_MAC) {
+            float* mm = mac + size_t(m) * 3 * nxy;
+            mm[ij] = rA;
+            mm[nxy + ij] = uA;
+            mm[2 * nxy + ij] = vA;
+        }
+        // rotate the window
+        uM = uA; vM = vA;
+        rA = rB; uA = uB; vA = vB;
+#pragma unroll
+        for (int q = 0; q < kQ; q++) { fA[q] = fB[q]; fB[q] = fC[q]; }
+    }
+}
+
+// moments of f for every member (lbm2euler-style, letkf.cu:340-355, but with v)
+__global__ void macros_kernel(const float* __restrict__ f, float* __restrict__ mac, Phys P) {
+    const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    if (ij >= P.nxy) return;
+    float fc[kQ];
+#pragma unroll
+    for (int q = 0; q < kQ; q++) fc[q] = f[(size_t(m) * kQ + q) * P.nxy + ij];
+    const float r = rf(fc);
+    float* mm = mac + size_t(m) * 3 * P.nxy;
+    mm[ij] = r;
+    mm[P.nxy + ij] = uf(fc, r, P.c);
+    mm[2 * P.nxy + ij] = vf(fc, r, P.c);
+}
+
+int strip_rows(const Phys& P) {
+    // enough CTAs to fill 148 SMs several times over, with a modest halo overhead
+    const long long members_rows = (long long)P.M * P.ny;
+    int ty = 16;
+    while (ty > 4 && members_rows / ty < 148 * 4) ty /= 2;
+    return ty;
+}
+
+}  // namespace
+
+void launch_ic_velocity(const double* modes, int n_modes, int nx, int ny, float* u, float* v, cudaStream_t s) {
+    dim3 block(128), grid((nx + 127) / 128, ny);
+    ic_velocity_kernel<<<grid, block, 0, s>>>(modes, n_modes, nx, ny, u, v);
+}
+
+void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s) {
+    const int threads = 256;
+    dim3 grid((c->P.nxy + threads - 1) / threads, nsteps);
+    const size_t sm = sizeof(float) * 7 * c->n_modes;
+    force_chunk_kernel<<<grid, threads, sm, s>>>(c->d_pool, c->d_sched, c->d_modes, c->n_modes, c->d_force, slot0,
+                                                 c->force_cap, c->P);
+}
+
+void launch_lbm_step(const lbl_ctx* c, const float* fin, float* fout, const float* force, float* mac_out,
+                     cudaStream_t s) {
+    const Phys& P = c->P;
+    const int ty = strip_rows(P);
+    dim3 grid((P.ny + ty - 1) / ty, P.M);
+    const size_t sm = sizeof(float) * 6 * P.nx;
+    if (mac_out)
+        lbm_step_kernel<true><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty);
+    else
+        lbm_step_kernel<false><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty);
+}
+
+void launch_macros(const lbl_ctx* c, const float* f, float* mac, cudaStream_t s) {
+    dim3 grid((c->P.nxy + 255) / 256, c->P.M);
+    macros_kernel<<<grid, 256, 0, s>>>(f, mac, c->P);
+}
+
+}  // namespace lbl

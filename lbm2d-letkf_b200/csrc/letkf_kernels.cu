@@ -1,0 +1,377 @@
+// letkf_kernels.cu -- LETKF analysis kernels for sm_100a (FP32, IEEE division/sqrt).
+//
+// The reference (letkf.cu:120-360, util/letkf_solver.h:235-349) builds, per grid
+// point, a 75-row observation window out of every member's H(x), multiplies it
+// with a dense 75x75 R^-1 through cuBLAS, eigen-decomposes Q with cuSOLVER
+// syevjBatched, and applies W through more cuBLAS calls, with MPI alltoalls in
+// between.  Here the whole ensemble is resident, so:
+//
+//   obs_ensemble_kernel  H(x) = (u, v, rho) of every member at every observation
+//                        site, minus the member mean  -> dY[var][site][member],
+//                        and the innovation yo - mean -> dyo[var][site]
+//                        (pack_yk letkf.cu:148-187, set_yo :230-269, ybar/dY/dyo
+//                        letkf_solver.h:239-243).  Mean over members depends only
+//                        on the site, so it is computed once per site.
+//   analysis_kernel<MP>  one group of MP lanes (lane = member) per grid point:
+//                        gather the localised window (R^-1 x Gaspari-Cohn weights
+//                        from a per-(i mod p, j mod p) table, zero-weight slots
+//                        dropped), Gram Q = (M-1)/beta I + dY^T R^-1 dY,
+//                        one-sided (Hestenes) Jacobi eigensolver in registers with
+//                        xor-pair parallel ordering, then
+//                        Xa = xbar + dX V (sqrt(M-1) Lambda^-1/2 V^T + Lambda^-1 V^T dY^T R^-1 dyo 1^T)
+//                        written straight into the member-major populations, plus
+//                        the lbm2euler macros (letkf.cu:336-357).
+#include <cmath>
+
+#include "lbl_internal.h"
+
+namespace lbl {
+namespace {
+
+__host__ __device__ constexpr int exq(int q) { return (q % 3) - 1; }
+__host__ __device__ constexpr int eyq(int q) { return (q / 3) - 1; }
+
+struct AnaParams {
+    int nx, ny, nxy, M;
+    int p, nsx, nsy, nsites;
+    int n_pat_max;          // entries per pattern row of the weight table
+    float diag;             // (M-1)/beta
+    float sqrt_m1;          // sqrt(M-1)
+    float tol;              // Jacobi off-diagonal tolerance
+    int max_sweeps;
+    float c;                // lattice speed for the macros
+    int write_v;            // 0 reproduces the reference's stale v after analysis
+};
+
+// ---------------------------------------------------------------------------
+// H(x) at every observation site for every member, centred on the member mean.
+// One warp per site; lanes stride over members.
+// ---------------------------------------------------------------------------
+__global__ void obs_ensemble_kernel(const float* __restrict__ f, const float* __restrict__ yo,
+                                    float* __restrict__ dY, float* __restrict__ dyo, AnaParams A) {
+    const int lane = threadIdx.x & 31;
+    const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (s >= A.nsites) return;
+    const int si = s % A.nsx, sj = s / A.nsx;
+    const int ij = si * A.p + A.nx * (sj * A.p);
+    constexpr int kPer = 2;  // members per lane (M <= 64)
+    float H[3][kPer];
+    float sum[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int t = 0; t < kPer; t++) {
+        const int m = lane + 32 * t;
+        H[0][t] = H[1][t] = H[2][t] = 0.f;
+        if (m < A.M) {
+            float fc[kQ];
+#pragma unroll
+            for (int q = 0; q < kQ; q++) fc[q] = __ldg(f + (size_t(m) * kQ + q) * A.nxy + ij);
+            float r = 0, mu = 0, mv = 0;
+#pragma unroll
+            for (int q = 0; q < kQ; q++) r += fc[q];
+#pragma unroll
+            for (int q = 0; q < kQ; q++) { mu += fc[q] * A.c * exq(q); mv += fc[q] * A.c * eyq(q); }
+            H[0][t] = mu / r;  // u
+            H[1][t] = mv / r;  // v
+            H[2][t] = r;       // rho
+            sum[0] += H[0][t]; sum[1] += H[1][t]; sum[2] += H[2][t];
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 3; v++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum[v] += __shfl_xor_sync(0xffffffffu, sum[v], o);
+#pragma unroll
+    for (int v = 0; v < 3; v++) {
+        const float mean = sum[v] / float(A.M);
+#pragma unroll
+        for (int t = 0; t < kPer; t++) {
+            const int m = lane + 32 * t;
+            if (m < A.M) dY[(size_t(v) * A.nsites + s) * A.M + m] = H[v][t] - mean;
+        }
+        if (lane == 0) dyo[size_t(v) * A.nsites + s] = yo[size_t(v) * A.nsites + s] - mean;
+    }
+}
+
+template <int MP>
+__device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+    for (int o = MP / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// The local analysis.  MP = member lanes per grid point (power of two >= M).
+// Table entry (int4): x = site dx, y = site dy (in sites), z = variable (0 u, 1 v,
+// 2 rho), w = weight bits (sigma^-2 x Gaspari-Cohn), per pattern (i%p, j%p).
+// ---------------------------------------------------------------------------
+template <int MP>
+__global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__ fin, float* __restrict__ fout,
+                                                       float* __restrict__ mac, const float* __restrict__ dY,
+                                                       const float* __restrict__ dyo,
+                                                       const int4* __restrict__ wtab,
+                                                       const int* __restrict__ wcnt, int* __restrict__ stats,
+                                                       AnaParams A) {
+    constexpr int GPW = 32 / MP;
+    extern __shared__ float smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int grp = lane / MP;
+    const int k = lane % MP;
+    const int gbase = lane - k;
+    const int point = (blockIdx.x * (blockDim.x >> 5) + warp) * GPW + grp;
+    const bool active = point < A.nxy;
+    const bool real_m = active && k < A.M;
+    const int M = A.M;
+
+    // per-group shared memory
+    const int per_grp = A.n_pat_max * MP + MP * MP + 2 * kQ * MP + 2 * MP;
+    float* base = smem + size_t(warp * GPW + grp) * per_grp;
+    float* sE = base;                          // [n_pat][MP] weighted window sqrt(w) dY
+    float* sV = sE + A.n_pat_max * MP;         // [MP][MP] eigenvectors, column j at j*MP
+    float* sDX = sV + MP * MP;                 // [9][MP]  dX
+    float* sD = sDX + kQ * MP;                 // [9][MP]  D = dX V
+    float* sS = sD + kQ * MP;                  // [MP]     sqrt(M-1)/sqrt(lambda)
+    float* sY = sS + MP;                       // [MP]     Lambda^-1 V^T c
+
+    // 1. forecast ensemble at the point: X, xbar, dX (letkf_solver.h:278-280)
+    float xq[kQ], xbar[kQ];
+    const int pt = active ? point : 0;
+#pragma unroll
+    for (int q = 0; q < kQ; q++) xq[q] = real_m ? __ldg(fin + (size_t(k) * kQ + q) * A.nxy + pt) : 0.f;
+#pragma unroll
+    for (int q = 0; q < kQ; q++) {
+        xbar[q] = group_sum<MP>(xq[q]) / float(M);
+        sDX[q * MP + k] = real_m ? xq[q] - xbar[q] : 0.f;
+    }
+
+    // 2. localised observation window (pack_yk/set_yo/set_rR geometry, letkf.cu:75-114,148-269)
+    const int i = pt % A.nx, j = pt / A.nx;
+    const int pat = (i % A.p) + A.p * (j % A.p);
+    const int bi = i / A.p, bj = j / A.p;
+    const int cnt = wcnt[pat];
+    const int4* ent = wtab + size_t(pat) * A.n_pat_max;
+    float ck = 0.f;  // (dY^T R^-1 dyo)_k
+    for (int o = 0; o < cnt; o++) {
+        const int4 e = ent[o];
+        int si = (bi + e.x) % A.nsx; si += si < 0 ? A.nsx : 0;
+        int sj = (bj + e.y) % A.nsy; sj += sj < 0 ? A.nsy : 0;
+        const int s = si + A.nsx * sj;
+        const float sw = sqrtf(__int_as_float(e.w));
+        const float d = real_m ? __ldg(dY + (size_t(e.z) * A.nsites + s) * M + k) : 0.f;
+        const float ev = sw * d;
+        sE[o * MP + k] = ev;
+        ck += ev * (sw * __ldg(dyo + size_t(e.z) * A.nsites + s));
+    }
+    __syncwarp();
+
+    // 3. Gram: column k of Q = (M-1)/beta I + E^T E (letkf_solver.h:252-254)
+    float qv[MP];
+#pragma unroll
+    for (int l = 0; l < MP; l++) qv[l] = 0.f;
+    for (int o = 0; o < cnt; o++) {
+        const float* row = sE + o * MP;
+        const float ek = row[k];
+#pragma unroll
+        for (int l = 0; l < MP; l += 4) {
+            const float4 r4 = *reinterpret_cast<const float4*>(row + l);
+            qv[l + 0] = fmaf(ek, r4.x, qv[l + 0]);
+            qv[l + 1] = fmaf(ek, r4.y, qv[l + 1]);
+            qv[l + 2] = fmaf(ek, r4.z, qv[l + 2]);
+            qv[l + 3] = fmaf(ek, r4.w, qv[l + 3]);
+        }
+    }
+#pragma unroll
+    for (int l = 0; l < MP; l++)
+        if (l == k && k < M) qv[l] += A.diag;
+
+    // 4. one-sided Jacobi: rotate column pairs (k, k^r) of Q until mutually
+    //    orthogonal; accumulated rotations V are the eigenvectors, Q V = V Lambda.
+    float vv[MP];
+#pragma unroll
+    for (int l = 0; l < MP; l++) vv[l] = (l == k) ? 1.f : 0.f;
+    const unsigned gmask = (MP == 32) ? 0xffffffffu : (((1u << MP) - 1u) << gbase);
+    int sweeps = 0;
+    bool converged = false;
+    for (int sw = 0; sw < A.max_sweeps; sw++) {
+        float a = 0.f;
+#pragma unroll
+        for (int l = 0; l < MP; l++) a = fmaf(qv[l], qv[l], a);
+        bool rot = false;
+#pragma unroll 1
+        for (int r = 1; r < MP; r++) {
+            float pq[MP];
+#pragma unroll
+            for (int l = 0; l < MP; l++) pq[l] = __shfl_xor_sync(0xffffffffu, qv[l], r);
+            float g = 0.f;
+#pragma unroll
+            for (int l = 0; l < MP; l++) g = fmaf(qv[l], pq[l], g);
+            const float b = __shfl_xor_sync(0xffffffffu, a, r);
+            const bool low = k < (k ^ r);
+            const float alo = low ? a : b, ahi = low ? b : a;
+            const bool doit = fabsf(g) > A.tol * sqrtf(alo * ahi);
+            float cs = 1.f, sn = 0.f, t = 0.f;
+            if (doit) {
+                const float zeta = (ahi - alo) / (2.f * g);
+                t = copysignf(1.f, zeta) / (fabsf(zeta) + sqrtf(1.f + zeta * zeta));
+                cs = 1.f / sqrtf(1.f + t * t);
+                sn = cs * t;
+            }
+            rot |= doit;
+#pragma unroll
+            for (int l = 0; l < MP; l++) {
+                const float pv = __shfl_xor_sync(0xffffffffu, vv[l], r);
+                if (low) {
+                    qv[l] = cs * qv[l] - sn * pq[l];
+                    vv[l] = cs * vv[l] - sn * pv;
+                } else {
+                    qv[l] = sn * pq[l] + cs * qv[l];
+                    vv[l] = sn * pv + cs * vv[l];
+                }
+            }
+            a = low ? a - t * g : a + t * g;
+        }
+        const unsigned ballot = __ballot_sync(0xffffffffu, rot);
+        if (!converged) {
+            sweeps = sw + 1;
+            if ((ballot & gmask) == 0u) converged = true;
+        }
+        if (ballot == 0u) break;
+    }
+
+    // 5. eigenvalue of column k: (Q V)_k = lambda_k v_k
+    float lam = 0.f;
+#pragma unroll
+    for (int l = 0; l < MP; l++) lam = fmaf(qv[l], vv[l], lam);
+
+    // 6. transform (letkf_solver.h:288-316)
+#pragma unroll
+    for (int l = 0; l < MP; l++) sV[k * MP + l] = vv[l];
+    float vc = 0.f;  // (V^T c)_k
+#pragma unroll
+    for (int l = 0; l < MP; l++) vc = fmaf(vv[l], __shfl_sync(0xffffffffu, ck, gbase + l), vc);
+    const bool col_ok = k < M;
+    sY[k] = col_ok ? vc / lam : 0.f;
+    sS[k] = col_ok ? A.sqrt_m1 / sqrtf(lam) : 0.f;
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < kQ; q++) {
+        float dsum = 0.f;
+#pragma unroll
+        for (int l = 0; l < MP; l++) dsum = fmaf(sDX[q * MP + l], vv[l], dsum);
+        sD[q * MP + k] = dsum;
+    }
+    __syncwarp();
+    float acc[kQ];
+#pragma unroll
+    for (int q = 0; q < kQ; q++) acc[q] = 0.f;
+#pragma unroll 4
+    for (int jj = 0; jj < MP; jj++) {
+        const float z = fmaf(sS[jj], sV[jj * MP + k], sY[jj]);
+#pragma unroll
+        for (int q = 0; q < kQ; q++) acc[q] = fmaf(sD[q * MP + jj], z, acc[q]);
+    }
+
+    // 7. write the analysis member k, refresh its macros (update_xk + lbm2euler)
+    if (real_m) {
+        float xa[kQ];
+        bool bad = false;
+#pragma unroll
+        for (int q = 0; q < kQ; q++) {
+            xa[q] = xbar[q] + acc[q];
+            bad |= !(xa[q] == xa[q]);
+            fout[(size_t(k) * kQ + q) * A.nxy + point] = xa[q];
+        }
+        float r = 0, mu = 0, mv = 0;
+#pragma unroll
+        for (int q = 0; q < kQ; q++) r += xa[q];
+#pragma unroll
+        for (int q = 0; q < kQ; q++) { mu += xa[q] * A.c * exq(q); mv += xa[q] * A.c * eyq(q); }
+        float* mm = mac + size_t(k) * 3 * A.nxy;
+        mm[point] = r;
+        mm[A.nxy + point] = mu / r;
+        if (A.write_v) mm[2 * A.nxy + point] = mv / r;
+        if (bad) atomicOr(stats + 2, 1);
+    }
+    if (active && k == 0) {
+        atomicMax(stats + 0, sweeps);
+        if (!converged) atomicAdd(stats + 1, 1);
+    }
+}
+
+AnaParams make_params(const lbl_ctx* c) {
+    AnaParams A;
+    A.nx = c->P.nx; A.ny = c->P.ny; A.nxy = c->P.nxy; A.M = c->P.M;
+    A.p = c->G.p; A.nsx = c->G.nsx; A.nsy = c->G.nsy; A.nsites = c->G.nsx * c->G.nsy;
+    A.n_pat_max = c->G.nobs;
+    const double beta = c->cfg.letkf_covinf;
+    A.diag = float((c->P.M - 1) / beta);
+    A.sqrt_m1 = float(std::sqrt(double(c->P.M - 1)));
+    A.tol = float(c->cfg.jacobi_tol);
+    A.max_sweeps = c->cfg.jacobi_max_sweeps;
+    A.c = c->P.c;
+    A.write_v = c->cfg.compat_stale_v ? 0 : 1;
+    return A;
+}
+
+int pad_pow2(int M) {
+    int mp = 4;
+    while (mp < M) mp *= 2;
+    return mp;
+}
+
+template <int MP>
+void launch_analysis_mp(const lbl_ctx* c, const float* fin, float* fout, float* mac, cudaStream_t s) {
+    const AnaParams A = make_params(c);
+    constexpr int GPW = 32 / MP;
+    const int warps = 4;
+    const int pts_per_cta = warps * GPW;
+    const int per_grp = A.n_pat_max * MP + MP * MP + 2 * kQ * MP + 2 * MP;
+    const size_t sm = sizeof(float) * size_t(per_grp) * warps * GPW;
+    const int grid = (A.nxy + pts_per_cta - 1) / pts_per_cta;
+    analysis_kernel<MP><<<grid, warps * 32, sm, s>>>(fin, fout, mac, c->d_dY, c->d_dyo,
+                                                      reinterpret_cast<const int4*>(c->d_wtab),
+                                                      c->d_wtab + size_t(4) * c->G.p * c->G.p * c->G.nobs,
+                                                      c->d_stats, A);
+}
+
+}  // namespace
+
+int analysis_supported(int M) { return M >= 2 && M <= kMaxMemberLanes; }
+
+// dynamic shared memory of one analysis CTA (4 warps) for M members and a window of nobs
+size_t analysis_smem_bytes(int M, int nobs) {
+    const int mp = pad_pow2(M);
+    const int per_grp = nobs * mp + mp * mp + 2 * kQ * mp + 2 * mp;
+    return sizeof(float) * size_t(per_grp) * 4 * (32 / mp);
+}
+
+// opt in to large dynamic shared memory once per device (not allowed during capture)
+int analysis_prepare() {
+    const int lim = 200 * 1024;
+    int rc = 0;
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    return rc;
+}
+
+void launch_obs_ensemble(const lbl_ctx* c, const float* f, cudaStream_t s) {
+    const AnaParams A = make_params(c);
+    const int threads = 256;
+    const long long total = (long long)A.nsites * 32;
+    const int grid = int((total + threads - 1) / threads);
+    obs_ensemble_kernel<<<grid, threads, 0, s>>>(f, c->d_yo, c->d_dY, c->d_dyo, A);
+}
+
+void launch_analysis(const lbl_ctx* c, const float* fin, float* fout, float* mac, cudaStream_t s) {
+    switch (pad_pow2(c->P.M)) {
+        case 4: launch_analysis_mp<4>(c, fin, fout, mac, s); break;
+        case 8: launch_analysis_mp<8>(c, fin, fout, mac, s); break;
+        case 16: launch_analysis_mp<16>(c, fin, fout, mac, s); break;
+        case 32: launch_analysis_mp<32>(c, fin, fout, mac, s); break;
+        default: break;
+    }
+}
+
+}  // namespace lbl

@@ -1,0 +1,355 @@
+"""Python bindings of liblbl, the B200 forecast-and-assimilate engine.
+
+The engine holds all M ensemble members of an LBM2D-LETKF experiment on one GPU.
+This module is a thin ctypes layer over the C ABI declared in include/lbl.h, plus
+functions named after the reference's host interface so that calling code reads
+like the reference's main loop (src/main.cu:80-116):
+
+    update(dat, t)                         -> src/lbm.h:16-29
+    DataAssimilator(dat).assimilate(dat,t) -> src/assimilate.h:54-68, src/letkf.cu:120-360
+    output(dat, t)                         -> src/io.cu:22-266
+
+The shared library is loaded from the package directory (built in-tree by
+``make -C lbm2d-letkf_b200``).  There is no fallback: if liblbl.so is missing or a
+call fails, an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+_PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG_DIR, "liblbl.so")
+
+ABI_VERSION = 1
+MODE_NATURE, MODE_OBSERVE, MODE_DA_LETKF = 0, 1, 2
+MODES = {"NATURE": MODE_NATURE, "OBSERVE": MODE_OBSERVE, "DA_LETKF": MODE_DA_LETKF}
+IC_REFERENCE, IC_K4EXP = 0, 1
+ENS_INDEPENDENT, ENS_PERTURBED = 0, 1
+TIMER_MAIN, TIMER_LETKF = 0, 1
+Q = 9
+
+ERRORS = {
+    -1: "LBL_ERR_ARG", -2: "LBL_ERR_CUDA", -3: "LBL_ERR_CURAND", -4: "LBL_ERR_IO",
+    -5: "LBL_ERR_NAN", -6: "LBL_ERR_STATE", -7: "LBL_ERR_NOMEM", -8: "LBL_ERR_UNSUPPORTED",
+    -9: "LBL_ERR_NOCONV",
+}
+
+# names of the exported C functions (must match include/lbl.h)
+EXPORTS = (
+    "lbl_config_default", "lbl_create", "lbl_destroy", "lbl_last_error", "lbl_version", "lbl_init",
+    "lbl_update", "lbl_update_async", "lbl_assimilate", "lbl_assimilate_async", "lbl_assimilate_files",
+    "lbl_cycle_async", "lbl_sync", "lbl_output", "lbl_get_f", "lbl_set_f", "lbl_get_fields",
+    "lbl_get_ens_stats", "lbl_get_force", "lbl_get_force_state", "lbl_get_observed",
+    "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_timer_csv", "lbl_timer_clear",
+    "lbl_timer_transit", "lbl_profile_step", "lbl_event_record", "lbl_event_elapsed",
+)
+
+
+class LblError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    """Mirror of lbl_config (include/lbl.h): the reference's config.h constants and -D knobs."""
+
+    _fields_ = [
+        ("abi_version", ctypes.c_int32), ("mode", ctypes.c_int32), ("nx", ctypes.c_int32),
+        ("ny", ctypes.c_int32), ("n_ens", ctypes.c_int32), ("iiter", ctypes.c_int32),
+        ("ioprune", ctypes.c_int32), ("daprune", ctypes.c_int32), ("da_xyprune", ctypes.c_int32),
+        ("letkf_rloc_len", ctypes.c_int32), ("iter_main", ctypes.c_int32), ("spinup", ctypes.c_int32),
+        ("ic_kind", ctypes.c_int32), ("ens_init", ctypes.c_int32), ("compat_stale_v", ctypes.c_int32),
+        ("jacobi_max_sweeps", ctypes.c_int32), ("write_mat", ctypes.c_int32), ("pad0", ctypes.c_int32),
+        ("letkf_covinf", ctypes.c_double), ("obs_error_rho", ctypes.c_double), ("obs_error_u", ctypes.c_double),
+        ("cs", ctypes.c_double), ("nu", ctypes.c_double), ("tau", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("rho_ref", ctypes.c_double), ("u_ref", ctypes.c_double), ("h_ref", ctypes.c_double),
+        ("kf", ctypes.c_double), ("fkf", ctypes.c_double), ("friction_rate", ctypes.c_double),
+        ("ic_amp", ctypes.c_double), ("ens_perturb", ctypes.c_double), ("jacobi_tol", ctypes.c_double),
+        ("force_seed", ctypes.c_uint64), ("obs_seed", ctypes.c_uint64),
+    ]
+
+    def copy(self) -> "Config":
+        c = Config()
+        ctypes.pointer(c)[0] = self
+        return c
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def load_library() -> ctypes.CDLL:
+    """Load liblbl.so from the package directory; raises if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"liblbl.so not built: {LIB_PATH} (run `make -C lbm2d-letkf_b200`)")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, I, F, D, U = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double), ctypes.c_size_t
+    IP = ctypes.POINTER(ctypes.c_int)
+    CP = ctypes.POINTER(Config)
+    sig = {
+        "lbl_config_default": (I, [CP, I, I, I]),
+        "lbl_create": (I, [CP, I, ctypes.POINTER(P)]),
+        "lbl_destroy": (I, [P]),
+        "lbl_last_error": (ctypes.c_char_p, [P]),
+        "lbl_version": (ctypes.c_char_p, []),
+        "lbl_init": (I, [P, I]),
+        "lbl_update": (I, [P, I, I]),
+        "lbl_update_async": (I, [P, I, I]),
+        "lbl_assimilate": (I, [P, I, F, F, F]),
+        "lbl_assimilate_async": (I, [P, I, F, F, F]),
+        "lbl_assimilate_files": (I, [P, I, ctypes.c_char_p]),
+        "lbl_cycle_async": (I, [P, I, F, F, F, I]),
+        "lbl_sync": (I, [P]),
+        "lbl_output": (I, [P, I, ctypes.c_char_p]),
+        "lbl_get_f": (I, [P, I, F]),
+        "lbl_set_f": (I, [P, I, F]),
+        "lbl_get_fields": (I, [P, I, F, F, F, F]),
+        "lbl_get_ens_stats": (I, [P, F, F, F, F]),
+        "lbl_get_force": (I, [P, F, F]),
+        "lbl_get_force_state": (I, [P, F, F, F, F, IP, IP]),
+        "lbl_get_observed": (I, [P, F, F, F, F]),
+        "lbl_get_letkf_stats": (I, [P, IP, IP, IP]),
+        "lbl_get_diagnostics": (I, [P, I, D, D, D]),
+        "lbl_rmse_uv": (I, [P, F, F, D]),
+        "lbl_timer_csv": (I, [P, I, ctypes.c_char_p, U]),
+        "lbl_timer_clear": (I, [P, I]),
+        "lbl_timer_transit": (I, [P, I, ctypes.c_char_p]),
+        "lbl_profile_step": (I, [P, I, D]),
+        "lbl_event_record": (I, [P, I]),
+        "lbl_event_elapsed": (I, [P, I, I, D]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _fp(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _f32(a, n: int) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32).reshape(-1)
+    if a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def config_default(mode="NATURE", nx: int = 256, n_ens: int = 1, **overrides) -> Config:
+    """The reference's defaults for a run mode at grid nx (= 64*SCALER), with overrides.
+
+    Override names are lbl_config fields (daprune, da_xyprune, letkf_rloc_len, letkf_covinf,
+    obs_error_u, cs, tau, ...)."""
+    lib = load_library()
+    m = MODES[mode] if isinstance(mode, str) else int(mode)
+    c = Config()
+    rc = lib.lbl_config_default(ctypes.byref(c), m, nx, n_ens)
+    if rc != 0:
+        raise LblError(rc, "lbl_config_default")
+    for k, v in overrides.items():
+        if not hasattr(c, k):
+            raise KeyError(f"unknown config field {k}")
+        setattr(c, k, v)
+    return c
+
+
+class Ensemble:
+    """All M members of one experiment on one GPU (the reference's `data` per rank x M,
+    plus its DataAssimilator)."""
+
+    def __init__(self, cfg: Config, device: int = 0):
+        self.lib = load_library()
+        self.cfg = cfg.copy()
+        self.nx, self.ny, self.M = cfg.nx, cfg.ny, cfg.n_ens
+        self.nxy = cfg.nx * cfg.ny
+        h = ctypes.c_void_p()
+        rc = self.lib.lbl_create(ctypes.byref(self.cfg), device, ctypes.byref(h))
+        self._h = h
+        if rc != 0:
+            msg = self.lib.lbl_last_error(h).decode() if h.value else "lbl_create"
+            if h.value:
+                self.lib.lbl_destroy(h)
+            self._h = ctypes.c_void_p()
+            raise LblError(rc, msg)
+
+    # -- plumbing ---------------------------------------------------------------
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise LblError(rc, f"{what}: {self.lib.lbl_last_error(self._h).decode()}")
+
+    def close(self):
+        if self._h and self._h.value:
+            self.lib.lbl_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the path ---------------------------------------------------------------
+    def init(self, ens_offset: int = 0):
+        self._check(self.lib.lbl_init(self._h, ens_offset), "lbl_init")
+
+    def update(self, t0: int = 0, nsteps: int = 1, sync: bool = True):
+        fn = self.lib.lbl_update if sync else self.lib.lbl_update_async
+        self._check(fn(self._h, t0, nsteps), "lbl_update")
+
+    def assimilate(self, t: int, rho_o, u_o, v_o, sync: bool = True):
+        ro, uo, vo = (_f32(a, self.nxy) for a in (rho_o, u_o, v_o))
+        fn = self.lib.lbl_assimilate if sync else self.lib.lbl_assimilate_async
+        self._check(fn(self._h, t, _fp(ro), _fp(uo), _fp(vo)), "lbl_assimilate")
+
+    def assimilate_files(self, t: int, io_prefix: str = "io"):
+        self._check(self.lib.lbl_assimilate_files(self._h, t, io_prefix.encode()), "lbl_assimilate_files")
+
+    def cycle_async(self, t: int, rho_o, u_o, v_o, n_fc: int):
+        if rho_o is None:
+            self._check(self.lib.lbl_cycle_async(self._h, t, None, None, None, n_fc), "lbl_cycle_async")
+            return
+        ro, uo, vo = (_f32(a, self.nxy) for a in (rho_o, u_o, v_o))
+        self._check(self.lib.lbl_cycle_async(self._h, t, _fp(ro), _fp(uo), _fp(vo), n_fc), "lbl_cycle_async")
+
+    def sync(self):
+        self._check(self.lib.lbl_sync(self._h), "lbl_sync")
+
+    def output(self, t: int, io_prefix: str = "io"):
+        self._check(self.lib.lbl_output(self._h, t, io_prefix.encode()), "lbl_output")
+
+    # -- accessors --------------------------------------------------------------
+    def get_f(self, member: int) -> np.ndarray:
+        out = np.empty(Q * self.nxy, np.float32)
+        self._check(self.lib.lbl_get_f(self._h, member, _fp(out)), "lbl_get_f")
+        return out.reshape(Q, self.ny, self.nx)
+
+    def set_f(self, member: int, f):
+        a = _f32(f, Q * self.nxy)
+        self._check(self.lib.lbl_set_f(self._h, member, _fp(a)), "lbl_set_f")
+
+    def get_fields(self, member: int) -> Tuple[np.ndarray, ...]:
+        r, u, v, w = (np.empty(self.nxy, np.float32) for _ in range(4))
+        self._check(self.lib.lbl_get_fields(self._h, member, _fp(r), _fp(u), _fp(v), _fp(w)), "lbl_get_fields")
+        return tuple(a.reshape(self.ny, self.nx) for a in (r, u, v, w))
+
+    def ens_stats(self) -> Tuple[np.ndarray, ...]:
+        a = [np.empty(self.nxy, np.float32) for _ in range(4)]
+        self._check(self.lib.lbl_get_ens_stats(self._h, *(_fp(x) for x in a)), "lbl_get_ens_stats")
+        return tuple(x.reshape(self.ny, self.nx) for x in a)
+
+    def force(self) -> Tuple[np.ndarray, np.ndarray]:
+        fx, fy = np.empty(self.nxy, np.float32), np.empty(self.nxy, np.float32)
+        self._check(self.lib.lbl_get_force(self._h, _fp(fx), _fp(fy)), "lbl_get_force")
+        return fx.reshape(self.ny, self.nx), fy.reshape(self.ny, self.nx)
+
+    def force_state(self) -> dict:
+        n = ctypes.c_int()
+        cur = ctypes.c_int()
+        self._check(self.lib.lbl_get_force_state(self._h, None, None, None, None, ctypes.byref(n), None),
+                    "lbl_get_force_state")
+        r, kx, ky, amp = (np.empty(4 * n.value, np.float32), np.empty(n.value, np.float32),
+                          np.empty(n.value, np.float32), np.empty(n.value, np.float32))
+        self._check(self.lib.lbl_get_force_state(self._h, _fp(r), _fp(kx), _fp(ky), _fp(amp), ctypes.byref(n),
+                                                 ctypes.byref(cur)), "lbl_get_force_state")
+        return {"randoms": r, "kx": kx, "ky": ky, "amp": amp, "n_modes": n.value, "cursor": cur.value}
+
+    def observed(self) -> Tuple[np.ndarray, ...]:
+        a = [np.empty(self.nxy, np.float32) for _ in range(4)]
+        self._check(self.lib.lbl_get_observed(self._h, *(_fp(x) for x in a)), "lbl_get_observed")
+        return tuple(x.reshape(self.ny, self.nx) for x in a)
+
+    def letkf_stats(self) -> dict:
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.lbl_get_letkf_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+                    "lbl_get_letkf_stats")
+        return {"max_sweeps": a.value, "n_noconv": b.value, "nan": c.value}
+
+    def diagnostics(self, member: int = -1) -> dict:
+        e, z, m = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.lbl_get_diagnostics(self._h, member, ctypes.byref(e), ctypes.byref(z), ctypes.byref(m)),
+                    "lbl_get_diagnostics")
+        return {"energy": e.value, "enstrophy": z.value, "mass": m.value}
+
+    def rmse_uv(self, u_true, v_true) -> float:
+        ut, vt = _f32(u_true, self.nxy), _f32(v_true, self.nxy)
+        r = ctypes.c_double()
+        self._check(self.lib.lbl_rmse_uv(self._h, _fp(ut), _fp(vt), ctypes.byref(r)), "lbl_rmse_uv")
+        return r.value
+
+    def timer_csv(self, which: int = TIMER_MAIN) -> str:
+        n = self.lib.lbl_timer_csv(self._h, which, None, 0)
+        if n < 0:
+            raise LblError(n, "lbl_timer_csv")
+        buf = ctypes.create_string_buffer(n + 1)
+        self.lib.lbl_timer_csv(self._h, which, buf, n + 1)
+        return buf.value.decode()
+
+    def profile_step(self, n: int) -> float:
+        """Average milliseconds per launch of the fused stream-collide kernel (CUDA events)."""
+        ms = ctypes.c_double()
+        self._check(self.lib.lbl_profile_step(self._h, n, ctypes.byref(ms)), "lbl_profile_step")
+        return ms.value
+
+    def event_record(self, slot: int):
+        """Record CUDA event `slot` (0..7) on the engine's stream."""
+        self._check(self.lib.lbl_event_record(self._h, slot), "lbl_event_record")
+
+    def event_elapsed(self, a: int, b: int) -> float:
+        """Milliseconds between recorded events a and b (waits for b)."""
+        ms = ctypes.c_double()
+        self._check(self.lib.lbl_event_elapsed(self._h, a, b, ctypes.byref(ms)), "lbl_event_elapsed")
+        return ms.value
+
+    def timer_transit(self, tag: str, which: int = TIMER_MAIN):
+        self._check(self.lib.lbl_timer_transit(self._h, which, tag.encode()), "lbl_timer_transit")
+
+    def timer_clear(self, which: int = TIMER_MAIN):
+        self._check(self.lib.lbl_timer_clear(self._h, which), "lbl_timer_clear")
+
+
+# --- functions named after the reference's host interface -----------------------
+def update(dat: Ensemble, t: int):
+    """One LBM step of every member (src/lbm.h:16-29)."""
+    dat.update(t, 1)
+
+
+class DataAssimilator:
+    """LETKF facade (src/assimilate.h:14-82); observations are read from `io_prefix`."""
+
+    def __init__(self, dat: Ensemble, io_prefix: str = "io"):
+        self.io_prefix = io_prefix
+
+    def assimilate(self, dat: Ensemble, t: int):
+        dat.assimilate_files(t, self.io_prefix)
+
+    def get_timer(self, dat: Ensemble) -> str:
+        return dat.timer_csv(TIMER_LETKF)
+
+
+def output(dat: Ensemble, t: int, io_prefix: str = "io"):
+    """Field files and ensemble statistics (src/io.cu:22-266)."""
+    dat.output(t, io_prefix)
+
+
+def version() -> str:
+    return load_library().lbl_version().decode()

@@ -1,0 +1,174 @@
+"""ORACLE (test infrastructure only): ctypes wrapper of liboracle.so, the FP64 CPU
+restatement of the reference's forecast-and-assimilate path (oracle.cpp).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only as the checker or the timed CPU baseline; the product path
+(liblbl.so) never calls it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_LBM = os.path.join(HERE, "_ref", "ref_lbm")
+Q = 9
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"oracle not built: {LIB_PATH} (run `make -C oracle liboracle.so`)")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, I = ctypes.c_void_p, ctypes.c_int
+    F = ctypes.POINTER(ctypes.c_float)
+    D = ctypes.POINTER(ctypes.c_double)
+    IP = ctypes.POINTER(ctypes.c_int)
+    sig = {
+        "orc_set_threads": (I, [I]),
+        "orc_create": (P, [P]),
+        "orc_destroy": (None, [P]),
+        "orc_ic_fields": (I, [P, I, F, F, F, F]),
+        "orc_init": (I, [P, I]),
+        "orc_force_modes": (I, [P, F, F, F, I]),
+        "orc_force": (I, [P, F, D, D]),
+        "orc_set_force": (I, [P, F, F]),
+        "orc_set_f": (I, [P, I, F]),
+        "orc_get_f": (I, [P, I, D]),
+        "orc_get_macros": (I, [P, I, D, D, D]),
+        "orc_step_noforce": (I, [P]),
+        "orc_step": (I, [P, I, F]),
+        "orc_vorticity_f32": (I, [P, F, F, F]),
+        "orc_observe": (I, [P, F, F, F, F, F, F, F]),
+        "orc_obs_weight": (I, [P, I, I, I, I, I, D, IP]),
+        "orc_assimilate": (I, [P, F, F, F, D]),
+        "orc_assimilate_rows": (I, [P, F, F, F, D, I, I]),
+        "orc_max_sweeps": (I, [P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _f(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32).reshape(-1)
+
+
+def set_threads(n: int) -> int:
+    return load().orc_set_threads(n)
+
+
+def ic_fields(cfg, seed: int):
+    """(r, u, v, f) of ensemble id `seed` exactly as stdata::init_lbm makes them (FP32)."""
+    lib = load()
+    nxy = cfg.nx * cfg.ny
+    r, u, v = (np.empty(nxy, np.float32) for _ in range(3))
+    f = np.empty(Q * nxy, np.float32)
+    lib.orc_ic_fields(ctypes.byref(cfg), seed, _f(r), _f(u), _f(v), _f(f))
+    sh = (cfg.ny, cfg.nx)
+    return r.reshape(sh), u.reshape(sh), v.reshape(sh), f.reshape((Q,) + sh)
+
+
+def force_modes(cfg):
+    lib = load()
+    kx, ky, amp = (np.empty(128, np.float32) for _ in range(3))
+    n = lib.orc_force_modes(ctypes.byref(cfg), _f(kx), _f(ky), _f(amp), 128)
+    return kx[:n].copy(), ky[:n].copy(), amp[:n].copy()
+
+
+def vorticity(cfg, u, v):
+    out = np.empty(cfg.nx * cfg.ny, np.float32)
+    load().orc_vorticity_f32(ctypes.byref(cfg), _f(_f32(u)), _f(_f32(v)), _f(out))
+    return out.reshape(cfg.ny, cfg.nx)
+
+
+class Oracle:
+    """FP64 CPU state of a whole ensemble (the oracle's counterpart of lbl.Ensemble)."""
+
+    def __init__(self, cfg):
+        self.lib = load()
+        self.cfg = cfg.copy()
+        self.nx, self.ny, self.M = cfg.nx, cfg.ny, cfg.n_ens
+        self.nxy = cfg.nx * cfg.ny
+        self.h = self.lib.orc_create(ctypes.byref(self.cfg))
+        if not self.h:
+            raise ValueError("orc_create rejected the configuration")
+
+    def close(self):
+        if self.h:
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self, ens_offset: int = 0):
+        self.lib.orc_init(self.h, ens_offset)
+
+    def set_f(self, m: int, f):
+        self.lib.orc_set_f(self.h, m, _f(_f32(f)))
+
+    def get_f(self, m: int) -> np.ndarray:
+        out = np.empty(Q * self.nxy, np.float64)
+        self.lib.orc_get_f(self.h, m, _d(out))
+        return out.reshape(Q, self.ny, self.nx)
+
+    def macros(self, m: int):
+        r, u, v = (np.empty(self.nxy, np.float64) for _ in range(3))
+        self.lib.orc_get_macros(self.h, m, _d(r), _d(u), _d(v))
+        return tuple(a.reshape(self.ny, self.nx) for a in (r, u, v))
+
+    def force(self, randoms):
+        fx, fy = np.empty(self.nxy, np.float64), np.empty(self.nxy, np.float64)
+        self.lib.orc_force(self.h, _f(_f32(randoms)), _d(fx), _d(fy))
+        return fx.reshape(self.ny, self.nx), fy.reshape(self.ny, self.nx)
+
+    def set_force(self, fx, fy):
+        self.lib.orc_set_force(self.h, _f(_f32(fx)), _f(_f32(fy)))
+
+    def step_noforce(self):
+        self.lib.orc_step_noforce(self.h)
+
+    def step(self, nsteps: int, randoms=None):
+        r = None if randoms is None else _f32(randoms)
+        self.lib.orc_step(self.h, nsteps, _f(r))
+
+    def observe(self, r, u, v):
+        ro, uo, vo, wo = (np.empty(self.nxy, np.float32) for _ in range(4))
+        self.lib.orc_observe(self.h, _f(_f32(r)), _f(_f32(u)), _f(_f32(v)), _f(ro), _f(uo), _f(vo), _f(wo))
+        return tuple(a.reshape(self.ny, self.nx) for a in (ro, uo, vo, wo))
+
+    def obs_weight(self, i, j, a, b, var):
+        w = ctypes.c_double()
+        valid = ctypes.c_int()
+        self.lib.orc_obs_weight(ctypes.byref(self.cfg), i, j, a, b, var, ctypes.byref(w), ctypes.byref(valid))
+        return w.value, bool(valid.value)
+
+    def assimilate_rows(self, rho_o, u_o, v_o, j0: int, j1: int):
+        return self.lib.orc_assimilate_rows(self.h, _f(_f32(rho_o)), _f(_f32(u_o)), _f(_f32(v_o)), None, j0, j1)
+
+    def assimilate(self, rho_o, u_o, v_o, want_lambda: bool = False):
+        lam = np.empty(self.nxy * self.M, np.float64) if want_lambda else None
+        sweeps = self.lib.orc_assimilate(self.h, _f(_f32(rho_o)), _f(_f32(u_o)), _f(_f32(v_o)), _d(lam))
+        return (sweeps, lam.reshape(self.ny, self.nx, self.M)) if want_lambda else sweeps

@@ -1,0 +1,78 @@
+// ref_lbm_harness.cu -- ORACLE TOOLING (test infrastructure only).
+//
+// A driver of our own around the reference's unmodified LBM sources
+// (src/lbm.cu, src/data.cu, compiled from where they lie by oracle/Makefile).  It
+// builds one reference `data` object (data.h:45-64: IC + forcing init) for a given
+// ensemble id and calls the reference's `update()` (lbm.h:16-29) step by step,
+// dumping the reference's own arrays (f, r, u, v, force_x, force_y, the cuRAND
+// normal buffer and its cursor) as raw little-endian float32 files.  The outputs
+// pin the CPU oracle and the CUDA engine against the reference itself.
+//
+// usage: ref_lbm <out_dir> <ensemble_id> <nsteps> <dump_step>[,<dump_step>...]
+#include <cstdio>
+#include <cstdlib>
+#include <set>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "config.h"
+#include "data.h"
+#include "lbm.h"
+
+static void dump(const std::string& name, const void* p, size_t bytes) {
+    std::FILE* fp = std::fopen(name.c_str(), "wb");
+    if (!fp) { std::fprintf(stderr, "cannot write %s\n", name.c_str()); std::exit(1); }
+    std::fwrite(p, 1, bytes, fp);
+    std::fclose(fp);
+}
+
+static void dump_state(data& dat, const std::string& dir, int step) {
+    cudaDeviceSynchronize();
+    const std::string pre = dir + "/s" + std::to_string(step) + "_";
+    const size_t nxy = size_t(config::nx) * config::ny;
+    dump(pre + "f.f32", dat.d().f.data(), sizeof(real) * nxy * config::Q);
+    dump(pre + "r.f32", dat.d().r.data(), sizeof(real) * nxy);
+    dump(pre + "u.f32", dat.d().u.data(), sizeof(real) * nxy);
+    dump(pre + "v.f32", dat.d().v.data(), sizeof(real) * nxy);
+    dump(pre + "fx.f32", dat.d0().force_x.data(), sizeof(real) * nxy);
+    dump(pre + "fy.f32", dat.d0().force_y.data(), sizeof(real) * nxy);
+    const int cursor = dat.d0().i_rand_outdated;
+    dump(pre + "cursor.i32", &cursor, sizeof(int));
+}
+
+int main(int argc, char** argv) {
+    if (argc < 5) { std::fprintf(stderr, "usage: %s out_dir ensemble_id nsteps dumps\n", argv[0]); return 2; }
+    const std::string dir = argv[1];
+    const int id = std::atoi(argv[2]);
+    const int nsteps = std::atoi(argv[3]);
+    std::set<int> dumps;
+    {
+        std::stringstream ss(argv[4]);
+        std::string tok;
+        while (std::getline(ss, tok, ',')) dumps.insert(std::atoi(tok.c_str()));
+    }
+    auto dat = data(id);
+    cudaDeviceSynchronize();
+    {  // forcing tables and the first normal buffer (serves the first 1023 forcing calls)
+        auto& d0 = dat.d0();
+        const int n = int(d0.force_amp.size());
+        dump(dir + "/modes_kx.f32", d0.force_kx.data(), sizeof(real) * n);
+        dump(dir + "/modes_ky.f32", d0.force_ky.data(), sizeof(real) * n);
+        dump(dir + "/modes_amp.f32", d0.force_amp.data(), sizeof(real) * n);
+        std::vector<float> buf(d0.n_rand_buf);
+        cudaMemcpy(buf.data(), d0.force_theta_d, sizeof(float) * buf.size(), cudaMemcpyDeviceToHost);
+        dump(dir + "/normals.f32", buf.data(), sizeof(float) * buf.size());
+    }
+    if (dumps.count(0)) dump_state(dat, dir, 0);
+    for (int s = 1; s <= nsteps; s++) {
+        update(dat, s - 1);
+        if (dumps.count(s)) dump_state(dat, dir, s);
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) { std::fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(e)); return 1; }
+    std::printf("ref_lbm: id %d, %d steps, dumps in %s\n", id, nsteps, dir.c_str());
+    return 0;
+}

@@ -1,0 +1,99 @@
+"""Output path and run modes on the GPU: OBSERVE files bit-exact against the oracle
+(io.cu:160-246), NATURE/DA_LETKF file layout and contents (io.cu:22-266), the
+ensemble statistics, and the lbl_run driver replaying main.cu's loop end to end."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG
+
+import lbl
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def read(path):
+    return np.fromfile(path, np.float32)
+
+
+def test_observe_files_bit_exact(tmp_path):
+    cfg = lbl.config_default("OBSERVE", 64, 1, da_xyprune=4, ioprune=1)
+    e = lbl.Ensemble(cfg)
+    e.init(0)
+    o = oracle.Oracle(cfg)  # its engine continues across outputs like the reference's static one
+    pre = str(tmp_path / "io")
+    for t in (0, cfg.iiter, 2 * cfg.iiter):
+        if t:
+            e.update(t - cfg.iiter, cfg.iiter)
+        e.output(t, pre)
+        r, u, v, w = e.get_fields(0)
+        want = o.observe(r, u, v)
+        step = f"{t // cfg.iiter:010d}"
+        for var, a in zip(("rho", "u", "v", "vor"), want):
+            got = read(f"{pre}/observed/ens0000/{var}_step{step}.dat")
+            np.testing.assert_array_equal(got, a.reshape(-1))  # NaN positions and bits identical
+        for var, a in zip(("rho", "u", "v", "vor"), (r, u, v, w)):
+            np.testing.assert_array_equal(read(f"{pre}/nature/ens0000/{var}_step{step}.dat"), a.reshape(-1))
+        assert not os.path.exists(f"{pre}/calc")  # OBSERVE writes no calc/ (io.cu:306-312)
+
+
+def test_nature_files_and_vorticity(tmp_path):
+    cfg = lbl.config_default("NATURE", 64, 2, ioprune=2)
+    e = lbl.Ensemble(cfg)
+    e.init(3)
+    pre = str(tmp_path / "io")
+    e.output(cfg.iiter, pre)  # off the IOPRUNE gate: nothing written
+    assert not os.path.exists(pre)
+    e.update(0, 2 * cfg.iiter)
+    e.output(2 * cfg.iiter, pre)
+    for k in range(2):
+        r, u, v, w = e.get_fields(k)
+        d = f"{pre}/calc/ens{k + 3:04d}"
+        np.testing.assert_array_equal(read(f"{d}/u_step0000000002.dat"), u.reshape(-1))
+        np.testing.assert_array_equal(read(f"{d}/vor_step0000000002.dat"), oracle.vorticity(cfg, u, v).reshape(-1))
+    assert not os.path.exists(f"{pre}/nature")  # ensemble id 0 is not in this run (ofs = 3)
+
+
+def test_da_output_with_ensemble_statistics(tmp_path):
+    cfg = lbl.config_default("DA_LETKF", 64, 4, ioprune=1)
+    e = lbl.Ensemble(cfg)
+    e.init(0)
+    e.update(0, 10)
+    pre = str(tmp_path / "io")
+    e.output(cfg.iiter, pre)
+    us = np.stack([e.get_fields(k)[1] for k in range(4)])
+    ws = np.stack([e.get_fields(k)[3] for k in range(4)])
+    np.testing.assert_allclose(read(f"{pre}/calc/ens_mean_u_step0000000001.dat"), us.mean(0).reshape(-1), rtol=1e-5, atol=1e-9)
+    np.testing.assert_allclose(read(f"{pre}/calc/ens_vor_mean_step0000000001.dat"), ws.mean(0).reshape(-1), rtol=1e-4, atol=1e-6)
+    std = read(f"{pre}/calc/ens_vor_std_step0000000001.dat")
+    ok = np.isfinite(std)
+    np.testing.assert_allclose(std[ok], ws.std(0).reshape(-1)[ok], rtol=2e-2, atol=1e-3)
+    for k in range(4):
+        assert os.path.exists(f"{pre}/calc/ens{k:04d}/rho_step0000000001.dat")
+    um, vm, wm, wsd = e.ens_stats()
+    np.testing.assert_allclose(um, us.mean(0), rtol=1e-5, atol=1e-9)
+
+
+def test_driver_observe_then_letkf(tmp_path):
+    """lbl_run replays main.cu: OBSERVE writes io/observed, DA_LETKF reads it."""
+    exe = os.path.join(PKG, "lbl_run")
+    pre = str(tmp_path / "io")
+    common = ["--nx=64", "--SPINUP=0", "--ITER_MAIN=100", "--IOPRUNE=2", "--DA_XYPRUNE=4", f"--PREFIX={pre}"]
+    subprocess.run([exe, "--mode=OBSERVE", *common], check=True, capture_output=True, timeout=300)
+    assert os.path.exists(f"{pre}/observed/ens0000/u_step0000000020.dat")
+    out = subprocess.run([exe, "--mode=DA_LETKF", "--n_ens=4", "--DAPRUNE=2", "--LETKF_RLOC_LEN=1",
+                          "--LETKF_COVINF=1.1", *common], check=True, capture_output=True, text=True, timeout=300)
+    assert "ensemble GLUPS" in out.stdout
+    main_csv = open(f"{pre}/elapsed_time_rank0.csv").read()
+    assert main_csv.startswith("#tag,sec\n")
+    tags = [l.split(",")[0] for l in main_csv.strip().split("\n")[1:]]
+    for tag in ("DA", "forecast", "output", "_sync.DA"):
+        assert tag in tags
+    letkf_csv = open(f"{pre}/letkf_elapsed_time_rank0.csv").read()
+    assert "solve," in letkf_csv and "load_obs," in letkf_csv
+    for k in range(4):
+        assert os.path.exists(f"{pre}/calc/ens{k:04d}/vor_step0000000020.dat")
+    assert os.path.exists(f"{pre}/calc/ens_vor_std_step0000000020.dat")

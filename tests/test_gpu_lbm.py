@@ -1,0 +1,167 @@
+"""Forecast path on the GPU, through the C ABI, against the reference's own run
+(golden fixtures) and the FP64 oracle: initial condition, forcing (cuRAND stream,
+cursor, field), fused stream-collide, macros, graphs and chunking."""
+import numpy as np
+import pytest
+
+from conftest import checksums, golden, rel_err
+
+import lbl
+import oracle
+
+pytestmark = pytest.mark.gpu
+N4 = 4 * 29
+
+
+def nature(nx=256, M=1, ofs=0, **kw):
+    e = lbl.Ensemble(lbl.config_default("NATURE", nx, M, **kw))
+    e.init(ofs)
+    return e
+
+
+def test_initial_condition_matches_oracle_bitwise():
+    e = nature(256)
+    r, u, v, f = oracle.ic_fields(e.cfg, 0)
+    np.testing.assert_array_max_ulp(e.get_f(0), f, maxulp=2)
+    rr, uu, vv, _ = e.get_fields(0)
+    np.testing.assert_array_max_ulp(uu, u, maxulp=2)
+    np.testing.assert_array_max_ulp(vv, v, maxulp=2)
+    np.testing.assert_array_equal(rr, r)
+
+
+@pytest.mark.parametrize("name,mode,seed_member", [("ref_lbm_id0.npz", "NATURE", 0), ("ref_lbm_id334.npz", "DA_LETKF", 0)])
+def test_initial_condition_matches_reference(name, mode, seed_member):
+    g = golden(name)
+    e = lbl.Ensemble(lbl.config_default(mode, 256, 2))
+    e.init(0)
+    f = e.get_f(seed_member)
+    rows = g["rows"]
+    np.testing.assert_array_max_ulp(f[:, rows, :], g["s0_rows_f"], maxulp=1)
+    np.testing.assert_allclose(checksums(f), g["s0_sums_f"], rtol=1e-7)
+
+
+def test_forcing_stream_and_cursor_match_reference():
+    g = golden("ref_lbm_id0.npz")
+    e = nature(256)
+    st = e.force_state()
+    np.testing.assert_array_equal(st["kx"], g["kx"])
+    np.testing.assert_array_equal(st["amp"], g["amp"])
+    assert st["cursor"] == int(g["s0_cursor"][0]) == N4
+    np.testing.assert_array_equal(st["randoms"], g["normals_head"][N4:2 * N4])  # cuRAND MTGP32, seed 1991
+    e.update(0, 1)
+    st = e.force_state()
+    assert st["cursor"] == int(g["s1_cursor"][0])
+    np.testing.assert_array_equal(st["randoms"], g["normals_head"][2 * N4:3 * N4])
+    fx, fy = e.force()
+    rows = g["rows"]
+    assert rel_err(fx[rows], g["s1_rows_fx"]) < 1e-6
+    assert rel_err(fy[rows], g["s1_rows_fy"]) < 1e-6
+
+
+def test_steps_match_reference_within_1e5():
+    """Populations after 1, 10 and 100 steps within 1e-5 relative of the reference's."""
+    g = golden("ref_lbm_id0.npz")
+    e = nature(256)
+    rows = g["rows"]
+    done = 0
+    worst = {}
+    for s in sorted(int(x) for x in g["steps"]):
+        if s > done:
+            e.update(done, s - done)
+            done = s
+        f = e.get_f(0).astype(np.float64)
+        ref = g[f"s{s}_rows_f"].astype(np.float64)
+        err = float(np.max(np.abs(f[:, rows, :] - ref) / np.abs(ref)))
+        worst[s] = err
+        assert err < 1e-5, (s, err)
+        np.testing.assert_allclose(checksums(f), g[f"s{s}_sums_f"], rtol=1e-6)
+        if s > 0:
+            r, u, v, _ = e.get_fields(0)
+            assert rel_err(u[rows], g[f"s{s}_rows_u"]) < 1e-4
+            assert rel_err(r[rows], g[f"s{s}_rows_r"]) < 1e-6
+    print("max relative error vs reference per step:", worst)
+
+
+def test_forcing_field_matches_oracle():
+    e = nature(128, M=1)
+    o = oracle.Oracle(e.cfg)
+    for _ in range(3):
+        e.update(0, 1)
+        st = e.force_state()
+        fx, fy = e.force()
+        ofx, ofy = o.force(st["randoms"])
+        assert rel_err(fx, ofx) < 2e-5
+        assert rel_err(fy, ofy) < 2e-5
+
+
+def test_stream_collide_matches_fp64_oracle():
+    """Engine forces injected into the oracle each step; 50 steps, 3 members."""
+    e = nature(128, M=3, ofs=5)
+    o = oracle.Oracle(e.cfg)
+    for m in range(3):
+        o.set_f(m, e.get_f(m))
+    for t in range(50):
+        e.update(t, 1)
+        fx, fy = e.force()
+        o.set_force(fx, fy)
+        o.step_noforce()
+    for m in range(3):
+        fe, fo = e.get_f(m).astype(np.float64), o.get_f(m)
+        assert np.max(np.abs(fe - fo) / np.abs(fo)) < 1e-5
+        r, u, v, _ = e.get_fields(m)
+        ro, uo, vo = o.macros(m)
+        assert rel_err(u, uo) < 1e-4 and rel_err(v, vo) < 1e-4
+        assert rel_err(r, ro) < 1e-6
+
+
+def test_chunking_and_graphs_are_bitwise_invariant():
+    a = nature(128, M=2)
+    b = nature(128, M=2)
+    a.update(0, 37)
+    for t in range(37):
+        b.update(t, 1)
+    for m in range(2):
+        np.testing.assert_array_equal(a.get_f(m), b.get_f(m))
+        np.testing.assert_array_equal(a.get_fields(m)[2], b.get_fields(m)[2])
+
+
+def test_members_are_independent_runs():
+    big = nature(128, M=3)
+    big.update(0, 10)
+    for k in range(3):
+        one = nature(128, M=1, ofs=k)
+        one.update(0, 10)
+        np.testing.assert_array_equal(big.get_f(k), one.get_f(0))
+
+
+def test_long_run_crosses_normal_refill():
+    """1100 steps cross the 1023-call refill of the cuRAND buffer (data.cu:241-247)."""
+    e = nature(64, M=1)
+    e.update(0, 1100)
+    st = e.force_state()
+    assert st["cursor"] == ((2 + 1100 - 1) % 1023) * N4
+    f = e.get_f(0)
+    assert np.all(np.isfinite(f))
+
+
+def test_diagnostics_fp64():
+    e = nature(128, M=2)
+    e.update(0, 5)
+    r, u, v, w = e.get_fields(1)
+    d = e.diagnostics(1)
+    np.testing.assert_allclose(d["energy"], 0.5 * np.mean(u.astype(np.float64) ** 2 + v.astype(np.float64) ** 2), rtol=1e-9)
+    np.testing.assert_allclose(d["mass"], np.mean(r.astype(np.float64)), rtol=1e-12)
+    np.testing.assert_allclose(d["enstrophy"], 0.5 * np.mean(w.astype(np.float64) ** 2), rtol=1e-4)
+
+
+def test_errors_are_reported_not_crashed():
+    with pytest.raises(lbl.LblError) as ei:
+        lbl.Ensemble(lbl.config_default("NATURE", 100, 1))
+    assert ei.value.code == -1
+    with pytest.raises(lbl.LblError) as ei:
+        lbl.Ensemble(lbl.config_default("DA_LETKF", 64, 1))
+    assert ei.value.code == -8
+    e = lbl.Ensemble(lbl.config_default("NATURE", 64, 1))
+    with pytest.raises(lbl.LblError) as ei:
+        e.update(0, 1)
+    assert ei.value.code == -6

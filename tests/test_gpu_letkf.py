@@ -1,0 +1,150 @@
+"""LETKF analysis on the GPU, through the C ABI, against the FP64 oracle on
+identical forecast ensembles and observations, for the reference's window
+geometries (p = 1 pointwise, p > 1 R-localised, LETKF_RLOC_LEN), ensemble sizes
+and inflation; plus the stale-v quirk, the DA gate, NaN reporting and the
+one-graph cycle."""
+import numpy as np
+import pytest
+
+import lbl
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def make_case(nx, M, p, L, beta, steps=30, sig_u=0.002, sig_r=1e-4, **kw):
+    cfg = lbl.config_default("DA_LETKF", nx, M, da_xyprune=p, letkf_rloc_len=L, letkf_covinf=beta,
+                             obs_error_u=sig_u, obs_error_rho=sig_r, daprune=1, **kw)
+    e = lbl.Ensemble(cfg)
+    e.init(0)
+    e.update(0, steps)
+    nat = lbl.Ensemble(lbl.config_default("NATURE", nx, 1))
+    nat.init(0)
+    nat.update(0, steps)
+    r, u, v, _ = nat.get_fields(0)
+    rng = np.random.default_rng(nx + M + p)
+    ro = (r + sig_r * rng.standard_normal(r.shape)).astype(np.float32)
+    uo = (u + sig_u * rng.standard_normal(u.shape)).astype(np.float32)
+    vo = (v + sig_u * rng.standard_normal(v.shape)).astype(np.float32)
+    off = np.ones_like(ro, bool)
+    off[::p, ::p] = False
+    for a in (ro, uo, vo):
+        a[off] = np.nan  # like io/observed files: NaN off the observation lattice
+    return cfg, e, (ro, uo, vo), u, v
+
+
+CASES = [  # nx, M, p, L, beta
+    (64, 4, 1, 0, 1.0),
+    (64, 8, 2, 0, 1.1),
+    (64, 16, 4, 1, 1.1),
+    (64, 6, 4, 1, 1.05),
+    (64, 32, 4, 1, 1.1),
+    (128, 16, 4, 2, 1.2),
+    (256, 16, 4, 1, 1.1),
+]
+
+
+@pytest.mark.parametrize("nx,M,p,L,beta", CASES)
+def test_analysis_matches_oracle(nx, M, p, L, beta):
+    cfg, e, obs, _, _ = make_case(nx, M, p, L, beta)
+    F = [e.get_f(m) for m in range(M)]
+    o = oracle.Oracle(cfg)
+    for m in range(M):
+        o.set_f(m, F[m])
+    t = cfg.iiter
+    e.assimilate(t, *obs)
+    o.assimilate(*obs)
+    st = e.letkf_stats()
+    assert st["nan"] == 0 and st["n_noconv"] == 0 and 1 <= st["max_sweeps"] <= 30, st
+    inc_e = np.stack([e.get_f(m).astype(np.float64) - F[m] for m in range(M)])
+    inc_o = np.stack([o.get_f(m) - F[m] for m in range(M)])
+    scale = np.max(np.abs(inc_o))
+    assert scale > 1e-6  # the analysis does something
+    # analysis increments within 1e-3 of their largest magnitude (FP32 Gram/Jacobi vs FP64)
+    assert np.max(np.abs(inc_e - inc_o)) / scale < 1e-3
+    # populations themselves within 1e-5 relative
+    fa = np.stack([o.get_f(m) for m in range(M)])
+    assert np.max(np.abs(np.stack([e.get_f(m) for m in range(M)]) - fa) / np.abs(fa)) < 1e-5
+
+
+def test_analysis_reduces_error():
+    cfg, e, obs, u_true, v_true = make_case(64, 16, 2, 0, 1.1)
+    before = e.rmse_uv(u_true, v_true)
+    e.assimilate(cfg.iiter, *obs)
+    after = e.rmse_uv(u_true, v_true)
+    assert after < 0.7 * before, (before, after)
+
+
+def test_stale_v_after_analysis():
+    for stale in (1, 0):
+        cfg, e, obs, _, _ = make_case(64, 4, 2, 0, 1.0, compat_stale_v=stale)
+        e.assimilate(cfg.iiter, *obs)
+        f = e.get_f(1).astype(np.float64)
+        r, u, v, _ = e.get_fields(1)
+        ey = np.array([(q // 3) - 1 for q in range(9)], float)
+        ex = np.array([(q % 3) - 1 for q in range(9)], float)
+        v_mom = np.tensordot(ey * 20, f, axes=(0, 0)) / f.sum(0)
+        u_mom = np.tensordot(ex * 20, f, axes=(0, 0)) / f.sum(0)
+        np.testing.assert_allclose(u, u_mom, rtol=1e-4, atol=1e-6)
+        if stale:
+            assert np.max(np.abs(v - v_mom)) > 1e-6  # letkf.cu:340-355 leaves v untouched
+        else:
+            np.testing.assert_allclose(v, v_mom, rtol=1e-4, atol=1e-6)
+
+
+def test_gate_skips_off_cycle():
+    cfg, e, obs, _, _ = make_case(64, 4, 2, 0, 1.0)
+    e2 = lbl.Ensemble(lbl.config_default("DA_LETKF", 64, 4, da_xyprune=2, daprune=5))
+    e2.init(0)
+    g0 = e2.get_f(0)
+    e2.assimilate(e2.cfg.iiter * 3, *obs)  # step 3 is not a multiple of DAPRUNE=5
+    np.testing.assert_array_equal(e2.get_f(0), g0)
+
+
+def test_nan_observation_is_reported():
+    cfg, e, (ro, uo, vo), _, _ = make_case(64, 4, 2, 0, 1.0)
+    uo = uo.copy()
+    uo[0, 0] = np.nan  # an observed site
+    with pytest.raises(lbl.LblError) as ei:
+        e.assimilate(cfg.iiter, ro, uo, vo)
+    assert ei.value.code == -5
+
+
+def test_cycle_graph_equals_separate_calls():
+    cfg, a, obs, _, _ = make_case(64, 8, 4, 1, 1.1)
+    b = lbl.Ensemble(cfg)
+    b.init(0)
+    b.update(0, 30)
+    t = cfg.iiter
+    a.cycle_async(t, *obs, 20)
+    a.sync()
+    b.assimilate(t, *obs)
+    b.update(t, 20)
+    for m in range(cfg.n_ens):
+        np.testing.assert_array_equal(a.get_f(m), b.get_f(m))
+    # NULL observation pointers reuse the observations already on the device
+    c = lbl.Ensemble(cfg)
+    c.init(0)
+    d = lbl.Ensemble(cfg)
+    d.init(0)
+    for x in (c, d):
+        x.update(0, 30)
+        x.cycle_async(t, *obs, 5)
+    c.cycle_async(2 * t, None, None, None, 5)
+    d.cycle_async(2 * t, *obs, 5)
+    c.sync()
+    d.sync()
+    for m in range(cfg.n_ens):
+        np.testing.assert_array_equal(c.get_f(m), d.get_f(m))
+
+
+def test_letkf_timer_tags():
+    cfg, e, obs, _, _ = make_case(64, 4, 2, 0, 1.0)
+    e.assimilate(cfg.iiter, *obs)
+    csv = e.timer_csv(lbl.TIMER_LETKF)
+    assert csv.startswith("#tag,sec\n")
+    tags = [line.split(",")[0] for line in csv.strip().split("\n")[1:]]
+    for tag in ("pack_xk", "pack_yk", "mpi_yk", "load_obs", "set_yo", "mpi_xk", "solve_comm_ovlp",
+                "mpi_barrier", "solve", "mpi_xsol", "update_xk", "lbm2euler"):
+        assert tag in tags
+    assert tags == sorted(tags)  # std::map order (util/timer.hpp:66-72)
