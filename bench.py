@@ -324,6 +324,22 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def profile_cycles(args):
+    """The workload's cycles only (no timing, no baseline): a clean launch list for ncu."""
+    import lbl
+    obs, _ = make_observations(lbl, 1)
+    ens = lbl.Ensemble(workload_config(lbl))
+    ens.init(0)
+    T = STEPS_PER_CYCLE
+    ens.cycle_async(0, None, None, None, T)
+    ens.cycle_async(T, *obs[0], T)
+    for c in range(args.warmup + args.steps):
+        ens.cycle_async((c + 2) * T, None, None, None, T)
+    ens.sync()
+    print("profile cycles done:", ens.letkf_stats())
+    ens.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -331,9 +347,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="run warmup + steps cycles of the workload and exit (for ncu captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.profile:
+        profile_cycles(args)
+        return
     if args.impl == "reference":
         # the CPU reference arm runs on rank 0 only; other ranks exit without work
         rank = int(os.environ.get("RANK", "0"))

@@ -76,10 +76,13 @@ def test_steps_match_reference_within_1e5():
         assert err < 1e-5, (s, err)
         np.testing.assert_allclose(checksums(f), g[f"s{s}_sums_f"], rtol=1e-6)
         if s > 0:
+            # u = c*sum(f e_x)/rho cancels O(0.1) populations down to O(1e-3): a 1e-5 bound on
+            # f allows ~1e-3 of max|u|; rho = sum(f) keeps the population bound
             r, u, v, _ = e.get_fields(0)
-            assert rel_err(u[rows], g[f"s{s}_rows_u"]) < 1e-4
-            assert rel_err(r[rows], g[f"s{s}_rows_r"]) < 1e-6
-    print("max relative error vs reference per step:", worst)
+            assert rel_err(u[rows], g[f"s{s}_rows_u"]) < 1e-3
+            assert rel_err(v[rows], g[f"s{s}_rows_v"]) < 1e-3
+            assert rel_err(r[rows], g[f"s{s}_rows_r"]) < 1e-5
+    print("max relative population error vs reference per step:", worst)
 
 
 def test_forcing_field_matches_oracle():
@@ -110,8 +113,8 @@ def test_stream_collide_matches_fp64_oracle():
         assert np.max(np.abs(fe - fo) / np.abs(fo)) < 1e-5
         r, u, v, _ = e.get_fields(m)
         ro, uo, vo = o.macros(m)
-        assert rel_err(u, uo) < 1e-4 and rel_err(v, vo) < 1e-4
-        assert rel_err(r, ro) < 1e-6
+        assert rel_err(u, uo) < 1e-3 and rel_err(v, vo) < 1e-3
+        assert rel_err(r, ro) < 1e-5  # FP32 storage of f vs FP64 over 50 steps
 
 
 def test_chunking_and_graphs_are_bitwise_invariant():
