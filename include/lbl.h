@@ -167,8 +167,8 @@ int lbl_get_force_state(lbl_ctx* ctx, float* randoms /* 4*n_modes */, float* kx,
 /* Observations generated by OBSERVE mode at the last output (host copies). */
 int lbl_get_observed(lbl_ctx* ctx, float* rho_o, float* u_o, float* v_o, float* vor_o);
 /* Analysis diagnostics of the last assimilate: max Jacobi sweeps, number of
- * grid points that hit the sweep limit, NaN flag. */
-int lbl_get_letkf_stats(lbl_ctx* ctx, int* max_sweeps, int* n_noconv, int* nan_flag);
+ * grid points that hit the sweep limit, NaN flag, sweeps summed over grid points. */
+int lbl_get_letkf_stats(lbl_ctx* ctx, int* max_sweeps, int* n_noconv, int* nan_flag, int* total_sweeps);
 /* FP64 domain reductions of member `member` (-1 = ensemble mean fields):
  * kinetic energy, enstrophy, mass (src/data.cu:458-542 inspect()). */
 int lbl_get_diagnostics(lbl_ctx* ctx, int member, double* energy, double* enstrophy, double* mass);

@@ -81,8 +81,10 @@ int set_device(lbl_ctx* ctx) {
 Phys derive_phys(const lbl_config& cfg) {
     Phys P{};
     P.nx = cfg.nx; P.ny = cfg.ny; P.M = cfg.n_ens; P.nxy = cfg.nx * cfg.ny;
+    // the reference's constexpr `real` arithmetic: h_ref is rounded to float first
+    // (config.h:158), then divided in float (config.h:250-251)
     P.c = float(cfg.u_ref) / float(cfg.cfl);                       // config.h:248 (constexpr real)
-    P.dx = float(cfg.h_ref / (cfg.ny - 1));                        // config.h:250
+    P.dx = float(cfg.h_ref) / float(cfg.ny - 1);                   // config.h:250
     P.dt = P.dx / P.c;                                             // config.h:251
     double nu = cfg.nu;
     if (cfg.tau > 0) nu = (cfg.tau - 0.5) * double(P.c) * double(P.c) * double(P.dt) / 3.0;
@@ -207,8 +209,8 @@ int upload_obs(lbl_ctx* ctx, const float* ro, const float* uo, const float* vo) 
 
 // enqueue: forcing chunk + n LBM steps starting from buffer `cur`; macros are
 // written on the last two steps (the only ones output/lbm2euler can observe).
-void enqueue_steps(lbl_ctx* ctx, int n, int cur, cudaStream_t s) {
-    launch_force_chunk(ctx, n, 0, s);
+void enqueue_steps(lbl_ctx* ctx, int n, int cur, cudaStream_t s, bool force_done = false) {
+    if (!force_done) launch_force_chunk(ctx, n, 0, s);
     for (int k = 0; k < n; k++) {
         const int src = (cur + k) & 1, dst = src ^ 1;
         const bool mac = k >= n - 2;
@@ -218,6 +220,7 @@ void enqueue_steps(lbl_ctx* ctx, int n, int cur, cudaStream_t s) {
 }
 
 void enqueue_analysis(lbl_ctx* ctx, int cur, cudaStream_t s) {
+    cudaMemsetAsync(ctx->d_stats, 0, sizeof(int) * 4, s);
     launch_obs_ensemble(ctx, ctx->f[cur], s);
     launch_analysis(ctx, ctx->f[cur], ctx->f[cur ^ 1], ctx->mac[cur ^ 1], s);
 }
@@ -230,8 +233,21 @@ int launch_graph(lbl_ctx* ctx, int kind, int n) {
         cudaGraph_t g = nullptr;
         LBL_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         int cur = ctx->cur;
-        if (kind == 1) { enqueue_analysis(ctx, cur, ctx->stream); cur ^= 1; }
-        if (n > 0) enqueue_steps(ctx, n, cur, ctx->stream);
+        if (kind == 1 && n > 0) {
+            // the forcing of the coming steps does not depend on the flow: compute it
+            // on a side branch while the analysis runs (different pipes: XU/FP64 vs FMA/SHFL)
+            cudaEventRecord(ctx->fork_ev, ctx->stream);
+            cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0);
+            launch_force_chunk(ctx, n, 0, ctx->side);
+            cudaEventRecord(ctx->join_ev, ctx->side);
+            enqueue_analysis(ctx, cur, ctx->stream);
+            cur ^= 1;
+            cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0);
+            enqueue_steps(ctx, n, cur, ctx->stream, true);
+        } else {
+            if (kind == 1) { enqueue_analysis(ctx, cur, ctx->stream); cur ^= 1; }
+            if (n > 0) enqueue_steps(ctx, n, cur, ctx->stream);
+        }
         const cudaError_t le = cudaGetLastError();
         const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &g);
         if (le != cudaSuccess || ee != cudaSuccess) {
@@ -332,6 +348,7 @@ int build_weight_table(lbl_ctx* ctx) {
                 for (int a = 0; a < G.nox; a++) {
                     const int da = a - (G.nl - G.off), db = b - (G.nl - G.off);
                     const int di = pi - da * G.p, dj = pj - db * G.p;   // i - io, j - jo
+                    (void)da; (void)db;
                     const bool valid = !(std::abs(di) > G.nl * G.p || std::abs(dj) > G.nl * G.p);
                     if (!valid) continue;
                     double gc = 1.0;
@@ -341,7 +358,9 @@ int build_weight_table(lbl_ctx* ctx) {
                         const float w = float(gc / (sig * sig));
                         if (!(w > 0.f)) continue;
                         int* e = tab.data() + (size_t(pat) * G.nobs + n) * 4;
-                        e[0] = da; e[1] = db; e[2] = var;
+                        e[0] = a + G.nox * b + var * G.nox * G.nox;  // window slot (letkf.cu:155, 183-185)
+                        e[1] = var;
+                        e[2] = 0;
                         std::memcpy(&e[3], &w, sizeof(float));
                         n++;
                     }
@@ -361,6 +380,9 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     ctx->G = derive_geo(*cfg);
     LBL_TRY(set_device(ctx));
     LBL_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    LBL_CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    LBL_CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+    LBL_CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
     const size_t nxy = size_t(ctx->P.nxy), M = size_t(ctx->P.M);
     for (int b = 0; b < 2; b++) {
         LBL_CK(cudaMalloc(&ctx->f[b], sizeof(float) * M * kQ * nxy));
@@ -389,10 +411,19 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
         const float total = float(cfg->fkf * cfg->u_ref / 1.0);
         for (int i = 0; i < n; i++) ctx->h_amp[i] = float(ctx->h_amp[i] * (total / asum));
         ctx->n_modes = n;
-        std::vector<float> tab(3 * n);
-        for (int i = 0; i < n; i++) { tab[i] = ctx->h_kx[i]; tab[n + i] = ctx->h_ky[i]; tab[2 * n + i] = ctx->h_amp[i]; }
-        LBL_CK(cudaMalloc(&ctx->d_modes, sizeof(float) * 3 * n));
-        LBL_CK(cudaMemcpy(ctx->d_modes, tab.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice));
+        std::vector<float> tab(2 * n);
+        std::vector<double> amps(2 * n);
+        for (int i = 0; i < n; i++) {
+            tab[i] = ctx->h_kx[i];
+            tab[n + i] = ctx->h_ky[i];
+            // amp*2*M_PI*ky, amp*2*M_PI*(-kx) of data.cu:342-343, evaluated left to right in FP64
+            amps[i] = double(ctx->h_amp[i] * 2) * M_PI * double(ctx->h_ky[i]);
+            amps[n + i] = double(ctx->h_amp[i] * 2) * M_PI * double(-ctx->h_kx[i]);
+        }
+        LBL_CK(cudaMalloc(&ctx->d_modes, sizeof(float) * 2 * n));
+        LBL_CK(cudaMemcpy(ctx->d_modes, tab.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice));
+        LBL_CK(cudaMalloc(&ctx->d_amps, sizeof(double) * 2 * n));
+        LBL_CK(cudaMemcpy(ctx->d_amps, amps.data(), sizeof(double) * 2 * n, cudaMemcpyHostToDevice));
         ctx->n_rand_buf = n * 4096;                                        // data.cu:297
         LBL_CK(cudaMalloc(&ctx->d_pool, sizeof(float) * ctx->pool_slots * size_t(ctx->n_rand_buf)));
     }
@@ -414,7 +445,7 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
         LBL_CK(cudaMalloc(&ctx->d_dyo, sizeof(float) * 3 * ns));
     }
     LBL_CK(cudaMalloc(&ctx->d_stats, sizeof(int) * 4));
-    LBL_CK(cudaMemset(ctx->d_stats, 0, sizeof(int) * 4));
+    LBL_CK(cudaMemset(ctx->d_stats, 0, sizeof(int) * 4));  // max sweeps, non-converged, NaN, sweep total
     LBL_CK(cudaMalloc(&ctx->d_red, sizeof(double) * 8));
     LBL_CK(cudaMalloc(&ctx->d_tmp, sizeof(float) * 2 * nxy));
     for (auto& e : ctx->ev) LBL_CK(cudaEventCreate(&e));
@@ -433,7 +464,7 @@ void destroy_impl(lbl_ctx* ctx) {
     ctx->graphs.clear();
     if (ctx->gen) curandDestroyGenerator(ctx->gen);
     for (int b = 0; b < 2; b++) { cudaFree(ctx->f[b]); cudaFree(ctx->mac[b]); }
-    cudaFree(ctx->d_modes); cudaFree(ctx->d_pool); cudaFree(ctx->d_force); cudaFree(ctx->d_sched);
+    cudaFree(ctx->d_modes); cudaFree(ctx->d_amps); cudaFree(ctx->d_pool); cudaFree(ctx->d_force); cudaFree(ctx->d_sched);
     cudaFree(ctx->d_wtab); cudaFree(ctx->d_yo); cudaFree(ctx->d_dY); cudaFree(ctx->d_dyo);
     cudaFree(ctx->d_stats); cudaFree(ctx->d_red); cudaFree(ctx->d_tmp);
     for (int b = 0; b < 2; b++) {
@@ -445,6 +476,9 @@ void destroy_impl(lbl_ctx* ctx) {
         for (auto& e : ctx->user_ev) cudaEventDestroy(e);
     }
     if (ctx->obs_engine) obs_engine_free(ctx->obs_engine);
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
 }
 
@@ -514,7 +548,7 @@ int assimilate_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
     timer_transit(tm, "_ignored");                                  // letkf.cu:121
     if (!da_due(ctx, t)) return LBL_OK;                             // letkf.cu:122-123
     if (!ro || !uo || !vo) return fail(ctx, LBL_ERR_ARG, "null observation pointer");
-    LBL_CK(cudaMemsetAsync(ctx->d_stats, 0, sizeof(int) * 3, ctx->stream));
+    LBL_CK(cudaMemsetAsync(ctx->d_stats, 0, sizeof(int) * 4, ctx->stream));
     const double h0 = wall_time();
     LBL_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     LBL_TRY(upload_obs(ctx, ro, uo, vo));
@@ -871,14 +905,15 @@ int lbl_get_observed(lbl_ctx* ctx, float* rho_o, float* u_o, float* v_o, float* 
     return LBL_OK;
 }
 
-int lbl_get_letkf_stats(lbl_ctx* ctx, int* max_sweeps, int* n_noconv, int* nan_flag) {
+int lbl_get_letkf_stats(lbl_ctx* ctx, int* max_sweeps, int* n_noconv, int* nan_flag, int* total_sweeps) {
     if (!ctx) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
     LBL_CK(cudaStreamSynchronize(ctx->stream));
-    LBL_CK(cudaMemcpy(ctx->h_stats, ctx->d_stats, sizeof(int) * 3, cudaMemcpyDeviceToHost));
+    LBL_CK(cudaMemcpy(ctx->h_stats, ctx->d_stats, sizeof(int) * 4, cudaMemcpyDeviceToHost));
     if (max_sweeps) *max_sweeps = ctx->h_stats[0];
     if (n_noconv) *n_noconv = ctx->h_stats[1];
     if (nan_flag) *nan_flag = ctx->h_stats[2];
+    if (total_sweeps) *total_sweeps = ctx->h_stats[3];
     return LBL_OK;
 }
 

@@ -65,6 +65,8 @@ struct lbl_ctx {
     bool initialised = false;
     std::string err;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;         // forcing branch of the cycle graph
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 
     // ensemble state, double buffered like data::d()/dn() (data.h:45-64)
     float* f[2] = {nullptr, nullptr};    // [M][9][ny][nx]
@@ -74,7 +76,8 @@ struct lbl_ctx {
     // forcing (data.cu:161-350)
     int n_modes = 0;
     float h_kx[lbl::kMaxModes], h_ky[lbl::kMaxModes], h_amp[lbl::kMaxModes];
-    float* d_modes = nullptr;            // [3][n_modes]
+    float* d_modes = nullptr;            // [2][n_modes] kx, ky
+    double* d_amps = nullptr;            // [2][n_modes] amp*2*pi*ky, amp*2*pi*(-kx) in FP64
     curandGenerator_t gen = nullptr;
     int n_rand_buf = 0;                  // 4096 * n_modes
     int i_rand_outdated = 0;             // cursor of data.cu:240-247
@@ -96,8 +99,8 @@ struct lbl_ctx {
     int yo_buf = 0;
     float* d_dY = nullptr;               // [3][nsites][M] H(x)-mean at sites
     float* d_dyo = nullptr;              // [3][nsites] yo - mean
-    int* d_stats = nullptr;              // [0] max sweeps, [1] non-converged points, [2] NaN flag
-    int h_stats[3] = {0, 0, 0};
+    int* d_stats = nullptr;              // [0] max sweeps, [1] non-converged points, [2] NaN flag, [3] sweep total
+    int h_stats[4] = {0, 0, 0, 0};
 
     // diagnostics scratch
     double* d_red = nullptr;             // reduction scratch (8 doubles)

@@ -12,6 +12,7 @@
 //   lbm_step_kernel     fused pull streaming + macros + Smagorinsky + BGK + force
 //                       (lbm.cu:24-160, lbm.h:31-109, lbm_collision_srt.h:8-16)
 //   macros_kernel       rho,u,v moments of f (lbm.h:72-109)
+#include <algorithm>
 #include <cmath>
 
 #include "lbl_internal.h"
@@ -102,13 +103,15 @@ __global__ void ic_velocity_kernel(const double* __restrict__ modes, int n, int 
 // that step s uses (the reference's force_theta_d[i_rand_outdated]).
 // ---------------------------------------------------------------------------
 __global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __restrict__ sched,
-                                   const float* __restrict__ modes, int n, float* __restrict__ force,
-                                   int slot0, int cap, Phys P) {
-    extern __shared__ float s_mode[];  // kx[n], ky[n], amp[n], r[4n]
+                                   const float* __restrict__ modes, const double* __restrict__ amps, int n,
+                                   float* __restrict__ force, int slot0, int cap, Phys P) {
+    extern __shared__ double s_amp[];  // ax[n], ay[n] (double), then kx[n], ky[n], r[4n] (float)
+    float* s_mode = reinterpret_cast<float*>(s_amp + 2 * n);
     const int s = blockIdx.y;
     const float* rnd = pool + sched[s];
-    for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) s_mode[k] = modes[k];
-    for (int k = threadIdx.x; k < 4 * n; k += blockDim.x) s_mode[3 * n + k] = rnd[k];
+    for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) s_amp[k] = amps[k];
+    for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) s_mode[k] = modes[k];
+    for (int k = threadIdx.x; k < 4 * n; k += blockDim.x) s_mode[2 * n + k] = rnd[k];
     __syncthreads();
     const int ij = blockIdx.x * blockDim.x + threadIdx.x;
     if (ij >= P.nxy) return;
@@ -118,8 +121,7 @@ __global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __
     const float y = float(j - ny / 2) * P.inv_ny;
     const float* force_kx = s_mode;
     const float* force_ky = s_mode + n;
-    const float* force_amp = s_mode + 2 * n;
-    const float* force_rand = s_mode + 3 * n;
+    const float* force_rand = s_mode + 2 * n;
     float f_x = 0;
     float f_y = 0;
     for (int k = 0; k < n; k++) {
@@ -130,9 +132,11 @@ __global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __
         const float cosi = cos(theta);
         const float r[4] = {force_rand[k + 0 * n], force_rand[k + 1 * n], force_rand[k + 2 * n],
                             force_rand[k + 3 * n]};
-        const float amp = force_amp[k];
-        f_x += amp * 2 * M_PI * ky * ((r[0] * kx + r[1] * ky) * sine + (r[2] * kx + r[3] * ky) * cosi);
-        f_y += amp * 2 * M_PI * (-kx) * ((r[0] * kx + r[1] * ky) * sine + (r[2] * kx + r[3] * ky) * cosi);
+        // amp*2*M_PI*ky (and *(-kx)) are per-mode FP64 products, precomputed on the host
+        // with the same IEEE operations the reference evaluates per cell
+        const float inner = (r[0] * kx + r[1] * ky) * sine + (r[2] * kx + r[3] * ky) * cosi;
+        f_x += s_amp[k] * inner;
+        f_y += s_amp[n + k] * inner;
     }
     float* F = force + size_t((slot0 + s) % cap) * 2 * P.nxy;
     F[ij] = f_x;
@@ -141,15 +145,17 @@ __global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __
 
 // ---------------------------------------------------------------------------
 // Fused LBM step.  One CTA = one member x one strip of TY rows, one thread per
-// column x.  Each thread marches up its column: it pulls row jj+1 (prefetched one
+// column x.  Each thread marches up its column: it pulls row j+2 (prefetched one
 // row ahead), computes that row's post-stream macros, shares u,v through a 3-row
-// shared-memory ring for the x+-1 neighbours, and finalises row jj (Smagorinsky
-// from the post-stream u,v stencil, BGK toward feq, Guo-less first-order force
-// with friction) straight from registers.  Rows j0-1 and j1 are pulled as halo so
-// that the whole step is one pass over f: 72 B/cell of compulsory traffic in FP32.
+// shared-memory ring for the x+-1 neighbours, and finalises row j (Smagorinsky
+// from the post-stream u,v stencil, BGK toward feq, first-order force with
+// friction) straight from registers.  Rows j0-1 and j1 are pulled as halo so that
+// the whole step is one pass over f: 72 B/cell of compulsory traffic in FP32.
+// Periodic wraps are branch-free selects on running row offsets (no integer
+// division in the loop).
 // ---------------------------------------------------------------------------
-template <bool WRITE_MAC>
-__global__ void __launch_bounds__(1024) lbm_step_kernel(const float* __restrict__ fin, float* __restrict__ fout,
+template <bool WRITE_MAC, int MAXT>
+__global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict__ fin, float* __restrict__ fout,
                                                         const float* __restrict__ force,
                                                         float* __restrict__ mac, Phys P, int TY) {
     extern __shared__ float s_uv[];  // [3][2][nx]
@@ -159,55 +165,65 @@ __global__ void __launch_bounds__(1024) lbm_step_kernel(const float* __restrict_
     const int j0 = blockIdx.x * TY;
     const int j1 = min(j0 + TY, ny);
     const float* __restrict__ fm = fin + size_t(m) * kQ * nxy;
-    float* __restrict__ fo = fout + size_t(m) * kQ * nxy;
+    float* __restrict__ fo = fout + size_t(m) * kQ * nxy + x;
     const int xm = (x == 0) ? nx - 1 : x - 1;
     const int xp = (x == nx - 1) ? 0 : x + 1;
-    const float* __restrict__ Fx = force;
-    const float* __restrict__ Fy = force + nxy;
+    const float* __restrict__ Fx = force + x;
+    const float* __restrict__ Fy = force + nxy + x;
 
+    // running row offsets (row*nx) of rows jj-1, jj, jj+1 for the row jj being pulled
+    auto wrap_row = [&](int r) { return (r < 0 ? r + ny : (r >= ny ? r - ny : r)) * nx; };
+    int o_m = wrap_row(j0 - 2), o_0 = wrap_row(j0 - 1), o_p = wrap_row(j0);
+    auto advance = [&]() {
+        o_m = o_0;
+        o_0 = o_p;
+        o_p = (o_p + nx == nxy) ? 0 : o_p + nx;
+    };
     // pull streaming: fc[q] = f[(i-ex, j-ey)] periodic (lbm.cu:82-87)
-    auto pull = [&](int jj, float (&fc)[kQ]) {
-        const int r0 = (jj + ny) % ny;
-        const int rm = (jj - 1 + ny) % ny;  // source row for ey = +1
-        const int rp = (jj + 1) % ny;       // source row for ey = -1
+    auto pull = [&](float (&fc)[kQ]) {
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
             const int col = ex_q(q) == -1 ? xp : (ex_q(q) == 0 ? x : xm);
-            const int row = ey_q(q) == -1 ? rp : (ey_q(q) == 0 ? r0 : rm);
-            fc[q] = __ldg(fm + size_t(q) * nxy + row * nx + col);
+            const int row = ey_q(q) == -1 ? o_p : (ey_q(q) == 0 ? o_0 : o_m);
+            fc[q] = __ldg(fm + q * nxy + row + col);
         }
     };
-    auto slot = [&](int row) { return ((row - j0 + 1) % 3) * 2 * nx; };
+    float* s_a = s_uv;           // ring of three rows of (u, v)
+    float* s_b = s_uv + 2 * nx;
+    float* s_c = s_uv + 4 * nx;
 
     float fA[kQ], fB[kQ], fC[kQ];
     float rA, uA, vA, rB, uB, vB, uM, vM;
     {  // halo row below the strip: only its u,v (own column) are needed
         float t[kQ];
-        pull(j0 - 1, t);
+        pull(t);
         const float r = rf(t);
         uM = uf(t, r, P.c);
         vM = vf(t, r, P.c);
     }
-    pull(j0, fA);
+    advance();
+    pull(fA);  // row j0
     rA = rf(fA);
     uA = uf(fA, rA, P.c);
     vA = vf(fA, rA, P.c);
-    s_uv[slot(j0) + x] = uA;
-    s_uv[slot(j0) + nx + x] = vA;
-    pull(j0 + 1, fB);
+    s_a[x] = uA;
+    s_a[nx + x] = vA;
+    advance();
+    pull(fB);  // row j0+1
+    int ij = j0 * nx;
 
     for (int jc = j0; jc < j1; jc++) {
-        if (jc + 2 <= j1) pull(jc + 2, fC);  // prefetch the row after next
+        advance();
+        if (jc + 2 <= j1) pull(fC);  // prefetch the row after next
         rB = rf(fB);
         uB = uf(fB, rB, P.c);
         vB = vf(fB, rB, P.c);
-        s_uv[slot(jc + 1) + x] = uB;
-        s_uv[slot(jc + 1) + nx + x] = vB;
+        s_b[x] = uB;
+        s_b[nx + x] = vB;
         __syncthreads();
 
         // Smagorinsky eddy viscosity from the post-stream velocity (lbm.cu:42-60)
-        const float* su = s_uv + slot(jc);
-        const float ue = su[xp], uw = su[xm], ve = su[nx + xp], vw = su[nx + xm];
+        const float ue = s_a[xp], uw = s_a[xm], ve = s_a[nx + xp], vw = s_a[nx + xm];
         const float ux = (ue - uw) / P.two_dx;
         const float uy = (uB - uM) / P.two_dx;
         const float vx = (ve - vw) / P.two_dx;
@@ -226,7 +242,6 @@ __global__ void __launch_bounds__(1024) lbm_step_kernel(const float* __restrict_
         const float omega = 1. / tau;
 
         // BGK (lbm_collision_srt.h:8-16) + force (lbm.cu:142-147)
-        const int ij = jc * nx + x;
         const float fxc = Fx[ij], fyc = Fy[ij];
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
@@ -237,18 +252,20 @@ __global__ void __launch_bounds__(1024) lbm_step_kernel(const float* __restrict_
 #pragma unroll
         for (int q = 0; q < kQ; q++) fA[q] += force_acc(fxc, fyc, q, rA, uA, vA, P);
 #pragma unroll
-        for (int q = 0; q < kQ; q++) fo[size_t(q) * nxy + ij] = fA[q];
+        for (int q = 0; q < kQ; q++) fo[q * nxy + ij] = fA[q];
         if (WRITE_MAC) {
-            float* mm = mac + size_t(m) * 3 * nxy;
+            float* mm = mac + size_t(m) * 3 * nxy + x;
             mm[ij] = rA;
             mm[nxy + ij] = uA;
             mm[2 * nxy + ij] = vA;
         }
-        // rotate the window
+        // rotate the window and the shared ring (a <- b <- c <- a)
         uM = uA; vM = vA;
         rA = rB; uA = uB; vA = vB;
 #pragma unroll
         for (int q = 0; q < kQ; q++) { fA[q] = fB[q]; fB[q] = fC[q]; }
+        float* t = s_a; s_a = s_b; s_b = s_c; s_c = t;
+        ij += nx;
     }
 }
 
@@ -267,12 +284,32 @@ __global__ void macros_kernel(const float* __restrict__ f, float* __restrict__ m
     mm[2 * P.nxy + ij] = vf(fc, r, P.c);
 }
 
+// Strip height: fill the GPU's resident CTA slots with as few waves as possible,
+// counting the two halo rows each strip pulls.
 int strip_rows(const Phys& P) {
-    // enough CTAs to fill 148 SMs several times over, with a modest halo overhead
-    const long long members_rows = (long long)P.M * P.ny;
-    int ty = 16;
-    while (ty > 4 && members_rows / ty < 148 * 4) ty /= 2;
-    return ty;
+    static int slots = 0, slots_nx = 0;
+    if (slots == 0 || slots_nx != P.nx) {
+        slots_nx = P.nx;
+        int dev = 0, sms = 148, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (P.nx <= 256)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 256>, P.nx,
+                                                          sizeof(float) * 6 * P.nx);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 1024>, P.nx,
+                                                          sizeof(float) * 6 * P.nx);
+        slots = std::max(1, per_sm) * sms;
+    }
+    int best = 4;
+    double best_cost = 1e30;
+    for (int ty = 2; ty <= 32; ty++) {
+        const long long strips = (long long)P.M * ((P.ny + ty - 1) / ty);
+        const long long waves = (strips + slots - 1) / slots;
+        const double cost = double(waves) * (ty + 1.0);
+        if (cost < best_cost - 1e-9) { best_cost = cost; best = ty; }
+    }
+    return best;
 }
 
 }  // namespace
@@ -285,9 +322,9 @@ void launch_ic_velocity(const double* modes, int n_modes, int nx, int ny, float*
 void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s) {
     const int threads = 256;
     dim3 grid((c->P.nxy + threads - 1) / threads, nsteps);
-    const size_t sm = sizeof(float) * 7 * c->n_modes;
-    force_chunk_kernel<<<grid, threads, sm, s>>>(c->d_pool, c->d_sched, c->d_modes, c->n_modes, c->d_force, slot0,
-                                                 c->force_cap, c->P);
+    const size_t sm = sizeof(double) * 2 * c->n_modes + sizeof(float) * 6 * c->n_modes;
+    force_chunk_kernel<<<grid, threads, sm, s>>>(c->d_pool, c->d_sched, c->d_modes, c->d_amps, c->n_modes, c->d_force,
+                                                 slot0, c->force_cap, c->P);
 }
 
 void launch_lbm_step(const lbl_ctx* c, const float* fin, float* fout, const float* force, float* mac_out,
@@ -296,10 +333,17 @@ void launch_lbm_step(const lbl_ctx* c, const float* fin, float* fout, const floa
     const int ty = strip_rows(P);
     dim3 grid((P.ny + ty - 1) / ty, P.M);
     const size_t sm = sizeof(float) * 6 * P.nx;
-    if (mac_out)
-        lbm_step_kernel<true><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty);
-    else
-        lbm_step_kernel<false><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty);
+    if (P.nx <= 256) {
+        if (mac_out)
+            lbm_step_kernel<true, 256><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty);
+        else
+            lbm_step_kernel<false, 256><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty);
+    } else {
+        if (mac_out)
+            lbm_step_kernel<true, 1024><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty);
+        else
+            lbm_step_kernel<false, 1024><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty);
+    }
 }
 
 void launch_macros(const lbl_ctx* c, const float* f, float* mac, cudaStream_t s) {

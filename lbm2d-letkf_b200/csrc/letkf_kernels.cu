@@ -34,7 +34,9 @@ __host__ __device__ constexpr int eyq(int q) { return (q / 3) - 1; }
 struct AnaParams {
     int nx, ny, nxy, M;
     int p, nsx, nsy, nsites;
-    int n_pat_max;          // entries per pattern row of the weight table
+    int n_pat_max;          // window slots = entries per pattern row of the weight table
+    int nox;                // window sites per row
+    int nl_off;             // n_obs_local - obs_offset (window origin, in sites)
     float diag;             // (M-1)/beta
     float sqrt_m1;          // sqrt(M-1)
     float tol;              // Jacobi off-diagonal tolerance
@@ -101,9 +103,15 @@ __device__ __forceinline__ float group_sum(float v) {
 
 // ---------------------------------------------------------------------------
 // The local analysis.  MP = member lanes per grid point (power of two >= M).
-// Table entry (int4): x = site dx, y = site dy (in sites), z = variable (0 u, 1 v,
-// 2 rho), w = weight bits (sigma^-2 x Gaspari-Cohn), per pattern (i%p, j%p).
+// A group of MP lanes walks a CW x CH tile of neighbouring grid points in snake
+// order.  The unweighted observation window of the current p x p block is cached
+// in shared memory, and every point's Jacobi starts from the previous point's
+// eigenvectors (A = Q V_prev), which leaves little to rotate.
+// Weight table entry (int4): x = window slot (a + nox*b + var*nox^2), w = weight
+// bits (sigma^-2 x Gaspari-Cohn), only w > 0, per pattern (i mod p, j mod p).
 // ---------------------------------------------------------------------------
+constexpr int kCW = 4, kCH = 2;  // chain tile (points in x, points in y)
+
 template <int MP>
 __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__ fin, float* __restrict__ fout,
                                                        float* __restrict__ mac, const float* __restrict__ dY,
@@ -118,183 +126,236 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
     const int grp = lane / MP;
     const int k = lane % MP;
     const int gbase = lane - k;
-    const int point = (blockIdx.x * (blockDim.x >> 5) + warp) * GPW + grp;
-    const bool active = point < A.nxy;
-    const bool real_m = active && k < A.M;
     const int M = A.M;
+    const bool real_k = k < M;
+    const int nobs = A.n_pat_max;  // window slots (3 * nox * nox)
+    const int nox2 = nobs / 3;
 
     // per-group shared memory
-    const int per_grp = A.n_pat_max * MP + MP * MP + 2 * kQ * MP + 2 * MP;
+    // every block below is a multiple of 4 floats, so all float4 accesses stay 16-B aligned
+    const int nobs_pad = (nobs + 3) & ~3;
+    const int per_grp = nobs * MP + nobs_pad + MP * MP + 2 * kQ * MP + 2 * MP;
     float* base = smem + size_t(warp * GPW + grp) * per_grp;
-    float* sE = base;                          // [n_pat][MP] weighted window sqrt(w) dY
-    float* sV = sE + A.n_pat_max * MP;         // [MP][MP] eigenvectors, column j at j*MP
-    float* sDX = sV + MP * MP;                 // [9][MP]  dX
+    float* sW = base;                          // [nobs][MP] window dY (unweighted)
+    float* sDyo = sW + nobs * MP;              // [nobs]     window innovations (padded to 4)
+    float* sQ = sDyo + nobs_pad;               // [MP][MP] Q columns, then V
+    float* sDX = sQ + MP * MP;                 // [9][MP]  dX
     float* sD = sDX + kQ * MP;                 // [9][MP]  D = dX V
     float* sS = sD + kQ * MP;                  // [MP]     sqrt(M-1)/sqrt(lambda)
     float* sY = sS + MP;                       // [MP]     Lambda^-1 V^T c
 
-    // 1. forecast ensemble at the point: X, xbar, dX (letkf_solver.h:278-280)
-    float xq[kQ], xbar[kQ];
-    const int pt = active ? point : 0;
-#pragma unroll
-    for (int q = 0; q < kQ; q++) xq[q] = real_m ? __ldg(fin + (size_t(k) * kQ + q) * A.nxy + pt) : 0.f;
-#pragma unroll
-    for (int q = 0; q < kQ; q++) {
-        xbar[q] = group_sum<MP>(xq[q]) / float(M);
-        sDX[q * MP + k] = real_m ? xq[q] - xbar[q] : 0.f;
-    }
+    const int tiles_x = (A.nx + kCW - 1) / kCW;
+    const int tile = (blockIdx.x * (blockDim.x >> 5) + warp) * GPW + grp;
+    const int x0 = (tile % tiles_x) * kCW;
+    const int y0 = (tile / tiles_x) * kCH;
+    const unsigned gmask = (MP == 32) ? 0xffffffffu : (((1u << MP) - 1u) << gbase);
 
-    // 2. localised observation window (pack_yk/set_yo/set_rR geometry, letkf.cu:75-114,148-269)
-    const int i = pt % A.nx, j = pt / A.nx;
-    const int pat = (i % A.p) + A.p * (j % A.p);
-    const int bi = i / A.p, bj = j / A.p;
-    const int cnt = wcnt[pat];
-    const int4* ent = wtab + size_t(pat) * A.n_pat_max;
-    float ck = 0.f;  // (dY^T R^-1 dyo)_k
-    for (int o = 0; o < cnt; o++) {
-        const int4 e = ent[o];
-        int si = (bi + e.x) % A.nsx; si += si < 0 ? A.nsx : 0;
-        int sj = (bj + e.y) % A.nsy; sj += sj < 0 ? A.nsy : 0;
-        const int s = si + A.nsx * sj;
-        const float sw = sqrtf(__int_as_float(e.w));
-        const float d = real_m ? __ldg(dY + (size_t(e.z) * A.nsites + s) * M + k) : 0.f;
-        const float ev = sw * d;
-        sE[o * MP + k] = ev;
-        ck += ev * (sw * __ldg(dyo + size_t(e.z) * A.nsites + s));
-    }
-    __syncwarp();
-
-    // 3. Gram: column k of Q = (M-1)/beta I + E^T E (letkf_solver.h:252-254)
-    float qv[MP];
-#pragma unroll
-    for (int l = 0; l < MP; l++) qv[l] = 0.f;
-    for (int o = 0; o < cnt; o++) {
-        const float* row = sE + o * MP;
-        const float ek = row[k];
-#pragma unroll
-        for (int l = 0; l < MP; l += 4) {
-            const float4 r4 = *reinterpret_cast<const float4*>(row + l);
-            qv[l + 0] = fmaf(ek, r4.x, qv[l + 0]);
-            qv[l + 1] = fmaf(ek, r4.y, qv[l + 1]);
-            qv[l + 2] = fmaf(ek, r4.z, qv[l + 2]);
-            qv[l + 3] = fmaf(ek, r4.w, qv[l + 3]);
-        }
-    }
-#pragma unroll
-    for (int l = 0; l < MP; l++)
-        if (l == k && k < M) qv[l] += A.diag;
-
-    // 4. one-sided Jacobi: rotate column pairs (k, k^r) of Q until mutually
-    //    orthogonal; accumulated rotations V are the eigenvectors, Q V = V Lambda.
-    float vv[MP];
+    float vv[MP];  // eigenvectors (column k), carried from point to point
 #pragma unroll
     for (int l = 0; l < MP; l++) vv[l] = (l == k) ? 1.f : 0.f;
-    const unsigned gmask = (MP == 32) ? 0xffffffffu : (((1u << MP) - 1u) << gbase);
-    int sweeps = 0;
-    bool converged = false;
-    for (int sw = 0; sw < A.max_sweeps; sw++) {
-        float a = 0.f;
-#pragma unroll
-        for (int l = 0; l < MP; l++) a = fmaf(qv[l], qv[l], a);
-        bool rot = false;
-#pragma unroll 1
-        for (int r = 1; r < MP; r++) {
-            float pq[MP];
-#pragma unroll
-            for (int l = 0; l < MP; l++) pq[l] = __shfl_xor_sync(0xffffffffu, qv[l], r);
-            float g = 0.f;
-#pragma unroll
-            for (int l = 0; l < MP; l++) g = fmaf(qv[l], pq[l], g);
-            const float b = __shfl_xor_sync(0xffffffffu, a, r);
-            const bool low = k < (k ^ r);
-            const float alo = low ? a : b, ahi = low ? b : a;
-            const bool doit = fabsf(g) > A.tol * sqrtf(alo * ahi);
-            float cs = 1.f, sn = 0.f, t = 0.f;
-            if (doit) {
-                const float zeta = (ahi - alo) / (2.f * g);
-                t = copysignf(1.f, zeta) / (fabsf(zeta) + sqrtf(1.f + zeta * zeta));
-                cs = 1.f / sqrtf(1.f + t * t);
-                sn = cs * t;
-            }
-            rot |= doit;
-#pragma unroll
-            for (int l = 0; l < MP; l++) {
-                const float pv = __shfl_xor_sync(0xffffffffu, vv[l], r);
-                if (low) {
-                    qv[l] = cs * qv[l] - sn * pq[l];
-                    vv[l] = cs * vv[l] - sn * pv;
-                } else {
-                    qv[l] = sn * pq[l] + cs * qv[l];
-                    vv[l] = sn * pv + cs * vv[l];
-                }
-            }
-            a = low ? a - t * g : a + t * g;
-        }
-        const unsigned ballot = __ballot_sync(0xffffffffu, rot);
-        if (!converged) {
-            sweeps = sw + 1;
-            if ((ballot & gmask) == 0u) converged = true;
-        }
-        if (ballot == 0u) break;
-    }
+    int cached_bi = -1, cached_bj = -1;
+    int max_sweeps = 0, noconv = 0, total_sweeps = 0;
+    bool bad = false;
 
-    // 5. eigenvalue of column k: (Q V)_k = lambda_k v_k
-    float lam = 0.f;
-#pragma unroll
-    for (int l = 0; l < MP; l++) lam = fmaf(qv[l], vv[l], lam);
+    for (int idx = 0; idx < kCW * kCH; idx++) {
+        const int r = idx / kCW;
+        const int cc = (r & 1) ? (kCW - 1 - idx % kCW) : (idx % kCW);
+        const int i = x0 + cc, j = y0 + r;
+        const bool active = (i < A.nx) && (j < A.ny);  // uniform within the group
+        const int point = active ? i + A.nx * j : 0;
+        const bool real_m = active && real_k;
 
-    // 6. transform (letkf_solver.h:288-316)
+        // 1. forecast ensemble at the point: X, xbar, dX (letkf_solver.h:278-280)
+        float xq[kQ], xbar[kQ];
 #pragma unroll
-    for (int l = 0; l < MP; l++) sV[k * MP + l] = vv[l];
-    float vc = 0.f;  // (V^T c)_k
-#pragma unroll
-    for (int l = 0; l < MP; l++) vc = fmaf(vv[l], __shfl_sync(0xffffffffu, ck, gbase + l), vc);
-    const bool col_ok = k < M;
-    sY[k] = col_ok ? vc / lam : 0.f;
-    sS[k] = col_ok ? A.sqrt_m1 / sqrtf(lam) : 0.f;
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < kQ; q++) {
-        float dsum = 0.f;
-#pragma unroll
-        for (int l = 0; l < MP; l++) dsum = fmaf(sDX[q * MP + l], vv[l], dsum);
-        sD[q * MP + k] = dsum;
-    }
-    __syncwarp();
-    float acc[kQ];
-#pragma unroll
-    for (int q = 0; q < kQ; q++) acc[q] = 0.f;
-#pragma unroll 4
-    for (int jj = 0; jj < MP; jj++) {
-        const float z = fmaf(sS[jj], sV[jj * MP + k], sY[jj]);
-#pragma unroll
-        for (int q = 0; q < kQ; q++) acc[q] = fmaf(sD[q * MP + jj], z, acc[q]);
-    }
-
-    // 7. write the analysis member k, refresh its macros (update_xk + lbm2euler)
-    if (real_m) {
-        float xa[kQ];
-        bool bad = false;
+        for (int q = 0; q < kQ; q++) xq[q] = real_m ? __ldg(fin + (size_t(k) * kQ + q) * A.nxy + point) : 0.f;
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
-            xa[q] = xbar[q] + acc[q];
-            bad |= !(xa[q] == xa[q]);
-            fout[(size_t(k) * kQ + q) * A.nxy + point] = xa[q];
+            xbar[q] = group_sum<MP>(xq[q]) / float(M);
+            sDX[q * MP + k] = real_m ? xq[q] - xbar[q] : 0.f;
         }
-        float r = 0, mu = 0, mv = 0;
+
+        // 2. observation window of the point's p x p block (pack_yk/set_yo geometry,
+        //    letkf.cu:148-269), gathered once per block from the site ensemble
+        const int bi = i / A.p, bj = j / A.p;
+        if (bi != cached_bi || bj != cached_bj) {
+            for (int sl = 0; sl < nobs; sl++) {
+                const int var = sl / nox2, ab = sl - var * nox2;
+                const int b = ab / A.nox, a = ab - b * A.nox;
+                int si = (bi + a - A.nl_off) % A.nsx; si += si < 0 ? A.nsx : 0;
+                int sj = (bj + b - A.nl_off) % A.nsy; sj += sj < 0 ? A.nsy : 0;
+                const int site = si + A.nsx * sj;
+                sW[sl * MP + k] = real_k ? __ldg(dY + (size_t(var) * A.nsites + site) * M + k) : 0.f;
+                if (k == 0) sDyo[sl] = __ldg(dyo + size_t(var) * A.nsites + site);
+            }
+            cached_bi = bi;
+            cached_bj = bj;
+        }
+        __syncwarp();
+
+        // 3. Gram: column k of Q = (M-1)/beta I + dY^T R^-1 dY (letkf_solver.h:252-254),
+        //    and c_k = (dY^T R^-1 dyo)_k
+        const int pat = (i % A.p) + A.p * (j % A.p);
+        const int cnt = wcnt[pat];
+        const int4* ent = wtab + size_t(pat) * nobs;
+        float qv[MP];
 #pragma unroll
-        for (int q = 0; q < kQ; q++) r += xa[q];
+        for (int l = 0; l < MP; l++) qv[l] = 0.f;
+        float ck = 0.f;
+        for (int o = 0; o < cnt; o++) {
+            const int4 e = ent[o];
+            const float* row = sW + e.x * MP;
+            const float ek = __int_as_float(e.w) * row[k];
+            ck = fmaf(ek, sDyo[e.x], ck);
 #pragma unroll
-        for (int q = 0; q < kQ; q++) { mu += xa[q] * A.c * exq(q); mv += xa[q] * A.c * eyq(q); }
-        float* mm = mac + size_t(k) * 3 * A.nxy;
-        mm[point] = r;
-        mm[A.nxy + point] = mu / r;
-        if (A.write_v) mm[2 * A.nxy + point] = mv / r;
-        if (bad) atomicOr(stats + 2, 1);
+            for (int l = 0; l < MP; l += 4) {
+                const float4 r4 = *reinterpret_cast<const float4*>(row + l);
+                qv[l + 0] = fmaf(ek, r4.x, qv[l + 0]);
+                qv[l + 1] = fmaf(ek, r4.y, qv[l + 1]);
+                qv[l + 2] = fmaf(ek, r4.z, qv[l + 2]);
+                qv[l + 3] = fmaf(ek, r4.w, qv[l + 3]);
+            }
+        }
+#pragma unroll
+        for (int l = 0; l < MP; l++)
+            if (l == k && k < M) qv[l] += A.diag;
+
+        // 4. warm start: A = Q V_prev (column k = sum_l Q_:l V_prev[l][k])
+        if (idx > 0) {
+#pragma unroll
+            for (int l = 0; l < MP; l++) sQ[k * MP + l] = qv[l];
+            __syncwarp();
+            float av[MP];
+#pragma unroll
+            for (int l = 0; l < MP; l++) av[l] = 0.f;
+#pragma unroll
+            for (int l = 0; l < MP; l++) {
+                const float vl = vv[l];
+#pragma unroll
+                for (int t = 0; t < MP; t += 4) {
+                    const float4 q4 = *reinterpret_cast<const float4*>(sQ + l * MP + t);
+                    av[t + 0] = fmaf(q4.x, vl, av[t + 0]);
+                    av[t + 1] = fmaf(q4.y, vl, av[t + 1]);
+                    av[t + 2] = fmaf(q4.z, vl, av[t + 2]);
+                    av[t + 3] = fmaf(q4.w, vl, av[t + 3]);
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int l = 0; l < MP; l++) qv[l] = av[l];
+        }
+
+        // 5. one-sided Jacobi: rotate column pairs (k, k^r) until mutually orthogonal;
+        //    accumulated rotations V are the eigenvectors, Q V = V Lambda.
+        int sweeps = 0;
+        bool converged = false;
+        for (int sw = 0; sw < A.max_sweeps; sw++) {
+            float a = 0.f;
+#pragma unroll
+            for (int l = 0; l < MP; l++) a = fmaf(qv[l], qv[l], a);
+            bool rot = false;
+#pragma unroll 1
+            for (int rr = 1; rr < MP; rr++) {
+                float pq[MP];
+#pragma unroll
+                for (int l = 0; l < MP; l++) pq[l] = __shfl_xor_sync(0xffffffffu, qv[l], rr);
+                float g = 0.f;
+#pragma unroll
+                for (int l = 0; l < MP; l++) g = fmaf(qv[l], pq[l], g);
+                const float b = __shfl_xor_sync(0xffffffffu, a, rr);
+                const bool low = k < (k ^ rr);
+                const float alo = low ? a : b, ahi = low ? b : a;
+                const bool doit = fabsf(g) > A.tol * sqrtf(alo * ahi);
+                float cs = 1.f, sn = 0.f, t = 0.f;
+                if (doit) {
+                    const float zeta = (ahi - alo) / (2.f * g);
+                    t = copysignf(1.f, zeta) / (fabsf(zeta) + sqrtf(1.f + zeta * zeta));
+                    cs = 1.f / sqrtf(1.f + t * t);
+                    sn = cs * t;
+                }
+                rot |= doit;
+#pragma unroll
+                for (int l = 0; l < MP; l++) {
+                    const float pv = __shfl_xor_sync(0xffffffffu, vv[l], rr);
+                    if (low) {
+                        qv[l] = cs * qv[l] - sn * pq[l];
+                        vv[l] = cs * vv[l] - sn * pv;
+                    } else {
+                        qv[l] = sn * pq[l] + cs * qv[l];
+                        vv[l] = sn * pv + cs * vv[l];
+                    }
+                }
+                a = low ? a - t * g : a + t * g;
+            }
+            const unsigned ballot = __ballot_sync(0xffffffffu, rot && active);
+            if (!converged) {
+                sweeps = sw + 1;
+                if ((ballot & gmask) == 0u) converged = true;
+            }
+            if (ballot == 0u) break;
+        }
+
+        // 6. eigenvalue of column k: (Q V)_k = lambda_k v_k; transform (letkf_solver.h:288-316)
+        float lam = 0.f;
+#pragma unroll
+        for (int l = 0; l < MP; l++) lam = fmaf(qv[l], vv[l], lam);
+#pragma unroll
+        for (int l = 0; l < MP; l++) sQ[k * MP + l] = vv[l];
+        float vc = 0.f;  // (V^T c)_k
+#pragma unroll
+        for (int l = 0; l < MP; l++) vc = fmaf(vv[l], __shfl_sync(0xffffffffu, ck, gbase + l), vc);
+        sY[k] = real_k ? vc / lam : 0.f;
+        sS[k] = real_k ? A.sqrt_m1 / sqrtf(lam) : 0.f;
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < kQ; q++) {
+            float dsum = 0.f;
+#pragma unroll
+            for (int l = 0; l < MP; l++) dsum = fmaf(sDX[q * MP + l], vv[l], dsum);
+            sD[q * MP + k] = dsum;
+        }
+        __syncwarp();
+        float acc[kQ];
+#pragma unroll
+        for (int q = 0; q < kQ; q++) acc[q] = 0.f;
+#pragma unroll 4
+        for (int jj = 0; jj < MP; jj++) {
+            const float z = fmaf(sS[jj], sQ[jj * MP + k], sY[jj]);
+#pragma unroll
+            for (int q = 0; q < kQ; q++) acc[q] = fmaf(sD[q * MP + jj], z, acc[q]);
+        }
+
+        // 7. write the analysis member k, refresh its macros (update_xk + lbm2euler)
+        if (real_m) {
+            float xa[kQ];
+#pragma unroll
+            for (int q = 0; q < kQ; q++) {
+                xa[q] = xbar[q] + acc[q];
+                bad |= !(xa[q] == xa[q]);
+                fout[(size_t(k) * kQ + q) * A.nxy + point] = xa[q];
+            }
+            float rsum = 0, mu = 0, mv = 0;
+#pragma unroll
+            for (int q = 0; q < kQ; q++) rsum += xa[q];
+#pragma unroll
+            for (int q = 0; q < kQ; q++) { mu += xa[q] * A.c * exq(q); mv += xa[q] * A.c * eyq(q); }
+            float* mm = mac + size_t(k) * 3 * A.nxy;
+            mm[point] = rsum;
+            mm[A.nxy + point] = mu / rsum;
+            if (A.write_v) mm[2 * A.nxy + point] = mv / rsum;
+        }
+        if (active) {
+            max_sweeps = max(max_sweeps, sweeps);
+            total_sweeps += sweeps;
+            noconv += converged ? 0 : 1;
+        }
+        __syncwarp();
     }
-    if (active && k == 0) {
-        atomicMax(stats + 0, sweeps);
-        if (!converged) atomicAdd(stats + 1, 1);
+    if (bad) atomicOr(stats + 2, 1);
+    if (k == 0 && total_sweeps > 0) {
+        atomicMax(stats + 0, max_sweeps);
+        if (noconv) atomicAdd(stats + 1, noconv);
+        atomicAdd(stats + 3, total_sweeps);
     }
 }
 
@@ -303,6 +364,8 @@ AnaParams make_params(const lbl_ctx* c) {
     A.nx = c->P.nx; A.ny = c->P.ny; A.nxy = c->P.nxy; A.M = c->P.M;
     A.p = c->G.p; A.nsx = c->G.nsx; A.nsy = c->G.nsy; A.nsites = c->G.nsx * c->G.nsy;
     A.n_pat_max = c->G.nobs;
+    A.nox = c->G.nox;
+    A.nl_off = c->G.nl - c->G.off;
     const double beta = c->cfg.letkf_covinf;
     A.diag = float((c->P.M - 1) / beta);
     A.sqrt_m1 = float(std::sqrt(double(c->P.M - 1)));
@@ -324,10 +387,10 @@ void launch_analysis_mp(const lbl_ctx* c, const float* fin, float* fout, float* 
     const AnaParams A = make_params(c);
     constexpr int GPW = 32 / MP;
     const int warps = 4;
-    const int pts_per_cta = warps * GPW;
-    const int per_grp = A.n_pat_max * MP + MP * MP + 2 * kQ * MP + 2 * MP;
-    const size_t sm = sizeof(float) * size_t(per_grp) * warps * GPW;
-    const int grid = (A.nxy + pts_per_cta - 1) / pts_per_cta;
+    const int groups_per_cta = warps * GPW;
+    const size_t sm = analysis_smem_bytes(A.M, A.n_pat_max);
+    const int tiles = ((A.nx + kCW - 1) / kCW) * ((A.ny + kCH - 1) / kCH);
+    const int grid = (tiles + groups_per_cta - 1) / groups_per_cta;
     analysis_kernel<MP><<<grid, warps * 32, sm, s>>>(fin, fout, mac, c->d_dY, c->d_dyo,
                                                       reinterpret_cast<const int4*>(c->d_wtab),
                                                       c->d_wtab + size_t(4) * c->G.p * c->G.p * c->G.nobs,
@@ -338,10 +401,10 @@ void launch_analysis_mp(const lbl_ctx* c, const float* fin, float* fout, float* 
 
 int analysis_supported(int M) { return M >= 2 && M <= kMaxMemberLanes; }
 
-// dynamic shared memory of one analysis CTA (4 warps) for M members and a window of nobs
+// dynamic shared memory of one analysis CTA (4 warps) for M members and a window of nobs slots
 size_t analysis_smem_bytes(int M, int nobs) {
     const int mp = pad_pow2(M);
-    const int per_grp = nobs * mp + mp * mp + 2 * kQ * mp + 2 * mp;
+    const int per_grp = nobs * mp + ((nobs + 3) & ~3) + mp * mp + 2 * kQ * mp + 2 * mp;
     return sizeof(float) * size_t(per_grp) * 4 * (32 / mp);
 }
 

@@ -118,7 +118,7 @@ def load_library() -> ctypes.CDLL:
         "lbl_get_force": (I, [P, F, F]),
         "lbl_get_force_state": (I, [P, F, F, F, F, IP, IP]),
         "lbl_get_observed": (I, [P, F, F, F, F]),
-        "lbl_get_letkf_stats": (I, [P, IP, IP, IP]),
+        "lbl_get_letkf_stats": (I, [P, IP, IP, IP, IP]),
         "lbl_get_diagnostics": (I, [P, I, D, D, D]),
         "lbl_rmse_uv": (I, [P, F, F, D]),
         "lbl_timer_csv": (I, [P, I, ctypes.c_char_p, U]),
@@ -279,10 +279,11 @@ class Ensemble:
         return tuple(x.reshape(self.ny, self.nx) for x in a)
 
     def letkf_stats(self) -> dict:
-        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        self._check(self.lib.lbl_get_letkf_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
-                    "lbl_get_letkf_stats")
-        return {"max_sweeps": a.value, "n_noconv": b.value, "nan": c.value}
+        a, b, c, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.lbl_get_letkf_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                                 ctypes.byref(d)), "lbl_get_letkf_stats")
+        return {"max_sweeps": a.value, "n_noconv": b.value, "nan": c.value,
+                "mean_sweeps": d.value / float(self.nxy)}
 
     def diagnostics(self, member: int = -1) -> dict:
         e, z, m = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()

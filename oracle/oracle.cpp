@@ -59,16 +59,21 @@ struct Derived {
 Derived derive(const lbl_config& cfg) {
     Derived d;
     d.nx = cfg.nx; d.ny = cfg.ny; d.M = cfg.n_ens;
-    d.c = cfg.u_ref / cfg.cfl;                        // config.h:248
-    d.dx = cfg.h_ref / (cfg.ny - 1);                  // config.h:250
-    d.dt = d.dx / d.c;                                // config.h:251
-    d.nu = cfg.tau > 0 ? (cfg.tau - 0.5) * d.c * d.c * d.dt / 3.0 : cfg.nu;  // config.h:253 inverted
-    d.cs = cfg.cs;
-    d.cs2 = d.c * d.c / 3.0;                          // lbm.h:50
+    // The physical constants are the reference's constexpr `real` (FP32) values
+    // (config.h:153-253), widened to FP64: the oracle solves the same discrete problem.
+    const float cf = float(cfg.u_ref) / float(cfg.cfl);              // config.h:248
+    const float dxf = float(cfg.h_ref) / float(cfg.ny - 1);          // config.h:250
+    const float dtf = dxf / cf;                                       // config.h:251
+    d.c = cf;
+    d.dx = dxf;
+    d.dt = dtf;
+    d.nu = float(cfg.tau > 0 ? (cfg.tau - 0.5) * double(cf) * double(cf) * double(dtf) / 3.0 : cfg.nu);
+    d.cs = cfg.cs;                                                    // a double in lbm.cu:59
+    d.cs2 = cf * cf / 3;                                              // lbm.h:50 (constexpr real)
     d.friction = cfg.friction_rate;
     d.u_ref = cfg.u_ref; d.rho_ref = cfg.rho_ref;
-    d.cf = float(cfg.u_ref) / float(cfg.cfl);
-    d.dxf = float(cfg.h_ref / (cfg.ny - 1));
+    d.cf = cf;
+    d.dxf = dxf;
     return d;
 }
 
@@ -405,8 +410,9 @@ int orc_step_noforce(orc_ctx* o) {
                 const double tau = 0.5 + 3. * nut / d.c / d.c / d.dt;
                 const double omega = 1. / tau;
                 const double rho = o->r[m * nxy + ij], u = um[ij], v = vm[ij];
-                const double Fx = (o->fx[ij] - d.friction / d.dt * u) * d.dt;
-                const double Fy = (o->fy[ij] - d.friction / d.dt * v) * d.dt;
+                const double fr_dt = double(float(d.friction) / float(d.dt));   // constexpr real (lbm.h:52)
+                const double Fx = (o->fx[ij] - fr_dt * u) * d.dt;
+                const double Fy = (o->fy[ij] - fr_dt * v) * d.dt;
                 for (int q = 0; q < Q; q++) {
                     double fq = fnm[size_t(q) * nxy + ij];
                     fq -= omega * (fq - feq(rho, u, v, q, d.c));
@@ -442,7 +448,7 @@ int orc_step(orc_ctx* o, int nsteps, const float* randoms) {
 // Vorticity exactly as io.cu:61-86 (host FP32, central differences, periodic).
 int orc_vorticity_f32(const lbl_config* cfg, const float* u, const float* v, float* vor) {
     const int nx = cfg->nx, ny = cfg->ny;
-    const float dx = float(cfg->h_ref / (cfg->ny - 1));
+    const float dx = float(cfg->h_ref) / float(cfg->ny - 1);   // constexpr real dx (config.h:250)
     for (int j = 0; j < ny; j++)
         for (int i = 0; i < nx; i++) {
             const int iw = (i - 1 + nx) % nx, ie = (i + 1) % nx, js = (j - 1 + ny) % ny, jn = (j + 1) % ny;

@@ -41,6 +41,7 @@ CASES = [  # nx, M, p, L, beta
     (64, 32, 4, 1, 1.1),
     (128, 16, 4, 2, 1.2),
     (256, 16, 4, 1, 1.1),
+    (96, 12, 4, 1, 1.1),
 ]
 
 
@@ -56,6 +57,7 @@ def test_analysis_matches_oracle(nx, M, p, L, beta):
     o.assimilate(*obs)
     st = e.letkf_stats()
     assert st["nan"] == 0 and st["n_noconv"] == 0 and 1 <= st["max_sweeps"] <= 30, st
+    print(f"nx={nx} M={M} p={p} L={L}: sweeps max {st['max_sweeps']} mean {st['mean_sweeps']:.2f}")
     inc_e = np.stack([e.get_f(m).astype(np.float64) - F[m] for m in range(M)])
     inc_o = np.stack([o.get_f(m) - F[m] for m in range(M)])
     scale = np.max(np.abs(inc_o))
