@@ -98,6 +98,10 @@ Phys derive_phys(const lbl_config& cfg) {
     P.tau_k = 3.0 / P.c_d / P.c_d / P.dt_d;
     P.inv_nx = 1.0f / float(cfg.nx);
     P.inv_ny = 1.0f / float(cfg.ny);
+    P.inv_c = 1.0f / P.c;
+    P.inv_c2 = 1.0f / (P.c * P.c);
+    P.inv_cs2 = 1.0f / P.cs2;
+    P.inv_two_dx = 1.0f / P.two_dx;
     return P;
 }
 

@@ -35,6 +35,9 @@ struct Phys {
     double tau_k;            // 3/c/c/dt chain, applied as ((3*nu)/c)/c)/dt in double
     double c_d, dt_d;        // c, dt widened to double for the tau chain
     float inv_nx, inv_ny;    // 1/nx, 1/ny for the forcing coordinates
+    // reciprocals of the constant divisors, rounded to float on the host: under
+    // -use_fast_math, x / constant rounds exactly like x * (1/constant)
+    float inv_c, inv_c2, inv_cs2, inv_two_dx;
 };
 
 // LETKF geometry (letkf.cu:29-56)

@@ -28,10 +28,11 @@ __host__ __device__ constexpr float w_q(int q) {                       // config
                                                            : float(1. / 36.);
 }
 
-// feq (lbm.h:31-39)
-__device__ __forceinline__ float feq(float rho, float u, float v, int q, float c) {
-    const float uc0 = (u * ex_q(q) + v * ey_q(q)) / c;
-    const float uu0 = (u * u + v * v) / (c * c);
+// feq (lbm.h:31-39); the divisions by the constants c and c*c are multiplications by
+// their host-rounded reciprocals, which round identically under -use_fast_math
+__device__ __forceinline__ float feq(float rho, float u, float v, int q, const Phys& P) {
+    const float uc0 = (u * ex_q(q) + v * ey_q(q)) * P.inv_c;
+    const float uu0 = (u * u + v * v) * P.inv_c2;
     return rho * w_q(q) * (float(1.) + float(3.) * uc0 + float(4.5) * uc0 * uc0 - float(1.5) * uu0);
 }
 
@@ -65,7 +66,7 @@ __device__ __forceinline__ float force_acc(float fx_, float fy_, int q, float rh
     const float wq = w_q(q);
     const float fx = (fx_ - P.fr_dt * u) * P.dt;
     const float fy = (fy_ - P.fr_dt * v) * P.dt;
-    const float f1 = (cx * fx + cy * fy) / P.cs2;
+    const float f1 = (cx * fx + cy * fy) * P.inv_cs2;
     float ret = f1;
     ret *= wq * rho;
     return ret;
@@ -224,10 +225,10 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
 
         // Smagorinsky eddy viscosity from the post-stream velocity (lbm.cu:42-60)
         const float ue = s_a[xp], uw = s_a[xm], ve = s_a[nx + xp], vw = s_a[nx + xm];
-        const float ux = (ue - uw) / P.two_dx;
-        const float uy = (uB - uM) / P.two_dx;
-        const float vx = (ve - vw) / P.two_dx;
-        const float vy = (vB - vM) / P.two_dx;
+        const float ux = (ue - uw) * P.inv_two_dx;
+        const float uy = (uB - uM) * P.inv_two_dx;
+        const float vx = (ve - vw) * P.inv_two_dx;
+        const float vy = (vB - vM) * P.inv_two_dx;
         const float s00 = ux;
         const float s01 = float(.5) * (uy + vx);
         const float s10 = s01;
@@ -245,7 +246,7 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
         const float fxc = Fx[ij], fyc = Fy[ij];
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
-            const float feqq = feq(rA, uA, vA, q, P.c);
+            const float feqq = feq(rA, uA, vA, q, P);
             const float fneq = fA[q] - feqq;
             fA[q] -= omega * fneq;
         }
