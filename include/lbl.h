@@ -185,6 +185,25 @@ int lbl_profile_step(lbl_ctx* ctx, int n, double* ms_per_launch);
 int lbl_event_record(lbl_ctx* ctx, int slot);
 int lbl_event_elapsed(lbl_ctx* ctx, int slot_a, int slot_b, double* ms);
 
+/* LETKF analysis for callers that cannot allocate device memory.  No counterpart
+ * in the reference: it serves code that owns every GPU buffer (a framework with
+ * its own caching allocator or memory budget, where a hidden cudaMalloc would
+ * overrun its pool and synchronise the device).  The caller passes device
+ * pointers to the forecast populations f_in [M][9][ny][nx], the output
+ * populations f_out and macros mac_out [M][3][ny][nx] (rho, u and, unless
+ * compat_stale_v, v), and the observations at the sites yo_sites
+ * [3][ny/p][nx/p] (u, v, rho; site (si, sj) is grid point (si*p, sj*p)).  The
+ * analysis scratch lives in one static device array of 8 MiB that every GPU
+ * loading liblbl holds until exit; configurations needing more are rejected with
+ * LBL_ERR_UNSUPPORTED.  All calls share that array: calls that overlap on the GPU
+ * race and must be serialised.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and must come before any stream capture.  stream is a
+ * cudaStream_t (NULL = legacy default stream); with host_stats (int[4]: max
+ * sweeps, non-converged points, NaN flag, sweep total) the call waits for the
+ * stream.  err (optional) receives a message of at most err_cap bytes. */
+int lbl_letkf_analysis_noalloc(const lbl_config* cfg, const float* f_in, float* f_out, float* mac_out,
+                               const float* yo_sites, void* stream, int* host_stats, char* err, size_t err_cap);
+
 /* Timers: writes the "#tag,sec" CSV (util/timer.hpp:66-72) into buf.
  * Returns the number of bytes needed (excluding NUL) or a negative status. */
 int lbl_timer_csv(lbl_ctx* ctx, int which, char* buf, size_t cap);

@@ -141,6 +141,24 @@ size_t analysis_smem_bytes(int M, int nobs);
 constexpr size_t kAnalysisSmemLimit = 200 * 1024;
 int analysis_prepare();
 
+// Explicit-pointer form of the analysis launch (no context), used by the entry
+// point that allocates no device memory (noalloc.cu).
+struct AnalysisArgs {
+    const float* f_in;        // [M][9][ny][nx]
+    float* f_out;             // [M][9][ny][nx]
+    float* mac_out;           // [M][3][ny][nx]
+    const float* yo;          // [3][nsites] u, v, rho at the sites
+    float* dY;                // [3][nsites][M] scratch
+    float* dyo;               // [3][nsites] scratch
+    const int* wtab;          // int4 [p*p][nobs] + int [p*p] counts
+    int* stats;               // int[4] scratch
+    int nx, ny, M, p, nox, nl_off, nobs;
+    float diag, sqrt_m1, tol, c;
+    int max_sweeps, write_v;
+};
+void launch_obs_ensemble_args(const AnalysisArgs& a, cudaStream_t s);
+void launch_analysis_args(const AnalysisArgs& a, cudaStream_t s);
+
 // ---- kernels (diag_kernels.cu) ----
 void launch_diag(const lbl_ctx* c, const float* mac, int member, double* red, cudaStream_t s);
 void launch_rmse(const lbl_ctx* c, const float* mac, const float* ut, const float* vt, double* red,

@@ -437,4 +437,54 @@ void launch_analysis(const lbl_ctx* c, const float* fin, float* fout, float* mac
     }
 }
 
+namespace {
+AnaParams params_from_args(const AnalysisArgs& a) {
+    AnaParams A;
+    A.nx = a.nx; A.ny = a.ny; A.nxy = a.nx * a.ny; A.M = a.M;
+    A.p = a.p; A.nsx = a.nx / a.p; A.nsy = a.ny / a.p; A.nsites = A.nsx * A.nsy;
+    A.n_pat_max = a.nobs;
+    A.nox = a.nox;
+    A.nl_off = a.nl_off;
+    A.diag = a.diag;
+    A.sqrt_m1 = a.sqrt_m1;
+    A.tol = a.tol;
+    A.max_sweeps = a.max_sweeps;
+    A.c = a.c;
+    A.write_v = a.write_v;
+    return A;
+}
+
+template <int MP>
+void launch_analysis_args_mp(const AnalysisArgs& a, cudaStream_t s) {
+    const AnaParams A = params_from_args(a);
+    constexpr int GPW = 32 / MP;
+    const int warps = 4;
+    const int groups_per_cta = warps * GPW;
+    const size_t sm = analysis_smem_bytes(A.M, A.n_pat_max);
+    const int tiles = ((A.nx + kCW - 1) / kCW) * ((A.ny + kCH - 1) / kCH);
+    const int grid = (tiles + groups_per_cta - 1) / groups_per_cta;
+    analysis_kernel<MP><<<grid, warps * 32, sm, s>>>(a.f_in, a.f_out, a.mac_out, a.dY, a.dyo,
+                                                      reinterpret_cast<const int4*>(a.wtab),
+                                                      a.wtab + size_t(4) * a.p * a.p * a.nobs, a.stats, A);
+}
+}  // namespace
+
+void launch_obs_ensemble_args(const AnalysisArgs& a, cudaStream_t s) {
+    const AnaParams A = params_from_args(a);
+    const int threads = 256;
+    const long long total = (long long)A.nsites * 32;
+    const int grid = int((total + threads - 1) / threads);
+    obs_ensemble_kernel<<<grid, threads, 0, s>>>(a.f_in, a.yo, a.dY, a.dyo, A);
+}
+
+void launch_analysis_args(const AnalysisArgs& a, cudaStream_t s) {
+    switch (pad_pow2(a.M)) {
+        case 4: launch_analysis_args_mp<4>(a, s); break;
+        case 8: launch_analysis_args_mp<8>(a, s); break;
+        case 16: launch_analysis_args_mp<16>(a, s); break;
+        case 32: launch_analysis_args_mp<32>(a, s); break;
+        default: break;
+    }
+}
+
 }  // namespace lbl

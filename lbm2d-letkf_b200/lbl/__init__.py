@@ -46,6 +46,7 @@ EXPORTS = (
     "lbl_get_ens_stats", "lbl_get_force", "lbl_get_force_state", "lbl_get_observed",
     "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_timer_csv", "lbl_timer_clear",
     "lbl_timer_transit", "lbl_profile_step", "lbl_event_record", "lbl_event_elapsed",
+    "lbl_letkf_analysis_noalloc",
 )
 
 
@@ -127,6 +128,7 @@ def load_library() -> ctypes.CDLL:
         "lbl_profile_step": (I, [P, I, D]),
         "lbl_event_record": (I, [P, I]),
         "lbl_event_elapsed": (I, [P, I, I, D]),
+        "lbl_letkf_analysis_noalloc": (I, [CP, P, P, P, P, P, IP, ctypes.c_char_p, U]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
