@@ -179,14 +179,20 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         //    letkf.cu:148-269), gathered once per block from the site ensemble
         const int bi = i / A.p, bj = j / A.p;
         if (bi != cached_bi || bj != cached_bj) {
-            for (int sl = 0; sl < nobs; sl++) {
-                const int var = sl / nox2, ab = sl - var * nox2;
-                const int b = ab / A.nox, a = ab - b * A.nox;
-                int si = (bi + a - A.nl_off) % A.nsx; si += si < 0 ? A.nsx : 0;
-                int sj = (bj + b - A.nl_off) % A.nsy; sj += sj < 0 ? A.nsy : 0;
-                const int site = si + A.nsx * sj;
-                sW[sl * MP + k] = real_k ? __ldg(dY + (size_t(var) * A.nsites + site) * M + k) : 0.f;
-                if (k == 0) sDyo[sl] = __ldg(dyo + size_t(var) * A.nsites + site);
+            for (int b = 0; b < A.nox; b++) {
+                int sj = (bj + b - A.nl_off) % A.nsy;
+                sj += sj < 0 ? A.nsy : 0;
+                for (int a = 0; a < A.nox; a++) {
+                    int si = (bi + a - A.nl_off) % A.nsx;
+                    si += si < 0 ? A.nsx : 0;
+                    const int site = si + A.nsx * sj;
+#pragma unroll
+                    for (int var = 0; var < 3; var++) {
+                        const int sl = a + A.nox * b + var * nox2;
+                        sW[sl * MP + k] = real_k ? __ldg(dY + (size_t(var) * A.nsites + site) * M + k) : 0.f;
+                        if (k == 0) sDyo[sl] = __ldg(dyo + size_t(var) * A.nsites + site);
+                    }
+                }
             }
             cached_bi = bi;
             cached_bj = bj;
@@ -246,31 +252,39 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         }
 
         // 5. one-sided Jacobi: rotate column pairs (k, k^r) until mutually orthogonal;
-        //    accumulated rotations V are the eigenvectors, Q V = V Lambda.
+        //    accumulated rotations V are the eigenvectors, Q V = V Lambda.  A sweep
+        //    whose largest relative off-diagonal |g|/sqrt(a b) stayed below 1e-4 ends the
+        //    iteration: convergence is quadratic, so the next sweep would be < 1e-8.
         int sweeps = 0;
         bool converged = false;
         for (int sw = 0; sw < A.max_sweeps; sw++) {
-            float a = 0.f;
+            float a0 = 0.f, a1 = 0.f;
 #pragma unroll
-            for (int l = 0; l < MP; l++) a = fmaf(qv[l], qv[l], a);
+            for (int l = 0; l < MP; l += 2) { a0 = fmaf(qv[l], qv[l], a0); a1 = fmaf(qv[l + 1], qv[l + 1], a1); }
+            float a = a0 + a1;
             bool rot = false;
+            float worst = 0.f;  // largest |g| / sqrt(a b) of the sweep
 #pragma unroll 1
             for (int rr = 1; rr < MP; rr++) {
                 float pq[MP];
 #pragma unroll
                 for (int l = 0; l < MP; l++) pq[l] = __shfl_xor_sync(0xffffffffu, qv[l], rr);
-                float g = 0.f;
+                float g0 = 0.f, g1 = 0.f;
 #pragma unroll
-                for (int l = 0; l < MP; l++) g = fmaf(qv[l], pq[l], g);
+                for (int l = 0; l < MP; l += 2) { g0 = fmaf(qv[l], pq[l], g0); g1 = fmaf(qv[l + 1], pq[l + 1], g1); }
+                const float g = g0 + g1;
                 const float b = __shfl_xor_sync(0xffffffffu, a, rr);
                 const bool low = k < (k ^ rr);
                 const float alo = low ? a : b, ahi = low ? b : a;
-                const bool doit = fabsf(g) > A.tol * sqrtf(alo * ahi);
+                const float nrm = sqrtf(alo * ahi);
+                const bool doit = fabsf(g) > A.tol * nrm;
                 float cs = 1.f, sn = 0.f, t = 0.f;
                 if (doit) {
-                    const float zeta = (ahi - alo) / (2.f * g);
-                    t = copysignf(1.f, zeta) / (fabsf(zeta) + sqrtf(1.f + zeta * zeta));
-                    cs = 1.f / sqrtf(1.f + t * t);
+                    // any exact rotation converges; cs^2 + sn^2 = 1 keeps V orthogonal
+                    worst = fmaxf(worst, __fdividef(fabsf(g), nrm));
+                    const float zeta = __fdividef(ahi - alo, 2.f * g);
+                    t = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.f)));
+                    cs = rsqrtf(fmaf(t, t, 1.f));
                     sn = cs * t;
                 }
                 rot |= doit;
@@ -287,7 +301,11 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
                 }
                 a = low ? a - t * g : a + t * g;
             }
-            const unsigned ballot = __ballot_sync(0xffffffffu, rot && active);
+            // group max of the sweep's relative off-diagonal
+#pragma unroll
+            for (int o = MP / 2; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+            const bool done = !rot || worst < 1e-4f;
+            const unsigned ballot = __ballot_sync(0xffffffffu, !done && active);
             if (!converged) {
                 sweeps = sw + 1;
                 if ((ballot & gmask) == 0u) converged = true;
