@@ -49,6 +49,12 @@ extern "C" {
 #define LBL_ERR_NOMEM      -7   /* device allocation failed                    */
 #define LBL_ERR_UNSUPPORTED -8  /* configuration not supported by this build   */
 #define LBL_ERR_NOCONV     -9   /* Jacobi eigensolver hit its sweep limit      */
+#define LBL_ERR_TIMEOUT   -10   /* a bounded wait inside a kernel gave up      */
+
+/* stream-collide kernel variants (lbl_config.lbm_variant) */
+#define LBL_LBM_AUTO   0    /* TMA-fed kernel where available, else direct loads */
+#define LBL_LBM_DIRECT 1    /* per-thread global loads                           */
+#define LBL_LBM_TMA    2    /* rows streamed into shared memory by the TMA unit  */
 
 /* run modes: the reference's -DTEST=<mode> (src/config.h:28-108) */
 #define LBL_MODE_NATURE   0
@@ -84,7 +90,7 @@ typedef struct lbl_config {
     int32_t compat_stale_v;  /* 1: after an analysis v is not refreshed (letkf.cu:340-355) */
     int32_t jacobi_max_sweeps; /* reference syevj: 100 (cu_matrix_eigensolver_wrapper.hpp:193) */
     int32_t write_mat;       /* reserved (LETKF matrix dumps); must be 0                  */
-    int32_t pad0;
+    int32_t lbm_variant;     /* LBL_LBM_* (stream-collide implementation)                 */
     double letkf_covinf;     /* LETKF_COVINF, multiplicative inflation beta (config.h:48-50) */
     double obs_error_rho;    /* OBS_ERROR_RHO (config.h:190-202)                          */
     double obs_error_u;      /* OBS_ERROR_U                                               */

@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "lbl_internal.h"
 
 using namespace lbl;
@@ -143,6 +145,7 @@ int validate(const lbl_config& c, std::string& err) {
     if (c.tau != 0 && !(c.tau > 0.5)) { err = "tau must be > 0.5 (or 0 to use nu)"; return LBL_ERR_ARG; }
     if (c.jacobi_max_sweeps < 1 || c.jacobi_max_sweeps > 1000) { err = "jacobi_max_sweeps out of range"; return LBL_ERR_ARG; }
     if (c.write_mat != 0) { err = "write_mat is not supported by this build"; return LBL_ERR_UNSUPPORTED; }
+    if (c.lbm_variant < LBL_LBM_AUTO || c.lbm_variant > LBL_LBM_TMA) { err = "unknown lbm_variant"; return LBL_ERR_ARG; }
     if (c.mode == LBL_MODE_DA_LETKF && !analysis_supported(c.n_ens)) {
         err = "DA_LETKF supports 2 <= n_ens <= 32 in this build"; return LBL_ERR_UNSUPPORTED;
     }
@@ -269,6 +272,17 @@ int launch_graph(lbl_ctx* ctx, int kind, int n) {
     return LBL_OK;
 }
 
+int check_timeout(lbl_ctx* ctx) {
+    int h = 0;
+    LBL_CK(cudaMemcpy(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        cudaMemset(ctx->d_err, 0, sizeof(int));
+        return fail(ctx, LBL_ERR_TIMEOUT, "stream-collide: a bounded shared-memory pipeline wait gave up (code " +
+                                              std::to_string(h) + ")");
+    }
+    return LBL_OK;
+}
+
 int read_stats(lbl_ctx* ctx) {
     LBL_CK(cudaMemcpy(ctx->h_stats, ctx->d_stats, sizeof(int) * 3, cudaMemcpyDeviceToHost));
     if (ctx->h_stats[2]) return fail(ctx, LBL_ERR_NAN, "NaN in the LETKF analysis (letkf_solver.h:352-364 sanity)");
@@ -376,6 +390,35 @@ int build_weight_table(lbl_ctx* ctx) {
     return LBL_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 3-D map over one population buffer: x (nx), y (ny), plane (member*9 + q); box = one
+// row segment of up to 256 floats
+bool make_population_map(const lbl_ctx* ctx, float* base, CUtensorMap* map) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {cuuint64_t(ctx->P.nx), cuuint64_t(ctx->P.ny), cuuint64_t(ctx->P.M) * kQ};
+    const cuuint64_t strides[2] = {cuuint64_t(ctx->P.nx) * sizeof(float), cuuint64_t(ctx->P.nxy) * sizeof(float)};
+    const cuuint32_t box[3] = {cuuint32_t(ctx->P.nx < 256 ? ctx->P.nx : 256), 1, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     ctx->cfg = *cfg;
     ctx->device = device;
@@ -452,6 +495,14 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     LBL_CK(cudaMemset(ctx->d_stats, 0, sizeof(int) * 4));  // max sweeps, non-converged, NaN, sweep total
     LBL_CK(cudaMalloc(&ctx->d_red, sizeof(double) * 8));
     LBL_CK(cudaMalloc(&ctx->d_tmp, sizeof(float) * 2 * nxy));
+    LBL_CK(cudaMalloc(&ctx->d_err, sizeof(int)));
+    LBL_CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
+    if (cfg->lbm_variant != LBL_LBM_DIRECT && lbm_tma_supported(cfg->nx)) {
+        ctx->use_tma = make_population_map(ctx, ctx->f[0], &ctx->tmap[0]) &&
+                       make_population_map(ctx, ctx->f[1], &ctx->tmap[1]) && lbm_tma_prepare(cfg->nx) == 0;
+    }
+    if (cfg->lbm_variant == LBL_LBM_TMA && !ctx->use_tma)
+        return fail(ctx, LBL_ERR_UNSUPPORTED, "TMA stream-collide unavailable for this grid (nx <= 512) or driver");
     for (auto& e : ctx->ev) LBL_CK(cudaEventCreate(&e));
     for (auto& e : ctx->user_ev) LBL_CK(cudaEventCreate(&e));
     ctx->have_events = true;
@@ -470,7 +521,7 @@ void destroy_impl(lbl_ctx* ctx) {
     for (int b = 0; b < 2; b++) { cudaFree(ctx->f[b]); cudaFree(ctx->mac[b]); }
     cudaFree(ctx->d_modes); cudaFree(ctx->d_amps); cudaFree(ctx->d_pool); cudaFree(ctx->d_force); cudaFree(ctx->d_sched);
     cudaFree(ctx->d_wtab); cudaFree(ctx->d_yo); cudaFree(ctx->d_dY); cudaFree(ctx->d_dyo);
-    cudaFree(ctx->d_stats); cudaFree(ctx->d_red); cudaFree(ctx->d_tmp);
+    cudaFree(ctx->d_stats); cudaFree(ctx->d_red); cudaFree(ctx->d_tmp); cudaFree(ctx->d_err);
     for (int b = 0; b < 2; b++) {
         if (ctx->h_yo[b]) cudaFreeHost(ctx->h_yo[b]);
         if (ctx->h_sched[b]) cudaFreeHost(ctx->h_sched[b]);
@@ -541,7 +592,10 @@ int update_impl(lbl_ctx* ctx, int nsteps, bool sync) {
         ctx->last_force_slot = n - 1;
         left -= n;
     }
-    if (sync) LBL_CK(cudaStreamSynchronize(ctx->stream));
+    if (sync) {
+        LBL_CK(cudaStreamSynchronize(ctx->stream));
+        LBL_TRY(check_timeout(ctx));
+    }
     return LBL_OK;
 }
 
@@ -677,6 +731,7 @@ int lbl_sync(lbl_ctx* ctx) {
     if (!ctx) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
     LBL_CK(cudaStreamSynchronize(ctx->stream));
+    LBL_TRY(check_timeout(ctx));
     if (ctx->cfg.mode == LBL_MODE_DA_LETKF) LBL_TRY(read_stats(ctx));
     return LBL_OK;
 }

@@ -2,6 +2,7 @@
 // liblbl translation units.  Not part of the public ABI (see include/lbl.h).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <curand.h>
 
@@ -113,6 +114,11 @@ struct lbl_ctx {
     void* obs_engine = nullptr;          // std::mt19937*
     std::vector<float> h_obs[4];         // last generated observed rho, u, v, vor
 
+    // TMA descriptors of the two population buffers (input side of a step)
+    CUtensorMap tmap[2];
+    bool use_tma = false;
+    int* d_err = nullptr;                // bounded-wait timeout flag of the TMA kernel
+
     // CUDA graphs keyed by (kind, n, parity)
     std::map<long long, cudaGraphExec_t> graphs;
 
@@ -131,6 +137,8 @@ void launch_ic_velocity(const double* modes /*[4][n]*/, int n_modes, int nx, int
 void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s);
 void launch_lbm_step(const lbl_ctx* c, const float* fin, float* fout, const float* force,
                      float* mac_out, cudaStream_t s);
+int lbm_tma_prepare(int nx);
+bool lbm_tma_supported(int nx);
 void launch_macros(const lbl_ctx* c, const float* f, float* mac, cudaStream_t s);
 
 // ---- kernels (letkf_kernels.cu) ----

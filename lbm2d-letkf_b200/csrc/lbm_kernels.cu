@@ -236,11 +236,13 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
         const float ss = sqrt(2 * (s00 * s00 + s01 * s10 + s10 * s01 + s11 * s11));
         const float nus = float(P.les_k * double(ss));
 
-        // relaxation (lbm.cu:132-139): tau in double from the float viscosity
+        // relaxation (lbm.cu:132-139): tau = 0.5 + 3 nu / c / c / dt in double from the float
+        // viscosity, as one FMA with the precomputed 3/c/c/dt; then omega = 1/tau correctly
+        // rounded in float (both differ from the reference's division chain only when a
+        // double result sits within one double ulp of a float rounding boundary)
         const float nu = P.nu + nus;
-        const float c = P.c, dt = P.dt;
-        const float tau = 0.5 + 3. * nu / c / c / dt;
-        const float omega = 1. / tau;
+        const float tau = float(fma(double(nu), P.tau_k, 0.5));
+        const float omega = __frcp_rn(tau);
 
         // BGK (lbm_collision_srt.h:8-16) + force (lbm.cu:142-147)
         const float fxc = Fx[ij], fyc = Fy[ij];
@@ -265,6 +267,207 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
         rA = rB; uA = uB; vA = vB;
 #pragma unroll
         for (int q = 0; q < kQ; q++) { fA[q] = fB[q]; fB[q] = fC[q]; }
+        float* t = s_a; s_a = s_b; s_b = s_c; s_c = t;
+        ij += nx;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// TMA-fed stream-collide (same arithmetic as lbm_step_kernel).  A producer warp
+// streams, for every pulled row jj of the strip (j0-1 .. j1), the nine source rows
+// f_q(:, jj - ey_q) into one stage of a shared-memory ring with
+// cp.async.bulk.tensor (one bulk copy per plane and 256-column box), signalling a
+// `full` mbarrier with the byte count; consumer warps read the pulled populations
+// straight from shared memory (x+-1 wrap by index) and release the stage on an
+// `empty` mbarrier.  Global loads thus cost one instruction per plane-row instead
+// of one per cell.  Every wait is bounded: on timeout the kernel records the stage
+// in *err and finishes without touching the ring again.
+// ---------------------------------------------------------------------------
+constexpr int kStages = 4;
+constexpr long long kWaitLimit = 1ll << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait; false (and *err set) when the limit is reached
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+    for (long long it = 0; it < kWaitLimit; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicCAS(err, 0, code);
+    return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void consumer_sync(int nthreads) {
+    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+template <bool WRITE_MAC>
+__global__ void __launch_bounds__(1024) lbm_step_tma_kernel(const __grid_constant__ CUtensorMap fin_map,
+                                                            float* __restrict__ fout,
+                                                            const float* __restrict__ force,
+                                                            float* __restrict__ mac, Phys P, int TY, int box,
+                                                            int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int nx = P.nx, ny = P.ny, nxy = P.nxy;
+    const int ncons = blockDim.x - 32;  // consumer threads, one column each
+    float* ring = reinterpret_cast<float*>(smem_raw);                 // [kStages][9][nx]
+    float* s_uv = ring + size_t(kStages) * kQ * nx;                     // [3][2][nx]
+    uint64_t* full = reinterpret_cast<uint64_t*>(s_uv + 6 * nx);        // [kStages]
+    uint64_t* empty = full + kStages;                                   // [kStages]
+    const int m = blockIdx.y;
+    const int j0 = blockIdx.x * TY;
+    const int j1 = min(j0 + TY, ny);
+    const int nrows = j1 - j0 + 2;  // pulled rows j0-1 .. j1
+    const int warp = threadIdx.x >> 5;
+    const int nwarps_c = ncons >> 5;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], nwarps_c);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp == nwarps_c) {  // ---------------- producer warp ----------------
+        if ((threadIdx.x & 31) == 0) {
+            bool ok = true;
+            int issued = 0;
+            const uint32_t bytes = uint32_t(kQ) * nx * sizeof(float);
+            for (int i = 0; i < nrows && ok; i++) {
+                const int s = i % kStages;
+                if (i >= kStages) ok = mbar_wait(&empty[s], ((i / kStages) - 1) & 1, err, 1);
+                if (!ok) break;
+                issued = i + 1;
+                mbar_expect_tx(&full[s], bytes);
+                const int jj = j0 - 1 + i;
+#pragma unroll
+                for (int q = 0; q < kQ; q++) {
+                    int y = jj - ey_q(q);
+                    y += (y < 0) ? ny : 0;
+                    y -= (y >= ny) ? ny : 0;
+                    float* dst = ring + (size_t(s) * kQ + q) * nx;
+                    for (int b = 0; b < nx; b += box) tma_load_3d(dst + b, &fin_map, b, y, m * kQ + q, &full[s]);
+                }
+            }
+            // drain: never leave the CTA with a bulk copy still writing shared memory
+            for (int i = max(0, issued - kStages); i < issued; i++) mbar_wait(&full[i % kStages], (i / kStages) & 1, err, 2);
+        }
+        return;
+    }
+
+    // ---------------- consumer warps ----------------
+    const int x = threadIdx.x;
+    const int xm = (x == 0) ? nx - 1 : x - 1;
+    const int xp = (x == nx - 1) ? 0 : x + 1;
+    float* __restrict__ fo = fout + size_t(m) * kQ * nxy + x;
+    const float* __restrict__ Fx = force + x;
+    const float* __restrict__ Fy = force + nxy + x;
+    bool good = true;
+    auto take = [&](int i, float (&fc)[kQ]) {  // pulled populations of ring row i
+        const int s = i % kStages;
+        if (good) good = mbar_wait(&full[s], (i / kStages) & 1, err, 3);
+        const float* st = ring + size_t(s) * kQ * nx;
+#pragma unroll
+        for (int q = 0; q < kQ; q++) {
+            const int col = ex_q(q) == -1 ? xp : (ex_q(q) == 0 ? x : xm);
+            fc[q] = good ? st[q * nx + col] : 0.f;
+        }
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(&empty[s]);
+    };
+    float* s_a = s_uv;
+    float* s_b = s_uv + 2 * nx;
+    float* s_c = s_uv + 4 * nx;
+    float fA[kQ], fB[kQ];
+    float rA, uA, vA, rB, uB, vB, uM, vM;
+    {
+        float t[kQ];
+        take(0, t);  // halo row j0-1: u,v only
+        const float r = rf(t);
+        uM = uf(t, r, P.c);
+        vM = vf(t, r, P.c);
+    }
+    take(1, fA);  // row j0
+    rA = rf(fA);
+    uA = uf(fA, rA, P.c);
+    vA = vf(fA, rA, P.c);
+    s_a[x] = uA;
+    s_a[nx + x] = vA;
+    int ij = j0 * nx;
+    for (int jc = j0; jc < j1; jc++) {
+        take(jc - j0 + 2, fB);  // row jc+1
+        rB = rf(fB);
+        uB = uf(fB, rB, P.c);
+        vB = vf(fB, rB, P.c);
+        s_b[x] = uB;
+        s_b[nx + x] = vB;
+        consumer_sync(ncons);
+
+        const float ue = s_a[xp], uw = s_a[xm], ve = s_a[nx + xp], vw = s_a[nx + xm];
+        const float ux = (ue - uw) * P.inv_two_dx;
+        const float uy = (uB - uM) * P.inv_two_dx;
+        const float vx = (ve - vw) * P.inv_two_dx;
+        const float vy = (vB - vM) * P.inv_two_dx;
+        const float s00 = ux;
+        const float s01 = float(.5) * (uy + vx);
+        const float s10 = s01;
+        const float s11 = vy;
+        const float ss = sqrt(2 * (s00 * s00 + s01 * s10 + s10 * s01 + s11 * s11));
+        const float nus = float(P.les_k * double(ss));
+        const float nu = P.nu + nus;
+        const float tau = float(fma(double(nu), P.tau_k, 0.5));
+        const float omega = __frcp_rn(tau);
+        const float fxc = Fx[ij], fyc = Fy[ij];
+#pragma unroll
+        for (int q = 0; q < kQ; q++) {
+            const float feqq = feq(rA, uA, vA, q, P);
+            const float fneq = fA[q] - feqq;
+            fA[q] -= omega * fneq;
+        }
+#pragma unroll
+        for (int q = 0; q < kQ; q++) fA[q] += force_acc(fxc, fyc, q, rA, uA, vA, P);
+        if (good) {
+#pragma unroll
+            for (int q = 0; q < kQ; q++) fo[q * nxy + ij] = fA[q];
+            if (WRITE_MAC) {
+                float* mm = mac + size_t(m) * 3 * nxy + x;
+                mm[ij] = rA;
+                mm[nxy + ij] = uA;
+                mm[2 * nxy + ij] = vA;
+            }
+        }
+        uM = uA; vM = vA;
+        rA = rB; uA = uB; vA = vB;
+#pragma unroll
+        for (int q = 0; q < kQ; q++) fA[q] = fB[q];
         float* t = s_a; s_a = s_b; s_b = s_c; s_c = t;
         ij += nx;
     }
@@ -328,11 +531,34 @@ void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s)
                                                  slot0, c->force_cap, c->P);
 }
 
+// one box per row (nx <= 256) or whole 256-column boxes (nx = 512): a partial box would
+// write past its plane in the shared ring
+bool lbm_tma_supported(int nx) { return (nx >= 32 && nx <= 256 && nx % 32 == 0) || nx == 512; }
+
+size_t lbm_tma_smem(int nx) { return sizeof(float) * (size_t(kStages) * kQ * nx + 6 * nx) + 2 * kStages * sizeof(uint64_t); }
+
+int lbm_tma_prepare(int nx) {
+    const int sm = int(lbm_tma_smem(nx));
+    int rc = int(cudaFuncSetAttribute(lbm_step_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    rc |= int(cudaFuncSetAttribute(lbm_step_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    return rc;
+}
+
 void launch_lbm_step(const lbl_ctx* c, const float* fin, float* fout, const float* force, float* mac_out,
                      cudaStream_t s) {
     const Phys& P = c->P;
     const int ty = strip_rows(P);
     dim3 grid((P.ny + ty - 1) / ty, P.M);
+    if (c->use_tma) {
+        const int b = (fin == c->f[0]) ? 0 : 1;
+        const size_t sm = lbm_tma_smem(P.nx);
+        const int box = P.nx < 256 ? P.nx : 256;
+        if (mac_out)
+            lbm_step_tma_kernel<true><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, mac_out, P, ty, box, c->d_err);
+        else
+            lbm_step_tma_kernel<false><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, nullptr, P, ty, box, c->d_err);
+        return;
+    }
     const size_t sm = sizeof(float) * 6 * P.nx;
     if (P.nx <= 256) {
         if (mac_out)

@@ -35,8 +35,9 @@ Q = 9
 ERRORS = {
     -1: "LBL_ERR_ARG", -2: "LBL_ERR_CUDA", -3: "LBL_ERR_CURAND", -4: "LBL_ERR_IO",
     -5: "LBL_ERR_NAN", -6: "LBL_ERR_STATE", -7: "LBL_ERR_NOMEM", -8: "LBL_ERR_UNSUPPORTED",
-    -9: "LBL_ERR_NOCONV",
+    -9: "LBL_ERR_NOCONV", -10: "LBL_ERR_TIMEOUT",
 }
+LBM_AUTO, LBM_DIRECT, LBM_TMA = 0, 1, 2
 
 # names of the exported C functions (must match include/lbl.h)
 EXPORTS = (
@@ -65,7 +66,7 @@ class Config(ctypes.Structure):
         ("ioprune", ctypes.c_int32), ("daprune", ctypes.c_int32), ("da_xyprune", ctypes.c_int32),
         ("letkf_rloc_len", ctypes.c_int32), ("iter_main", ctypes.c_int32), ("spinup", ctypes.c_int32),
         ("ic_kind", ctypes.c_int32), ("ens_init", ctypes.c_int32), ("compat_stale_v", ctypes.c_int32),
-        ("jacobi_max_sweeps", ctypes.c_int32), ("write_mat", ctypes.c_int32), ("pad0", ctypes.c_int32),
+        ("jacobi_max_sweeps", ctypes.c_int32), ("write_mat", ctypes.c_int32), ("lbm_variant", ctypes.c_int32),
         ("letkf_covinf", ctypes.c_double), ("obs_error_rho", ctypes.c_double), ("obs_error_u", ctypes.c_double),
         ("cs", ctypes.c_double), ("nu", ctypes.c_double), ("tau", ctypes.c_double), ("cfl", ctypes.c_double),
         ("rho_ref", ctypes.c_double), ("u_ref", ctypes.c_double), ("h_ref", ctypes.c_double),

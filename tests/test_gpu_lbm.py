@@ -179,3 +179,22 @@ def test_errors_are_reported_not_crashed():
         e.update(0, 1)
     assert ei.value.code == -6
 
+
+@pytest.mark.parametrize("nx", [64, 256, 512])
+def test_stream_collide_variants_agree(nx):
+    """The TMA-fed and the direct-load stream-collide compute the same arithmetic."""
+    out = {}
+    for variant in (lbl.LBM_DIRECT, lbl.LBM_TMA):
+        e = lbl.Ensemble(lbl.config_default("NATURE", nx, 2, lbm_variant=variant))
+        e.init(0)
+        e.update(0, 25)
+        out[variant] = [e.get_f(m).astype(np.float64) for m in range(2)] + [e.get_fields(1)[1]]
+    for a, b in zip(out[lbl.LBM_DIRECT][:2], out[lbl.LBM_TMA][:2]):
+        assert np.max(np.abs(a - b) / np.abs(a)) < 1e-6
+    np.testing.assert_allclose(out[lbl.LBM_TMA][2], out[lbl.LBM_DIRECT][2], rtol=1e-4, atol=1e-7)
+
+
+def test_tma_variant_rejected_where_unsupported():
+    with pytest.raises(lbl.LblError) as ei:
+        lbl.Ensemble(lbl.config_default("NATURE", 384, 1, lbm_variant=lbl.LBM_TMA))
+    assert ei.value.code == -8
