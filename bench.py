@@ -189,12 +189,18 @@ def init_dist():
 
 
 def reduce_max(dist, x, device):
+    """Max of x over ranks (device None: a CPU tensor, for gloo)."""
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+    t = torch.tensor([x], dtype=torch.float64, device="cpu" if device is None else f"cuda:{device}")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(world, cycles_per_rank, ms_max):
+    """Whole-job cycles/s of `world` independent replicas timed by the slowest rank."""
+    return world * cycles_per_rank / (ms_max / 1e3)
 
 
 def barrier(dist):
@@ -230,7 +236,7 @@ def run_engine(args, dist, rank, world, device):
         ens.sync()
     clk.__exit__(None, None, None)
     ms_max = reduce_max(dist, ms, device)
-    value = world * K / (ms_max / 1e3)
+    value = replica_value(world, K, ms_max)
     stats = ens.letkf_stats()
 
     # ---- e2e: host observations in, RMSE out, every cycle -----------------------------
@@ -249,7 +255,7 @@ def run_engine(args, dist, rank, world, device):
         rmse.append(e2e_ens.rmse_uv(*truth[c + 1]))
     e2e_ens.event_record(1)
     ms_e2e = reduce_max(dist, e2e_ens.event_elapsed(0, 1), device)
-    e2e_value = world * K / (ms_e2e / 1e3)
+    e2e_value = replica_value(world, K, ms_e2e)
     nsites = (NX // P_OBS) ** 2
     h2d = 3 * nsites * 4 + 2 * NX * NX * 4 + 4 * T
     d2h = 8
