@@ -497,7 +497,7 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     LBL_CK(cudaMalloc(&ctx->d_tmp, sizeof(float) * 2 * nxy));
     LBL_CK(cudaMalloc(&ctx->d_err, sizeof(int)));
     LBL_CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
-    if (cfg->lbm_variant != LBL_LBM_DIRECT && lbm_tma_supported(cfg->nx)) {
+    if (cfg->lbm_variant == LBL_LBM_TMA && lbm_tma_supported(cfg->nx)) {
         ctx->use_tma = make_population_map(ctx, ctx->f[0], &ctx->tmap[0]) &&
                        make_population_map(ctx, ctx->f[1], &ctx->tmap[1]) && lbm_tma_prepare(cfg->nx) == 0;
     }

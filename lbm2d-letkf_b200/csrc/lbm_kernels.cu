@@ -28,11 +28,25 @@ __host__ __device__ constexpr float w_q(int q) {                       // config
                                                            : float(1. / 36.);
 }
 
-// feq (lbm.h:31-39); the divisions by the constants c and c*c are multiplications by
-// their host-rounded reciprocals, which round identically under -use_fast_math
-__device__ __forceinline__ float feq(float rho, float u, float v, int q, const Phys& P) {
-    const float uc0 = (u * ex_q(q) + v * ey_q(q)) * P.inv_c;
-    const float uu0 = (u * u + v * v) * P.inv_c2;
+// The D2Q9 helpers below skip the e = 0 terms at compile time (x*0 cannot be folded
+// under IEEE rules, yet adding it never changes a finite result), and turn the
+// divisions by the constants c, c*c and cs2 into multiplications by host-rounded
+// reciprocals, which round identically under -use_fast_math.
+
+// u*ex + v*ey for the lattice direction q
+template <int q>
+__device__ __forceinline__ float edot(float u, float v) {
+    constexpr int ex = ex_q(q), ey = ey_q(q);
+    if (ex == 0 && ey == 0) return 0.f;
+    if (ex == 0) return ey > 0 ? v : -v;
+    if (ey == 0) return ex > 0 ? u : -u;
+    return (ex > 0 ? u : -u) + (ey > 0 ? v : -v);
+}
+
+// feq (lbm.h:31-39)
+template <int q>
+__device__ __forceinline__ float feq_q(float rho, float u, float v, float uu0, const Phys& P) {
+    const float uc0 = edot<q>(u, v) * P.inv_c;
     return rho * w_q(q) * (float(1.) + float(3.) * uc0 + float(4.5) * uc0 * uc0 - float(1.5) * uu0);
 }
 
@@ -46,30 +60,75 @@ __device__ __forceinline__ float rf(const float (&f)[kQ]) {
 __device__ __forceinline__ float uf(const float (&f)[kQ], float rho, float c) {
     float ret = 0;
 #pragma unroll
-    for (int q = 0; q < kQ; q++) ret += f[q] * c * ex_q(q);
+    for (int q = 0; q < kQ; q++)
+        if (ex_q(q) != 0) ret = fmaf(f[q], c * ex_q(q), ret);
     ret /= rho;
     return ret;
 }
 __device__ __forceinline__ float vf(const float (&f)[kQ], float rho, float c) {
     float ret = 0;
 #pragma unroll
-    for (int q = 0; q < kQ; q++) ret += f[q] * c * ey_q(q);
+    for (int q = 0; q < kQ; q++)
+        if (ey_q(q) != 0) ret = fmaf(f[q], c * ey_q(q), ret);
     ret /= rho;
     return ret;
 }
 
-// force_acc (lbm.h:41-70; first-order term only, FORCE_SECOND_ORDER off)
-__device__ __forceinline__ float force_acc(float fx_, float fy_, int q, float rho, float u, float v,
-                                           const Phys& P) {
-    const float cx = P.u_ref * ex_q(q);
-    const float cy = P.u_ref * ey_q(q);
-    const float wq = w_q(q);
-    const float fx = (fx_ - P.fr_dt * u) * P.dt;
-    const float fy = (fy_ - P.fr_dt * v) * P.dt;
-    const float f1 = (cx * fx + cy * fy) * P.inv_cs2;
+// force_acc (lbm.h:41-70; first-order term only, FORCE_SECOND_ORDER off), with
+// fx = (fx_ - friction/dt*u)*dt and fy precomputed per cell
+template <int q>
+__device__ __forceinline__ float force_acc_q(float fx, float fy, float rho, const Phys& P) {
+    const float f1 = edot<q>(P.u_ref * fx, P.u_ref * fy) * P.inv_cs2;
     float ret = f1;
-    ret *= wq * rho;
+    ret *= w_q(q) * rho;
     return ret;
+}
+
+// BGK toward feq plus the force term for all nine populations (lbm_collision_srt.h:8-16,
+// lbm.cu:142-147)
+__device__ __forceinline__ void collide(float (&f)[kQ], float rho, float u, float v, float omega, float fxc,
+                                        float fyc, const Phys& P) {
+    const float uu0 = (u * u + v * v) * P.inv_c2;
+    const float fx = (fxc - P.fr_dt * u) * P.dt;
+    const float fy = (fyc - P.fr_dt * v) * P.dt;
+#define LBL_COLLIDE_Q(q)                                  \
+    {                                                     \
+        const float feqq = feq_q<q>(rho, u, v, uu0, P);  \
+        const float fneq = f[q] - feqq;                   \
+        f[q] -= omega * fneq;                             \
+    }
+    LBL_COLLIDE_Q(0) LBL_COLLIDE_Q(1) LBL_COLLIDE_Q(2) LBL_COLLIDE_Q(3) LBL_COLLIDE_Q(4)
+    LBL_COLLIDE_Q(5) LBL_COLLIDE_Q(6) LBL_COLLIDE_Q(7) LBL_COLLIDE_Q(8)
+#undef LBL_COLLIDE_Q
+    f[0] += force_acc_q<0>(fx, fy, rho, P);
+    f[1] += force_acc_q<1>(fx, fy, rho, P);
+    f[2] += force_acc_q<2>(fx, fy, rho, P);
+    f[3] += force_acc_q<3>(fx, fy, rho, P);
+    f[4] += force_acc_q<4>(fx, fy, rho, P);
+    f[5] += force_acc_q<5>(fx, fy, rho, P);
+    f[6] += force_acc_q<6>(fx, fy, rho, P);
+    f[7] += force_acc_q<7>(fx, fy, rho, P);
+    f[8] += force_acc_q<8>(fx, fy, rho, P);
+}
+
+// Smagorinsky relaxation rate from the post-stream velocity stencil (lbm.cu:42-60,
+// 132-139): tau = 0.5 + 3 nu / c / c / dt in double from the float viscosity, as one
+// FMA with the precomputed 3/c/c/dt; omega = 1/tau correctly rounded in float.
+__device__ __forceinline__ float les_omega(float ue, float uw, float ve, float vw, float un, float us, float vn,
+                                           float vs, const Phys& P) {
+    const float ux = (ue - uw) * P.inv_two_dx;
+    const float uy = (un - us) * P.inv_two_dx;
+    const float vx = (ve - vw) * P.inv_two_dx;
+    const float vy = (vn - vs) * P.inv_two_dx;
+    const float s00 = ux;
+    const float s01 = float(.5) * (uy + vx);
+    const float s10 = s01;
+    const float s11 = vy;
+    const float ss = sqrt(2 * (s00 * s00 + s01 * s10 + s10 * s01 + s11 * s11));
+    const float nus = float(P.les_k * double(ss));
+    const float nu = P.nu + nus;
+    const float tau = float(fma(double(nu), P.tau_k, 0.5));
+    return __frcp_rn(tau);
 }
 
 // ---------------------------------------------------------------------------
@@ -152,15 +211,15 @@ __global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __
 // from the post-stream u,v stencil, BGK toward feq, first-order force with
 // friction) straight from registers.  Rows j0-1 and j1 are pulled as halo so that
 // the whole step is one pass over f: 72 B/cell of compulsory traffic in FP32.
-// Periodic wraps are branch-free selects on running row offsets (no integer
-// division in the loop).
+// NX > 0 fixes the (square) grid at compile time so that plane and row offsets are
+// immediates; NX = 0 reads nx, ny from P.
 // ---------------------------------------------------------------------------
-template <bool WRITE_MAC, int MAXT>
+template <bool WRITE_MAC, int MAXT, int NX>
 __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict__ fin, float* __restrict__ fout,
                                                         const float* __restrict__ force,
                                                         float* __restrict__ mac, Phys P, int TY) {
     extern __shared__ float s_uv[];  // [3][2][nx]
-    const int nx = P.nx, ny = P.ny, nxy = P.nxy;
+    const int nx = NX ? NX : P.nx, ny = NX ? NX : P.ny, nxy = NX ? NX * NX : P.nxy;
     const int x = threadIdx.x;
     const int m = blockIdx.y;
     const int j0 = blockIdx.x * TY;
@@ -189,7 +248,7 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
             fc[q] = __ldg(fm + q * nxy + row + col);
         }
     };
-    float* s_a = s_uv;           // ring of three rows of (u, v)
+    float* s_a = s_uv;  // ring of three rows of (u, v)
     float* s_b = s_uv + 2 * nx;
     float* s_c = s_uv + 4 * nx;
 
@@ -223,37 +282,8 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
         s_b[nx + x] = vB;
         __syncthreads();
 
-        // Smagorinsky eddy viscosity from the post-stream velocity (lbm.cu:42-60)
-        const float ue = s_a[xp], uw = s_a[xm], ve = s_a[nx + xp], vw = s_a[nx + xm];
-        const float ux = (ue - uw) * P.inv_two_dx;
-        const float uy = (uB - uM) * P.inv_two_dx;
-        const float vx = (ve - vw) * P.inv_two_dx;
-        const float vy = (vB - vM) * P.inv_two_dx;
-        const float s00 = ux;
-        const float s01 = float(.5) * (uy + vx);
-        const float s10 = s01;
-        const float s11 = vy;
-        const float ss = sqrt(2 * (s00 * s00 + s01 * s10 + s10 * s01 + s11 * s11));
-        const float nus = float(P.les_k * double(ss));
-
-        // relaxation (lbm.cu:132-139): tau = 0.5 + 3 nu / c / c / dt in double from the float
-        // viscosity, as one FMA with the precomputed 3/c/c/dt; then omega = 1/tau correctly
-        // rounded in float (both differ from the reference's division chain only when a
-        // double result sits within one double ulp of a float rounding boundary)
-        const float nu = P.nu + nus;
-        const float tau = float(fma(double(nu), P.tau_k, 0.5));
-        const float omega = __frcp_rn(tau);
-
-        // BGK (lbm_collision_srt.h:8-16) + force (lbm.cu:142-147)
-        const float fxc = Fx[ij], fyc = Fy[ij];
-#pragma unroll
-        for (int q = 0; q < kQ; q++) {
-            const float feqq = feq(rA, uA, vA, q, P);
-            const float fneq = fA[q] - feqq;
-            fA[q] -= omega * fneq;
-        }
-#pragma unroll
-        for (int q = 0; q < kQ; q++) fA[q] += force_acc(fxc, fyc, q, rA, uA, vA, P);
+        const float omega = les_omega(s_a[xp], s_a[xm], s_a[nx + xp], s_a[nx + xm], uB, uM, vB, vM, P);
+        collide(fA, rA, uA, vA, omega, Fx[ij], Fy[ij], P);
 #pragma unroll
         for (int q = 0; q < kQ; q++) fo[q * nxy + ij] = fA[q];
         if (WRITE_MAC) {
@@ -283,7 +313,7 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
 // of one per cell.  Every wait is bounded: on timeout the kernel records the stage
 // in *err and finishes without touching the ring again.
 // ---------------------------------------------------------------------------
-constexpr int kStages = 4;
+constexpr int kStages = 6;
 constexpr long long kWaitLimit = 1ll << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -327,15 +357,15 @@ __device__ __forceinline__ void consumer_sync(int nthreads) {
     asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
 
-template <bool WRITE_MAC>
+template <bool WRITE_MAC, int NX>
 __global__ void __launch_bounds__(1024) lbm_step_tma_kernel(const __grid_constant__ CUtensorMap fin_map,
                                                             float* __restrict__ fout,
                                                             const float* __restrict__ force,
                                                             float* __restrict__ mac, Phys P, int TY, int box,
                                                             int* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    const int nx = P.nx, ny = P.ny, nxy = P.nxy;
-    const int ncons = blockDim.x - 32;  // consumer threads, one column each
+    const int nx = NX ? NX : P.nx, ny = NX ? NX : P.ny, nxy = NX ? NX * NX : P.nxy;
+    const int ncons = nx;  // consumer threads, one column each
     float* ring = reinterpret_cast<float*>(smem_raw);                 // [kStages][9][nx]
     float* s_uv = ring + size_t(kStages) * kQ * nx;                     // [3][2][nx]
     uint64_t* full = reinterpret_cast<uint64_t*>(s_uv + 6 * nx);        // [kStages]
@@ -398,7 +428,7 @@ __global__ void __launch_bounds__(1024) lbm_step_tma_kernel(const __grid_constan
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
             const int col = ex_q(q) == -1 ? xp : (ex_q(q) == 0 ? x : xm);
-            fc[q] = good ? st[q * nx + col] : 0.f;
+            fc[q] = st[q * nx + col];
         }
         __syncwarp();
         if ((threadIdx.x & 31) == 0) mbar_arrive(&empty[s]);
@@ -431,29 +461,8 @@ __global__ void __launch_bounds__(1024) lbm_step_tma_kernel(const __grid_constan
         s_b[nx + x] = vB;
         consumer_sync(ncons);
 
-        const float ue = s_a[xp], uw = s_a[xm], ve = s_a[nx + xp], vw = s_a[nx + xm];
-        const float ux = (ue - uw) * P.inv_two_dx;
-        const float uy = (uB - uM) * P.inv_two_dx;
-        const float vx = (ve - vw) * P.inv_two_dx;
-        const float vy = (vB - vM) * P.inv_two_dx;
-        const float s00 = ux;
-        const float s01 = float(.5) * (uy + vx);
-        const float s10 = s01;
-        const float s11 = vy;
-        const float ss = sqrt(2 * (s00 * s00 + s01 * s10 + s10 * s01 + s11 * s11));
-        const float nus = float(P.les_k * double(ss));
-        const float nu = P.nu + nus;
-        const float tau = float(fma(double(nu), P.tau_k, 0.5));
-        const float omega = __frcp_rn(tau);
-        const float fxc = Fx[ij], fyc = Fy[ij];
-#pragma unroll
-        for (int q = 0; q < kQ; q++) {
-            const float feqq = feq(rA, uA, vA, q, P);
-            const float fneq = fA[q] - feqq;
-            fA[q] -= omega * fneq;
-        }
-#pragma unroll
-        for (int q = 0; q < kQ; q++) fA[q] += force_acc(fxc, fyc, q, rA, uA, vA, P);
+        const float omega = les_omega(s_a[xp], s_a[xm], s_a[nx + xp], s_a[nx + xm], uB, uM, vB, vM, P);
+        collide(fA, rA, uA, vA, omega, Fx[ij], Fy[ij], P);
         if (good) {
 #pragma unroll
             for (int q = 0; q < kQ; q++) fo[q * nxy + ij] = fA[q];
@@ -490,26 +499,31 @@ __global__ void macros_kernel(const float* __restrict__ f, float* __restrict__ m
 
 // Strip height: fill the GPU's resident CTA slots with as few waves as possible,
 // counting the two halo rows each strip pulls.
-int strip_rows(const Phys& P) {
-    static int slots = 0, slots_nx = 0;
-    if (slots == 0 || slots_nx != P.nx) {
-        slots_nx = P.nx;
+int strip_rows(const Phys& P, bool tma) {
+    static int slots[2] = {0, 0}, slots_nx[2] = {0, 0};
+    const int t = tma ? 1 : 0;
+    if (slots[t] == 0 || slots_nx[t] != P.nx) {
+        slots_nx[t] = P.nx;
         int dev = 0, sms = 148, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (P.nx <= 256)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 256>, P.nx,
+        if (tma)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_tma_kernel<false, 0>, P.nx + 32,
+                                                          sizeof(float) * (size_t(kStages) * kQ * P.nx + 6 * P.nx) +
+                                                              2 * kStages * sizeof(uint64_t));
+        else if (P.nx <= 256)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 256, 0>, P.nx,
                                                           sizeof(float) * 6 * P.nx);
         else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 1024>, P.nx,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 1024, 0>, P.nx,
                                                           sizeof(float) * 6 * P.nx);
-        slots = std::max(1, per_sm) * sms;
+        slots[t] = std::max(1, per_sm) * sms;
     }
     int best = 4;
     double best_cost = 1e30;
     for (int ty = 2; ty <= 32; ty++) {
         const long long strips = (long long)P.M * ((P.ny + ty - 1) / ty);
-        const long long waves = (strips + slots - 1) / slots;
+        const long long waves = (strips + slots[t] - 1) / slots[t];
         const double cost = double(waves) * (ty + 1.0);
         if (cost < best_cost - 1e-9) { best_cost = cost; best = ty; }
     }
@@ -537,39 +551,70 @@ bool lbm_tma_supported(int nx) { return (nx >= 32 && nx <= 256 && nx % 32 == 0) 
 
 size_t lbm_tma_smem(int nx) { return sizeof(float) * (size_t(kStages) * kQ * nx + 6 * nx) + 2 * kStages * sizeof(uint64_t); }
 
+namespace {
+template <int NX>
+int tma_prepare_nx(int sm) {
+    int rc = int(cudaFuncSetAttribute(lbm_step_tma_kernel<false, NX>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    rc |= int(cudaFuncSetAttribute(lbm_step_tma_kernel<true, NX>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    return rc;
+}
+
+template <int NX>
+void launch_tma(const lbl_ctx* c, dim3 grid, int ty, int b, float* fout, const float* force, float* mac_out,
+                cudaStream_t s) {
+    const Phys& P = c->P;
+    const size_t sm = lbm_tma_smem(P.nx);
+    const int box = P.nx < 256 ? P.nx : 256;
+    if (mac_out)
+        lbm_step_tma_kernel<true, NX><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, mac_out, P, ty, box, c->d_err);
+    else
+        lbm_step_tma_kernel<false, NX><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, nullptr, P, ty, box, c->d_err);
+}
+
+template <int MAXT, int NX>
+void launch_direct(const lbl_ctx* c, dim3 grid, int ty, const float* fin, float* fout, const float* force,
+                   float* mac_out, cudaStream_t s) {
+    const Phys& P = c->P;
+    const size_t sm = sizeof(float) * 6 * P.nx;
+    if (mac_out)
+        lbm_step_kernel<true, MAXT, NX><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty);
+    else
+        lbm_step_kernel<false, MAXT, NX><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty);
+}
+}  // namespace
+
 int lbm_tma_prepare(int nx) {
     const int sm = int(lbm_tma_smem(nx));
-    int rc = int(cudaFuncSetAttribute(lbm_step_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    rc |= int(cudaFuncSetAttribute(lbm_step_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-    return rc;
+    return tma_prepare_nx<0>(sm) | tma_prepare_nx<64>(sm) | tma_prepare_nx<128>(sm) | tma_prepare_nx<256>(sm) |
+           tma_prepare_nx<512>(sm);
 }
 
 void launch_lbm_step(const lbl_ctx* c, const float* fin, float* fout, const float* force, float* mac_out,
                      cudaStream_t s) {
     const Phys& P = c->P;
-    const int ty = strip_rows(P);
+    const int sq = (P.nx == P.ny) ? P.nx : 0;
+    const int ty = strip_rows(P, c->use_tma);
     dim3 grid((P.ny + ty - 1) / ty, P.M);
     if (c->use_tma) {
         const int b = (fin == c->f[0]) ? 0 : 1;
-        const size_t sm = lbm_tma_smem(P.nx);
-        const int box = P.nx < 256 ? P.nx : 256;
-        if (mac_out)
-            lbm_step_tma_kernel<true><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, mac_out, P, ty, box, c->d_err);
-        else
-            lbm_step_tma_kernel<false><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, nullptr, P, ty, box, c->d_err);
+        switch (sq) {
+            case 64: launch_tma<64>(c, grid, ty, b, fout, force, mac_out, s); break;
+            case 128: launch_tma<128>(c, grid, ty, b, fout, force, mac_out, s); break;
+            case 256: launch_tma<256>(c, grid, ty, b, fout, force, mac_out, s); break;
+            case 512: launch_tma<512>(c, grid, ty, b, fout, force, mac_out, s); break;
+            default: launch_tma<0>(c, grid, ty, b, fout, force, mac_out, s); break;
+        }
         return;
     }
-    const size_t sm = sizeof(float) * 6 * P.nx;
-    if (P.nx <= 256) {
-        if (mac_out)
-            lbm_step_kernel<true, 256><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty);
-        else
-            lbm_step_kernel<false, 256><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty);
-    } else {
-        if (mac_out)
-            lbm_step_kernel<true, 1024><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty);
-        else
-            lbm_step_kernel<false, 1024><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty);
+    switch (sq) {
+        case 64: launch_direct<256, 64>(c, grid, ty, fin, fout, force, mac_out, s); break;
+        case 128: launch_direct<256, 128>(c, grid, ty, fin, fout, force, mac_out, s); break;
+        case 256: launch_direct<256, 256>(c, grid, ty, fin, fout, force, mac_out, s); break;
+        case 512: launch_direct<1024, 512>(c, grid, ty, fin, fout, force, mac_out, s); break;
+        case 1024: launch_direct<1024, 1024>(c, grid, ty, fin, fout, force, mac_out, s); break;
+        default:
+            if (P.nx <= 256) launch_direct<256, 0>(c, grid, ty, fin, fout, force, mac_out, s);
+            else launch_direct<1024, 0>(c, grid, ty, fin, fout, force, mac_out, s);
     }
 }
 

@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
     // per-group shared memory
     // every block below is a multiple of 4 floats, so all float4 accesses stay 16-B aligned
     const int nobs_pad = (nobs + 3) & ~3;
-    const int per_grp = nobs * MP + nobs_pad + MP * MP + 2 * kQ * MP + 2 * MP;
+    const int per_grp = nobs * MP + nobs_pad + MP * MP + 2 * kQ * MP + 2 * MP + 12;
     float* base = smem + size_t(warp * GPW + grp) * per_grp;
     float* sW = base;                          // [nobs][MP] window dY (unweighted)
     float* sDyo = sW + nobs * MP;              // [nobs]     window innovations (padded to 4)
@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
     float* sD = sDX + kQ * MP;                 // [9][MP]  D = dX V
     float* sS = sD + kQ * MP;                  // [MP]     sqrt(M-1)/sqrt(lambda)
     float* sY = sS + MP;                       // [MP]     Lambda^-1 V^T c
+    float* sXbar = sY + MP;                    // [9]      ensemble mean (12 reserved)
 
     const int tiles_x = (A.nx + kCW - 1) / kCW;
     const int tile = (blockIdx.x * (blockDim.x >> 5) + warp) * GPW + grp;
@@ -166,13 +167,16 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         const bool real_m = active && real_k;
 
         // 1. forecast ensemble at the point: X, xbar, dX (letkf_solver.h:278-280)
-        float xq[kQ], xbar[kQ];
+        {
+            float xq[kQ];
 #pragma unroll
-        for (int q = 0; q < kQ; q++) xq[q] = real_m ? __ldg(fin + (size_t(k) * kQ + q) * A.nxy + point) : 0.f;
+            for (int q = 0; q < kQ; q++) xq[q] = real_m ? __ldg(fin + (size_t(k) * kQ + q) * A.nxy + point) : 0.f;
 #pragma unroll
-        for (int q = 0; q < kQ; q++) {
-            xbar[q] = group_sum<MP>(xq[q]) / float(M);
-            sDX[q * MP + k] = real_m ? xq[q] - xbar[q] : 0.f;
+            for (int q = 0; q < kQ; q++) {
+                const float xb = group_sum<MP>(xq[q]) / float(M);
+                sDX[q * MP + k] = real_m ? xq[q] - xb : 0.f;
+                if (k == 0) sXbar[q] = xb;
+            }
         }
 
         // 2. observation window of the point's p x p block (pack_yk/set_yo geometry,
@@ -348,7 +352,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
             float xa[kQ];
 #pragma unroll
             for (int q = 0; q < kQ; q++) {
-                xa[q] = xbar[q] + acc[q];
+                xa[q] = sXbar[q] + acc[q];
                 bad |= !(xa[q] == xa[q]);
                 fout[(size_t(k) * kQ + q) * A.nxy + point] = xa[q];
             }
@@ -422,7 +426,7 @@ int analysis_supported(int M) { return M >= 2 && M <= kMaxMemberLanes; }
 // dynamic shared memory of one analysis CTA (4 warps) for M members and a window of nobs slots
 size_t analysis_smem_bytes(int M, int nobs) {
     const int mp = pad_pow2(M);
-    const int per_grp = nobs * mp + ((nobs + 3) & ~3) + mp * mp + 2 * kQ * mp + 2 * mp;
+    const int per_grp = nobs * mp + ((nobs + 3) & ~3) + mp * mp + 2 * kQ * mp + 2 * mp + 12;
     return sizeof(float) * size_t(per_grp) * 4 * (32 / mp);
 }
 
