@@ -220,20 +220,37 @@ def run_engine(args, dist, rank, world, device):
     ens.cycle_async(0, None, None, None, T)
     ens.sync()
 
+    # Timed cycles: the 16-member state (37.7 MB per population buffer) fits in the
+    # 126 MB L2, so L2 is flushed (a 256 MB write) between timed cycles, outside the
+    # timed intervals; each cycle is timed on the engine's stream with CUDA events.
+    import torch
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")
+
+    def flush_l2():
+        flush.zero_()
+        torch.cuda.synchronize(device)
+
     # ---- value: resident observations --------------------------------------------
     clk = ClockSampler(device).__enter__()  # sampled from warm-up to the end of the timed region
     ens.cycle_async(T, *obs[0], T)  # uploads the observations once
     for c in range(1, W):
         ens.cycle_async((c + 1) * T, None, None, None, T)
     ens.sync()
+    torch.cuda.synchronize(device)
     barrier(dist)
-    if True:
+    ms = ms_ana = ms_fc = 0.0
+    for c in range(K):
+        flush_l2()
         ens.event_record(0)
-        for c in range(K):
-            ens.cycle_async((W + c + 1) * T, None, None, None, T)
+        ens.cycle_async((W + c + 1) * T, None, None, None, T)
         ens.event_record(1)
-        ms = ens.event_elapsed(0, 1)
-        ens.sync()
+        ms += ens.event_elapsed(0, 1)
+        a, f = ens.cycle_phases()
+        ms_ana += a
+        ms_fc += f
+    ens.sync()
+    torch.cuda.synchronize(device)
+    barrier(dist)
     clk.__exit__(None, None, None)
     ms_max = reduce_max(dist, ms, device)
     value = replica_value(world, K, ms_max)
@@ -247,40 +264,51 @@ def run_engine(args, dist, rank, world, device):
         e2e_ens.cycle_async((c + 1) * T, *obs[c], T)
         e2e_ens.rmse_uv(*truth[c + 1])
     e2e_ens.sync()
+    torch.cuda.synchronize(device)
     barrier(dist)
     rmse = []
-    e2e_ens.event_record(0)
+    ms_e2e = 0.0
     for c in range(W, W + K):
+        flush_l2()
+        e2e_ens.event_record(0)
         e2e_ens.cycle_async((c + 1) * T, *obs[c], T)
         rmse.append(e2e_ens.rmse_uv(*truth[c + 1]))
-    e2e_ens.event_record(1)
-    ms_e2e = reduce_max(dist, e2e_ens.event_elapsed(0, 1), device)
+        e2e_ens.event_record(1)
+        ms_e2e += e2e_ens.event_elapsed(0, 1)
+    torch.cuda.synchronize(device)
+    barrier(dist)
+    ms_e2e = reduce_max(dist, ms_e2e, device)
     e2e_value = replica_value(world, K, ms_e2e)
     nsites = (NX // P_OBS) ** 2
     h2d = 3 * nsites * 4 + 2 * NX * NX * 4 + 4 * T
     d2h = 8
 
-    # ---- roofline of the stream-collide kernel ------------------------------------------
-    ens.profile_step(20)
-    ms_step = ens.profile_step(200)
+    # ---- roofline of the stream-collide kernel, live in the timed cycles ----------------
+    # the forecast phase of each cycle graph is T back-to-back stream-collide launches
+    ms_step = ms_fc / (K * T)
     bytes_per_launch = 72.0 * M * NX * NX
     achieved = bytes_per_launch / (ms_step * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
     traffic = ncu_traffic()
+    ens.profile_step(20)
+    ms_isolated = ens.profile_step(200)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded nature run + Gaussian observation noise)",
         "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "l2": "working set 221 MB (f ping-pong 151 MB + forcing 67 MB) > 126 MB L2",
+                   "l2": "flushed (256 MB write) between timed cycles, outside the timed intervals",
                    "observations": "value leg reuses the resident observations; e2e uploads them every cycle"},
         "glups": M * NX * NX * T * K * world / (ms_max / 1e3) / 1e9,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "forecast_rmse_uv_last": rmse[-1] if rmse else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "lbm_step_kernel", "ms_per_launch": ms_step,
-                     "algorithmic_bytes_per_launch": bytes_per_launch, "peak_kind": peak_kind},
+                     "algorithmic_bytes_per_launch": bytes_per_launch, "peak_kind": peak_kind,
+                     "timed": "forecast phase of the timed cycles (in-graph events), 100 launches per cycle",
+                     "ms_per_launch_back_to_back": ms_isolated},
+        "phases_ms_per_cycle": {"analysis_with_forcing_beside": ms_ana / K, "forecast": ms_fc / K},
         "gpu_launches": K * (T + 3),
         "letkf": stats,
         "clocks": clk.summary(),

@@ -185,6 +185,14 @@ int lbl_rmse_uv(lbl_ctx* ctx, const float* u_true, const float* v_true, double* 
  * context's stream, timed with CUDA events; *ms_per_launch = average per launch.
  * The state advances by n steps with the last computed force field. */
 int lbl_profile_step(lbl_ctx* ctx, int n, double* ms_per_launch);
+/* Device time of the phases of the last graph that lbl_update / lbl_update_async /
+ * lbl_cycle_async launched, from events recorded inside the graph: *analysis_ms =
+ * observation operator + LETKF analysis (with the forcing chunk beside it; 0 for a
+ * forecast-only graph), *forecast_ms = the n stream-collide launches (a forecast-only
+ * graph runs its forcing chunk first and counts it here).  Waits for the
+ * graph to finish.  No counterpart in the reference (its util/timer.hpp timers are
+ * host clocks around synchronised calls; those are lbl_timer_*). */
+int lbl_get_cycle_phases(lbl_ctx* ctx, double* analysis_ms, double* forecast_ms);
 
 /* CUDA events on the context's stream, for device-side timing by callers:
  * slot in [0, 8).  lbl_event_elapsed waits for slot b and returns ms from a to b. */

@@ -240,6 +240,8 @@ int launch_graph(lbl_ctx* ctx, int kind, int n) {
         cudaGraph_t g = nullptr;
         LBL_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         int cur = ctx->cur;
+        // phase events become event-record nodes of the graph (device timestamps of each launch)
+        cudaEventRecordWithFlags(ctx->ev[10], ctx->stream, cudaEventRecordExternal);
         if (kind == 1 && n > 0) {
             // the forcing of the coming steps does not depend on the flow: compute it
             // on a side branch while the analysis runs (different pipes: XU/FP64 vs FMA/SHFL)
@@ -250,11 +252,14 @@ int launch_graph(lbl_ctx* ctx, int kind, int n) {
             enqueue_analysis(ctx, cur, ctx->stream);
             cur ^= 1;
             cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0);
+            cudaEventRecordWithFlags(ctx->ev[11], ctx->stream, cudaEventRecordExternal);
             enqueue_steps(ctx, n, cur, ctx->stream, true);
         } else {
             if (kind == 1) { enqueue_analysis(ctx, cur, ctx->stream); cur ^= 1; }
+            cudaEventRecordWithFlags(ctx->ev[11], ctx->stream, cudaEventRecordExternal);
             if (n > 0) enqueue_steps(ctx, n, cur, ctx->stream);
         }
+        cudaEventRecordWithFlags(ctx->ev[12], ctx->stream, cudaEventRecordExternal);
         const cudaError_t le = cudaGetLastError();
         const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &g);
         if (le != cudaSuccess || ee != cudaSuccess) {
@@ -269,6 +274,7 @@ int launch_graph(lbl_ctx* ctx, int kind, int n) {
         it = ctx->graphs.emplace(key, ge).first;
     }
     LBL_CK(cudaGraphLaunch(it->second, ctx->stream));
+    ctx->phases = kind == 1 ? 2 : 1;
     return LBL_OK;
 }
 
@@ -1022,6 +1028,19 @@ int lbl_profile_step(lbl_ctx* ctx, int n, double* ms_per_launch) {
     float ms = 0;
     LBL_CK(cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]));
     *ms_per_launch = double(ms) / n;
+    return LBL_OK;
+}
+
+int lbl_get_cycle_phases(lbl_ctx* ctx, double* analysis_ms, double* forecast_ms) {
+    if (!ctx || !analysis_ms || !forecast_ms) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    if (!ctx->phases) return fail(ctx, LBL_ERR_STATE, "lbl_get_cycle_phases before any forecast or cycle");
+    LBL_CK(cudaEventSynchronize(ctx->ev[12]));
+    float a = 0, f = 0;
+    LBL_CK(cudaEventElapsedTime(&a, ctx->ev[10], ctx->ev[11]));
+    LBL_CK(cudaEventElapsedTime(&f, ctx->ev[11], ctx->ev[12]));
+    *analysis_ms = ctx->phases == 2 ? a : 0.0;
+    *forecast_ms = f;
     return LBL_OK;
 }
 

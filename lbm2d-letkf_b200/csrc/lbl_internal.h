@@ -67,6 +67,7 @@ struct lbl_ctx {
     int device = 0;
     int ens_offset = 0;
     bool initialised = false;
+    int phases = 0;                      // phase events of the last graph: 0 none, 1 forecast, 2 analysis + forecast
     std::string err;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;         // forcing branch of the cycle graph
@@ -124,7 +125,8 @@ struct lbl_ctx {
 
     // timers
     lbl::TimerMap timers[2];
-    cudaEvent_t ev[16] = {};             // 0-3 stage timing, 4-5 sched staging, 6-7 obs staging, 8-9 profile
+    cudaEvent_t ev[16] = {};             // 0-3 stage timing, 4-5 sched staging, 6-7 obs staging, 8-9 profile,
+                                         // 10-12 phase events recorded inside the graphs
     cudaEvent_t user_ev[8] = {};         // lbl_event_record slots
     bool have_events = false;
 };

@@ -134,14 +134,13 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
     // per-group shared memory
     // every block below is a multiple of 4 floats, so all float4 accesses stay 16-B aligned
     const int nobs_pad = (nobs + 3) & ~3;
-    const int per_grp = nobs * MP + nobs_pad + MP * MP + 2 * kQ * MP + 2 * MP + 12;
+    const int per_grp = nobs * MP + nobs_pad + MP * MP + kQ * MP + 2 * MP + 12;
     float* base = smem + size_t(warp * GPW + grp) * per_grp;
     float* sW = base;                          // [nobs][MP] window dY (unweighted)
     float* sDyo = sW + nobs * MP;              // [nobs]     window innovations (padded to 4)
     float* sQ = sDyo + nobs_pad;               // [MP][MP] Q columns, then V
-    float* sDX = sQ + MP * MP;                 // [9][MP]  dX
-    float* sD = sDX + kQ * MP;                 // [9][MP]  D = dX V
-    float* sS = sD + kQ * MP;                  // [MP]     sqrt(M-1)/sqrt(lambda)
+    float* sDX = sQ + MP * MP;                 // [9][MP]  dX, then D = dX V in place
+    float* sS = sDX + kQ * MP;                 // [MP]     sqrt(M-1)/sqrt(lambda)
     float* sY = sS + MP;                       // [MP]     Lambda^-1 V^T c
     float* sXbar = sY + MP;                    // [9]      ensemble mean (12 reserved)
 
@@ -255,10 +254,12 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
             for (int l = 0; l < MP; l++) qv[l] = av[l];
         }
 
-        // 5. one-sided Jacobi: rotate column pairs (k, k^r) until mutually orthogonal;
-        //    accumulated rotations V are the eigenvectors, Q V = V Lambda.  A sweep
-        //    whose largest relative off-diagonal |g|/sqrt(a b) stayed below 1e-4 ends the
-        //    iteration: convergence is quadratic, so the next sweep would be < 1e-8.
+        // 5. one-sided Jacobi: rotate column pairs (k, k^r) of A = Q V until mutually
+        //    orthogonal.  V is not accumulated: for SPD Q, A with orthogonal columns is
+        //    V Lambda (A^T A = V^T Q^2 V diagonal makes V diagonalise Q), so column k of
+        //    V is a_k / |a_k| and lambda_k = |a_k|.  A sweep whose largest relative
+        //    off-diagonal |g|/sqrt(a b) stayed below 1e-4 ends the iteration: convergence
+        //    is quadratic, so after that sweep's rotations it is below 1e-8.
         int sweeps = 0;
         bool converged = false;
         for (int sw = 0; sw < A.max_sweeps; sw++) {
@@ -282,28 +283,18 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
                 const float alo = low ? a : b, ahi = low ? b : a;
                 const float nrm = sqrtf(alo * ahi);
                 const bool doit = fabsf(g) > A.tol * nrm;
-                float cs = 1.f, sn = 0.f, t = 0.f;
                 if (doit) {
-                    // any exact rotation converges; cs^2 + sn^2 = 1 keeps V orthogonal
+                    // any exact rotation converges; cs^2 + sn^2 = 1 keeps the columns' span
                     worst = fmaxf(worst, __fdividef(fabsf(g), nrm));
                     const float zeta = __fdividef(ahi - alo, 2.f * g);
-                    t = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.f)));
-                    cs = rsqrtf(fmaf(t, t, 1.f));
-                    sn = cs * t;
+                    const float t = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.f)));
+                    const float cs = rsqrtf(fmaf(t, t, 1.f));
+                    const float sn = low ? -(cs * t) : cs * t;  // low: cs a - sn b; high: sn a + cs b
+#pragma unroll
+                    for (int l = 0; l < MP; l++) qv[l] = fmaf(sn, pq[l], cs * qv[l]);
+                    a = low ? a - t * g : a + t * g;
                 }
                 rot |= doit;
-#pragma unroll
-                for (int l = 0; l < MP; l++) {
-                    const float pv = __shfl_xor_sync(0xffffffffu, vv[l], rr);
-                    if (low) {
-                        qv[l] = cs * qv[l] - sn * pq[l];
-                        vv[l] = cs * vv[l] - sn * pv;
-                    } else {
-                        qv[l] = sn * pq[l] + cs * qv[l];
-                        vv[l] = sn * pv + cs * vv[l];
-                    }
-                }
-                a = low ? a - t * g : a + t * g;
             }
             // group max of the sweep's relative off-diagonal
 #pragma unroll
@@ -317,10 +308,24 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
             if (ballot == 0u) break;
         }
 
-        // 6. eigenvalue of column k: (Q V)_k = lambda_k v_k; transform (letkf_solver.h:288-316)
+        // 6. eigenpair of column k: lambda_k = |a_k|, v_k = a_k / lambda_k (padding
+        //    columns are zero and keep the unit vector); transform (letkf_solver.h:288-316)
         float lam = 0.f;
+        {
+            float n0 = 0.f, n1 = 0.f;
 #pragma unroll
-        for (int l = 0; l < MP; l++) lam = fmaf(qv[l], vv[l], lam);
+            for (int l = 0; l < MP; l += 2) { n0 = fmaf(qv[l], qv[l], n0); n1 = fmaf(qv[l + 1], qv[l + 1], n1); }
+            const float n2 = n0 + n1;
+            if (n2 > 0.f) {
+                lam = sqrtf(n2);
+                const float inv = 1.f / lam;
+#pragma unroll
+                for (int l = 0; l < MP; l++) vv[l] = qv[l] * inv;
+            } else {
+#pragma unroll
+                for (int l = 0; l < MP; l++) vv[l] = (l == k) ? 1.f : 0.f;
+            }
+        }
 #pragma unroll
         for (int l = 0; l < MP; l++) sQ[k * MP + l] = vv[l];
         float vc = 0.f;  // (V^T c)_k
@@ -329,12 +334,17 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         sY[k] = real_k ? vc / lam : 0.f;
         sS[k] = real_k ? A.sqrt_m1 / sqrtf(lam) : 0.f;
         __syncwarp();
+        {
+            float dsum[kQ];
 #pragma unroll
-        for (int q = 0; q < kQ; q++) {
-            float dsum = 0.f;
+            for (int q = 0; q < kQ; q++) {
+                dsum[q] = 0.f;
 #pragma unroll
-            for (int l = 0; l < MP; l++) dsum = fmaf(sDX[q * MP + l], vv[l], dsum);
-            sD[q * MP + k] = dsum;
+                for (int l = 0; l < MP; l++) dsum[q] = fmaf(sDX[q * MP + l], vv[l], dsum[q]);
+            }
+            __syncwarp();  // every lane has read dX before D overwrites it
+#pragma unroll
+            for (int q = 0; q < kQ; q++) sDX[q * MP + k] = dsum[q];
         }
         __syncwarp();
         float acc[kQ];
@@ -344,7 +354,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         for (int jj = 0; jj < MP; jj++) {
             const float z = fmaf(sS[jj], sQ[jj * MP + k], sY[jj]);
 #pragma unroll
-            for (int q = 0; q < kQ; q++) acc[q] = fmaf(sD[q * MP + jj], z, acc[q]);
+            for (int q = 0; q < kQ; q++) acc[q] = fmaf(sDX[q * MP + jj], z, acc[q]);
         }
 
         // 7. write the analysis member k, refresh its macros (update_xk + lbm2euler)
@@ -426,7 +436,7 @@ int analysis_supported(int M) { return M >= 2 && M <= kMaxMemberLanes; }
 // dynamic shared memory of one analysis CTA (4 warps) for M members and a window of nobs slots
 size_t analysis_smem_bytes(int M, int nobs) {
     const int mp = pad_pow2(M);
-    const int per_grp = nobs * mp + ((nobs + 3) & ~3) + mp * mp + 2 * kQ * mp + 2 * mp + 12;
+    const int per_grp = nobs * mp + ((nobs + 3) & ~3) + mp * mp + kQ * mp + 2 * mp + 12;
     return sizeof(float) * size_t(per_grp) * 4 * (32 / mp);
 }
 

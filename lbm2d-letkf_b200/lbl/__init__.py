@@ -46,7 +46,7 @@ EXPORTS = (
     "lbl_cycle_async", "lbl_sync", "lbl_output", "lbl_get_f", "lbl_set_f", "lbl_get_fields",
     "lbl_get_ens_stats", "lbl_get_force", "lbl_get_force_state", "lbl_get_observed",
     "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_timer_csv", "lbl_timer_clear",
-    "lbl_timer_transit", "lbl_profile_step", "lbl_event_record", "lbl_event_elapsed",
+    "lbl_timer_transit", "lbl_profile_step", "lbl_get_cycle_phases", "lbl_event_record", "lbl_event_elapsed",
     "lbl_letkf_analysis_noalloc",
 )
 
@@ -127,6 +127,7 @@ def load_library() -> ctypes.CDLL:
         "lbl_timer_clear": (I, [P, I]),
         "lbl_timer_transit": (I, [P, I, ctypes.c_char_p]),
         "lbl_profile_step": (I, [P, I, D]),
+        "lbl_get_cycle_phases": (I, [P, D, D]),
         "lbl_event_record": (I, [P, I]),
         "lbl_event_elapsed": (I, [P, I, I, D]),
         "lbl_letkf_analysis_noalloc": (I, [CP, P, P, P, P, P, IP, ctypes.c_char_p, U]),
@@ -313,6 +314,12 @@ class Ensemble:
         ms = ctypes.c_double()
         self._check(self.lib.lbl_profile_step(self._h, n, ctypes.byref(ms)), "lbl_profile_step")
         return ms.value
+
+    def cycle_phases(self) -> tuple:
+        """(analysis_ms, forecast_ms) of the last graph, from events recorded inside it."""
+        a, f = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.lbl_get_cycle_phases(self._h, ctypes.byref(a), ctypes.byref(f)), "lbl_get_cycle_phases")
+        return a.value, f.value
 
     def event_record(self, slot: int):
         """Record CUDA event `slot` (0..7) on the engine's stream."""

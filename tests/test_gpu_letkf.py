@@ -177,3 +177,17 @@ def test_letkf_timer_tags():
                 "mpi_barrier", "solve", "mpi_xsol", "update_xk", "lbm2euler"):
         assert tag in tags
     assert tags == sorted(tags)  # std::map order (util/timer.hpp:66-72)
+
+
+def test_cycle_phase_events():
+    cfg, e, obs, _, _ = make_case(64, 8, 4, 1, 1.1)
+    t = cfg.iiter
+    e.cycle_async(t, *obs, 20)
+    ana, fc = e.cycle_phases()
+    assert ana > 0 and fc > 0
+    e.update(2 * t, 10)  # a forecast-only graph has no analysis phase
+    ana, fc = e.cycle_phases()
+    assert ana == 0 and fc > 0
+    fresh = lbl.Ensemble(cfg)
+    with pytest.raises(lbl.LblError):
+        fresh.cycle_phases()  # nothing launched yet
