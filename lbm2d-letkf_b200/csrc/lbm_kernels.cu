@@ -203,6 +203,80 @@ __global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __
     F[P.nxy + ij] = f_y;
 }
 
+// x rounded to the nearest float (ties to even), kept in FP64: the FP64 -> FP32 -> FP64
+// round trip of a float accumulator, done on the integer pipe.  Valid for finite x
+// with |x| in the normal float range or zero (partial force sums are O(1e-3..1)).
+__device__ __forceinline__ double round_to_float(double x) {
+    unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
+    b += 0x0FFFFFFFull + ((b >> 29) & 1ull);
+    b &= ~0x1FFFFFFFull;
+    return __longlong_as_double(static_cast<long long>(b));
+}
+
+// The same forcing with the step loop inside the thread.  theta, sin and cos depend
+// only on the cell and the mode, so each thread evaluates them once for its cell and
+// keeps them in registers (at most kRegModes modes); the per-step random
+// combinations (r0 kx + r1 ky, r2 kx + r3 ky) are staged in shared memory for the
+// CTA's steps.  Every expression keeps the reference's shape and the accumulators
+// keep its float rounding after each mode, so the field is the one above.
+constexpr int kRegModes = 32;
+
+__global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __restrict__ pool,
+                                                              const int* __restrict__ sched,
+                                                              const float* __restrict__ modes,
+                                                              const double* __restrict__ amps, int n, int nsteps,
+                                                              int steps_per_cta, float* __restrict__ force, int slot0,
+                                                              int cap, Phys P) {
+    extern __shared__ double2 s_axy[];  // (ax, ay)[n] (double), then (A, B)[steps_per_cta][n] (float2)
+    float2* s_ab = reinterpret_cast<float2*>(s_axy + n);
+    const int s0 = blockIdx.y * steps_per_cta;
+    const int ns = min(steps_per_cta, nsteps - s0);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) s_axy[k] = make_double2(amps[k], amps[n + k]);
+    for (int e = threadIdx.x; e < ns * n; e += blockDim.x) {
+        const int ls = e / n, k = e - ls * n;
+        const float* r = pool + sched[s0 + ls];
+        const float kx = modes[k], ky = modes[n + k];
+        const float a = r[k] * kx + r[n + k] * ky;
+        const float b = r[2 * n + k] * kx + r[3 * n + k] * ky;
+        s_ab[e] = make_float2(a, b);
+    }
+    __syncthreads();
+    const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= P.nxy) return;
+    const int nx = P.nx, ny = P.ny;
+    const int i = ij % nx, j = ij / nx;
+    const float x = float(i - nx / 2) * P.inv_nx;
+    const float y = float(j - ny / 2) * P.inv_ny;
+    float sn[kRegModes], cn[kRegModes];
+#pragma unroll
+    for (int k = 0; k < kRegModes; k++) {
+        if (k < n) {
+            const float kx = modes[k];
+            const float ky = modes[n + k];
+            const float theta = 2 * M_PI * (kx * x + ky * y);
+            sn[k] = sin(theta);
+            cn[k] = cos(theta);
+        }
+    }
+    for (int ls = 0; ls < ns; ls++) {
+        const float2* ab = s_ab + ls * n;
+        double f_x = 0, f_y = 0;
+#pragma unroll
+        for (int k = 0; k < kRegModes; k++) {
+            if (k < n) {
+                const float2 c = ab[k];
+                const double2 am = s_axy[k];
+                const float inner = c.x * sn[k] + c.y * cn[k];
+                f_x = round_to_float(f_x + am.x * inner);
+                f_y = round_to_float(f_y + am.y * inner);
+            }
+        }
+        float* F = force + size_t((slot0 + s0 + ls) % cap) * 2 * P.nxy;
+        F[ij] = float(f_x);
+        F[P.nxy + ij] = float(f_y);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Fused LBM step.  One CTA = one member x one strip of TY rows, one thread per
 // column x.  Each thread marches up its column: it pulls row j+2 (prefetched one
@@ -539,9 +613,24 @@ void launch_ic_velocity(const double* modes, int n_modes, int nx, int ny, float*
 
 void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s) {
     const int threads = 256;
-    dim3 grid((c->P.nxy + threads - 1) / threads, nsteps);
-    const size_t sm = sizeof(double) * 2 * c->n_modes + sizeof(float) * 6 * c->n_modes;
-    force_chunk_kernel<<<grid, threads, sm, s>>>(c->d_pool, c->d_sched, c->d_modes, c->d_amps, c->n_modes, c->d_force,
+    const int cells = (c->P.nxy + threads - 1) / threads;
+    const int n = c->n_modes;
+    if (n <= kRegModes) {
+        // split the steps over enough CTAs to fill the GPU four times over
+        int sms = 148, dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int ys = std::max(1, std::min(nsteps, (4 * sms + cells - 1) / cells));
+        const int spc = (nsteps + ys - 1) / ys;
+        dim3 grid(cells, (nsteps + spc - 1) / spc);
+        const size_t sm = sizeof(double2) * n + sizeof(float2) * size_t(spc) * n;
+        force_chunk_reg_kernel<<<grid, threads, sm, s>>>(c->d_pool, c->d_sched, c->d_modes, c->d_amps, n, nsteps,
+                                                         spc, c->d_force, slot0, c->force_cap, c->P);
+        return;
+    }
+    dim3 grid(cells, nsteps);
+    const size_t sm = sizeof(double) * 2 * n + sizeof(float) * 6 * n;
+    force_chunk_kernel<<<grid, threads, sm, s>>>(c->d_pool, c->d_sched, c->d_modes, c->d_amps, n, c->d_force,
                                                  slot0, c->force_cap, c->P);
 }
 

@@ -54,8 +54,8 @@ def test_forcing_stream_and_cursor_match_reference():
     np.testing.assert_array_equal(st["randoms"], g["normals_head"][2 * N4:3 * N4])
     fx, fy = e.force()
     rows = g["rows"]
-    assert rel_err(fx[rows], g["s1_rows_fx"]) < 1e-6
-    assert rel_err(fy[rows], g["s1_rows_fy"]) < 1e-6
+    np.testing.assert_array_equal(fx[rows], g["s1_rows_fx"])  # bit-exact
+    np.testing.assert_array_equal(fy[rows], g["s1_rows_fy"])
 
 
 def test_steps_match_reference_within_1e5():
@@ -86,6 +86,10 @@ def test_steps_match_reference_within_1e5():
         assert elem < 3e-5, (s, elem)
         np.testing.assert_allclose(checksums(f), g[f"s{s}_sums_f"], rtol=1e-6)
         if s > 0:
+            # the forcing of step s is bit-exact (the chunks here are 1, 9 and 90 steps)
+            fx, fy = e.force()
+            np.testing.assert_array_equal(fx[rows], g[f"s{s}_rows_fx"])
+            np.testing.assert_array_equal(fy[rows], g[f"s{s}_rows_fy"])
             # u = c*sum(f e_x)/rho cancels O(0.1) populations down to O(1e-3): a 1e-5 bound on
             # f allows ~1e-3 of max|u|; rho = sum(f) keeps the population bound
             r, u, v, _ = e.get_fields(0)
@@ -95,9 +99,11 @@ def test_steps_match_reference_within_1e5():
     print("population error vs reference per step (normwise, elementwise max):", worst)
 
 
-def test_forcing_field_matches_oracle():
-    e = nature(128, M=1)
+@pytest.mark.parametrize("kf", [4.0, 8.0])  # 29 modes (register kernel), 61 (per-step kernel)
+def test_forcing_field_matches_oracle(kf):
+    e = nature(128, M=1, kf=kf)
     o = oracle.Oracle(e.cfg)
+    assert (e.force_state()["n_modes"] <= 32) == (kf == 4.0)
     for _ in range(3):
         e.update(0, 1)
         st = e.force_state()
