@@ -477,6 +477,7 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
         LBL_CK(cudaMemcpy(ctx->d_modes, tab.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice));
         LBL_CK(cudaMalloc(&ctx->d_amps, sizeof(double) * 2 * n));
         LBL_CK(cudaMemcpy(ctx->d_amps, amps.data(), sizeof(double) * 2 * n, cudaMemcpyHostToDevice));
+        std::copy(amps.begin(), amps.end(), ctx->h_amps);
         ctx->n_rand_buf = n * 4096;                                        // data.cu:297
         LBL_CK(cudaMalloc(&ctx->d_pool, sizeof(float) * ctx->pool_slots * size_t(ctx->n_rand_buf)));
     }

@@ -81,6 +81,7 @@ struct lbl_ctx {
     // forcing (data.cu:161-350)
     int n_modes = 0;
     float h_kx[lbl::kMaxModes], h_ky[lbl::kMaxModes], h_amp[lbl::kMaxModes];
+    double h_amps[2 * lbl::kMaxModes];   // the FP64 per-mode factors held in d_amps
     float* d_modes = nullptr;            // [2][n_modes] kx, ky
     double* d_amps = nullptr;            // [2][n_modes] amp*2*pi*ky, amp*2*pi*(-kx) in FP64
     curandGenerator_t gen = nullptr;

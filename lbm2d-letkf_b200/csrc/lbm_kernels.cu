@@ -217,21 +217,43 @@ __device__ __forceinline__ double round_to_float(double x) {
 // only on the cell and the mode, so each thread evaluates them once for its cell and
 // keeps them in registers (at most kRegModes modes); the per-step random
 // combinations (r0 kx + r1 ky, r2 kx + r3 ky) are staged in shared memory for the
-// CTA's steps.  Every expression keeps the reference's shape and the accumulators
-// keep its float rounding after each mode, so the field is the one above.
+// CTA's steps, and the FP64 amplitudes travel as kernel parameters (constant-bank
+// operands).  Two steps advance together for instruction-level parallelism.  Every
+// expression keeps the reference's shape and the accumulators keep its float
+// rounding after each mode, so the field is the one above.
 constexpr int kRegModes = 32;
+struct ForceAmps {
+    double ax[kRegModes], ay[kRegModes];  // amp*2*pi*ky, amp*2*pi*(-kx)
+};
+
+template <int NS>
+__device__ __forceinline__ void force_steps(const float2* __restrict__ ab, int n, const float (&sn)[kRegModes],
+                                            const float (&cn)[kRegModes], const ForceAmps& A, double (&fx)[NS],
+                                            double (&fy)[NS]) {
+#pragma unroll
+    for (int t = 0; t < NS; t++) fx[t] = fy[t] = 0;
+#pragma unroll
+    for (int k = 0; k < kRegModes; k++) {
+        if (k < n) {
+#pragma unroll
+            for (int t = 0; t < NS; t++) {
+                const float2 c = ab[t * n + k];
+                const float inner = c.x * sn[k] + c.y * cn[k];
+                fx[t] = round_to_float(fx[t] + A.ax[k] * inner);
+                fy[t] = round_to_float(fy[t] + A.ay[k] * inner);
+            }
+        }
+    }
+}
 
 __global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __restrict__ pool,
                                                               const int* __restrict__ sched,
-                                                              const float* __restrict__ modes,
-                                                              const double* __restrict__ amps, int n, int nsteps,
-                                                              int steps_per_cta, float* __restrict__ force, int slot0,
-                                                              int cap, Phys P) {
-    extern __shared__ double2 s_axy[];  // (ax, ay)[n] (double), then (A, B)[steps_per_cta][n] (float2)
-    float2* s_ab = reinterpret_cast<float2*>(s_axy + n);
+                                                              const float* __restrict__ modes, const ForceAmps amps,
+                                                              int n, int nsteps, int steps_per_cta,
+                                                              float* __restrict__ force, int slot0, int cap, Phys P) {
+    extern __shared__ float2 s_ab[];  // (A, B)[steps_per_cta][n]
     const int s0 = blockIdx.y * steps_per_cta;
     const int ns = min(steps_per_cta, nsteps - s0);
-    for (int k = threadIdx.x; k < n; k += blockDim.x) s_axy[k] = make_double2(amps[k], amps[n + k]);
     for (int e = threadIdx.x; e < ns * n; e += blockDim.x) {
         const int ls = e / n, k = e - ls * n;
         const float* r = pool + sched[s0 + ls];
@@ -258,22 +280,23 @@ __global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __res
             cn[k] = cos(theta);
         }
     }
-    for (int ls = 0; ls < ns; ls++) {
-        const float2* ab = s_ab + ls * n;
-        double f_x = 0, f_y = 0;
+    int ls = 0;
+    for (; ls + 1 < ns; ls += 2) {
+        double fx[2], fy[2];
+        force_steps<2>(s_ab + ls * n, n, sn, cn, amps, fx, fy);
 #pragma unroll
-        for (int k = 0; k < kRegModes; k++) {
-            if (k < n) {
-                const float2 c = ab[k];
-                const double2 am = s_axy[k];
-                const float inner = c.x * sn[k] + c.y * cn[k];
-                f_x = round_to_float(f_x + am.x * inner);
-                f_y = round_to_float(f_y + am.y * inner);
-            }
+        for (int t = 0; t < 2; t++) {
+            float* F = force + size_t((slot0 + s0 + ls + t) % cap) * 2 * P.nxy;
+            F[ij] = float(fx[t]);
+            F[P.nxy + ij] = float(fy[t]);
         }
+    }
+    if (ls < ns) {
+        double fx[1], fy[1];
+        force_steps<1>(s_ab + ls * n, n, sn, cn, amps, fx, fy);
         float* F = force + size_t((slot0 + s0 + ls) % cap) * 2 * P.nxy;
-        F[ij] = float(f_x);
-        F[P.nxy + ij] = float(f_y);
+        F[ij] = float(fx[0]);
+        F[P.nxy + ij] = float(fy[0]);
     }
 }
 
@@ -623,9 +646,11 @@ void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s)
         const int ys = std::max(1, std::min(nsteps, (4 * sms + cells - 1) / cells));
         const int spc = (nsteps + ys - 1) / ys;
         dim3 grid(cells, (nsteps + spc - 1) / spc);
-        const size_t sm = sizeof(double2) * n + sizeof(float2) * size_t(spc) * n;
-        force_chunk_reg_kernel<<<grid, threads, sm, s>>>(c->d_pool, c->d_sched, c->d_modes, c->d_amps, n, nsteps,
-                                                         spc, c->d_force, slot0, c->force_cap, c->P);
+        const size_t sm = sizeof(float2) * size_t(spc) * n;
+        ForceAmps A{};
+        for (int k = 0; k < n; k++) { A.ax[k] = c->h_amps[k]; A.ay[k] = c->h_amps[n + k]; }
+        force_chunk_reg_kernel<<<grid, threads, sm, s>>>(c->d_pool, c->d_sched, c->d_modes, A, n, nsteps, spc,
+                                                         c->d_force, slot0, c->force_cap, c->P);
         return;
     }
     dim3 grid(cells, nsteps);
