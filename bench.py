@@ -374,6 +374,29 @@ def profile_cycles(args):
     ens.close()
 
 
+def lbm_sweep(args):
+    """Stream-collide alone at the given grids (NXxM,...): back-to-back launches on the
+    engine's stream, CUDA events, one JSON line per size.  Sizes whose population
+    buffers exceed the 126 MB L2 measure the HBM-bound regime."""
+    import lbl
+    for spec in args.lbm.split(","):
+        nx, m = (int(v) for v in spec.lower().split("x"))
+        e = lbl.Ensemble(lbl.config_default("NATURE", nx, m))
+        e.init(0)
+        e.update(0, 2)
+        e.profile_step(max(3, args.warmup))
+        ms = e.profile_step(max(1, args.steps))
+        bytes_launch = 72.0 * m * nx * nx
+        peak, peak_kind = measured_peak()
+        gbs = bytes_launch / (ms * 1e-3) / 1e9
+        print(json.dumps({"lbm_stream_collide": {
+            "nx": nx, "ny": nx, "members": m, "launches": args.steps, "ms_per_launch": ms,
+            "glups": m * nx * nx / (ms * 1e-3) / 1e9, "algorithmic_bytes_per_launch": bytes_launch,
+            "population_buffer_mb": bytes_launch / 2 / 1e6, "achieved_gbs": gbs, "peak_gbs": peak,
+            "frac": gbs / peak, "peak_kind": peak_kind}}), flush=True)
+        e.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -383,9 +406,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="run warmup + steps cycles of the workload and exit (for ncu captures)")
+    ap.add_argument("--lbm", default=None, metavar="NXxM[,NXxM...]",
+                    help="time the stream-collide alone at these grids and exit")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.lbm:
+        lbm_sweep(args)
+        return
     if args.profile:
         profile_cycles(args)
         return
