@@ -345,57 +345,57 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
             fc[q] = __ldg(fm + q * nxy + row + col);
         }
     };
-    float* s_a = s_uv;  // ring of three rows of (u, v)
-    float* s_b = s_uv + 2 * nx;
-    float* s_c = s_uv + 4 * nx;
-
-    float fA[kQ], fB[kQ], fC[kQ];
-    float rA, uA, vA, rB, uB, vB, uM, vM;
+    // Three row slots rotate roles (A = row being finalised, B = next row, C = the row
+    // after, prefetched); the march is unrolled by three so that the rotation is a
+    // renaming of registers, not a copy.  Slot k's (u, v) also lives in the shared
+    // ring s_uv[k]; u[c], v[c] hold the row below A (the previous A).
+    float f[3][kQ], r[3], u[3], v[3];
     {  // halo row below the strip: only its u,v (own column) are needed
-        float t[kQ];
-        pull(t);
-        const float r = rf(t);
-        uM = uf(t, r, P.c);
-        vM = vf(t, r, P.c);
+        pull(f[2]);
+        const float rr = rf(f[2]);
+        u[2] = uf(f[2], rr, P.c);
+        v[2] = vf(f[2], rr, P.c);
     }
     advance();
-    pull(fA);  // row j0
-    rA = rf(fA);
-    uA = uf(fA, rA, P.c);
-    vA = vf(fA, rA, P.c);
-    s_a[x] = uA;
-    s_a[nx + x] = vA;
+    pull(f[0]);  // row j0
+    r[0] = rf(f[0]);
+    u[0] = uf(f[0], r[0], P.c);
+    v[0] = vf(f[0], r[0], P.c);
+    s_uv[x] = u[0];
+    s_uv[nx + x] = v[0];
     advance();
-    pull(fB);  // row j0+1
+    pull(f[1]);  // row j0+1
     int ij = j0 * nx;
 
-    for (int jc = j0; jc < j1; jc++) {
+    auto row = [&](float (&fa)[kQ], float (&fb)[kQ], float (&fc)[kQ], float& ra, float& ua, float& va, float& rb,
+                   float& ub, float& vb, float uc, float vc, float* sa, float* sb, int jc) {
         advance();
-        if (jc + 2 <= j1) pull(fC);  // prefetch the row after next
-        rB = rf(fB);
-        uB = uf(fB, rB, P.c);
-        vB = vf(fB, rB, P.c);
-        s_b[x] = uB;
-        s_b[nx + x] = vB;
+        if (jc + 2 <= j1) pull(fc);  // prefetch the row after next
+        rb = rf(fb);
+        ub = uf(fb, rb, P.c);
+        vb = vf(fb, rb, P.c);
+        sb[x] = ub;
+        sb[nx + x] = vb;
         __syncthreads();
-
-        const float omega = les_omega(s_a[xp], s_a[xm], s_a[nx + xp], s_a[nx + xm], uB, uM, vB, vM, P);
-        collide(fA, rA, uA, vA, omega, Fx[ij], Fy[ij], P);
+        const float omega = les_omega(sa[xp], sa[xm], sa[nx + xp], sa[nx + xm], ub, uc, vb, vc, P);
+        collide(fa, ra, ua, va, omega, Fx[ij], Fy[ij], P);
 #pragma unroll
-        for (int q = 0; q < kQ; q++) fo[q * nxy + ij] = fA[q];
+        for (int q = 0; q < kQ; q++) fo[q * nxy + ij] = fa[q];
         if (WRITE_MAC) {
             float* mm = mac + size_t(m) * 3 * nxy + x;
-            mm[ij] = rA;
-            mm[nxy + ij] = uA;
-            mm[2 * nxy + ij] = vA;
+            mm[ij] = ra;
+            mm[nxy + ij] = ua;
+            mm[2 * nxy + ij] = va;
         }
-        // rotate the window and the shared ring (a <- b <- c <- a)
-        uM = uA; vM = vA;
-        rA = rB; uA = uB; vA = vB;
-#pragma unroll
-        for (int q = 0; q < kQ; q++) { fA[q] = fB[q]; fB[q] = fC[q]; }
-        float* t = s_a; s_a = s_b; s_b = s_c; s_c = t;
         ij += nx;
+    };
+    float* s0 = s_uv;
+    float* s1 = s_uv + 2 * nx;
+    float* s2 = s_uv + 4 * nx;
+    for (int jc = j0; jc < j1; jc += 3) {
+        row(f[0], f[1], f[2], r[0], u[0], v[0], r[1], u[1], v[1], u[2], v[2], s0, s1, jc);
+        if (jc + 1 < j1) row(f[1], f[2], f[0], r[1], u[1], v[1], r[2], u[2], v[2], u[0], v[0], s1, s2, jc + 1);
+        if (jc + 2 < j1) row(f[2], f[0], f[1], r[2], u[2], v[2], r[0], u[0], v[0], u[1], v[1], s2, s0, jc + 2);
     }
 }
 

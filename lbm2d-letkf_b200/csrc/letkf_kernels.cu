@@ -39,7 +39,9 @@ struct AnaParams {
     int nl_off;             // n_obs_local - obs_offset (window origin, in sites)
     float diag;             // (M-1)/beta
     float sqrt_m1;          // sqrt(M-1)
-    float tol;              // Jacobi off-diagonal tolerance
+    float tol;              // Jacobi off-diagonal tolerance: pairs below tol are not rotated
+    float stop;             // sqrt(tol): a sweep whose worst relative off-diagonal is below it ends the
+                            // iteration, since the sweep's own rotations leave about stop^2 = tol
     int max_sweeps;
     float c;                // lattice speed for the macros
     int write_v;            // 0 reproduces the reference's stale v after analysis
@@ -258,8 +260,9 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         //    orthogonal.  V is not accumulated: for SPD Q, A with orthogonal columns is
         //    V Lambda (A^T A = V^T Q^2 V diagonal makes V diagonalise Q), so column k of
         //    V is a_k / |a_k| and lambda_k = |a_k|.  A sweep whose largest relative
-        //    off-diagonal |g|/sqrt(a b) stayed below 1e-4 ends the iteration: convergence
-        //    is quadratic, so after that sweep's rotations it is below 1e-8.
+        //    off-diagonal |g|/sqrt(a b) stayed below sqrt(tol) ends the iteration:
+        //    convergence is quadratic, so that sweep's rotations leave about tol, the
+        //    relative off-diagonal norm at which the reference's syevj stops.
         int sweeps = 0;
         bool converged = false;
         for (int sw = 0; sw < A.max_sweeps; sw++) {
@@ -299,7 +302,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
             // group max of the sweep's relative off-diagonal
 #pragma unroll
             for (int o = MP / 2; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
-            const bool done = !rot || worst < 1e-4f;
+            const bool done = !rot || worst < A.stop;
             const unsigned ballot = __ballot_sync(0xffffffffu, !done && active);
             if (!converged) {
                 sweeps = sw + 1;
@@ -402,6 +405,7 @@ AnaParams make_params(const lbl_ctx* c) {
     A.diag = float((c->P.M - 1) / beta);
     A.sqrt_m1 = float(std::sqrt(double(c->P.M - 1)));
     A.tol = float(c->cfg.jacobi_tol);
+    A.stop = float(std::sqrt(c->cfg.jacobi_tol));
     A.max_sweeps = c->cfg.jacobi_max_sweeps;
     A.c = c->P.c;
     A.write_v = c->cfg.compat_stale_v ? 0 : 1;
@@ -480,6 +484,7 @@ AnaParams params_from_args(const AnalysisArgs& a) {
     A.diag = a.diag;
     A.sqrt_m1 = a.sqrt_m1;
     A.tol = a.tol;
+    A.stop = std::sqrt(a.tol);
     A.max_sweeps = a.max_sweeps;
     A.c = a.c;
     A.write_v = a.write_v;

@@ -57,10 +57,11 @@ def test_analysis_matches_oracle(nx, M, p, L, beta):
     o.assimilate(*obs)
     st = e.letkf_stats()
     assert st["nan"] == 0 and st["n_noconv"] == 0 and 1 <= st["max_sweeps"] <= 30, st
-    print(f"nx={nx} M={M} p={p} L={L}: sweeps max {st['max_sweeps']} mean {st['mean_sweeps']:.2f}")
     inc_e = np.stack([e.get_f(m).astype(np.float64) - F[m] for m in range(M)])
     inc_o = np.stack([o.get_f(m) - F[m] for m in range(M)])
     scale = np.max(np.abs(inc_o))
+    print(f"nx={nx} M={M} p={p} L={L}: sweeps max {st['max_sweeps']} mean {st['mean_sweeps']:.2f}, "
+          f"increment error {np.max(np.abs(inc_e - inc_o)) / scale:.2e} of the largest increment")
     assert scale > 1e-6  # the analysis does something
     # analysis increments within 1e-3 of their largest magnitude (FP32 Gram/Jacobi vs FP64)
     assert np.max(np.abs(inc_e - inc_o)) / scale < 1e-3
