@@ -204,13 +204,16 @@ __global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __
 }
 
 // x rounded to the nearest float (ties to even), kept in FP64: the FP64 -> FP32 -> FP64
-// round trip of a float accumulator, done on the integer pipe.  Valid for finite x
-// with |x| in the normal float range or zero (partial force sums are O(1e-3..1)).
+// round trip of a float accumulator.  C = 1.5 * 2^(e+29), with 2^e <= |x| < 2^(e+1)
+// taken from x's exponent field, puts x + C in a binade whose ulp is x's float ulp;
+// C is a multiple of that ulp with an even significand, so the FP64 addition rounds
+// x to float precision with ties to even, and subtracting C back is exact.  Valid
+// for finite x with |x| in the normal float range or zero (partial force sums are
+// O(1e-3..1)).
 __device__ __forceinline__ double round_to_float(double x) {
-    unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
-    b += 0x0FFFFFFFull + ((b >> 29) & 1ull);
-    b &= ~0x1FFFFFFFull;
-    return __longlong_as_double(static_cast<long long>(b));
+    const int c_hi = (__double2hiint(x) & 0x7FF00000) + 0x01D80000;  // exponent + 29, significand 1.5
+    const double c = __hiloint2double(c_hi, 0);
+    return __dadd_rn(__dadd_rn(x, c), -c);
 }
 
 // The same forcing with the step loop inside the thread.  theta, sin and cos depend
