@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define LBL_ABI_VERSION 1
+#define LBL_ABI_VERSION 2
 
 /* status codes */
 #define LBL_OK              0
@@ -60,6 +60,7 @@ extern "C" {
 #define LBL_MODE_NATURE   0
 #define LBL_MODE_OBSERVE  1
 #define LBL_MODE_DA_LETKF 2
+#define LBL_MODE_DA_NUDGING 3  /* DA_NUDGING: relax f toward feq of the observations (src/nudging.cu:40-143) */
 
 /* initial condition kinds */
 #define LBL_IC_REFERENCE  0  /* src/data.cu:53-120: band exp(-(k-kf)^2/5), |k-kf|<=10, max|u| = ic_amp */
@@ -109,6 +110,12 @@ typedef struct lbl_config {
     double jacobi_tol;       /* reference syevj: 1e-6 (cu_matrix_eigensolver_wrapper.hpp:192) */
     uint64_t force_seed;     /* cuRAND MTGP32 seed, 1991 (data.cu:294)                    */
     uint64_t obs_seed;       /* OBSERVE noise engine seed 334 (io.cu:321)                 */
+    /* appended in ABI version 2 */
+    int32_t da_dummy;        /* DA_DUMMY (config.h:71-74): a DA run without analyses (main.cu:94) */
+    int32_t da_quadra;       /* DA_QUADRA (config.h:63-65): nudge only x < nx/2 (odd), y < ny/2 (>= 2) */
+    int32_t da_obs_ruv;      /* 1: DA_OBS_RUV, rho observed (config.h:44); 0: DA_OBS_UV, model rho */
+    int32_t reserved0;       /* must be 0                                                 */
+    double da_nud_rate;      /* DA_NUD_RATE, nudging weight alpha, 0.1 (config.h:67-69)   */
 } lbl_config;
 
 typedef struct lbl_ctx lbl_ctx;

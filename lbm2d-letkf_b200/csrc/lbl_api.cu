@@ -129,7 +129,15 @@ Geo derive_geo(const lbl_config& cfg) {
 
 int validate(const lbl_config& c, std::string& err) {
     if (c.abi_version != LBL_ABI_VERSION) { err = "abi_version mismatch"; return LBL_ERR_ARG; }
-    if (c.mode < LBL_MODE_NATURE || c.mode > LBL_MODE_DA_LETKF) { err = "unknown mode"; return LBL_ERR_ARG; }
+    if (c.mode < LBL_MODE_NATURE || c.mode > LBL_MODE_DA_NUDGING) { err = "unknown mode"; return LBL_ERR_ARG; }
+    if (c.da_dummy != 0 && c.mode != LBL_MODE_DA_LETKF && c.mode != LBL_MODE_DA_NUDGING) {
+        err = "da_dummy needs DA_LETKF or DA_NUDGING (config.h:38-41)"; return LBL_ERR_ARG;
+    }
+    if (c.da_quadra < 0 || c.da_quadra > 3) { err = "DA_QUADRA out of range [0, 3]"; return LBL_ERR_ARG; }
+    if (c.mode == LBL_MODE_DA_NUDGING && !(c.da_nud_rate >= 0 && c.da_nud_rate <= 1)) {
+        err = "DA_NUD_RATE must lie in [0, 1]"; return LBL_ERR_ARG;
+    }
+    if (c.reserved0 != 0) { err = "reserved0 must be 0"; return LBL_ERR_ARG; }
     if (c.nx < 32 || c.ny < 8 || c.nx > 1024 || c.nx % 32 != 0) {
         err = "nx must be a multiple of 32 in [32, 1024] and ny >= 8"; return LBL_ERR_ARG;
     }
@@ -226,10 +234,17 @@ void enqueue_steps(lbl_ctx* ctx, int n, int cur, cudaStream_t s, bool force_done
     }
 }
 
-void enqueue_analysis(lbl_ctx* ctx, int cur, cudaStream_t s) {
+// enqueue the assimilation of the resident observations into buffer `cur`; returns the
+// buffer that holds the result (the LETKF writes the other buffer, nudging works in place)
+int enqueue_analysis(lbl_ctx* ctx, int cur, cudaStream_t s) {
+    if (ctx->cfg.mode == LBL_MODE_DA_NUDGING) {
+        launch_nudging(ctx, ctx->f[cur], ctx->mac[cur], s);
+        return cur;
+    }
     cudaMemsetAsync(ctx->d_stats, 0, sizeof(int) * 4, s);
     launch_obs_ensemble(ctx, ctx->f[cur], s);
     launch_analysis(ctx, ctx->f[cur], ctx->f[cur ^ 1], ctx->mac[cur ^ 1], s);
+    return cur ^ 1;
 }
 
 // Build (once) and launch a graph.  kind: 0 = steps, 1 = cycle (analysis + steps).
@@ -249,13 +264,12 @@ int launch_graph(lbl_ctx* ctx, int kind, int n) {
             cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0);
             launch_force_chunk(ctx, n, 0, ctx->side);
             cudaEventRecord(ctx->join_ev, ctx->side);
-            enqueue_analysis(ctx, cur, ctx->stream);
-            cur ^= 1;
+            cur = enqueue_analysis(ctx, cur, ctx->stream);
             cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0);
             cudaEventRecordWithFlags(ctx->ev[11], ctx->stream, cudaEventRecordExternal);
             enqueue_steps(ctx, n, cur, ctx->stream, true);
         } else {
-            if (kind == 1) { enqueue_analysis(ctx, cur, ctx->stream); cur ^= 1; }
+            if (kind == 1) cur = enqueue_analysis(ctx, cur, ctx->stream);
             cudaEventRecordWithFlags(ctx->ev[11], ctx->stream, cudaEventRecordExternal);
             if (n > 0) enqueue_steps(ctx, n, cur, ctx->stream);
         }
@@ -296,6 +310,9 @@ int read_stats(lbl_ctx* ctx) {
 }
 
 bool da_due(const lbl_ctx* ctx, int t) { return ((t / ctx->cfg.iiter) % ctx->cfg.daprune) == 0; }
+
+// the reference's DATA_ASSIMILATION run modes (config.h:32-53)
+bool is_da_mode(int mode) { return mode == LBL_MODE_DA_LETKF || mode == LBL_MODE_DA_NUDGING; }
 
 // initial velocity of one ensemble id on the device, rescaled on the host (FP32)
 int ic_member(lbl_ctx* ctx, int seed, std::vector<float>& u, std::vector<float>& v) {
@@ -489,12 +506,15 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     LBL_CKR(curandCreateGenerator(&ctx->gen, CURAND_RNG_PSEUDO_MTGP32));   // data.cu:293-294
     LBL_CKR(curandSetPseudoRandomGeneratorSeed(ctx->gen, cfg->force_seed));
     LBL_CKR(curandSetStream(ctx->gen, ctx->stream));
-    // LETKF buffers
+    // observation sites (both DA modes) and LETKF buffers
+    if (cfg->mode == LBL_MODE_DA_LETKF || cfg->mode == LBL_MODE_DA_NUDGING) {
+        const size_t ns = size_t(ctx->G.nsx) * ctx->G.nsy;
+        LBL_CK(cudaMalloc(&ctx->d_yo, sizeof(float) * 3 * ns));
+        for (int b = 0; b < 2; b++) LBL_CK(cudaMallocHost(&ctx->h_yo[b], sizeof(float) * 3 * ns));
+    }
     if (cfg->mode == LBL_MODE_DA_LETKF) {
         const size_t ns = size_t(ctx->G.nsx) * ctx->G.nsy;
         LBL_TRY(build_weight_table(ctx));
-        LBL_CK(cudaMalloc(&ctx->d_yo, sizeof(float) * 3 * ns));
-        for (int b = 0; b < 2; b++) LBL_CK(cudaMallocHost(&ctx->h_yo[b], sizeof(float) * 3 * ns));
         LBL_CK(cudaMalloc(&ctx->d_dY, sizeof(float) * 3 * ns * M));
         LBL_CK(cudaMalloc(&ctx->d_dyo, sizeof(float) * 3 * ns));
     }
@@ -550,7 +570,7 @@ int init_impl(lbl_ctx* ctx, int ens_offset) {
     const int M = ctx->P.M;
     ctx->ens_offset = ens_offset;
     ctx->cur = 0;
-    const int add = cfg.mode == LBL_MODE_DA_LETKF ? 334 : 0;       // data.cu:31-35
+    const int add = is_da_mode(cfg.mode) ? 334 : 0;                // data.cu:31-35 (DATA_ASSIMILATION)
     std::vector<float> un, vn;
     if (cfg.ens_init == LBL_ENS_PERTURBED) LBL_TRY(ic_member(ctx, ens_offset, un, vn));
     std::vector<float> fh(kQ * nxy), mh(3 * nxy);
@@ -606,9 +626,23 @@ int update_impl(lbl_ctx* ctx, int nsteps, bool sync) {
     return LBL_OK;
 }
 
+// DA_NUDGING (nudging.cu:40-143): every member's f relaxes toward feq of the observed
+// (bilinearly interpolated) rho, u, v, in place; the macros are not refreshed.
+int nudging_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const float* vo, bool sync) {
+    if (!da_due(ctx, t)) return LBL_OK;                             // nudging.cu:43-44
+    if (!ro || !uo || !vo) return fail(ctx, LBL_ERR_ARG, "null observation pointer");
+    LBL_TRY(upload_obs(ctx, ro, uo, vo));
+    launch_nudging(ctx, ctx->f[ctx->cur], ctx->mac[ctx->cur], ctx->stream);
+    LBL_CK(cudaGetLastError());
+    if (sync) LBL_CK(cudaStreamSynchronize(ctx->stream));
+    return LBL_OK;
+}
+
 int assimilate_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const float* vo, bool sync) {
     if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate before lbl_init");
-    if (ctx->cfg.mode != LBL_MODE_DA_LETKF) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate needs mode DA_LETKF");
+    if (!is_da_mode(ctx->cfg.mode)) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate needs mode DA_LETKF or DA_NUDGING");
+    if (ctx->cfg.da_dummy) return LBL_OK;                           // DA_DUMMY: no assimilation (main.cu:94)
+    if (ctx->cfg.mode == LBL_MODE_DA_NUDGING) return nudging_impl(ctx, t, ro, uo, vo, sync);
     TimerMap& tm = ctx->timers[LBL_TIMER_LETKF];
     timer_transit(tm, "_ignored");                                  // letkf.cu:121
     if (!da_due(ctx, t)) return LBL_OK;                             // letkf.cu:122-123
@@ -694,6 +728,10 @@ int lbl_config_default(lbl_config* c, int mode, int nx, int n_ens) {
     c->jacobi_tol = 1e-6;                    // cu_matrix_eigensolver_wrapper.hpp:192
     c->force_seed = 1991;                    // data.cu:294
     c->obs_seed = 334;                       // io.cu:321
+    c->da_dummy = 0;                         // config.h:71 (commented out)
+    c->da_quadra = 0;                        // config.h:63-65
+    c->da_obs_ruv = 1;                       // config.h:44 (DA_OBS_RUV)
+    c->da_nud_rate = 0.1;                    // config.h:67-69
     return LBL_OK;
 }
 
@@ -757,13 +795,19 @@ int lbl_assimilate_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, 
 
 int lbl_assimilate_files(lbl_ctx* ctx, int t, const char* io_prefix) {
     if (!ctx || !io_prefix) return LBL_ERR_ARG;
-    if (ctx->cfg.mode != LBL_MODE_DA_LETKF) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate needs mode DA_LETKF");
-    if (!da_due(ctx, t)) { timer_transit(ctx->timers[LBL_TIMER_LETKF], "_ignored"); return LBL_OK; }
+    if (!is_da_mode(ctx->cfg.mode)) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate needs mode DA_LETKF or DA_NUDGING");
+    if (ctx->cfg.da_dummy) return LBL_OK;                           // DA_DUMMY (main.cu:94)
+    if (!da_due(ctx, t)) {
+        if (ctx->cfg.mode == LBL_MODE_DA_LETKF) timer_transit(ctx->timers[LBL_TIMER_LETKF], "_ignored");
+        return LBL_OK;
+    }
     const size_t nxy = size_t(ctx->P.nxy);
-    std::vector<float> ro(nxy), uo(nxy), vo(nxy);
+    std::vector<float> ro(nxy, 0.f), uo(nxy), vo(nxy);
     const std::string step = to_string_aligned(t / ctx->cfg.iiter, 10);
     const std::string dir = std::string(io_prefix) + "/observed/ens0000/";
-    LBL_TRY(read_dat(dir + "rho_step" + step + ".dat", ro.data(), nxy, ctx->err));
+    // nudging reads the rho file only under DA_OBS_RUV (nudging.cu:72-80)
+    if (ctx->cfg.mode == LBL_MODE_DA_LETKF || ctx->cfg.da_obs_ruv)
+        LBL_TRY(read_dat(dir + "rho_step" + step + ".dat", ro.data(), nxy, ctx->err));
     LBL_TRY(read_dat(dir + "u_step" + step + ".dat", uo.data(), nxy, ctx->err));
     LBL_TRY(read_dat(dir + "v_step" + step + ".dat", vo.data(), nxy, ctx->err));
     return lbl_assimilate(ctx, t, ro.data(), uo.data(), vo.data());
@@ -774,11 +818,11 @@ int lbl_cycle_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
     LBL_TRY(set_device(ctx));
     if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_cycle_async before lbl_init");
     if (n_fc < 0 || n_fc > ctx->force_cap) return fail(ctx, LBL_ERR_ARG, "n_fc out of range for one graph");
-    const bool due = ctx->cfg.mode == LBL_MODE_DA_LETKF && t > 0 && da_due(ctx, t);
+    const bool due = is_da_mode(ctx->cfg.mode) && !ctx->cfg.da_dummy && t > 0 && da_due(ctx, t);
     if (due && ro && uo && vo) LBL_TRY(upload_obs(ctx, ro, uo, vo));  // NULL: resident observations
     if (n_fc > 0) LBL_TRY(schedule_force(ctx, n_fc));
     LBL_TRY(launch_graph(ctx, due ? 1 : 0, n_fc));
-    if (due) ctx->cur ^= 1;
+    if (due && ctx->cfg.mode == LBL_MODE_DA_LETKF) ctx->cur ^= 1;
     ctx->cur ^= (n_fc & 1);
     if (n_fc > 0) ctx->last_force_slot = n_fc - 1;
     return LBL_OK;

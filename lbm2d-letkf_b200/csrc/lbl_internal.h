@@ -146,6 +146,7 @@ void launch_macros(const lbl_ctx* c, const float* f, float* mac, cudaStream_t s)
 
 // ---- kernels (letkf_kernels.cu) ----
 void launch_obs_ensemble(const lbl_ctx* c, const float* f, cudaStream_t s);
+void launch_nudging(const lbl_ctx* c, float* f, const float* mac, cudaStream_t s);
 void launch_analysis(const lbl_ctx* c, const float* fin, float* fout, float* mac_out, cudaStream_t s);
 int analysis_supported(int M);
 size_t analysis_smem_bytes(int M, int nobs);

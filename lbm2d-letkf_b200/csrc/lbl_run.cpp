@@ -4,10 +4,11 @@
 // DROP_FORMER_HALF_TIMER rule, the io/ file layout and the elapsed_time CSVs
 // follow the reference.
 //
-// usage: lbl_run --mode=NATURE|OBSERVE|DA_LETKF [--nx=256] [--n_ens=M] [--KEY=VALUE ...] [ens_offset]
+// usage: lbl_run --mode=NATURE|OBSERVE|DA_LETKF|DA_NUDGING [--nx=256] [--n_ens=M] [--KEY=VALUE ...] [ens_offset]
 //   KEY is one of the reference's knobs: DAPRUNE IOPRUNE DA_XYPRUNE LETKF_RLOC_LEN
-//   LETKF_COVINF OBS_ERROR_RHO OBS_ERROR_U, or SPINUP ITER_MAIN IIITER CS NU TAU
-//   IC (reference|k4exp) IC_AMP ENS_INIT (independent|perturbed) ENS_PERTURB PREFIX DEVICE
+//   LETKF_COVINF OBS_ERROR_RHO OBS_ERROR_U DA_DUMMY DA_QUADRA DA_NUD_RATE DA_OBS_UV, or
+//   SPINUP ITER_MAIN IIITER CS NU TAU IC (reference|k4exp) IC_AMP
+//   ENS_INIT (independent|perturbed) ENS_PERTURB PREFIX DEVICE
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -63,7 +64,11 @@ int main(int argc, char** argv) {
             ofs = std::atoi(s.c_str());  // main.cu:42-45: argv[1] = ensemble offset
         }
     }
-    const int mode = mode_s == "OBSERVE" ? LBL_MODE_OBSERVE : mode_s == "DA_LETKF" ? LBL_MODE_DA_LETKF : LBL_MODE_NATURE;
+    const int mode = mode_s == "OBSERVE"      ? LBL_MODE_OBSERVE
+                     : mode_s == "DA_LETKF"   ? LBL_MODE_DA_LETKF
+                     : mode_s == "DA_NUDGING" ? LBL_MODE_DA_NUDGING
+                                              : LBL_MODE_NATURE;
+    const bool da = mode == LBL_MODE_DA_LETKF || mode == LBL_MODE_DA_NUDGING;  // DATA_ASSIMILATION
     lbl_config cfg;
     lbl_config_default(&cfg, mode, nx, M);
     for (auto& p : kv) {
@@ -86,6 +91,10 @@ int main(int argc, char** argv) {
         else if (k == "IC_AMP") cfg.ic_amp = std::atof(v);
         else if (k == "ENS_INIT") cfg.ens_init = std::string(v) == "perturbed" ? LBL_ENS_PERTURBED : LBL_ENS_INDEPENDENT;
         else if (k == "ENS_PERTURB") cfg.ens_perturb = std::atof(v);
+        else if (k == "DA_DUMMY") cfg.da_dummy = std::atoi(v);
+        else if (k == "DA_QUADRA") cfg.da_quadra = std::atoi(v);
+        else if (k == "DA_NUD_RATE") cfg.da_nud_rate = std::atof(v);
+        else if (k == "DA_OBS_UV") cfg.da_obs_ruv = std::atoi(v) ? 0 : 1;
         else { std::fprintf(stderr, "lbl_run: unknown option --%s\n", k.c_str()); return 2; }
     }
 
@@ -108,14 +117,15 @@ int main(int argc, char** argv) {
         std::printf("spin-up finished\n");
     }
     lbl_timer_transit(ctx, T, "_main");
-    const int iter_total = mode == LBL_MODE_OBSERVE ? cfg.iter_main + 1 : cfg.iter_main;  // config.h:144-151
+    const int iter_total = (mode == LBL_MODE_OBSERVE || (da && cfg.da_dummy)) ? cfg.iter_main + 1  // config.h:144-151
+                                                                                : cfg.iter_main;
     for (int tt = 0; tt < iter_total / cfg.iiter + 1; tt++) {
         const int t = tt * cfg.iiter;
         if (mode == LBL_MODE_DA_LETKF && t == iter_total / 2) {  // DROP_FORMER_HALF_TIMER, main.cu:85-92
             lbl_timer_clear(ctx, T);
             lbl_timer_clear(ctx, LBL_TIMER_LETKF);
         }
-        if (mode == LBL_MODE_DA_LETKF) {
+        if (da && !cfg.da_dummy) {                                   // main.cu:94
             lbl_timer_transit(ctx, T, "DA");
             if (t > 0) check(ctx, lbl_assimilate_files(ctx, t, prefix.c_str()), "assimilate");
             lbl_timer_transit(ctx, T, "_sync.DA");
@@ -130,14 +140,14 @@ int main(int argc, char** argv) {
     lbl_timer_transit(ctx, T, "_ignored");
 
     const std::string main_csv = timer_text(ctx, T);
-    const double fc = timer_get(main_csv, "forecast"), out = timer_get(main_csv, "output"), da = timer_get(main_csv, "DA");
+    const double fc = timer_get(main_csv, "forecast"), out = timer_get(main_csv, "output"), t_da = timer_get(main_csv, "DA");
     std::printf("\nElapsed time%s:\n%s", mode == LBL_MODE_DA_LETKF ? " for latter half loop" : "", main_csv.c_str());
     const double lu = double(nx) * nx * iter_total;
     // main.cu:128-133 prints these per member with the full iter_total (2x overstated
     // in DA_LETKF, where the timers cover the latter half only); the ensemble rates
     // below count every member and the steps the timers actually cover.
     std::printf("core MLUPS (reference formula, per member): %g\n", 1e-6 * lu / fc);
-    std::printf("total MLUPS (reference formula, per member): %g\n", 1e-6 * lu / (fc + out + da));
+    std::printf("total MLUPS (reference formula, per member): %g\n", 1e-6 * lu / (fc + out + t_da));
     const double covered = mode == LBL_MODE_DA_LETKF ? 0.5 : 1.0;
     std::printf("ensemble GLUPS (forecast tag): %g\n", 1e-9 * lu * M * covered / fc);
     if (mode == LBL_MODE_DA_LETKF) std::printf("LETKF breakdown:\n%s", timer_text(ctx, LBL_TIMER_LETKF).c_str());

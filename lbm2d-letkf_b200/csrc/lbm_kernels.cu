@@ -203,6 +203,69 @@ __global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __
     F[P.nxy + ij] = f_y;
 }
 
+// ---------------------------------------------------------------------------
+// DA_NUDGING (nudging.cu:40-143, DA_OBS_RUV or DA_OBS_UV): every member's f relaxes
+// in place toward feq of the observed rho, u, v, f = alpha feq_obs + (1 - alpha) f.
+// With DA_XYPRUNE p > 1 the site observations are interpolated bilinearly, the
+// weights in FP64 as in the reference; DA_QUADRA restricts the nudged quadrant.
+// yo holds the site observations [u, v, rho][site]; mac the current macros (rho is
+// taken from the model under DA_OBS_UV).  The macros are not refreshed, as there.
+// ---------------------------------------------------------------------------
+template <int q>
+__device__ __forceinline__ void nudge_q(float* fm, int nxy, float rho, float u, float v, float uu0, float alpha,
+                                        const Phys& P) {
+    const float f_calc = fm[q * nxy];
+    const float f_obse = feq_q<q>(rho, u, v, uu0, P);
+    fm[q * nxy] = alpha * f_obse + (1 - alpha) * f_calc;
+}
+
+__global__ void nudging_kernel(float* __restrict__ f, const float* __restrict__ mac, const float* __restrict__ yo,
+                               Phys P, int p, int nsx, int nsy, float alpha, int quadra, int ruv) {
+    const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    if (ij >= P.nxy) return;
+    const int nx = P.nx, ny = P.ny, nxy = P.nxy;
+    const int i = ij % nx, j = ij / nx;
+    if (quadra % 2 == 1 && !(i < nx / 2)) return;  // skip_east (nudging.cu:26, 93)
+    if (quadra >= 2 && !(j < ny / 2)) return;      // skip_north (nudging.cu:27, 95)
+    const int ns = nsx * nsy;
+    const float* du = yo;
+    const float* dv = yo + ns;
+    const float* dr = yo + 2 * ns;
+    float u_obse = 0, v_obse = 0, rho_obse = 0;
+    if (p == 1) {
+        u_obse = du[ij];
+        v_obse = dv[ij];
+        if (ruv) rho_obse = dr[ij];
+    } else {
+        // corners (iw, js) .. (iw + p, js + p), periodic: sites of the p-lattice
+        const int iw = (i / p) * p, js = (j / p) * p;
+        const int sw = iw / p, se = (sw + 1) % nsx, ss = js / p, sn = (ss + 1) % nsy;
+        const int ij0 = sw + nsx * ss, ije = se + nsx * ss, ijn = sw + nsx * sn, ijen = se + nsx * sn;
+        const float ir = (i - iw) / float(p);
+        const float jr = (j - js) / float(p);
+        u_obse = (1. - ir) * (1. - jr) * du[ij0] + ir * (1. - jr) * du[ije] + (1. - ir) * jr * du[ijn] +
+                 ir * jr * du[ijen];
+        v_obse = (1. - ir) * (1. - jr) * dv[ij0] + ir * (1. - jr) * dv[ije] + (1. - ir) * jr * dv[ijn] +
+                 ir * jr * dv[ijen];
+        if (ruv)
+            rho_obse = (1. - ir) * (1. - jr) * dr[ij0] + ir * (1. - jr) * dr[ije] + (1. - ir) * jr * dr[ijn] +
+                       ir * jr * dr[ijen];
+    }
+    if (!ruv) rho_obse = mac[size_t(m) * 3 * nxy + ij];  // DA_OBS_UV: rho_calc (nudging.cu:128-131)
+    const float uu0 = (u_obse * u_obse + v_obse * v_obse) * P.inv_c2;
+    float* fm = f + size_t(m) * kQ * nxy + ij;
+    nudge_q<0>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
+    nudge_q<1>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
+    nudge_q<2>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
+    nudge_q<3>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
+    nudge_q<4>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
+    nudge_q<5>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
+    nudge_q<6>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
+    nudge_q<7>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
+    nudge_q<8>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
+}
+
 // x rounded to the nearest float (ties to even), kept in FP64: the FP64 -> FP32 -> FP64
 // round trip of a float accumulator.  C = 1.5 * 2^(e+29), with 2^e <= |x| < 2^(e+1)
 // taken from x's exponent field, puts x + C in a binade whose ulp is x's float ulp;
@@ -635,6 +698,13 @@ int strip_rows(const Phys& P, bool tma) {
 void launch_ic_velocity(const double* modes, int n_modes, int nx, int ny, float* u, float* v, cudaStream_t s) {
     dim3 block(128), grid((nx + 127) / 128, ny);
     ic_velocity_kernel<<<grid, block, 0, s>>>(modes, n_modes, nx, ny, u, v);
+}
+
+void launch_nudging(const lbl_ctx* c, float* f, const float* mac, cudaStream_t s) {
+    const int threads = 256;
+    dim3 grid((c->P.nxy + threads - 1) / threads, c->P.M);
+    nudging_kernel<<<grid, threads, 0, s>>>(f, mac, c->d_yo, c->P, c->G.p, c->G.nsx, c->G.nsy,
+                                            float(c->cfg.da_nud_rate), c->cfg.da_quadra, c->cfg.da_obs_ruv);
 }
 
 void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s) {

@@ -24,9 +24,9 @@ import numpy as np
 _PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(_PKG_DIR, "liblbl.so")
 
-ABI_VERSION = 1
-MODE_NATURE, MODE_OBSERVE, MODE_DA_LETKF = 0, 1, 2
-MODES = {"NATURE": MODE_NATURE, "OBSERVE": MODE_OBSERVE, "DA_LETKF": MODE_DA_LETKF}
+ABI_VERSION = 2
+MODE_NATURE, MODE_OBSERVE, MODE_DA_LETKF, MODE_DA_NUDGING = 0, 1, 2, 3
+MODES = {"NATURE": MODE_NATURE, "OBSERVE": MODE_OBSERVE, "DA_LETKF": MODE_DA_LETKF, "DA_NUDGING": MODE_DA_NUDGING}
 IC_REFERENCE, IC_K4EXP = 0, 1
 ENS_INDEPENDENT, ENS_PERTURBED = 0, 1
 TIMER_MAIN, TIMER_LETKF = 0, 1
@@ -73,6 +73,8 @@ class Config(ctypes.Structure):
         ("kf", ctypes.c_double), ("fkf", ctypes.c_double), ("friction_rate", ctypes.c_double),
         ("ic_amp", ctypes.c_double), ("ens_perturb", ctypes.c_double), ("jacobi_tol", ctypes.c_double),
         ("force_seed", ctypes.c_uint64), ("obs_seed", ctypes.c_uint64),
+        ("da_dummy", ctypes.c_int32), ("da_quadra", ctypes.c_int32), ("da_obs_ruv", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32), ("da_nud_rate", ctypes.c_double),
     ]
 
     def copy(self) -> "Config":

@@ -354,6 +354,17 @@ int orc_get_f(orc_ctx* o, int m, double* f) {
     return 0;
 }
 
+int orc_set_macros(orc_ctx* o, int m, const float* r, const float* u, const float* v) {
+    const size_t n = size_t(o->cfg.nx) * o->cfg.ny;
+    if (m < 0 || m >= o->cfg.n_ens) return -1;
+    for (size_t i = 0; i < n; i++) {
+        if (r) o->r[m * n + i] = r[i];
+        if (u) o->u[m * n + i] = u[i];
+        if (v) o->v[m * n + i] = v[i];
+    }
+    return 0;
+}
+
 int orc_get_macros(orc_ctx* o, int m, double* r, double* u, double* v) {
     const size_t n = size_t(o->cfg.nx) * o->cfg.ny;
     if (m < 0 || m >= o->cfg.n_ens) return -1;
@@ -711,5 +722,46 @@ int orc_assimilate_rows(orc_ctx* o, const float* ro, const float* uo, const floa
 }
 
 int orc_max_sweeps(orc_ctx* o) { return o->max_sweeps_seen; }
+
+// DA_NUDGING (nudging.cu:40-143): f <- alpha feq(rho_o, u_o, v_o) + (1 - alpha) f for every
+// member, in FP64.  ro, uo, vo are full fields (NaN off the p-lattice, never read);
+// with p > 1 the lattice values are interpolated bilinearly between (iw, js) and
+// (iw + p, js + p), periodic (nudging.cu:98-127).  DA_QUADRA masks x >= nx/2 (odd)
+// and y >= ny/2 (>= 2); DA_OBS_UV (da_obs_ruv = 0) takes rho from the model.
+int orc_nudge(orc_ctx* o, const float* ro, const float* uo, const float* vo) {
+    const lbl_config& cfg = o->cfg;
+    const int nx = cfg.nx, ny = cfg.ny, p = cfg.da_xyprune;
+    const size_t nxy = size_t(nx) * ny;
+    const double alpha = float(cfg.da_nud_rate);
+    const bool skip_east = cfg.da_quadra % 2 == 1, skip_north = cfg.da_quadra >= 2;
+    auto at = [&](const float* a, int i, int j) { return double(a[size_t((i % nx + nx) % nx) + size_t(nx) * ((j % ny + ny) % ny)]); };
+    for (int m = 0; m < cfg.n_ens; m++) {
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) {
+                if (skip_east && !(i < nx / 2)) continue;
+                if (skip_north && !(j < ny / 2)) continue;
+                const size_t ij = size_t(i) + size_t(nx) * j;
+                double u, v, r;
+                if (p == 1) {
+                    u = uo[ij]; v = vo[ij]; r = ro[ij];
+                } else {
+                    const int iw = (i / p) * p, js = (j / p) * p;
+                    const double ir = double(i - iw) / p, jr = double(j - js) / p;
+                    auto itp = [&](const float* a) {
+                        return (1 - ir) * (1 - jr) * at(a, iw, js) + ir * (1 - jr) * at(a, iw + p, js) +
+                               (1 - ir) * jr * at(a, iw, js + p) + ir * jr * at(a, iw + p, js + p);
+                    };
+                    u = itp(uo); v = itp(vo); r = itp(ro);
+                }
+                if (!cfg.da_obs_ruv) r = o->r[m * nxy + ij];
+                for (int q = 0; q < Q; q++) {
+                    double& fq = o->f[(m * Q + q) * nxy + ij];
+                    fq = alpha * feq(r, u, v, q, o->d.c) + (1 - alpha) * fq;
+                }
+            }
+    }
+    return 0;
+}
 
 }  // extern "C"

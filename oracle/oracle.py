@@ -43,6 +43,7 @@ def load():
         "orc_set_f": (I, [P, I, F]),
         "orc_get_f": (I, [P, I, D]),
         "orc_get_macros": (I, [P, I, D, D, D]),
+        "orc_set_macros": (I, [P, I, F, F, F]),
         "orc_step_noforce": (I, [P]),
         "orc_step": (I, [P, I, F]),
         "orc_vorticity_f32": (I, [P, F, F, F]),
@@ -51,6 +52,7 @@ def load():
         "orc_assimilate": (I, [P, F, F, F, D]),
         "orc_assimilate_rows": (I, [P, F, F, F, D, I, I]),
         "orc_max_sweeps": (I, [P]),
+        "orc_nudge": (I, [P, F, F, F]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -139,6 +141,11 @@ class Oracle:
         self.lib.orc_get_macros(self.h, m, _d(r), _d(u), _d(v))
         return tuple(a.reshape(self.ny, self.nx) for a in (r, u, v))
 
+    def set_macros(self, m: int, r=None, u=None, v=None):
+        """Overwrite member m's current macros (any of r, u, v; None keeps it)."""
+        a = [None if x is None else _f32(x) for x in (r, u, v)]
+        self.lib.orc_set_macros(self.h, m, *(_f(x) for x in a))
+
     def force(self, randoms):
         fx, fy = np.empty(self.nxy, np.float64), np.empty(self.nxy, np.float64)
         self.lib.orc_force(self.h, _f(_f32(randoms)), _d(fx), _d(fy))
@@ -167,6 +174,10 @@ class Oracle:
 
     def assimilate_rows(self, rho_o, u_o, v_o, j0: int, j1: int):
         return self.lib.orc_assimilate_rows(self.h, _f(_f32(rho_o)), _f(_f32(u_o)), _f(_f32(v_o)), None, j0, j1)
+
+    def nudge(self, rho_o, u_o, v_o):
+        """DA_NUDGING (nudging.cu:40-143) of every member, FP64."""
+        return self.lib.orc_nudge(self.h, _f(_f32(rho_o)), _f(_f32(u_o)), _f(_f32(v_o)))
 
     def assimilate(self, rho_o, u_o, v_o, want_lambda: bool = False):
         lam = np.empty(self.nxy * self.M, np.float64) if want_lambda else None
