@@ -225,6 +225,26 @@ int lbl_event_elapsed(lbl_ctx* ctx, int slot_a, int slot_b, double* ms);
 int lbl_letkf_analysis_noalloc(const lbl_config* cfg, const float* f_in, float* f_out, float* mac_out,
                                const float* yo_sites, void* stream, int* host_stats, char* err, size_t err_cap);
 
+/* Evaluation measures over the files lbl_output writes (host only; no context, no
+ * GPU).  err (optional) receives a message of at most err_cap bytes.
+ *
+ * lbl_bindiff: RMSE of u and v together between dir0/<var>_step%010d.dat and dir1's
+ * (bindiff/main.cpp:27-69): sqrt(sum (a-b)^2 / count), differences in float, sums
+ * in long double; *count = values compared. */
+int lbl_bindiff(const char* dir0, const char* dir1, int step, double* rmse, long long* count, char* err,
+                size_t err_cap);
+/* lbl_ensemble_stat: ensemble_stat/main.cpp:33-170 with the grid size taken from the
+ * files: per-cell member mean and standard deviation (long double, kept as float) of
+ * ens_dir/ens%04d, then against nature_dir/ens0000: out[0] spread and out[1] RMSE of
+ * (u, v) together, out[2] rho spread, out[3] rho RMSE, out[4] max of the mean (u, v). */
+int lbl_ensemble_stat(const char* nature_dir, const char* ens_dir, int n_ens, int step, double* out, char* err,
+                      size_t err_cap);
+/* lbl_energy_spectrum: postprocess/fourier.ipynb cell 2 for one (u, v) [ny][nx]:
+ * F = DFT/(nx*ny); over the non-negative wavenumbers i, j <= nx/2, shell
+ * k = int(sqrt(i^2 + j^2) + 0.5) <= nx/2 accumulates |(Fu^2 + Fv^2)/2| (complex
+ * squares, as the notebook).  ek receives nx/2 + 1 values (FP64). */
+int lbl_energy_spectrum(const float* u, const float* v, int nx, int ny, double* ek);
+
 /* Timers: writes the "#tag,sec" CSV (util/timer.hpp:66-72) into buf.
  * Returns the number of bytes needed (excluding NUL) or a negative status. */
 int lbl_timer_csv(lbl_ctx* ctx, int which, char* buf, size_t cap);

@@ -47,7 +47,7 @@ EXPORTS = (
     "lbl_get_ens_stats", "lbl_get_force", "lbl_get_force_state", "lbl_get_observed",
     "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_timer_csv", "lbl_timer_clear",
     "lbl_timer_transit", "lbl_profile_step", "lbl_get_cycle_phases", "lbl_event_record", "lbl_event_elapsed",
-    "lbl_letkf_analysis_noalloc",
+    "lbl_letkf_analysis_noalloc", "lbl_bindiff", "lbl_ensemble_stat", "lbl_energy_spectrum",
 )
 
 
@@ -133,6 +133,10 @@ def load_library() -> ctypes.CDLL:
         "lbl_event_record": (I, [P, I]),
         "lbl_event_elapsed": (I, [P, I, I, D]),
         "lbl_letkf_analysis_noalloc": (I, [CP, P, P, P, P, P, IP, ctypes.c_char_p, U]),
+        "lbl_bindiff": (I, [ctypes.c_char_p, ctypes.c_char_p, I, D, ctypes.POINTER(ctypes.c_longlong),
+                            ctypes.c_char_p, U]),
+        "lbl_ensemble_stat": (I, [ctypes.c_char_p, ctypes.c_char_p, I, I, D, ctypes.c_char_p, U]),
+        "lbl_energy_spectrum": (I, [F, F, I, I, D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -366,3 +370,40 @@ def output(dat: Ensemble, t: int, io_prefix: str = "io"):
 
 def version() -> str:
     return load_library().lbl_version().decode()
+
+
+# ---- evaluation measures over the output files (host only) ----------------------------
+
+def bindiff(dir0: str, dir1: str, step: int) -> Tuple[float, int]:
+    """RMSE of (u, v) between two output directories at one step (bindiff/main.cpp)."""
+    lib = load_library()
+    r, n = ctypes.c_double(), ctypes.c_longlong()
+    err = ctypes.create_string_buffer(512)
+    rc = lib.lbl_bindiff(dir0.encode(), dir1.encode(), step, ctypes.byref(r), ctypes.byref(n), err, 512)
+    if rc != 0:
+        raise LblError(rc, err.value.decode())
+    return r.value, n.value
+
+
+def ensemble_stat(nature_dir: str, ens_dir: str, n_ens: int, step: int) -> dict:
+    """Spread and RMSE of the ensemble mean against nature (ensemble_stat/main.cpp)."""
+    lib = load_library()
+    out = (ctypes.c_double * 5)()
+    err = ctypes.create_string_buffer(512)
+    rc = lib.lbl_ensemble_stat(nature_dir.encode(), ens_dir.encode(), n_ens, step, out, err, 512)
+    if rc != 0:
+        raise LblError(rc, err.value.decode())
+    return dict(zip(("spread", "rmse", "rho_spread", "rho_rmse", "max"), list(out)))
+
+
+def energy_spectrum(u, v) -> np.ndarray:
+    """E(k), k = 0..nx/2, of postprocess/fourier.ipynb cell 2 for one (u, v) field."""
+    lib = load_library()
+    u = np.ascontiguousarray(u, dtype=np.float32)
+    v = np.ascontiguousarray(v, dtype=np.float32)
+    ny, nx = u.shape
+    ek = np.empty(nx // 2 + 1, np.float64)
+    rc = lib.lbl_energy_spectrum(_fp(u), _fp(v), nx, ny, ek.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    if rc != 0:
+        raise LblError(rc, "lbl_energy_spectrum")
+    return ek
