@@ -90,7 +90,7 @@ typedef struct lbl_config {
     int32_t ens_init;        /* LBL_ENS_*                                                 */
     int32_t compat_stale_v;  /* 1: after an analysis v is not refreshed (letkf.cu:340-355) */
     int32_t jacobi_max_sweeps; /* reference syevj: 100 (cu_matrix_eigensolver_wrapper.hpp:193) */
-    int32_t write_mat;       /* reserved (LETKF matrix dumps); must be 0                  */
+    int32_t write_mat;       /* need_save_mat (letkf.cu:33): dump the LETKF matrices each analysis */
     int32_t lbm_variant;     /* LBL_LBM_* (stream-collide implementation)                 */
     double letkf_covinf;     /* LETKF_COVINF, multiplicative inflation beta (config.h:48-50) */
     double obs_error_rho;    /* OBS_ERROR_RHO (config.h:190-202)                          */
@@ -224,6 +224,19 @@ int lbl_event_elapsed(lbl_ctx* ctx, int slot_a, int slot_b, double* ms);
  * stream.  err (optional) receives a message of at most err_cap bytes. */
 int lbl_letkf_analysis_noalloc(const lbl_config* cfg, const float* f_in, float* f_out, float* mac_out,
                                const float* yo_sites, void* stream, int* host_stats, char* err, size_t err_cap);
+
+/* Directory prefix (config::prefix, "io" by default, config.h:287) under which the
+ * LETKF matrix dumps go when cfg.write_mat is set: <prefix>/letkf/mat/ens<r>/
+ * <label>.float_<rows>_<cols>_<batch>.<t>.h5 (letkf.cu:276-306, cu_matrix.hpp:97-117),
+ * r = the reference rank whose batch is rows [r*ny/M, (r+1)*ny/M), labels _dYf _dyo
+ * _Q _V _Xf _dXf _Pa _dWa _Xa _Wa _AI _Z _Lambda _Wma.  lbl_assimilate_files sets
+ * it to its io_prefix. */
+int lbl_set_io_prefix(lbl_ctx* ctx, const char* io_prefix);
+
+/* The HDF5 writer of the matrix dumps, without libhdf5: one file with one contiguous
+ * dataset "data" of dims {d0, d1, d2} (C order over data), float32 or float64
+ * (is_double), like H5Fcreate + H5LTmake_dataset (cu_matrix.hpp:108-117). */
+int lbl_h5_write_dataset(const char* path, uint64_t d0, uint64_t d1, uint64_t d2, const void* data, int is_double);
 
 /* Evaluation measures over the files lbl_output writes (host only; no context, no
  * GPU).  err (optional) receives a message of at most err_cap bytes.

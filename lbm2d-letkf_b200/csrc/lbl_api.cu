@@ -152,7 +152,11 @@ int validate(const lbl_config& c, std::string& err) {
     if (!(c.cfl > 0) || !(c.u_ref > 0) || !(c.h_ref > 0)) { err = "cfl, u_ref, h_ref must be > 0"; return LBL_ERR_ARG; }
     if (c.tau != 0 && !(c.tau > 0.5)) { err = "tau must be > 0.5 (or 0 to use nu)"; return LBL_ERR_ARG; }
     if (c.jacobi_max_sweeps < 1 || c.jacobi_max_sweeps > 1000) { err = "jacobi_max_sweeps out of range"; return LBL_ERR_ARG; }
-    if (c.write_mat != 0) { err = "write_mat is not supported by this build"; return LBL_ERR_UNSUPPORTED; }
+    if (c.write_mat != 0 && c.mode != LBL_MODE_DA_LETKF) { err = "write_mat needs DA_LETKF"; return LBL_ERR_ARG; }
+    if (c.write_mat != 0 && c.ny % c.n_ens != 0) {  // letkf.cu:34-35, 74: whole rows per rank
+        err = "write_mat needs ny divisible by n_ens (the reference's batch per rank is whole rows)";
+        return LBL_ERR_ARG;
+    }
     if (c.lbm_variant < LBL_LBM_AUTO || c.lbm_variant > LBL_LBM_TMA) { err = "unknown lbm_variant"; return LBL_ERR_ARG; }
     if (c.mode == LBL_MODE_DA_LETKF && !analysis_supported(c.n_ens)) {
         err = "DA_LETKF supports 2 <= n_ens <= 32 in this build"; return LBL_ERR_UNSUPPORTED;
@@ -548,7 +552,7 @@ void destroy_impl(lbl_ctx* ctx) {
     for (int b = 0; b < 2; b++) { cudaFree(ctx->f[b]); cudaFree(ctx->mac[b]); }
     cudaFree(ctx->d_modes); cudaFree(ctx->d_amps); cudaFree(ctx->d_pool); cudaFree(ctx->d_force); cudaFree(ctx->d_sched);
     cudaFree(ctx->d_wtab); cudaFree(ctx->d_yo); cudaFree(ctx->d_dY); cudaFree(ctx->d_dyo);
-    cudaFree(ctx->d_stats); cudaFree(ctx->d_red); cudaFree(ctx->d_tmp); cudaFree(ctx->d_err);
+    cudaFree(ctx->d_stats); cudaFree(ctx->d_red); cudaFree(ctx->d_tmp); cudaFree(ctx->d_err); cudaFree(ctx->d_dump);
     for (int b = 0; b < 2; b++) {
         if (ctx->h_yo[b]) cudaFreeHost(ctx->h_yo[b]);
         if (ctx->h_sched[b]) cudaFreeHost(ctx->h_sched[b]);
@@ -626,6 +630,45 @@ int update_impl(lbl_ctx* ctx, int nsteps, bool sync) {
     return LBL_OK;
 }
 
+// need_save_mat (letkf.cu:33, 276-306; letkf_solver.h:243-345): the matrices of every
+// point, written per reference rank r (the rows [r*ny/M, (r+1)*ny/M)) to
+// <prefix>/letkf/mat/ens<r>/<label>.float_<rows>_<cols>_<batch>.<t>.h5 (cu_matrix.hpp:97-117).
+// fin is the forecast the analysis started from.
+int dump_matrices(lbl_ctx* ctx, int t, const float* fin) {
+    const int M = ctx->P.M, ny = ctx->P.ny, rows = ny / M, nobs = ctx->G.nobs;
+    const size_t nb = size_t(rows) * ctx->P.nx;
+    size_t sz[kDumpCount], total = 0;
+    dump_sizes(M, nobs, nb, sz);
+    for (size_t z : sz) total += z;
+    if (!ctx->d_dump) LBL_CK(cudaMalloc(&ctx->d_dump, sizeof(float) * total));
+    ctx->h_dump.resize(total);
+    const uint64_t shape[kDumpCount][2] = {{uint64_t(nobs), uint64_t(M)}, {uint64_t(nobs), 1}, {uint64_t(M), uint64_t(M)},
+                                           {uint64_t(M), uint64_t(M)}, {kQ, uint64_t(M)}, {kQ, uint64_t(M)},
+                                           {uint64_t(M), uint64_t(M)}, {uint64_t(M), uint64_t(M)}, {kQ, uint64_t(M)},
+                                           {uint64_t(M), uint64_t(M)}, {kQ, uint64_t(M)}, {uint64_t(M), uint64_t(M)},
+                                           {uint64_t(M), uint64_t(M)}, {uint64_t(M), uint64_t(M)}};
+    for (int r = 0; r < M; r++) {
+        launch_analysis_dump(ctx, fin, ctx->d_dump, r * rows, (r + 1) * rows, ctx->stream);
+        LBL_CK(cudaGetLastError());
+        LBL_CK(cudaMemcpyAsync(ctx->h_dump.data(), ctx->d_dump, sizeof(float) * total, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+        LBL_CK(cudaStreamSynchronize(ctx->stream));
+        const std::string dir = ctx->io_prefix + "/letkf/mat/ens" + std::to_string(r);
+        if (mkdir_p(dir) != 0) return fail(ctx, LBL_ERR_IO, "could not create " + dir);
+        const float* p = ctx->h_dump.data();
+        for (int i = 0; i < kDumpCount; i++) {
+            const uint64_t dims[3] = {shape[i][0], shape[i][1], uint64_t(nb)};
+            const std::string name = dir + "/" + kDumpLabels[i] + ".float_" + std::to_string(dims[0]) + "_" +
+                                     std::to_string(dims[1]) + "_" + std::to_string(nb) + "." + std::to_string(t) +
+                                     ".h5";
+            std::string e;
+            if (write_h5_dataset(name, dims, p, false, e) != LBL_OK) return fail(ctx, LBL_ERR_IO, e);
+            p += sz[i];
+        }
+    }
+    return LBL_OK;
+}
+
 // DA_NUDGING (nudging.cu:40-143): every member's f relaxes toward feq of the observed
 // (bilinearly interpolated) rho, u, v, in place; the macros are not refreshed.
 int nudging_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const float* vo, bool sync) {
@@ -658,6 +701,11 @@ int assimilate_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
     launch_analysis(ctx, ctx->f[ctx->cur], ctx->f[ctx->cur ^ 1], ctx->mac[ctx->cur ^ 1], ctx->stream);
     LBL_CK(cudaGetLastError());
     LBL_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    if (ctx->cfg.write_mat) {
+        const double d0 = wall_time();
+        LBL_TRY(dump_matrices(ctx, t, ctx->f[ctx->cur]));
+        timer_add(tm, "solve", wall_time() - d0);                   // the dumps sit in solve_evd/solve_xa
+    }
     ctx->cur ^= 1;                                                   // dat.swap(), letkf.cu:357
     if (sync) {
         LBL_CK(cudaEventSynchronize(ctx->ev[3]));
@@ -810,6 +858,7 @@ int lbl_assimilate_files(lbl_ctx* ctx, int t, const char* io_prefix) {
         LBL_TRY(read_dat(dir + "rho_step" + step + ".dat", ro.data(), nxy, ctx->err));
     LBL_TRY(read_dat(dir + "u_step" + step + ".dat", uo.data(), nxy, ctx->err));
     LBL_TRY(read_dat(dir + "v_step" + step + ".dat", vo.data(), nxy, ctx->err));
+    ctx->io_prefix = io_prefix;                                     // config::prefix for the matrix dumps
     return lbl_assimilate(ctx, t, ro.data(), uo.data(), vo.data());
 }
 
@@ -819,6 +868,12 @@ int lbl_cycle_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
     if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_cycle_async before lbl_init");
     if (n_fc < 0 || n_fc > ctx->force_cap) return fail(ctx, LBL_ERR_ARG, "n_fc out of range for one graph");
     const bool due = is_da_mode(ctx->cfg.mode) && !ctx->cfg.da_dummy && t > 0 && da_due(ctx, t);
+    if (due && ctx->cfg.write_mat) {
+        // matrix dumps write files: the analysis runs outside the graph, the forecast in one
+        if (!(ro && uo && vo)) return fail(ctx, LBL_ERR_ARG, "write_mat needs the observations in each call");
+        LBL_TRY(assimilate_impl(ctx, t, ro, uo, vo, true));
+        return lbl_cycle_async(ctx, -1, nullptr, nullptr, nullptr, n_fc);
+    }
     if (due && ro && uo && vo) LBL_TRY(upload_obs(ctx, ro, uo, vo));  // NULL: resident observations
     if (n_fc > 0) LBL_TRY(schedule_force(ctx, n_fc));
     LBL_TRY(launch_graph(ctx, due ? 1 : 0, n_fc));
@@ -1074,6 +1129,19 @@ int lbl_profile_step(lbl_ctx* ctx, int n, double* ms_per_launch) {
     LBL_CK(cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]));
     *ms_per_launch = double(ms) / n;
     return LBL_OK;
+}
+
+int lbl_set_io_prefix(lbl_ctx* ctx, const char* io_prefix) {
+    if (!ctx || !io_prefix) return LBL_ERR_ARG;
+    ctx->io_prefix = io_prefix;
+    return LBL_OK;
+}
+
+int lbl_h5_write_dataset(const char* path, uint64_t d0, uint64_t d1, uint64_t d2, const void* data, int is_double) {
+    if (!path || (!data && d0 * d1 * d2 > 0)) return LBL_ERR_ARG;
+    const uint64_t dims[3] = {d0, d1, d2};
+    std::string e;
+    return write_h5_dataset(path, dims, data, is_double != 0, e);
 }
 
 int lbl_get_cycle_phases(lbl_ctx* ctx, double* analysis_ms, double* forecast_ms) {

@@ -111,6 +111,9 @@ struct lbl_ctx {
     // diagnostics scratch
     double* d_red = nullptr;             // reduction scratch (8 doubles)
     float* d_tmp = nullptr;              // nxy*2 floats (truth fields)
+    float* d_dump = nullptr;             // LETKF matrix dump of one chunk (write_mat only)
+    std::vector<float> h_dump;
+    std::string io_prefix = "io";        // config::prefix (config.h:287) for the matrix dumps
 
     // OBSERVE noise engine state lives host side (io.cu:321 function-static engine)
     void* obs_engine = nullptr;          // std::mt19937*
@@ -148,6 +151,16 @@ void launch_macros(const lbl_ctx* c, const float* f, float* mac, cudaStream_t s)
 void launch_obs_ensemble(const lbl_ctx* c, const float* f, cudaStream_t s);
 void launch_nudging(const lbl_ctx* c, float* f, const float* mac, cudaStream_t s);
 void launch_analysis(const lbl_ctx* c, const float* fin, float* fout, float* mac_out, cudaStream_t s);
+// LETKF matrix dumps (need_save_mat, letkf_solver.h:243-345): the 14 matrices of the
+// rows [j0, j1), each [rows][cols][points] column-major with the point slowest, laid
+// out one after the other in buf in the order of kDumpLabels
+constexpr int kDumpCount = 14;
+constexpr const char* kDumpLabels[kDumpCount] = {"_dYf", "_dyo", "_Q", "_V", "_Xf", "_dXf", "_Pa",
+                                                 "_dWa", "_Xa", "_Wa", "_AI", "_Z", "_Lambda", "_Wma"};
+void dump_sizes(int M, int nobs, size_t nb, size_t* sz);
+void launch_analysis_dump(const lbl_ctx* c, const float* fin, float* buf, int j0, int j1, cudaStream_t s);
+int write_h5_dataset(const std::string& path, const uint64_t dims[3], const void* data, bool is_double,
+                     std::string& err);
 int analysis_supported(int M);
 size_t analysis_smem_bytes(int M, int nobs);
 constexpr size_t kAnalysisSmemLimit = 200 * 1024;

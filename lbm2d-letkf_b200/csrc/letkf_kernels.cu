@@ -45,6 +45,15 @@ struct AnaParams {
     int max_sweeps;
     float c;                // lattice speed for the macros
     int write_v;            // 0 reproduces the reference's stale v after analysis
+    int tile_y0;            // first tile row (0 for the whole grid)
+};
+
+// Matrix dump of one chunk of whole rows [j0, j1) (the batch of one reference rank):
+// every matrix of letkf_solver.h:243-345 per point b = point - point0, column-major
+// with the point slowest, as cu_matrix::save lays them out.
+struct DumpPtrs {
+    float *dYf, *dyo, *Q, *V, *Xf, *dXf, *Pa, *dWa, *Xa, *Wa, *AI, *Z, *Lambda, *Wma;
+    int j0, j1, point0;
 };
 
 // ---------------------------------------------------------------------------
@@ -114,13 +123,15 @@ __device__ __forceinline__ float group_sum(float v) {
 // ---------------------------------------------------------------------------
 constexpr int kCW = 4, kCH = 2;  // chain tile (points in x, points in y)
 
-template <int MP>
+// DUMP = true recomputes the tiles that cover the rows of D and, instead of writing
+// the analysis, writes every intermediate matrix of those rows (need_save_mat).
+template <int MP, bool DUMP>
 __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__ fin, float* __restrict__ fout,
                                                        float* __restrict__ mac, const float* __restrict__ dY,
                                                        const float* __restrict__ dyo,
                                                        const int4* __restrict__ wtab,
                                                        const int* __restrict__ wcnt, int* __restrict__ stats,
-                                                       AnaParams A) {
+                                                       AnaParams A, DumpPtrs D) {
     constexpr int GPW = 32 / MP;
     extern __shared__ float smem[];
     const int lane = threadIdx.x & 31;
@@ -149,7 +160,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
     const int tiles_x = (A.nx + kCW - 1) / kCW;
     const int tile = (blockIdx.x * (blockDim.x >> 5) + warp) * GPW + grp;
     const int x0 = (tile % tiles_x) * kCW;
-    const int y0 = (tile / tiles_x) * kCH;
+    const int y0 = (A.tile_y0 + tile / tiles_x) * kCH;
     const unsigned gmask = (MP == 32) ? 0xffffffffu : (((1u << MP) - 1u) << gbase);
 
     float vv[MP];  // eigenvectors (column k), carried from point to point
@@ -166,6 +177,8 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         const bool active = (i < A.nx) && (j < A.ny);  // uniform within the group
         const int point = active ? i + A.nx * j : 0;
         const bool real_m = active && real_k;
+        const bool dump = DUMP && active && j >= D.j0 && j < D.j1;
+        const size_t b = dump ? size_t(point - D.point0) : 0;
 
         // 1. forecast ensemble at the point: X, xbar, dX (letkf_solver.h:278-280)
         {
@@ -177,6 +190,10 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
                 const float xb = group_sum<MP>(xq[q]) / float(M);
                 sDX[q * MP + k] = real_m ? xq[q] - xb : 0.f;
                 if (k == 0) sXbar[q] = xb;
+                if (DUMP && dump && real_k) {
+                    D.Xf[q + kQ * (k + M * b)] = xq[q];
+                    D.dXf[q + kQ * (k + M * b)] = xq[q] - xb;
+                }
             }
         }
 
@@ -203,6 +220,11 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
             cached_bj = bj;
         }
         __syncwarp();
+        if (DUMP && dump) {
+            if (real_k)
+                for (int sl = 0; sl < nobs; sl++) D.dYf[sl + size_t(nobs) * (k + M * b)] = sW[sl * MP + k];
+            for (int sl = k; sl < nobs; sl += MP) D.dyo[sl + nobs * b] = sDyo[sl];
+        }
 
         // 3. Gram: column k of Q = (M-1)/beta I + dY^T R^-1 dY (letkf_solver.h:252-254),
         //    and c_k = (dY^T R^-1 dyo)_k
@@ -230,6 +252,8 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
 #pragma unroll
         for (int l = 0; l < MP; l++)
             if (l == k && k < M) qv[l] += A.diag;
+        if (DUMP && dump && real_k)
+            for (int l = 0; l < M; l++) D.Q[l + M * (k + M * b)] = qv[l];
 
         // 4. warm start: A = Q V_prev (column k = sum_l Q_:l V_prev[l][k])
         if (idx > 0) {
@@ -337,6 +361,33 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         sY[k] = real_k ? vc / lam : 0.f;
         sS[k] = real_k ? A.sqrt_m1 / sqrtf(lam) : 0.f;
         __syncwarp();
+        if (DUMP) {
+            // V, Lambda; P = V Lambda^-1 V^T, dW = sqrt(M-1) V Lambda^-1/2 V^T, w = V Lambda^-1 V^T c,
+            // W = dW + w 1^T, Z = W - I, Wma = w 1^T (letkf_solver.h:263-345); column k per lane
+            float lamj[MP];
+#pragma unroll
+            for (int jj = 0; jj < MP; jj++) lamj[jj] = __shfl_sync(0xffffffffu, lam, gbase + jj);
+            if (dump && real_k) {
+                const size_t o = size_t(M) * (k + M * b);
+                for (int l = 0; l < M; l++) {
+                    float pa = 0.f, dw = 0.f, w = 0.f;
+                    for (int jj = 0; jj < M; jj++) {
+                        const float vl = sQ[jj * MP + l], vk = sQ[jj * MP + k];
+                        pa = fmaf(vl * vk, 1.f / lamj[jj], pa);
+                        dw = fmaf(vl * vk, 1.f / sqrtf(lamj[jj]), dw);
+                        w = fmaf(vl, sY[jj], w);
+                    }
+                    dw *= A.sqrt_m1;
+                    D.V[o + l] = vv[l];
+                    D.Lambda[o + l] = (l == k) ? lam : 0.f;
+                    D.Pa[o + l] = pa;
+                    D.dWa[o + l] = dw;
+                    D.Wa[o + l] = dw + w;
+                    D.Z[o + l] = dw + w - ((l == k) ? 1.f : 0.f);
+                    D.Wma[o + l] = w;
+                }
+            }
+        }
         {
             float dsum[kQ];
 #pragma unroll
@@ -361,7 +412,16 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         }
 
         // 7. write the analysis member k, refresh its macros (update_xk + lbm2euler)
-        if (real_m) {
+        if (DUMP) {
+            if (dump && real_k)
+#pragma unroll
+                for (int q = 0; q < kQ; q++) {
+                    const float xa = sXbar[q] + acc[q];
+                    const float xf = __ldg(fin + (size_t(k) * kQ + q) * A.nxy + point);
+                    D.Xa[q + kQ * (k + M * b)] = xa;
+                    D.AI[q + kQ * (k + M * b)] = xa - xf;
+                }
+        } else if (real_m) {
             float xa[kQ];
 #pragma unroll
             for (int q = 0; q < kQ; q++) {
@@ -386,6 +446,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         }
         __syncwarp();
     }
+    if (DUMP) return;
     if (bad) atomicOr(stats + 2, 1);
     if (k == 0 && total_sweeps > 0) {
         atomicMax(stats + 0, max_sweeps);
@@ -395,7 +456,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
 }
 
 AnaParams make_params(const lbl_ctx* c) {
-    AnaParams A;
+    AnaParams A{};  // every field zero unless set below
     A.nx = c->P.nx; A.ny = c->P.ny; A.nxy = c->P.nxy; A.M = c->P.M;
     A.p = c->G.p; A.nsx = c->G.nsx; A.nsy = c->G.nsy; A.nsites = c->G.nsx * c->G.nsy;
     A.n_pat_max = c->G.nobs;
@@ -409,6 +470,7 @@ AnaParams make_params(const lbl_ctx* c) {
     A.max_sweeps = c->cfg.jacobi_max_sweeps;
     A.c = c->P.c;
     A.write_v = c->cfg.compat_stale_v ? 0 : 1;
+    A.tile_y0 = 0;
     return A;
 }
 
@@ -427,10 +489,28 @@ void launch_analysis_mp(const lbl_ctx* c, const float* fin, float* fout, float* 
     const size_t sm = analysis_smem_bytes(A.M, A.n_pat_max);
     const int tiles = ((A.nx + kCW - 1) / kCW) * ((A.ny + kCH - 1) / kCH);
     const int grid = (tiles + groups_per_cta - 1) / groups_per_cta;
-    analysis_kernel<MP><<<grid, warps * 32, sm, s>>>(fin, fout, mac, c->d_dY, c->d_dyo,
-                                                      reinterpret_cast<const int4*>(c->d_wtab),
-                                                      c->d_wtab + size_t(4) * c->G.p * c->G.p * c->G.nobs,
-                                                      c->d_stats, A);
+    analysis_kernel<MP, false><<<grid, warps * 32, sm, s>>>(fin, fout, mac, c->d_dY, c->d_dyo,
+                                                             reinterpret_cast<const int4*>(c->d_wtab),
+                                                             c->d_wtab + size_t(4) * c->G.p * c->G.p * c->G.nobs,
+                                                             c->d_stats, A, DumpPtrs{});
+}
+
+// the matrices of the rows [j0, j1): the tiles that cover them, recomputed exactly
+template <int MP>
+void launch_dump_mp(const lbl_ctx* c, const float* fin, const DumpPtrs& D, cudaStream_t s) {
+    AnaParams A = make_params(c);
+    constexpr int GPW = 32 / MP;
+    const int warps = 4;
+    const int groups_per_cta = warps * GPW;
+    const size_t sm = analysis_smem_bytes(A.M, A.n_pat_max);
+    const int ty0 = D.j0 / kCH, ty1 = (D.j1 - 1) / kCH + 1;
+    A.tile_y0 = ty0;
+    const int tiles = ((A.nx + kCW - 1) / kCW) * (ty1 - ty0);
+    const int grid = (tiles + groups_per_cta - 1) / groups_per_cta;
+    analysis_kernel<MP, true><<<grid, warps * 32, sm, s>>>(fin, nullptr, nullptr, c->d_dY, c->d_dyo,
+                                                            reinterpret_cast<const int4*>(c->d_wtab),
+                                                            c->d_wtab + size_t(4) * c->G.p * c->G.p * c->G.nobs,
+                                                            c->d_stats, A, D);
 }
 
 }  // namespace
@@ -448,10 +528,14 @@ size_t analysis_smem_bytes(int M, int nobs) {
 int analysis_prepare() {
     const int lim = 200 * 1024;
     int rc = 0;
-    rc |= int(cudaFuncSetAttribute(analysis_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    rc |= int(cudaFuncSetAttribute(analysis_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    rc |= int(cudaFuncSetAttribute(analysis_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    rc |= int(cudaFuncSetAttribute(analysis_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
     return rc;
 }
 
@@ -461,6 +545,31 @@ void launch_obs_ensemble(const lbl_ctx* c, const float* f, cudaStream_t s) {
     const long long total = (long long)A.nsites * 32;
     const int grid = int((total + threads - 1) / threads);
     obs_ensemble_kernel<<<grid, threads, 0, s>>>(f, c->d_yo, c->d_dY, c->d_dyo, A);
+}
+
+// sizes (floats) of the 14 dumped matrices for nb points, in the order of kDumpLabels
+void dump_sizes(int M, int nobs, size_t nb, size_t* sz) {
+    const size_t e = size_t(M), o = size_t(nobs);
+    const size_t per[kDumpCount] = {o * e, o, e * e, e * e, kQ * e, kQ * e, e * e, e * e, kQ * e, e * e, kQ * e,
+                                    e * e, e * e, e * e};
+    for (int i = 0; i < kDumpCount; i++) sz[i] = per[i] * nb;
+}
+
+void launch_analysis_dump(const lbl_ctx* c, const float* fin, float* buf, int j0, int j1, cudaStream_t s) {
+    const size_t nb = size_t(j1 - j0) * c->P.nx;
+    size_t sz[kDumpCount];
+    dump_sizes(c->P.M, c->G.nobs, nb, sz);
+    float* ptr[kDumpCount];
+    for (int i = 0; i < kDumpCount; i++) { ptr[i] = buf; buf += sz[i]; }
+    DumpPtrs D{ptr[0], ptr[1], ptr[2], ptr[3], ptr[4], ptr[5], ptr[6], ptr[7], ptr[8], ptr[9], ptr[10], ptr[11],
+               ptr[12], ptr[13], j0, j1, j0 * c->P.nx};
+    switch (pad_pow2(c->P.M)) {
+        case 4: launch_dump_mp<4>(c, fin, D, s); break;
+        case 8: launch_dump_mp<8>(c, fin, D, s); break;
+        case 16: launch_dump_mp<16>(c, fin, D, s); break;
+        case 32: launch_dump_mp<32>(c, fin, D, s); break;
+        default: break;
+    }
 }
 
 void launch_analysis(const lbl_ctx* c, const float* fin, float* fout, float* mac, cudaStream_t s) {
@@ -475,7 +584,7 @@ void launch_analysis(const lbl_ctx* c, const float* fin, float* fout, float* mac
 
 namespace {
 AnaParams params_from_args(const AnalysisArgs& a) {
-    AnaParams A;
+    AnaParams A{};  // every field zero unless set below
     A.nx = a.nx; A.ny = a.ny; A.nxy = a.nx * a.ny; A.M = a.M;
     A.p = a.p; A.nsx = a.nx / a.p; A.nsy = a.ny / a.p; A.nsites = A.nsx * A.nsy;
     A.n_pat_max = a.nobs;
@@ -488,6 +597,7 @@ AnaParams params_from_args(const AnalysisArgs& a) {
     A.max_sweeps = a.max_sweeps;
     A.c = a.c;
     A.write_v = a.write_v;
+    A.tile_y0 = 0;
     return A;
 }
 
@@ -500,9 +610,10 @@ void launch_analysis_args_mp(const AnalysisArgs& a, cudaStream_t s) {
     const size_t sm = analysis_smem_bytes(A.M, A.n_pat_max);
     const int tiles = ((A.nx + kCW - 1) / kCW) * ((A.ny + kCH - 1) / kCH);
     const int grid = (tiles + groups_per_cta - 1) / groups_per_cta;
-    analysis_kernel<MP><<<grid, warps * 32, sm, s>>>(a.f_in, a.f_out, a.mac_out, a.dY, a.dyo,
-                                                      reinterpret_cast<const int4*>(a.wtab),
-                                                      a.wtab + size_t(4) * a.p * a.p * a.nobs, a.stats, A);
+    analysis_kernel<MP, false><<<grid, warps * 32, sm, s>>>(a.f_in, a.f_out, a.mac_out, a.dY, a.dyo,
+                                                             reinterpret_cast<const int4*>(a.wtab),
+                                                             a.wtab + size_t(4) * a.p * a.p * a.nobs, a.stats, A,
+                                                             DumpPtrs{});
 }
 }  // namespace
 

@@ -48,6 +48,7 @@ EXPORTS = (
     "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_timer_csv", "lbl_timer_clear",
     "lbl_timer_transit", "lbl_profile_step", "lbl_get_cycle_phases", "lbl_event_record", "lbl_event_elapsed",
     "lbl_letkf_analysis_noalloc", "lbl_bindiff", "lbl_ensemble_stat", "lbl_energy_spectrum",
+    "lbl_set_io_prefix", "lbl_h5_write_dataset",
 )
 
 
@@ -137,6 +138,8 @@ def load_library() -> ctypes.CDLL:
                             ctypes.c_char_p, U]),
         "lbl_ensemble_stat": (I, [ctypes.c_char_p, ctypes.c_char_p, I, I, D, ctypes.c_char_p, U]),
         "lbl_energy_spectrum": (I, [F, F, I, I, D]),
+        "lbl_set_io_prefix": (I, [P, ctypes.c_char_p]),
+        "lbl_h5_write_dataset": (I, [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, P, I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -320,6 +323,10 @@ class Ensemble:
         ms = ctypes.c_double()
         self._check(self.lib.lbl_profile_step(self._h, n, ctypes.byref(ms)), "lbl_profile_step")
         return ms.value
+
+    def set_io_prefix(self, prefix: str):
+        """Directory prefix of the LETKF matrix dumps (cfg.write_mat)."""
+        self._check(self.lib.lbl_set_io_prefix(self._h, prefix.encode()), "lbl_set_io_prefix")
 
     def cycle_phases(self) -> tuple:
         """(analysis_ms, forecast_ms) of the last graph, from events recorded inside it."""

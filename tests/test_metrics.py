@@ -109,3 +109,20 @@ def test_cli_tools_keep_the_reference_formats(tmp_path):
                          capture_output=True, text=True, check=True)
     ek = [float(r.split(",")[1]) for r in out.stdout.strip().split("\n")]
     assert len(ek) == 9 and abs(ek[0] - 0.5) < 1e-12 and sum(ek[1:]) < 1e-12  # uniform u = 1: E(0) = 1/2
+
+
+def test_h5_writer_round_trip(tmp_path):
+    """The matrix-dump HDF5 writer against a reader written from the format specification."""
+    import ctypes
+    from h5_parse import read_datasets
+    lib = lbl.load_library()
+    rng = np.random.default_rng(1)
+    for dtype, is_double in ((np.float32, 0), (np.float64, 1)):
+        a = rng.standard_normal((3, 5, 7)).astype(dtype)
+        path = str(tmp_path / f"_Q.float_3_5_7.{is_double}.h5")
+        rc = lib.lbl_h5_write_dataset(path.encode(), 3, 5, 7, a.ctypes.data_as(ctypes.c_void_p), is_double)
+        assert rc == 0
+        ds = read_datasets(path)
+        assert list(ds) == ["data"]
+        assert ds["data"].dtype == dtype and ds["data"].shape == (3, 5, 7)
+        np.testing.assert_array_equal(ds["data"], a)
