@@ -153,13 +153,16 @@ int validate(const lbl_config& c, std::string& err) {
     if (c.tau != 0 && !(c.tau > 0.5)) { err = "tau must be > 0.5 (or 0 to use nu)"; return LBL_ERR_ARG; }
     if (c.jacobi_max_sweeps < 1 || c.jacobi_max_sweeps > 1000) { err = "jacobi_max_sweeps out of range"; return LBL_ERR_ARG; }
     if (c.write_mat != 0 && c.mode != LBL_MODE_DA_LETKF) { err = "write_mat needs DA_LETKF"; return LBL_ERR_ARG; }
+    if (c.write_mat != 0 && c.n_ens > kMaxMemberLanes) {
+        err = "write_mat supports n_ens <= 32 in this build"; return LBL_ERR_UNSUPPORTED;
+    }
     if (c.write_mat != 0 && c.ny % c.n_ens != 0) {  // letkf.cu:34-35, 74: whole rows per rank
         err = "write_mat needs ny divisible by n_ens (the reference's batch per rank is whole rows)";
         return LBL_ERR_ARG;
     }
     if (c.lbm_variant < LBL_LBM_AUTO || c.lbm_variant > LBL_LBM_TMA) { err = "unknown lbm_variant"; return LBL_ERR_ARG; }
     if (c.mode == LBL_MODE_DA_LETKF && !analysis_supported(c.n_ens)) {
-        err = "DA_LETKF supports 2 <= n_ens <= 32 in this build"; return LBL_ERR_UNSUPPORTED;
+        err = "DA_LETKF supports 2 <= n_ens <= 64 in this build"; return LBL_ERR_UNSUPPORTED;
     }
     if (c.mode == LBL_MODE_DA_LETKF && analysis_smem_bytes(c.n_ens, derive_geo(c).nobs) > kAnalysisSmemLimit) {
         err = "observation window too large for the analysis kernel's shared memory (reduce LETKF_RLOC_LEN)";

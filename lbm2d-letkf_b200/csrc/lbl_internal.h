@@ -18,7 +18,8 @@ namespace lbl {
 constexpr int kQ = 9;
 constexpr int kMaxModes = 128;     // forcing modes (29 at kf=4)
 constexpr int kMaxNobs = 3 * 33 * 33;  // observation window slots (RLOC_LEN <= 8)
-constexpr int kMaxMemberLanes = 32;    // register-resident analysis kernel handles M <= 32
+constexpr int kMaxMemberLanes = 32;    // warp-resident analysis kernel handles M <= 32
+constexpr int kMaxAnalysisMembers = 64; // the 64-thread analysis kernel handles 32 < M <= 64
 
 // Physical constants derived once per context, in the precision the reference
 // evaluates them in (config.h:248-254 are constexpr `real` = float).

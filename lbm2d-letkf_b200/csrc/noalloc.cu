@@ -101,7 +101,8 @@ int analysis_noalloc_impl(const lbl_config* cfg, const float* f_in, float* f_out
     if (c.abi_version != LBL_ABI_VERSION) return noalloc_fail(LBL_ERR_ARG, "abi_version mismatch");
     if (c.nx < 32 || c.nx > 1024 || c.nx % 32 != 0 || c.ny < 8)
         return noalloc_fail(LBL_ERR_ARG, "nx must be a multiple of 32 in [32, 1024] and ny >= 8");
-    if (!lbl::analysis_supported(c.n_ens)) return noalloc_fail(LBL_ERR_UNSUPPORTED, "n_ens must be in [2, 32]");
+    if (c.n_ens < 2 || c.n_ens > lbl::kMaxMemberLanes)
+        return noalloc_fail(LBL_ERR_UNSUPPORTED, "n_ens must be in [2, 32]");
     if (c.da_xyprune < 1 || c.nx % c.da_xyprune || c.ny % c.da_xyprune)
         return noalloc_fail(LBL_ERR_ARG, "DA_XYPRUNE must divide nx and ny");
     if (c.letkf_rloc_len < 0 || c.letkf_rloc_len > 8) return noalloc_fail(LBL_ERR_ARG, "LETKF_RLOC_LEN out of range");

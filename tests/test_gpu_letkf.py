@@ -42,6 +42,9 @@ CASES = [  # nx, M, p, L, beta
     (128, 16, 4, 2, 1.2),
     (256, 16, 4, 1, 1.1),
     (96, 12, 4, 1, 1.1),
+    (64, 64, 4, 1, 1.1),   # 32 < M <= 64: the 64-thread analysis kernel (C2's ensemble size)
+    (64, 48, 4, 1, 1.1),
+    (64, 40, 2, 0, 1.05),
 ]
 
 
