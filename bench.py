@@ -51,14 +51,20 @@ STEPS_PER_CYCLE = 100
 P_OBS = 4
 METRIC = "DA cycles/s"
 UNIT = "cycles/s"
-WORKLOAD = ("DA_LETKF OSSE, M=16 members resident on 1 GPU, 256x256 D2Q9 BGK+Smagorinsky (Cs 0.1, tau 0.51), "
-            "obs (u,v,rho) every 4th point (4096 sites), GC localisation radius 4 cells (75 obs/point), "
-            "inflation 1.1, 100 LBM steps + 1 LETKF analysis per cycle, FP32")
+WORKLOADS = {
+    "C1": (256, 16, "DA_LETKF OSSE, M=16 members resident on 1 GPU, 256x256 D2Q9 BGK+Smagorinsky (Cs 0.1, tau 0.51), "
+                    "obs (u,v,rho) every 4th point (4096 sites), GC localisation radius 4 cells (75 obs/point), "
+                    "inflation 1.1, 100 LBM steps + 1 LETKF analysis per cycle, FP32"),
+    "C2": (512, 64, "DA_LETKF OSSE, M=64 members resident on 1 GPU, 512x512 D2Q9 BGK+Smagorinsky (Cs 0.1, tau 0.51), "
+                    "obs (u,v,rho) every 4th point (16384 sites), GC localisation radius 4 cells (75 obs/point), "
+                    "inflation 1.1, 100 LBM steps + 1 LETKF analysis per cycle, FP32 storage"),
+}
+WORKLOAD = WORKLOADS["C1"][2]
 
 
-def workload_config(lbl, mode="DA_LETKF", n_ens=M):
+def workload_config(lbl, mode="DA_LETKF", n_ens=None):
     return lbl.config_default(
-        mode, NX, n_ens, da_xyprune=P_OBS, letkf_rloc_len=1, letkf_covinf=1.1, obs_error_u=0.1,
+        mode, NX, M if n_ens is None else n_ens, da_xyprune=P_OBS, letkf_rloc_len=1, letkf_covinf=1.1, obs_error_u=0.1,
         obs_error_rho=0.01, daprune=5, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP, ic_amp=1.0,
         ens_init=lbl.ENS_PERTURBED, ens_perturb=0.1)
 
@@ -73,7 +79,7 @@ def measured_peak():
 
 def ncu_traffic():
     """DRAM bytes per stream-collide launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "lbm_step_kernel_256x256_M16.md")
+    path = os.path.join(ROOT, "profiles", f"lbm_step_kernel_{NX}x{NX}_M{M}.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -406,11 +412,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="run warmup + steps cycles of the workload and exit (for ncu captures)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="C1",
+                    help="C1 (the headline, 256^2 x 16) or C2 (512^2 x 64)")
     ap.add_argument("--lbm", default=None, metavar="NXxM[,NXxM...]",
                     help="time the stream-collide alone at these grids and exit")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    global NX, M, WORKLOAD
+    NX, M, WORKLOAD = WORKLOADS[args.workload]
     if args.lbm:
         lbm_sweep(args)
         return

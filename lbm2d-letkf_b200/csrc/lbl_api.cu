@@ -505,7 +505,8 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
         ctx->n_rand_buf = n * 4096;                                        // data.cu:297
         LBL_CK(cudaMalloc(&ctx->d_pool, sizeof(float) * ctx->pool_slots * size_t(ctx->n_rand_buf)));
     }
-    ctx->force_cap = int(std::max<long long>(8, std::min<long long>(1023, (64ll << 20) / (8ll * nxy))));
+    // steps of forcing one graph can hold: 256 MB of fields (512 steps at 256^2, 128 at 512^2)
+    ctx->force_cap = int(std::max<long long>(8, std::min<long long>(1023, (256ll << 20) / (8ll * nxy))));
     LBL_CK(cudaMalloc(&ctx->d_force, sizeof(float) * 2 * nxy * ctx->force_cap));
     LBL_CK(cudaMemset(ctx->d_force, 0, sizeof(float) * 2 * nxy * ctx->force_cap));
     LBL_CK(cudaMalloc(&ctx->d_sched, sizeof(int) * ctx->force_cap));
@@ -869,7 +870,13 @@ int lbl_cycle_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
     if (!ctx) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
     if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_cycle_async before lbl_init");
-    if (n_fc < 0 || n_fc > ctx->force_cap) return fail(ctx, LBL_ERR_ARG, "n_fc out of range for one graph");
+    if (n_fc < 0) return fail(ctx, LBL_ERR_ARG, "n_fc < 0");
+    if (n_fc > ctx->force_cap) {
+        // more steps than one graph's forcing buffer: the cycle graph takes the first
+        // force_cap steps, forecast graphs the rest
+        LBL_TRY(lbl_cycle_async(ctx, t, ro, uo, vo, ctx->force_cap));
+        return update_impl(ctx, n_fc - ctx->force_cap, false);
+    }
     const bool due = is_da_mode(ctx->cfg.mode) && !ctx->cfg.da_dummy && t > 0 && da_due(ctx, t);
     if (due && ctx->cfg.write_mat) {
         // matrix dumps write files: the analysis runs outside the graph, the forecast in one

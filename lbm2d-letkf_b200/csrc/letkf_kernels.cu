@@ -457,30 +457,40 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
 
 // ---------------------------------------------------------------------------
 // The local analysis for 32 < M <= 64 (the C2 ensembles; the reference runs them
-// through EigenG-Batched).  One CTA of 64 threads walks one CW x CH tile of points,
-// thread k = member k.  The algorithm is the one above; what a warp did with
-// shuffles goes through shared memory here: each Jacobi round every thread
-// publishes its column of A (when it changed) in a 64 x 64 exchange matrix and
-// reads its partner's, with a barrier on each side.
+// through EigenG-Batched).  One CTA of 128 threads walks one CW x CH tile of points;
+// thread t owns rows [32h, 32h + 32) (h = t & 1) of member column k = t >> 1, and
+// the two halves of a column combine their partial dot products with one shuffle.
+// The algorithm is the one above; the Jacobi's partner columns go through a 64 x 64
+// shared exchange matrix: each round a thread publishes its half column (when it
+// changed) and reads its partner's half once, with a barrier on each side.
 // ---------------------------------------------------------------------------
-constexpr int kWide = 64;
+constexpr int kWide = 64;             // member columns
+constexpr int kHalf = 32;             // rows per thread
+constexpr int kWideThreads = 2 * kWide;
 
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+// float offset of 16-byte chunk c4 (rows 4 c4 .. 4 c4 + 3) of half column hb in the exchange
+// matrix: chunks are XOR-swizzled by hb so that the eight threads of a quarter warp,
+// which touch eight different half columns at the same chunk, hit eight bank groups
+__device__ __forceinline__ int sa_chunk(int hb, int c4) { return hb * kHalf + 4 * (c4 ^ (hb & 7)); }
+// sum of the two halves of a column (adjacent lanes)
+__device__ __forceinline__ float pair_sum(float v) { return v + __shfl_xor_sync(0xffffffffu, v, 1); }
 
-__global__ void __launch_bounds__(kWide) analysis_wide_kernel(const float* __restrict__ fin,
-                                                              float* __restrict__ fout, float* __restrict__ mac,
-                                                              const float* __restrict__ dY,
-                                                              const float* __restrict__ dyo,
-                                                              const int4* __restrict__ wtab,
-                                                              const int* __restrict__ wcnt, int* __restrict__ stats,
-                                                              AnaParams A) {
+__global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const float* __restrict__ fin,
+                                                                     float* __restrict__ fout, float* __restrict__ mac,
+                                                                     const float* __restrict__ dY,
+                                                                     const float* __restrict__ dyo,
+                                                                     const int4* __restrict__ wtab,
+                                                                     const int* __restrict__ wcnt,
+                                                                     int* __restrict__ stats, AnaParams A) {
     extern __shared__ float smem[];
-    const int k = threadIdx.x;
-    const int warp = k >> 5, lane = k & 31;
+    const int t = threadIdx.x;
+    const int k = t >> 1, h = t & 1, r0 = kHalf * h;
+    const int warp = t >> 5, lane = t & 31;
     const int M = A.M;
     const bool real_k = k < M;
     const int nobs = A.n_pat_max;
@@ -488,53 +498,51 @@ __global__ void __launch_bounds__(kWide) analysis_wide_kernel(const float* __res
     const int nobs_pad = (nobs + 3) & ~3;
     float* sW = smem;                    // [nobs][64] window dY (unweighted)
     float* sDyo = sW + nobs * kWide;     // [nobs]     window innovations (padded to 4)
-    float* sA = sDyo + nobs_pad;         // [64][64]   Q columns, the Jacobi exchange, then V
+    float* sA = sDyo + nobs_pad;         // [128][32]  half columns: Q, the Jacobi exchange, then V (swizzled)
     float* sDX = sA + kWide * kWide;     // [9][64]    dX, then D = dX V in place
     float* sS = sDX + kQ * kWide;        // [64]       sqrt(M-1)/sqrt(lambda)
     float* sY = sS + kWide;              // [64]       Lambda^-1 V^T c
-    float* sC = sY + kWide;              // [64]       c = dY^T R^-1 dyo
-    float* sN = sC + kWide;              // [64]       squared column norms of A
+    float* sN = sY + kWide;              // [64]       squared column norms of A (Jacobi rounds), and
+    float* sC = sN;                      //            c = dY^T R^-1 dyo (transform), and
+    float* sRed = sN;                    //            per-warp partial sums [4][12] (between those)
     float* sXbar = sN + kWide;           // [12]       ensemble mean
-    float* sRed = sXbar + 12;            // [2][12]    per-warp partial sums
-    float* sV = sRed + 24;               // [64][64]   eigenvectors, column k at sV[l*64 + k] (thread-private)
+    float* sV = sXbar + 12;              // [64][64]   eigenvectors, V[l][k] at sV[l*64 + k]
 
     const int tiles_x = (A.nx + kCW - 1) / kCW;
     const int tile = blockIdx.x;
     const int x0 = (tile % tiles_x) * kCW;
     const int y0 = (A.tile_y0 + tile / tiles_x) * kCH;
 
-    // eigenvectors, carried from point to point (column k belongs to thread k)
-    for (int l = 0; l < kWide; l++) sV[l * kWide + k] = (l == k) ? 1.f : 0.f;
+    for (int l = 0; l < kHalf; l++) sV[(r0 + l) * kWide + k] = (r0 + l == k) ? 1.f : 0.f;
     int cached_bi = -1, cached_bj = -1;
     int max_sweeps = 0, noconv = 0, total_sweeps = 0;
     bool bad = false;
 
     for (int idx = 0; idx < kCW * kCH; idx++) {
-        const int r = idx / kCW;
-        const int cc = (r & 1) ? (kCW - 1 - idx % kCW) : (idx % kCW);
-        const int i = x0 + cc, j = y0 + r;
+        const int rr_ = idx / kCW;
+        const int cc = (rr_ & 1) ? (kCW - 1 - idx % kCW) : (idx % kCW);
+        const int i = x0 + cc, j = y0 + rr_;
         const bool active = (i < A.nx) && (j < A.ny);  // uniform within the CTA
         if (!active) continue;
         const int point = i + A.nx * j;
 
-        // 1. X, xbar, dX (letkf_solver.h:278-280)
+        // 1. X, xbar, dX (letkf_solver.h:278-280); the h = 0 thread of a column loads it
         {
-            float xq[kQ], part[kQ];
+            float xq[kQ];
 #pragma unroll
             for (int q = 0; q < kQ; q++) {
-                xq[q] = real_k ? __ldg(fin + (size_t(k) * kQ + q) * A.nxy + point) : 0.f;
-                part[q] = warp_sum(xq[q]);
+                xq[q] = (real_k && h == 0) ? __ldg(fin + (size_t(k) * kQ + q) * A.nxy + point) : 0.f;
+                const float part = warp_sum(xq[q]);
+                if (lane == 0) sRed[warp * 12 + q] = part;
             }
-            if (lane == 0)
-#pragma unroll
-                for (int q = 0; q < kQ; q++) sRed[warp * 12 + q] = part[q];
             __syncthreads();
+            if (h == 0)
 #pragma unroll
-            for (int q = 0; q < kQ; q++) {
-                const float xb = (sRed[q] + sRed[12 + q]) / float(M);
-                sDX[q * kWide + k] = real_k ? xq[q] - xb : 0.f;
-                if (k == 0) sXbar[q] = xb;
-            }
+                for (int q = 0; q < kQ; q++) {
+                    const float xb = (sRed[q] + sRed[12 + q] + sRed[24 + q] + sRed[36 + q]) / float(M);
+                    sDX[q * kWide + k] = real_k ? xq[q] - xb : 0.f;
+                    if (k == 0) sXbar[q] = xb;
+                }
         }
 
         // 2. observation window of the point's p x p block, once per block
@@ -547,8 +555,7 @@ __global__ void __launch_bounds__(kWide) analysis_wide_kernel(const float* __res
                     int si = (bi + a - A.nl_off) % A.nsx;
                     si += si < 0 ? A.nsx : 0;
                     const int site = si + A.nsx * sj;
-#pragma unroll
-                    for (int var = 0; var < 3; var++) {
+                    for (int var = h; var < 3; var += 2) {
                         const int sl = a + A.nox * b + var * nox2;
                         sW[sl * kWide + k] = real_k ? __ldg(dY + (size_t(var) * A.nsites + site) * M + k) : 0.f;
                         if (k == 0) sDyo[sl] = __ldg(dyo + size_t(var) * A.nsites + site);
@@ -560,13 +567,13 @@ __global__ void __launch_bounds__(kWide) analysis_wide_kernel(const float* __res
         }
         __syncthreads();
 
-        // 3. Gram column k and c_k (letkf_solver.h:252-254)
+        // 3. Gram: rows [r0, r0 + 32) of column k, and c_k (letkf_solver.h:252-254)
         const int pat = (i % A.p) + A.p * (j % A.p);
         const int cnt = wcnt[pat];
         const int4* ent = wtab + size_t(pat) * nobs;
-        float qv[kWide];
+        float qv[kHalf];
 #pragma unroll
-        for (int l = 0; l < kWide; l++) qv[l] = 0.f;
+        for (int l = 0; l < kHalf; l++) qv[l] = 0.f;
         float ck = 0.f;
         for (int o = 0; o < cnt; o++) {
             const int4 e = ent[o];
@@ -574,8 +581,8 @@ __global__ void __launch_bounds__(kWide) analysis_wide_kernel(const float* __res
             const float ek = __int_as_float(e.w) * row[k];
             ck = fmaf(ek, sDyo[e.x], ck);
 #pragma unroll
-            for (int l = 0; l < kWide; l += 4) {
-                const float4 r4 = *reinterpret_cast<const float4*>(row + l);
+            for (int l = 0; l < kHalf; l += 4) {
+                const float4 r4 = *reinterpret_cast<const float4*>(row + r0 + l);
                 qv[l + 0] = fmaf(ek, r4.x, qv[l + 0]);
                 qv[l + 1] = fmaf(ek, r4.y, qv[l + 1]);
                 qv[l + 2] = fmaf(ek, r4.z, qv[l + 2]);
@@ -583,65 +590,64 @@ __global__ void __launch_bounds__(kWide) analysis_wide_kernel(const float* __res
             }
         }
 #pragma unroll
-        for (int l = 0; l < kWide; l++)
-            if (l == k && k < M) qv[l] += A.diag;
+        for (int l = 0; l < kHalf; l++)
+            if (r0 + l == k && k < M) qv[l] += A.diag;
 
-        // 4. warm start A = Q V_prev: Q's columns go through sA, qv accumulates A's column k
+        // 4. warm start A = Q V_prev: Q's columns go through sA
         if (idx > 0) {
 #pragma unroll
-            for (int l = 0; l < kWide; l += 4)
-                *reinterpret_cast<float4*>(sA + k * kWide + l) = make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
+            for (int l = 0; l < kHalf; l += 4)
+                *reinterpret_cast<float4*>(sA + sa_chunk(2 * k + h, l >> 2)) = make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
             __syncthreads();
 #pragma unroll
-            for (int t = 0; t < kWide; t++) qv[t] = 0.f;
-            for (int l = 0; l < kWide; l++) {
-                const float vl = sV[l * kWide + k];
+            for (int l = 0; l < kHalf; l++) qv[l] = 0.f;
+            for (int c = 0; c < kWide; c++) {
+                const float vc = sV[c * kWide + k];
 #pragma unroll
-                for (int t = 0; t < kWide; t += 4) {
-                    const float4 q4 = *reinterpret_cast<const float4*>(sA + l * kWide + t);
-                    qv[t + 0] = fmaf(q4.x, vl, qv[t + 0]);
-                    qv[t + 1] = fmaf(q4.y, vl, qv[t + 1]);
-                    qv[t + 2] = fmaf(q4.z, vl, qv[t + 2]);
-                    qv[t + 3] = fmaf(q4.w, vl, qv[t + 3]);
+                for (int l = 0; l < kHalf; l += 4) {
+                    const float4 q4 = *reinterpret_cast<const float4*>(sA + sa_chunk(2 * c + h, l >> 2));
+                    qv[l + 0] = fmaf(q4.x, vc, qv[l + 0]);
+                    qv[l + 1] = fmaf(q4.y, vc, qv[l + 1]);
+                    qv[l + 2] = fmaf(q4.z, vc, qv[l + 2]);
+                    qv[l + 3] = fmaf(q4.w, vc, qv[l + 3]);
                 }
             }
             __syncthreads();  // sA is the Jacobi exchange next
         }
 
-        // 5. one-sided Jacobi on the columns of A (see analysis_kernel): round rr pairs
-        //    k with k ^ rr through sA; V is recovered as A / |a| at the end
+        // 5. one-sided Jacobi on the columns of A (see analysis_kernel)
         int sweeps = 0;
         bool converged = false;
         for (int sw = 0; sw < A.max_sweeps; sw++) {
             float a0 = 0.f, a1 = 0.f;
 #pragma unroll
-            for (int l = 0; l < kWide; l += 2) { a0 = fmaf(qv[l], qv[l], a0); a1 = fmaf(qv[l + 1], qv[l + 1], a1); }
-            float a = a0 + a1;
+            for (int l = 0; l < kHalf; l += 2) { a0 = fmaf(qv[l], qv[l], a0); a1 = fmaf(qv[l + 1], qv[l + 1], a1); }
+            float a = pair_sum(a0 + a1);
             bool rot = false, dirty = true;
             float worst = 0.f;
             for (int rr = 1; rr < kWide; rr++) {
                 const int pk = k ^ rr;
                 if (dirty) {
 #pragma unroll
-                    for (int l = 0; l < kWide; l += 4)
-                        *reinterpret_cast<float4*>(sA + k * kWide + l) =
+                    for (int l = 0; l < kHalf; l += 4)
+                        *reinterpret_cast<float4*>(sA + sa_chunk(2 * k + h, l >> 2)) =
                             make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
                     dirty = false;
                 }
-                sN[k] = a;
+                if (h == 0) sN[k] = a;
                 __syncthreads();
-                const float* pc = sA + pk * kWide;
+                float pq[kHalf];
+#pragma unroll
+                for (int l = 0; l < kHalf; l += 4) {
+                    const float4 p4 = *reinterpret_cast<const float4*>(sA + sa_chunk(2 * pk + h, l >> 2));
+                    pq[l] = p4.x; pq[l + 1] = p4.y; pq[l + 2] = p4.z; pq[l + 3] = p4.w;
+                }
+                const float b = sN[pk];
+                __syncthreads();  // the partner's half is in registers: sA may change
                 float g0 = 0.f, g1 = 0.f;
 #pragma unroll
-                for (int l = 0; l < kWide; l += 4) {
-                    const float4 p4 = *reinterpret_cast<const float4*>(pc + l);
-                    g0 = fmaf(qv[l], p4.x, g0);
-                    g1 = fmaf(qv[l + 1], p4.y, g1);
-                    g0 = fmaf(qv[l + 2], p4.z, g0);
-                    g1 = fmaf(qv[l + 3], p4.w, g1);
-                }
-                const float g = g0 + g1;
-                const float b = sN[pk];
+                for (int l = 0; l < kHalf; l += 2) { g0 = fmaf(qv[l], pq[l], g0); g1 = fmaf(qv[l + 1], pq[l + 1], g1); }
+                const float g = pair_sum(g0 + g1);
                 const bool low = k < pk;
                 const float alo = low ? a : b, ahi = low ? b : a;
                 const float nrm = sqrtf(alo * ahi);
@@ -649,22 +655,15 @@ __global__ void __launch_bounds__(kWide) analysis_wide_kernel(const float* __res
                 if (doit) {
                     worst = fmaxf(worst, __fdividef(fabsf(g), nrm));
                     const float zeta = __fdividef(ahi - alo, 2.f * g);
-                    const float t = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.f)));
-                    const float cs = rsqrtf(fmaf(t, t, 1.f));
-                    const float sn = low ? -(cs * t) : cs * t;
+                    const float tt = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.f)));
+                    const float cs = rsqrtf(fmaf(tt, tt, 1.f));
+                    const float sn = low ? -(cs * tt) : cs * tt;
 #pragma unroll
-                    for (int l = 0; l < kWide; l += 4) {
-                        const float4 p4 = *reinterpret_cast<const float4*>(pc + l);
-                        qv[l + 0] = fmaf(sn, p4.x, cs * qv[l + 0]);
-                        qv[l + 1] = fmaf(sn, p4.y, cs * qv[l + 1]);
-                        qv[l + 2] = fmaf(sn, p4.z, cs * qv[l + 2]);
-                        qv[l + 3] = fmaf(sn, p4.w, cs * qv[l + 3]);
-                    }
-                    a = low ? a - t * g : a + t * g;
+                    for (int l = 0; l < kHalf; l++) qv[l] = fmaf(sn, pq[l], cs * qv[l]);
+                    a = low ? a - tt * g : a + tt * g;
                     dirty = true;
                 }
                 rot |= doit;
-                __syncthreads();  // the partner has read this column before it changes
             }
             // CTA-wide max of the sweep's relative off-diagonal, and whether any pair rotated
             float wmax = worst;
@@ -672,7 +671,7 @@ __global__ void __launch_bounds__(kWide) analysis_wide_kernel(const float* __res
             for (int o = 16; o > 0; o >>= 1) wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
             if (lane == 0) sRed[warp * 12] = wmax;
             const int any_rot = __syncthreads_or(rot ? 1 : 0);
-            wmax = fmaxf(sRed[0], sRed[12]);
+            wmax = fmaxf(fmaxf(sRed[0], sRed[12]), fmaxf(sRed[24], sRed[36]));
             sweeps = sw + 1;
             const bool done = !any_rot || wmax < A.stop;
             __syncthreads();
@@ -684,56 +683,61 @@ __global__ void __launch_bounds__(kWide) analysis_wide_kernel(const float* __res
         {
             float n0 = 0.f, n1 = 0.f;
 #pragma unroll
-            for (int l = 0; l < kWide; l += 2) { n0 = fmaf(qv[l], qv[l], n0); n1 = fmaf(qv[l + 1], qv[l + 1], n1); }
-            const float n2 = n0 + n1;
+            for (int l = 0; l < kHalf; l += 2) { n0 = fmaf(qv[l], qv[l], n0); n1 = fmaf(qv[l + 1], qv[l + 1], n1); }
+            const float n2 = pair_sum(n0 + n1);
             if (n2 > 0.f) {
                 lam = sqrtf(n2);
                 const float inv = 1.f / lam;
 #pragma unroll
-                for (int l = 0; l < kWide; l++) qv[l] *= inv;
+                for (int l = 0; l < kHalf; l++) qv[l] *= inv;
             } else {
 #pragma unroll
-                for (int l = 0; l < kWide; l++) qv[l] = (l == k) ? 1.f : 0.f;
+                for (int l = 0; l < kHalf; l++) qv[l] = (r0 + l == k) ? 1.f : 0.f;
             }
         }
-        // qv now holds v_k; V goes to sV (column k) and, transposed for the transform, to sA
+        // qv holds rows [r0, r0 + 32) of v_k: into sV (row-major) and sA (column-major)
 #pragma unroll
-        for (int l = 0; l < kWide; l++) sV[l * kWide + k] = qv[l];
+        for (int l = 0; l < kHalf; l++) sV[(r0 + l) * kWide + k] = qv[l];
 #pragma unroll
-        for (int l = 0; l < kWide; l += 4)
-            *reinterpret_cast<float4*>(sA + k * kWide + l) = make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
-        sC[k] = ck;
+        for (int l = 0; l < kHalf; l += 4)
+            *reinterpret_cast<float4*>(sA + sa_chunk(2 * k + h, l >> 2)) = make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
+        if (h == 0) sC[k] = ck;
         __syncthreads();
         float vc = 0.f;  // (V^T c)_k
 #pragma unroll
-        for (int l = 0; l < kWide; l++) vc = fmaf(qv[l], sC[l], vc);
-        sY[k] = real_k ? vc / lam : 0.f;
-        sS[k] = real_k ? A.sqrt_m1 / sqrtf(lam) : 0.f;
-        {
-            float dsum[kQ];
+        for (int l = 0; l < kHalf; l++) vc = fmaf(qv[l], sC[r0 + l], vc);
+        vc = pair_sum(vc);
+        float dsum[kQ];
 #pragma unroll
-            for (int q = 0; q < kQ; q++) {
-                dsum[q] = 0.f;
+        for (int q = 0; q < kQ; q++) {
+            float d = 0.f;
 #pragma unroll
-                for (int l = 0; l < kWide; l++) dsum[q] = fmaf(sDX[q * kWide + l], qv[l], dsum[q]);
-            }
-            __syncthreads();  // every thread has read dX before D overwrites it
+            for (int l = 0; l < kHalf; l++) d = fmaf(sDX[q * kWide + r0 + l], qv[l], d);
+            dsum[q] = pair_sum(d);
+        }
+        __syncthreads();  // every thread has read dX before D overwrites it
+        if (h == 0) {
+            sY[k] = real_k ? vc / lam : 0.f;
+            sS[k] = real_k ? A.sqrt_m1 / sqrtf(lam) : 0.f;
 #pragma unroll
             for (int q = 0; q < kQ; q++) sDX[q * kWide + k] = dsum[q];
         }
         __syncthreads();
+        // Xa_k = xbar + sum_jj D[:, jj] z_jj, z_jj = sS[jj] V[k][jj] + sY[jj]; halves split jj
         float acc[kQ];
 #pragma unroll
         for (int q = 0; q < kQ; q++) acc[q] = 0.f;
 #pragma unroll 4
-        for (int jj = 0; jj < kWide; jj++) {
-            const float z = fmaf(sS[jj], sA[jj * kWide + k], sY[jj]);
+        for (int jj = r0; jj < r0 + kHalf; jj++) {
+            const float z = fmaf(sS[jj], sA[sa_chunk(2 * jj + (k >> 5), (k & 31) >> 2) + (k & 3)], sY[jj]);
 #pragma unroll
             for (int q = 0; q < kQ; q++) acc[q] = fmaf(sDX[q * kWide + jj], z, acc[q]);
         }
+#pragma unroll
+        for (int q = 0; q < kQ; q++) acc[q] = pair_sum(acc[q]);
 
         // 7. the analysis member k and its macros (update_xk + lbm2euler)
-        if (real_k) {
+        if (real_k && h == 0) {
             float xa[kQ];
 #pragma unroll
             for (int q = 0; q < kQ; q++) {
@@ -757,7 +761,7 @@ __global__ void __launch_bounds__(kWide) analysis_wide_kernel(const float* __res
         __syncthreads();  // the next point rewrites sDX, sA, sXbar
     }
     if (bad) atomicOr(stats + 2, 1);
-    if (k == 0 && total_sweeps > 0) {
+    if (t == 0 && total_sweeps > 0) {
         atomicMax(stats + 0, max_sweeps);
         if (noconv) atomicAdd(stats + 1, noconv);
         atomicAdd(stats + 3, total_sweeps);
@@ -829,8 +833,8 @@ int analysis_supported(int M) { return M >= 2 && M <= kMaxAnalysisMembers; }
 // dynamic shared memory of one analysis CTA (4 warps) for M members and a window of nobs slots
 size_t analysis_smem_bytes(int M, int nobs) {
     if (M > 32)  // analysis_wide_kernel: one 64-thread CTA
-        return sizeof(float) * (size_t(nobs) * kWide + ((nobs + 3) & ~3) + 2 * kWide * kWide + kQ * kWide + 4 * kWide +
-                                12 + 24);
+        return sizeof(float) * (size_t(nobs) * kWide + ((nobs + 3) & ~3) + 2 * kWide * kWide + kQ * kWide + 3 * kWide +
+                                12);
     const int mp = pad_pow2(M);
     const int per_grp = nobs * mp + ((nobs + 3) & ~3) + mp * mp + kQ * mp + 2 * mp + 12;
     return sizeof(float) * size_t(per_grp) * 4 * (32 / mp);
@@ -888,7 +892,7 @@ void launch_analysis_dump(const lbl_ctx* c, const float* fin, float* buf, int j0
 void launch_analysis_wide(const lbl_ctx* c, const float* fin, float* fout, float* mac, cudaStream_t s) {
     const AnaParams A = make_params(c);
     const int tiles = ((A.nx + kCW - 1) / kCW) * ((A.ny + kCH - 1) / kCH);
-    analysis_wide_kernel<<<tiles, kWide, analysis_smem_bytes(A.M, A.n_pat_max), s>>>(
+    analysis_wide_kernel<<<tiles, kWideThreads, analysis_smem_bytes(A.M, A.n_pat_max), s>>>(
         fin, fout, mac, c->d_dY, c->d_dyo, reinterpret_cast<const int4*>(c->d_wtab),
         c->d_wtab + size_t(4) * c->G.p * c->G.p * c->G.nobs, c->d_stats, A);
 }

@@ -195,3 +195,27 @@ def test_cycle_phase_events():
     fresh = lbl.Ensemble(cfg)
     with pytest.raises(lbl.LblError):
         fresh.cycle_phases()  # nothing launched yet
+
+
+def test_cycle_longer_than_one_forcing_buffer():
+    """At 1024^2 one graph holds 32 steps of forcing: a 45-step cycle is split over graphs
+    and still equals the analysis followed by 45 separate steps."""
+    kw = dict(da_xyprune=8, letkf_rloc_len=0, letkf_covinf=1.1, obs_error_u=0.002, obs_error_rho=1e-4, daprune=1)
+    cfg = lbl.config_default("DA_LETKF", 1024, 2, **kw)
+    a, b = lbl.Ensemble(cfg), lbl.Ensemble(cfg)
+    rng = np.random.default_rng(3)
+    obs = []
+    for s_ in (1e-4, 2e-3, 2e-3):
+        o_ = np.full((1024, 1024), np.nan, np.float32)
+        o_[::8, ::8] = (1.0 if s_ == 1e-4 else 0.0) + s_ * rng.standard_normal((128, 128))
+        obs.append(o_)
+    for x in (a, b):
+        x.init(0)
+        x.update(0, 3)
+    t = cfg.iiter
+    a.cycle_async(t, *obs, 45)
+    a.sync()
+    b.assimilate(t, *obs)
+    b.update(t, 45)
+    for m in range(2):
+        np.testing.assert_array_equal(a.get_f(m), b.get_f(m))
