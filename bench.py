@@ -62,11 +62,14 @@ WORKLOADS = {
 WORKLOAD = WORKLOADS["C1"][2]
 
 
+STORAGE = 0  # lbl_config.storage of the ensemble (the nature run stays FP32)
+
+
 def workload_config(lbl, mode="DA_LETKF", n_ens=None):
     return lbl.config_default(
         mode, NX, M if n_ens is None else n_ens, da_xyprune=P_OBS, letkf_rloc_len=1, letkf_covinf=1.1, obs_error_u=0.1,
         obs_error_rho=0.01, daprune=5, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP, ic_amp=1.0,
-        ens_init=lbl.ENS_PERTURBED, ens_perturb=0.1)
+        ens_init=lbl.ENS_PERTURBED, ens_perturb=0.1, storage=STORAGE if mode != "NATURE" else 0)
 
 
 def measured_peak():
@@ -79,6 +82,8 @@ def measured_peak():
 
 def ncu_traffic():
     """DRAM bytes per stream-collide launch from the committed ncu summary, if any."""
+    if STORAGE:
+        return None
     path = os.path.join(ROOT, "profiles", f"lbm_step_kernel_{NX}x{NX}_M{M}.md")
     try:
         for line in open(path):
@@ -292,7 +297,7 @@ def run_engine(args, dist, rank, world, device):
     # ---- roofline of the stream-collide kernel, live in the timed cycles ----------------
     # the forecast phase of each cycle graph is T back-to-back stream-collide launches
     ms_step = ms_fc / (K * T)
-    bytes_per_launch = 72.0 * M * NX * NX
+    bytes_per_launch = (36.0 if STORAGE else 72.0) * M * NX * NX
     achieved = bytes_per_launch / (ms_step * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
     traffic = ncu_traffic()
@@ -302,7 +307,8 @@ def run_engine(args, dist, rank, world, device):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded nature run + Gaussian observation noise)",
+        "dtype": "f16 storage, f32 compute" if STORAGE else "f32",
+        "data": "synthetic (seeded nature run + Gaussian observation noise)",
         "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                    "l2": "flushed (256 MB write) between timed cycles, outside the timed intervals",
                    "observations": "value leg reuses the resident observations; e2e uploads them every cycle"},
@@ -387,16 +393,17 @@ def lbm_sweep(args):
     import lbl
     for spec in args.lbm.split(","):
         nx, m = (int(v) for v in spec.lower().split("x"))
-        e = lbl.Ensemble(lbl.config_default("NATURE", nx, m))
+        e = lbl.Ensemble(lbl.config_default("NATURE", nx, m, storage=STORAGE))
         e.init(0)
         e.update(0, 2)
         e.profile_step(max(3, args.warmup))
         ms = e.profile_step(max(1, args.steps))
-        bytes_launch = 72.0 * m * nx * nx
+        bytes_launch = (36.0 if STORAGE else 72.0) * m * nx * nx
         peak, peak_kind = measured_peak()
         gbs = bytes_launch / (ms * 1e-3) / 1e9
         print(json.dumps({"lbm_stream_collide": {
-            "nx": nx, "ny": nx, "members": m, "launches": args.steps, "ms_per_launch": ms,
+            "nx": nx, "ny": nx, "members": m, "storage": "f16 deviations" if STORAGE else "f32",
+            "launches": args.steps, "ms_per_launch": ms,
             "glups": m * nx * nx / (ms * 1e-3) / 1e9, "algorithmic_bytes_per_launch": bytes_launch,
             "population_buffer_mb": bytes_launch / 2 / 1e6, "achieved_gbs": gbs, "peak_gbs": peak,
             "frac": gbs / peak, "peak_kind": peak_kind}}), flush=True)
@@ -414,13 +421,18 @@ def main():
                     help="run warmup + steps cycles of the workload and exit (for ncu captures)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="C1",
                     help="C1 (the headline, 256^2 x 16) or C2 (512^2 x 64)")
+    ap.add_argument("--storage", choices=["f32", "f16"], default="f32",
+                    help="population storage: f32, or the precision form's f16 deviations f - w_q")
     ap.add_argument("--lbm", default=None, metavar="NXxM[,NXxM...]",
                     help="time the stream-collide alone at these grids and exit")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global NX, M, WORKLOAD
+    global NX, M, WORKLOAD, STORAGE
     NX, M, WORKLOAD = WORKLOADS[args.workload]
+    STORAGE = 1 if args.storage == "f16" else 0
+    if STORAGE:
+        WORKLOAD = WORKLOAD.replace("FP32 storage", "FP16 deviation storage").replace(", FP32", ", FP16 deviation storage")
     if args.lbm:
         lbm_sweep(args)
         return

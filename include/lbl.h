@@ -56,6 +56,10 @@ extern "C" {
 #define LBL_LBM_DIRECT 1    /* per-thread global loads                           */
 #define LBL_LBM_TMA    2    /* rows streamed into shared memory by the TMA unit  */
 
+/* population storage (lbl_config.storage) */
+#define LBL_STORAGE_F32 0    /* FP32 populations (the reference's `real`)                   */
+#define LBL_STORAGE_F16 1    /* FP16 deviations f - w_q from the lattice weights, FP32 collide */
+
 /* run modes: the reference's -DTEST=<mode> (src/config.h:28-108) */
 #define LBL_MODE_NATURE   0
 #define LBL_MODE_OBSERVE  1
@@ -116,6 +120,8 @@ typedef struct lbl_config {
     int32_t da_obs_ruv;      /* 1: DA_OBS_RUV, rho observed (config.h:44); 0: DA_OBS_UV, model rho */
     int32_t reserved0;       /* must be 0                                                 */
     double da_nud_rate;      /* DA_NUD_RATE, nudging weight alpha, 0.1 (config.h:67-69)   */
+    int32_t storage;         /* LBL_STORAGE_* (the precision form stores FP16 deviations)  */
+    int32_t reserved1;       /* must be 0                                                 */
 } lbl_config;
 
 typedef struct lbl_ctx lbl_ctx;

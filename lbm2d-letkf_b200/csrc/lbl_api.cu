@@ -137,7 +137,11 @@ int validate(const lbl_config& c, std::string& err) {
     if (c.mode == LBL_MODE_DA_NUDGING && !(c.da_nud_rate >= 0 && c.da_nud_rate <= 1)) {
         err = "DA_NUD_RATE must lie in [0, 1]"; return LBL_ERR_ARG;
     }
-    if (c.reserved0 != 0) { err = "reserved0 must be 0"; return LBL_ERR_ARG; }
+    if (c.reserved0 != 0 || c.reserved1 != 0) { err = "reserved fields must be 0"; return LBL_ERR_ARG; }
+    if (c.storage != LBL_STORAGE_F32 && c.storage != LBL_STORAGE_F16) { err = "unknown storage"; return LBL_ERR_ARG; }
+    if (c.storage == LBL_STORAGE_F16 && c.lbm_variant == LBL_LBM_TMA) {
+        err = "the TMA stream-collide reads FP32 populations only"; return LBL_ERR_UNSUPPORTED;
+    }
     if (c.nx < 32 || c.ny < 8 || c.nx > 1024 || c.nx % 32 != 0) {
         err = "nx must be a multiple of 32 in [32, 1024] and ny >= 8"; return LBL_ERR_ARG;
     }
@@ -236,21 +240,36 @@ void enqueue_steps(lbl_ctx* ctx, int n, int cur, cudaStream_t s, bool force_done
     for (int k = 0; k < n; k++) {
         const int src = (cur + k) & 1, dst = src ^ 1;
         const bool mac = k >= n - 2;
-        launch_lbm_step(ctx, ctx->f[src], ctx->f[dst], ctx->d_force + size_t(k) * 2 * ctx->P.nxy,
+        launch_lbm_step(ctx, src, dst, ctx->d_force + size_t(k) * 2 * ctx->P.nxy,
                         mac ? ctx->mac[dst] : nullptr, s);
     }
+}
+
+// The FP32 populations the LETKF reads (forecast) and writes (analysis) for buffer cur:
+// the buffers themselves, or, with FP16 storage, FP32 copies expanded before and
+// compressed after the analysis.
+const float* analysis_input(lbl_ctx* ctx, int cur, cudaStream_t s) {
+    if (!ctx->f16) return ctx->f[cur];
+    launch_expand(ctx, ctx->h[cur], ctx->fs[0], s);
+    return ctx->fs[0];
+}
+float* analysis_output(lbl_ctx* ctx, int cur) { return ctx->f16 ? ctx->fs[1] : ctx->f[cur ^ 1]; }
+void analysis_commit(lbl_ctx* ctx, int cur, cudaStream_t s) {
+    if (ctx->f16) launch_compress(ctx, ctx->fs[1], ctx->h[cur ^ 1], s);
 }
 
 // enqueue the assimilation of the resident observations into buffer `cur`; returns the
 // buffer that holds the result (the LETKF writes the other buffer, nudging works in place)
 int enqueue_analysis(lbl_ctx* ctx, int cur, cudaStream_t s) {
     if (ctx->cfg.mode == LBL_MODE_DA_NUDGING) {
-        launch_nudging(ctx, ctx->f[cur], ctx->mac[cur], s);
+        launch_nudging(ctx, cur, ctx->mac[cur], s);
         return cur;
     }
     cudaMemsetAsync(ctx->d_stats, 0, sizeof(int) * 4, s);
-    launch_obs_ensemble(ctx, ctx->f[cur], s);
-    launch_analysis(ctx, ctx->f[cur], ctx->f[cur ^ 1], ctx->mac[cur ^ 1], s);
+    const float* fin = analysis_input(ctx, cur, s);
+    launch_obs_ensemble(ctx, fin, s);
+    launch_analysis(ctx, fin, analysis_output(ctx, cur), ctx->mac[cur ^ 1], s);
+    analysis_commit(ctx, cur, s);
     return cur ^ 1;
 }
 
@@ -461,8 +480,14 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     LBL_CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
     LBL_CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
     const size_t nxy = size_t(ctx->P.nxy), M = size_t(ctx->P.M);
+    ctx->f16 = cfg->storage == LBL_STORAGE_F16;
     for (int b = 0; b < 2; b++) {
-        LBL_CK(cudaMalloc(&ctx->f[b], sizeof(float) * M * kQ * nxy));
+        if (ctx->f16) {
+            LBL_CK(cudaMalloc(&ctx->h[b], sizeof(__half) * M * kQ * nxy));
+            if (cfg->mode == LBL_MODE_DA_LETKF) LBL_CK(cudaMalloc(&ctx->fs[b], sizeof(float) * M * kQ * nxy));
+        } else {
+            LBL_CK(cudaMalloc(&ctx->f[b], sizeof(float) * M * kQ * nxy));
+        }
         LBL_CK(cudaMalloc(&ctx->mac[b], sizeof(float) * M * 3 * nxy));
         LBL_CK(cudaMemset(ctx->mac[b], 0, sizeof(float) * M * 3 * nxy));
     }
@@ -532,7 +557,7 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     LBL_CK(cudaMalloc(&ctx->d_tmp, sizeof(float) * 2 * nxy));
     LBL_CK(cudaMalloc(&ctx->d_err, sizeof(int)));
     LBL_CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
-    if (cfg->lbm_variant == LBL_LBM_TMA && lbm_tma_supported(cfg->nx)) {
+    if (cfg->lbm_variant == LBL_LBM_TMA && !ctx->f16 && lbm_tma_supported(cfg->nx)) {
         ctx->use_tma = make_population_map(ctx, ctx->f[0], &ctx->tmap[0]) &&
                        make_population_map(ctx, ctx->f[1], &ctx->tmap[1]) && lbm_tma_prepare(cfg->nx) == 0;
     }
@@ -553,7 +578,9 @@ void destroy_impl(lbl_ctx* ctx) {
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
     ctx->graphs.clear();
     if (ctx->gen) curandDestroyGenerator(ctx->gen);
-    for (int b = 0; b < 2; b++) { cudaFree(ctx->f[b]); cudaFree(ctx->mac[b]); }
+    for (int b = 0; b < 2; b++) {
+        cudaFree(ctx->f[b]); cudaFree(ctx->h[b]); cudaFree(ctx->fs[b]); cudaFree(ctx->mac[b]);
+    }
     cudaFree(ctx->d_modes); cudaFree(ctx->d_amps); cudaFree(ctx->d_pool); cudaFree(ctx->d_force); cudaFree(ctx->d_sched);
     cudaFree(ctx->d_wtab); cudaFree(ctx->d_yo); cudaFree(ctx->d_dY); cudaFree(ctx->d_dyo);
     cudaFree(ctx->d_stats); cudaFree(ctx->d_red); cudaFree(ctx->d_tmp); cudaFree(ctx->d_err); cudaFree(ctx->d_dump);
@@ -570,6 +597,31 @@ void destroy_impl(lbl_ctx* ctx) {
     if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+}
+
+// one member's FP32 populations [9][ny][nx] to/from buffer b, converting for FP16 storage
+int upload_member(lbl_ctx* ctx, int b, int m, const float* f) {
+    const size_t n = size_t(kQ) * ctx->P.nxy;
+    if (!ctx->f16) {
+        LBL_CK(cudaMemcpy(ctx->f[b] + size_t(m) * n, f, sizeof(float) * n, cudaMemcpyHostToDevice));
+        return LBL_OK;
+    }
+    std::vector<__half> h(n);
+    for (size_t e = 0; e < n; e++) h[e] = __float2half_rn(f[e] - wq_h(int(e / ctx->P.nxy)));
+    LBL_CK(cudaMemcpy(ctx->h[b] + size_t(m) * n, h.data(), sizeof(__half) * n, cudaMemcpyHostToDevice));
+    return LBL_OK;
+}
+
+int download_member(lbl_ctx* ctx, int b, int m, float* f) {
+    const size_t n = size_t(kQ) * ctx->P.nxy;
+    if (!ctx->f16) {
+        LBL_CK(cudaMemcpy(f, ctx->f[b] + size_t(m) * n, sizeof(float) * n, cudaMemcpyDeviceToHost));
+        return LBL_OK;
+    }
+    std::vector<__half> h(n);
+    LBL_CK(cudaMemcpy(h.data(), ctx->h[b] + size_t(m) * n, sizeof(__half) * n, cudaMemcpyDeviceToHost));
+    for (size_t e = 0; e < n; e++) f[e] = wq_h(int(e / ctx->P.nxy)) + __half2float(h[e]);
+    return LBL_OK;
 }
 
 int init_impl(lbl_ctx* ctx, int ens_offset) {
@@ -595,8 +647,7 @@ int init_impl(lbl_ctx* ctx, int ens_offset) {
             mh[ij] = r0; mh[nxy + ij] = u[ij]; mh[2 * nxy + ij] = v[ij];
         }
         for (int b = 0; b < 2; b++) {  // data_0_ and data_1_ both start from the IC (data.h:55)
-            LBL_CK(cudaMemcpy(ctx->f[b] + size_t(m) * kQ * nxy, fh.data(), sizeof(float) * kQ * nxy,
-                              cudaMemcpyHostToDevice));
+            LBL_TRY(upload_member(ctx, b, m, fh.data()));
             LBL_CK(cudaMemcpy(ctx->mac[b] + size_t(m) * 3 * nxy, mh.data(), sizeof(float) * 3 * nxy,
                               cudaMemcpyHostToDevice));
         }
@@ -679,7 +730,7 @@ int nudging_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const fl
     if (!da_due(ctx, t)) return LBL_OK;                             // nudging.cu:43-44
     if (!ro || !uo || !vo) return fail(ctx, LBL_ERR_ARG, "null observation pointer");
     LBL_TRY(upload_obs(ctx, ro, uo, vo));
-    launch_nudging(ctx, ctx->f[ctx->cur], ctx->mac[ctx->cur], ctx->stream);
+    launch_nudging(ctx, ctx->cur, ctx->mac[ctx->cur], ctx->stream);
     LBL_CK(cudaGetLastError());
     if (sync) LBL_CK(cudaStreamSynchronize(ctx->stream));
     return LBL_OK;
@@ -700,14 +751,16 @@ int assimilate_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
     LBL_TRY(upload_obs(ctx, ro, uo, vo));
     const double h1 = wall_time();
     LBL_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    launch_obs_ensemble(ctx, ctx->f[ctx->cur], ctx->stream);
+    const float* fin = analysis_input(ctx, ctx->cur, ctx->stream);
+    launch_obs_ensemble(ctx, fin, ctx->stream);
     LBL_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    launch_analysis(ctx, ctx->f[ctx->cur], ctx->f[ctx->cur ^ 1], ctx->mac[ctx->cur ^ 1], ctx->stream);
+    launch_analysis(ctx, fin, analysis_output(ctx, ctx->cur), ctx->mac[ctx->cur ^ 1], ctx->stream);
+    analysis_commit(ctx, ctx->cur, ctx->stream);
     LBL_CK(cudaGetLastError());
     LBL_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     if (ctx->cfg.write_mat) {
         const double d0 = wall_time();
-        LBL_TRY(dump_matrices(ctx, t, ctx->f[ctx->cur]));
+        LBL_TRY(dump_matrices(ctx, t, fin));
         timer_add(tm, "solve", wall_time() - d0);                   // the dumps sit in solve_evd/solve_xa
     }
     ctx->cur ^= 1;                                                   // dat.swap(), letkf.cu:357
@@ -979,19 +1032,16 @@ int lbl_output(lbl_ctx* ctx, int t, const char* io_prefix) {
 int lbl_get_f(lbl_ctx* ctx, int member, float* f) {
     if (!ctx || !f || member < 0 || member >= ctx->P.M) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
-    const size_t n = size_t(kQ) * ctx->P.nxy;
     LBL_CK(cudaStreamSynchronize(ctx->stream));
-    LBL_CK(cudaMemcpy(f, ctx->f[ctx->cur] + member * n, sizeof(float) * n, cudaMemcpyDeviceToHost));
-    return LBL_OK;
+    return download_member(ctx, ctx->cur, member, f);
 }
 
 int lbl_set_f(lbl_ctx* ctx, int member, const float* f) {
     if (!ctx || !f || member < 0 || member >= ctx->P.M) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
-    const size_t n = size_t(kQ) * ctx->P.nxy;
     LBL_CK(cudaStreamSynchronize(ctx->stream));
-    LBL_CK(cudaMemcpy(ctx->f[ctx->cur] + member * n, f, sizeof(float) * n, cudaMemcpyHostToDevice));
-    launch_macros(ctx, ctx->f[ctx->cur], ctx->mac[ctx->cur], ctx->stream);
+    LBL_TRY(upload_member(ctx, ctx->cur, member, f));
+    launch_macros(ctx, ctx->cur, ctx->mac[ctx->cur], ctx->stream);
     LBL_CK(cudaGetLastError());
     LBL_CK(cudaStreamSynchronize(ctx->stream));
     return LBL_OK;
@@ -1129,7 +1179,7 @@ int lbl_profile_step(lbl_ctx* ctx, int n, double* ms_per_launch) {
     const float* force = ctx->d_force + size_t(ctx->last_force_slot) * 2 * ctx->P.nxy;
     LBL_CK(cudaEventRecord(ctx->ev[8], ctx->stream));
     for (int k = 0; k < n; k++) {
-        launch_lbm_step(ctx, ctx->f[ctx->cur], ctx->f[ctx->cur ^ 1], force, nullptr, ctx->stream);
+        launch_lbm_step(ctx, ctx->cur, ctx->cur ^ 1, force, nullptr, ctx->stream);
         ctx->cur ^= 1;
     }
     LBL_CK(cudaGetLastError());

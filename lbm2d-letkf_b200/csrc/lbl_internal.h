@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <curand.h>
 
@@ -75,7 +76,10 @@ struct lbl_ctx {
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 
     // ensemble state, double buffered like data::d()/dn() (data.h:45-64)
-    float* f[2] = {nullptr, nullptr};    // [M][9][ny][nx]
+    float* f[2] = {nullptr, nullptr};    // [M][9][ny][nx] FP32 populations (LBL_STORAGE_F32)
+    __half* h[2] = {nullptr, nullptr};   // [M][9][ny][nx] FP16 deviations f - w_q (LBL_STORAGE_F16)
+    float* fs[2] = {nullptr, nullptr};   // FP32 forecast / analysis copies for the analysis (FP16 storage)
+    bool f16 = false;                    // storage == LBL_STORAGE_F16
     float* mac[2] = {nullptr, nullptr};  // [M][3][ny][nx]  rho, u, v (post-stream macros)
     int cur = 0;                         // index of d()
 
@@ -142,15 +146,18 @@ namespace lbl {
 void launch_ic_velocity(const double* modes /*[4][n]*/, int n_modes, int nx, int ny,
                         float* u, float* v, cudaStream_t s);
 void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s);
-void launch_lbm_step(const lbl_ctx* c, const float* fin, float* fout, const float* force,
-                     float* mac_out, cudaStream_t s);
+// one step from population buffer src to dst (FP32 or FP16 storage)
+void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s);
+// FP16 deviation storage <-> FP32 populations, all members
+void launch_expand(const lbl_ctx* c, const __half* h, float* f, cudaStream_t s);
+void launch_compress(const lbl_ctx* c, const float* f, __half* h, cudaStream_t s);
 int lbm_tma_prepare(int nx);
 bool lbm_tma_supported(int nx);
-void launch_macros(const lbl_ctx* c, const float* f, float* mac, cudaStream_t s);
+void launch_macros(const lbl_ctx* c, int buf, float* mac, cudaStream_t s);
 
 // ---- kernels (letkf_kernels.cu) ----
 void launch_obs_ensemble(const lbl_ctx* c, const float* f, cudaStream_t s);
-void launch_nudging(const lbl_ctx* c, float* f, const float* mac, cudaStream_t s);
+void launch_nudging(const lbl_ctx* c, int buf, const float* mac, cudaStream_t s);
 void launch_analysis(const lbl_ctx* c, const float* fin, float* fout, float* mac_out, cudaStream_t s);
 // LETKF matrix dumps (need_save_mat, letkf_solver.h:243-345): the 14 matrices of the
 // rows [j0, j1), each [rows][cols][points] column-major with the point slowest, laid

@@ -28,6 +28,28 @@ __host__ __device__ constexpr float w_q(int q) {                       // config
                                                            : float(1. / 36.);
 }
 
+__device__ __forceinline__ float w_q_rt(int q) {
+    return q == 4 ? float(4. / 9.) : ((q & 1) ? float(1. / 9.) : float(1. / 36.));
+}
+
+// ---------------------------------------------------------------------------
+// Population storage: FP32 values, or FP16 deviations f - w_q from the lattice
+// weights (the precision form): every load widens to FP32 and every store narrows
+// after the FP32 collide, so only the bytes in HBM change.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct Store;
+template <>
+struct Store<float> {
+    static __device__ __forceinline__ float ld(const float* p, float) { return __ldg(p); }
+    static __device__ __forceinline__ void st(float* p, float v, float) { *p = v; }
+};
+template <>
+struct Store<__half> {
+    static __device__ __forceinline__ float ld(const __half* p, float w) { return w + __half2float(__ldg(p)); }
+    static __device__ __forceinline__ void st(__half* p, float v, float w) { *p = __float2half_rn(v - w); }
+};
+
 // The D2Q9 helpers below skip the e = 0 terms at compile time (x*0 cannot be folded
 // under IEEE rules, yet adding it never changes a finite result), and turn the
 // divisions by the constants c, c*c and cs2 into multiplications by host-rounded
@@ -211,15 +233,16 @@ __global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __
 // yo holds the site observations [u, v, rho][site]; mac the current macros (rho is
 // taken from the model under DA_OBS_UV).  The macros are not refreshed, as there.
 // ---------------------------------------------------------------------------
-template <int q>
-__device__ __forceinline__ void nudge_q(float* fm, int nxy, float rho, float u, float v, float uu0, float alpha,
+template <int q, typename T>
+__device__ __forceinline__ void nudge_q(T* fm, int nxy, float rho, float u, float v, float uu0, float alpha,
                                         const Phys& P) {
-    const float f_calc = fm[q * nxy];
+    const float f_calc = Store<T>::ld(fm + q * nxy, w_q(q));
     const float f_obse = feq_q<q>(rho, u, v, uu0, P);
-    fm[q * nxy] = alpha * f_obse + (1 - alpha) * f_calc;
+    Store<T>::st(fm + q * nxy, alpha * f_obse + (1 - alpha) * f_calc, w_q(q));
 }
 
-__global__ void nudging_kernel(float* __restrict__ f, const float* __restrict__ mac, const float* __restrict__ yo,
+template <typename T>
+__global__ void nudging_kernel(T* __restrict__ f, const float* __restrict__ mac, const float* __restrict__ yo,
                                Phys P, int p, int nsx, int nsy, float alpha, int quadra, int ruv) {
     const int ij = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
@@ -254,7 +277,7 @@ __global__ void nudging_kernel(float* __restrict__ f, const float* __restrict__ 
     }
     if (!ruv) rho_obse = mac[size_t(m) * 3 * nxy + ij];  // DA_OBS_UV: rho_calc (nudging.cu:128-131)
     const float uu0 = (u_obse * u_obse + v_obse * v_obse) * P.inv_c2;
-    float* fm = f + size_t(m) * kQ * nxy + ij;
+    T* fm = f + size_t(m) * kQ * nxy + ij;
     nudge_q<0>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
     nudge_q<1>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
     nudge_q<2>(fm, nxy, rho_obse, u_obse, v_obse, uu0, alpha, P);
@@ -377,8 +400,8 @@ __global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __res
 // NX > 0 fixes the (square) grid at compile time so that plane and row offsets are
 // immediates; NX = 0 reads nx, ny from P.
 // ---------------------------------------------------------------------------
-template <bool WRITE_MAC, int MAXT, int NX>
-__global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict__ fin, float* __restrict__ fout,
+template <bool WRITE_MAC, int MAXT, int NX, typename T>
+__global__ void __launch_bounds__(MAXT) lbm_step_kernel(const T* __restrict__ fin, T* __restrict__ fout,
                                                         const float* __restrict__ force,
                                                         float* __restrict__ mac, Phys P, int TY) {
     extern __shared__ float s_uv[];  // [3][2][nx]
@@ -387,8 +410,8 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
     const int m = blockIdx.y;
     const int j0 = blockIdx.x * TY;
     const int j1 = min(j0 + TY, ny);
-    const float* __restrict__ fm = fin + size_t(m) * kQ * nxy;
-    float* __restrict__ fo = fout + size_t(m) * kQ * nxy + x;
+    const T* __restrict__ fm = fin + size_t(m) * kQ * nxy;
+    T* __restrict__ fo = fout + size_t(m) * kQ * nxy + x;
     const int xm = (x == 0) ? nx - 1 : x - 1;
     const int xp = (x == nx - 1) ? 0 : x + 1;
     const float* __restrict__ Fx = force + x;
@@ -408,7 +431,7 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
         for (int q = 0; q < kQ; q++) {
             const int col = ex_q(q) == -1 ? xp : (ex_q(q) == 0 ? x : xm);
             const int row = ey_q(q) == -1 ? o_p : (ey_q(q) == 0 ? o_0 : o_m);
-            fc[q] = __ldg(fm + q * nxy + row + col);
+            fc[q] = Store<T>::ld(fm + q * nxy + row + col, w_q(q));
         }
     };
     // Three row slots rotate roles (A = row being finalised, B = next row, C = the row
@@ -446,7 +469,7 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const float* __restrict_
         const float omega = les_omega(sa[xp], sa[xm], sa[nx + xp], sa[nx + xm], ub, uc, vb, vc, P);
         collide(fa, ra, ua, va, omega, Fx[ij], Fy[ij], P);
 #pragma unroll
-        for (int q = 0; q < kQ; q++) fo[q * nxy + ij] = fa[q];
+        for (int q = 0; q < kQ; q++) Store<T>::st(fo + q * nxy + ij, fa[q], w_q(q));
         if (WRITE_MAC) {
             float* mm = mac + size_t(m) * 3 * nxy + x;
             mm[ij] = ra;
@@ -646,13 +669,14 @@ __global__ void __launch_bounds__(1024) lbm_step_tma_kernel(const __grid_constan
 }
 
 // moments of f for every member (lbm2euler-style, letkf.cu:340-355, but with v)
-__global__ void macros_kernel(const float* __restrict__ f, float* __restrict__ mac, Phys P) {
+template <typename T>
+__global__ void macros_kernel(const T* __restrict__ f, float* __restrict__ mac, Phys P) {
     const int ij = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
     if (ij >= P.nxy) return;
     float fc[kQ];
 #pragma unroll
-    for (int q = 0; q < kQ; q++) fc[q] = f[(size_t(m) * kQ + q) * P.nxy + ij];
+    for (int q = 0; q < kQ; q++) fc[q] = Store<T>::ld(f + (size_t(m) * kQ + q) * P.nxy + ij, w_q(q));
     const float r = rf(fc);
     float* mm = mac + size_t(m) * 3 * P.nxy;
     mm[ij] = r;
@@ -675,10 +699,10 @@ int strip_rows(const Phys& P, bool tma) {
                                                           sizeof(float) * (size_t(kStages) * kQ * P.nx + 6 * P.nx) +
                                                               2 * kStages * sizeof(uint64_t));
         else if (P.nx <= 256)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 256, 0>, P.nx,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 256, 0, float>, P.nx,
                                                           sizeof(float) * 6 * P.nx);
         else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 1024, 0>, P.nx,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 1024, 0, float>, P.nx,
                                                           sizeof(float) * 6 * P.nx);
         slots[t] = std::max(1, per_sm) * sms;
     }
@@ -700,11 +724,16 @@ void launch_ic_velocity(const double* modes, int n_modes, int nx, int ny, float*
     ic_velocity_kernel<<<grid, block, 0, s>>>(modes, n_modes, nx, ny, u, v);
 }
 
-void launch_nudging(const lbl_ctx* c, float* f, const float* mac, cudaStream_t s) {
+void launch_nudging(const lbl_ctx* c, int buf, const float* mac, cudaStream_t s) {
     const int threads = 256;
     dim3 grid((c->P.nxy + threads - 1) / threads, c->P.M);
-    nudging_kernel<<<grid, threads, 0, s>>>(f, mac, c->d_yo, c->P, c->G.p, c->G.nsx, c->G.nsy,
-                                            float(c->cfg.da_nud_rate), c->cfg.da_quadra, c->cfg.da_obs_ruv);
+    const float alpha = float(c->cfg.da_nud_rate);
+    if (c->f16)
+        nudging_kernel<__half><<<grid, threads, 0, s>>>(c->h[buf], mac, c->d_yo, c->P, c->G.p, c->G.nsx, c->G.nsy,
+                                                        alpha, c->cfg.da_quadra, c->cfg.da_obs_ruv);
+    else
+        nudging_kernel<float><<<grid, threads, 0, s>>>(c->f[buf], mac, c->d_yo, c->P, c->G.p, c->G.nsx, c->G.nsy,
+                                                       alpha, c->cfg.da_quadra, c->cfg.da_obs_ruv);
 }
 
 void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s) {
@@ -758,15 +787,24 @@ void launch_tma(const lbl_ctx* c, dim3 grid, int ty, int b, float* fout, const f
         lbm_step_tma_kernel<false, NX><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, nullptr, P, ty, box, c->d_err);
 }
 
-template <int MAXT, int NX>
-void launch_direct(const lbl_ctx* c, dim3 grid, int ty, const float* fin, float* fout, const float* force,
-                   float* mac_out, cudaStream_t s) {
+template <int MAXT, int NX, typename T>
+void launch_direct_t(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout, const float* force,
+                     float* mac_out, cudaStream_t s) {
     const Phys& P = c->P;
     const size_t sm = sizeof(float) * 6 * P.nx;
     if (mac_out)
-        lbm_step_kernel<true, MAXT, NX><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty);
+        lbm_step_kernel<true, MAXT, NX, T><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty);
     else
-        lbm_step_kernel<false, MAXT, NX><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty);
+        lbm_step_kernel<false, MAXT, NX, T><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty);
+}
+
+template <int MAXT, int NX>
+void launch_direct(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
+                   cudaStream_t s) {
+    if (c->f16)
+        launch_direct_t<MAXT, NX, __half>(c, grid, ty, c->h[src], c->h[dst], force, mac_out, s);
+    else
+        launch_direct_t<MAXT, NX, float>(c, grid, ty, c->f[src], c->f[dst], force, mac_out, s);
 }
 }  // namespace
 
@@ -776,38 +814,63 @@ int lbm_tma_prepare(int nx) {
            tma_prepare_nx<512>(sm);
 }
 
-void launch_lbm_step(const lbl_ctx* c, const float* fin, float* fout, const float* force, float* mac_out,
-                     cudaStream_t s) {
+void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s) {
     const Phys& P = c->P;
     const int sq = (P.nx == P.ny) ? P.nx : 0;
     const int ty = strip_rows(P, c->use_tma);
     dim3 grid((P.ny + ty - 1) / ty, P.M);
     if (c->use_tma) {
-        const int b = (fin == c->f[0]) ? 0 : 1;
+        float* fout = c->f[dst];
         switch (sq) {
-            case 64: launch_tma<64>(c, grid, ty, b, fout, force, mac_out, s); break;
-            case 128: launch_tma<128>(c, grid, ty, b, fout, force, mac_out, s); break;
-            case 256: launch_tma<256>(c, grid, ty, b, fout, force, mac_out, s); break;
-            case 512: launch_tma<512>(c, grid, ty, b, fout, force, mac_out, s); break;
-            default: launch_tma<0>(c, grid, ty, b, fout, force, mac_out, s); break;
+            case 64: launch_tma<64>(c, grid, ty, src, fout, force, mac_out, s); break;
+            case 128: launch_tma<128>(c, grid, ty, src, fout, force, mac_out, s); break;
+            case 256: launch_tma<256>(c, grid, ty, src, fout, force, mac_out, s); break;
+            case 512: launch_tma<512>(c, grid, ty, src, fout, force, mac_out, s); break;
+            default: launch_tma<0>(c, grid, ty, src, fout, force, mac_out, s); break;
         }
         return;
     }
     switch (sq) {
-        case 64: launch_direct<256, 64>(c, grid, ty, fin, fout, force, mac_out, s); break;
-        case 128: launch_direct<256, 128>(c, grid, ty, fin, fout, force, mac_out, s); break;
-        case 256: launch_direct<256, 256>(c, grid, ty, fin, fout, force, mac_out, s); break;
-        case 512: launch_direct<1024, 512>(c, grid, ty, fin, fout, force, mac_out, s); break;
-        case 1024: launch_direct<1024, 1024>(c, grid, ty, fin, fout, force, mac_out, s); break;
+        case 64: launch_direct<256, 64>(c, grid, ty, src, dst, force, mac_out, s); break;
+        case 128: launch_direct<256, 128>(c, grid, ty, src, dst, force, mac_out, s); break;
+        case 256: launch_direct<256, 256>(c, grid, ty, src, dst, force, mac_out, s); break;
+        case 512: launch_direct<1024, 512>(c, grid, ty, src, dst, force, mac_out, s); break;
+        case 1024: launch_direct<1024, 1024>(c, grid, ty, src, dst, force, mac_out, s); break;
         default:
-            if (P.nx <= 256) launch_direct<256, 0>(c, grid, ty, fin, fout, force, mac_out, s);
-            else launch_direct<1024, 0>(c, grid, ty, fin, fout, force, mac_out, s);
+            if (P.nx <= 256) launch_direct<256, 0>(c, grid, ty, src, dst, force, mac_out, s);
+            else launch_direct<1024, 0>(c, grid, ty, src, dst, force, mac_out, s);
     }
 }
 
-void launch_macros(const lbl_ctx* c, const float* f, float* mac, cudaStream_t s) {
+void launch_macros(const lbl_ctx* c, int buf, float* mac, cudaStream_t s) {
     dim3 grid((c->P.nxy + 255) / 256, c->P.M);
-    macros_kernel<<<grid, 256, 0, s>>>(f, mac, c->P);
+    if (c->f16)
+        macros_kernel<__half><<<grid, 256, 0, s>>>(c->h[buf], mac, c->P);
+    else
+        macros_kernel<float><<<grid, 256, 0, s>>>(c->f[buf], mac, c->P);
+}
+
+// FP16 deviation storage <-> FP32 populations, element-wise over [M][9][ny][nx]
+__global__ void expand_kernel(const __half* __restrict__ h, float* __restrict__ f, size_t n, int nxy) {
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x) * blockDim.x) {
+        const int q = int((e / nxy) % kQ);
+        f[e] = w_q_rt(q) + __half2float(h[e]);
+    }
+}
+__global__ void compress_kernel(const float* __restrict__ f, __half* __restrict__ h, size_t n, int nxy) {
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x) * blockDim.x) {
+        const int q = int((e / nxy) % kQ);
+        h[e] = __float2half_rn(f[e] - w_q_rt(q));
+    }
+}
+
+void launch_expand(const lbl_ctx* c, const __half* h, float* f, cudaStream_t s) {
+    const size_t n = size_t(c->P.M) * kQ * c->P.nxy;
+    expand_kernel<<<4 * 148, 256, 0, s>>>(h, f, n, c->P.nxy);
+}
+void launch_compress(const lbl_ctx* c, const float* f, __half* h, cudaStream_t s) {
+    const size_t n = size_t(c->P.M) * kQ * c->P.nxy;
+    compress_kernel<<<4 * 148, 256, 0, s>>>(f, h, n, c->P.nxy);
 }
 
 }  // namespace lbl

@@ -38,6 +38,7 @@ ERRORS = {
     -9: "LBL_ERR_NOCONV", -10: "LBL_ERR_TIMEOUT",
 }
 LBM_AUTO, LBM_DIRECT, LBM_TMA = 0, 1, 2
+STORAGE_F32, STORAGE_F16 = 0, 1
 
 # names of the exported C functions (must match include/lbl.h)
 EXPORTS = (
@@ -76,6 +77,7 @@ class Config(ctypes.Structure):
         ("force_seed", ctypes.c_uint64), ("obs_seed", ctypes.c_uint64),
         ("da_dummy", ctypes.c_int32), ("da_quadra", ctypes.c_int32), ("da_obs_ruv", ctypes.c_int32),
         ("reserved0", ctypes.c_int32), ("da_nud_rate", ctypes.c_double),
+        ("storage", ctypes.c_int32), ("reserved1", ctypes.c_int32),
     ]
 
     def copy(self) -> "Config":
