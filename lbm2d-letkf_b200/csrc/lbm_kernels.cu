@@ -72,85 +72,122 @@ __device__ __forceinline__ float feq_q(float rho, float u, float v, float uu0, c
     return rho * w_q(q) * (float(1.) + float(3.) * uc0 + float(4.5) * uc0 * uc0 - float(1.5) * uu0);
 }
 
-// rf / uf / vf (lbm.h:72-109; VELOCITY_FORCE_CORRECTION and ICLBM are off)
-__device__ __forceinline__ float rf(const float (&f)[kQ]) {
-    float ret = 0;
-#pragma unroll
-    for (int q = 0; q < kQ; q++) ret += f[q];
-    return ret;
-}
-__device__ __forceinline__ float uf(const float (&f)[kQ], float rho, float c) {
-    float ret = 0;
-#pragma unroll
-    for (int q = 0; q < kQ; q++)
-        if (ex_q(q) != 0) ret = fmaf(f[q], c * ex_q(q), ret);
-    ret /= rho;
-    return ret;
-}
-__device__ __forceinline__ float vf(const float (&f)[kQ], float rho, float c) {
-    float ret = 0;
-#pragma unroll
-    for (int q = 0; q < kQ; q++)
-        if (ey_q(q) != 0) ret = fmaf(f[q], c * ey_q(q), ret);
-    ret /= rho;
-    return ret;
+// ---------------------------------------------------------------------------
+// Arithmetic of the stream-collide.  Every operation below is one explicitly rounded
+// IEEE operation (__fadd_rn, __fmul_rn, __fmaf_rn, ...) in a fixed order, so the
+// rounding sequence is the one written here rather than a compiler's choice of
+// contractions; divisions and square roots follow -use_fast_math, and the relaxation
+// time is computed in FP64.  (V is the lane type; the kernels use float.)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float vadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float vsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float vmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+template <typename V> __device__ __forceinline__ V splat(float s);
+template <> __device__ __forceinline__ float splat<float>(float s) { return s; }
+__device__ __forceinline__ float vdiv(float a, float b) { return a / b; }
+__device__ __forceinline__ float vneg(float a) { return -a; }
+
+// (u ex + v ey) * s for direction q, the signs folded into the constant
+template <int q, typename V>
+__device__ __forceinline__ V edot_s(V u, V v, float s) {
+    constexpr int ex = ex_q(q), ey = ey_q(q);
+    if (ex == 0 && ey == 0) return splat<V>(0.f);
+    if (ex == 0) return vmul(v, splat<V>(ey * s));
+    if (ey == 0) return vmul(u, splat<V>(ex * s));
+    if (ex == ey) return vmul(vadd(u, v), splat<V>(ex * s));
+    return vmul(vsub(u, v), splat<V>(ex * s));
 }
 
-// force_acc (lbm.h:41-70; first-order term only, FORCE_SECOND_ORDER off), with
-// fx = (fx_ - friction/dt*u)*dt and fy precomputed per cell
-template <int q>
-__device__ __forceinline__ float force_acc_q(float fx, float fy, float rho, const Phys& P) {
-    const float f1 = edot<q>(P.u_ref * fx, P.u_ref * fy) * P.inv_cs2;
-    float ret = f1;
-    ret *= w_q(q) * rho;
-    return ret;
-}
-
-// BGK toward feq plus the force term for all nine populations (lbm_collision_srt.h:8-16,
-// lbm.cu:142-147)
-__device__ __forceinline__ void collide(float (&f)[kQ], float rho, float u, float v, float omega, float fxc,
-                                        float fyc, const Phys& P) {
-    const float uu0 = (u * u + v * v) * P.inv_c2;
-    const float fx = (fxc - P.fr_dt * u) * P.dt;
-    const float fy = (fyc - P.fr_dt * v) * P.dt;
-#define LBL_COLLIDE_Q(q)                                  \
-    {                                                     \
-        const float feqq = feq_q<q>(rho, u, v, uu0, P);  \
-        const float fneq = f[q] - feqq;                   \
-        f[q] -= omega * fneq;                             \
-    }
-    LBL_COLLIDE_Q(0) LBL_COLLIDE_Q(1) LBL_COLLIDE_Q(2) LBL_COLLIDE_Q(3) LBL_COLLIDE_Q(4)
-    LBL_COLLIDE_Q(5) LBL_COLLIDE_Q(6) LBL_COLLIDE_Q(7) LBL_COLLIDE_Q(8)
-#undef LBL_COLLIDE_Q
-    f[0] += force_acc_q<0>(fx, fy, rho, P);
-    f[1] += force_acc_q<1>(fx, fy, rho, P);
-    f[2] += force_acc_q<2>(fx, fy, rho, P);
-    f[3] += force_acc_q<3>(fx, fy, rho, P);
-    f[4] += force_acc_q<4>(fx, fy, rho, P);
-    f[5] += force_acc_q<5>(fx, fy, rho, P);
-    f[6] += force_acc_q<6>(fx, fy, rho, P);
-    f[7] += force_acc_q<7>(fx, fy, rho, P);
-    f[8] += force_acc_q<8>(fx, fy, rho, P);
+// rho, u, v of a pulled row (lbm.h:72-109): rho = f0 + f1 + ..., u = sum f c ex / rho
+template <typename V>
+__device__ __forceinline__ void macros_v(const V (&f)[kQ], V& r, V& u, V& v, float c) {
+    r = f[0];
+#pragma unroll
+    for (int q = 1; q < kQ; q++) r = vadd(r, f[q]);
+    V su = vmul(f[0], splat<V>(c * ex_q(0)));  // q = 0, 2, 3, 5, 6, 8 have ex != 0
+    su = vfma(f[2], splat<V>(c * ex_q(2)), su);
+    su = vfma(f[3], splat<V>(c * ex_q(3)), su);
+    su = vfma(f[5], splat<V>(c * ex_q(5)), su);
+    su = vfma(f[6], splat<V>(c * ex_q(6)), su);
+    su = vfma(f[8], splat<V>(c * ex_q(8)), su);
+    V sv = vmul(f[0], splat<V>(c * ey_q(0)));  // q = 0, 1, 2, 6, 7, 8 have ey != 0
+    sv = vfma(f[1], splat<V>(c * ey_q(1)), sv);
+    sv = vfma(f[2], splat<V>(c * ey_q(2)), sv);
+    sv = vfma(f[6], splat<V>(c * ey_q(6)), sv);
+    sv = vfma(f[7], splat<V>(c * ey_q(7)), sv);
+    sv = vfma(f[8], splat<V>(c * ey_q(8)), sv);
+    u = vdiv(su, r);
+    v = vdiv(sv, r);
 }
 
 // Smagorinsky relaxation rate from the post-stream velocity stencil (lbm.cu:42-60,
-// 132-139): tau = 0.5 + 3 nu / c / c / dt in double from the float viscosity, as one
-// FMA with the precomputed 3/c/c/dt; omega = 1/tau correctly rounded in float.
-__device__ __forceinline__ float les_omega(float ue, float uw, float ve, float vw, float un, float us, float vn,
-                                           float vs, const Phys& P) {
-    const float ux = (ue - uw) * P.inv_two_dx;
-    const float uy = (un - us) * P.inv_two_dx;
-    const float vx = (ve - vw) * P.inv_two_dx;
-    const float vy = (vn - vs) * P.inv_two_dx;
-    const float s00 = ux;
-    const float s01 = float(.5) * (uy + vx);
-    const float s10 = s01;
-    const float s11 = vy;
-    const float ss = sqrt(2 * (s00 * s00 + s01 * s10 + s10 * s01 + s11 * s11));
+// 132-139): S from central differences, nu_t = cs^2 dx^2 sqrt(2 S:S) in double from
+// the float S, tau = 0.5 + 3 nu / c / c / dt as one FP64 FMA with the precomputed
+// 3/c/c/dt, omega = 1/tau correctly rounded in float.
+__device__ __forceinline__ float omega_of(float ss2, const Phys& P) {
+    const float ss = sqrtf(ss2);
     const float nus = float(P.les_k * double(ss));
     const float nu = P.nu + nus;
     const float tau = float(fma(double(nu), P.tau_k, 0.5));
     return __frcp_rn(tau);
+}
+template <typename V>
+__device__ __forceinline__ V les_omega_v(V ue, V uw, V ve, V vw, V un, V us, V vn, V vs, const Phys& P) {
+    const V k2 = splat<V>(P.inv_two_dx);
+    const V ux = vmul(vsub(ue, uw), k2);  // s00
+    const V uy = vmul(vsub(un, us), k2);
+    const V vx = vmul(vsub(ve, vw), k2);
+    const V vy = vmul(vsub(vn, vs), k2);  // s11
+    const V s01 = vmul(splat<V>(.5f), vadd(uy, vx));
+    V t = vmul(ux, ux);
+    t = vfma(s01, s01, t);  // s01 s10
+    t = vfma(s01, s01, t);  // s10 s01
+    t = vfma(vy, vy, t);
+    t = vmul(splat<V>(2.f), t);
+    return omega_of(t, P);
+}
+
+// BGK toward feq (lbm.h:31-39, lbm_collision_srt.h:8-16) plus the first-order force
+// with friction (lbm.h:41-70, lbm.cu:142-147): fx = (fx_ - friction/dt u) dt, ...
+template <int q, typename V>
+__device__ __forceinline__ void collide_q(V& fq, V rho, V u, V v, V uu0, V nomega, V gx, V gy, const Phys& P) {
+    const V uc0 = edot_s<q>(u, v, P.inv_c);
+    V t = vfma(splat<V>(3.f), uc0, splat<V>(1.f));
+    t = vfma(vmul(splat<V>(4.5f), uc0), uc0, t);
+    t = vfma(splat<V>(-1.5f), uu0, t);
+    const V rw = vmul(rho, splat<V>(w_q(q)));
+    const V feq = vmul(rw, t);
+    fq = vfma(nomega, vsub(fq, feq), fq);
+    if (q != 4) fq = vfma(edot_s<q>(gx, gy, P.inv_cs2), rw, fq);
+}
+template <typename V>
+__device__ __forceinline__ void collide_v(V (&f)[kQ], V rho, V u, V v, V omega, float fxc, float fyc,
+                                          const Phys& P) {
+    const V uu0 = vmul(vfma(u, u, vmul(v, v)), splat<V>(P.inv_c2));
+    const V fx = vmul(vfma(splat<V>(-P.fr_dt), u, splat<V>(fxc)), splat<V>(P.dt));
+    const V fy = vmul(vfma(splat<V>(-P.fr_dt), v, splat<V>(fyc)), splat<V>(P.dt));
+    const V gx = vmul(splat<V>(P.u_ref), fx), gy = vmul(splat<V>(P.u_ref), fy);
+    const V nomega = vneg(omega);
+    collide_q<0>(f[0], rho, u, v, uu0, nomega, gx, gy, P);
+    collide_q<1>(f[1], rho, u, v, uu0, nomega, gx, gy, P);
+    collide_q<2>(f[2], rho, u, v, uu0, nomega, gx, gy, P);
+    collide_q<3>(f[3], rho, u, v, uu0, nomega, gx, gy, P);
+    collide_q<4>(f[4], rho, u, v, uu0, nomega, gx, gy, P);
+    collide_q<5>(f[5], rho, u, v, uu0, nomega, gx, gy, P);
+    collide_q<6>(f[6], rho, u, v, uu0, nomega, gx, gy, P);
+    collide_q<7>(f[7], rho, u, v, uu0, nomega, gx, gy, P);
+    collide_q<8>(f[8], rho, u, v, uu0, nomega, gx, gy, P);
+}
+
+// the one-member forms the scalar kernels call
+__device__ __forceinline__ void collide(float (&f)[kQ], float rho, float u, float v, float omega, float fxc,
+                                        float fyc, const Phys& P) {
+    collide_v<float>(f, rho, u, v, omega, fxc, fyc, P);
+}
+__device__ __forceinline__ float les_omega(float ue, float uw, float ve, float vw, float un, float us, float vn,
+                                           float vs, const Phys& P) {
+    return les_omega_v<float>(ue, uw, ve, vw, un, us, vn, vs, P);
 }
 
 // ---------------------------------------------------------------------------
@@ -441,15 +478,12 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const T* __restrict__ fi
     float f[3][kQ], r[3], u[3], v[3];
     {  // halo row below the strip: only its u,v (own column) are needed
         pull(f[2]);
-        const float rr = rf(f[2]);
-        u[2] = uf(f[2], rr, P.c);
-        v[2] = vf(f[2], rr, P.c);
+        float rr;
+        macros_v(f[2], rr, u[2], v[2], P.c);
     }
     advance();
     pull(f[0]);  // row j0
-    r[0] = rf(f[0]);
-    u[0] = uf(f[0], r[0], P.c);
-    v[0] = vf(f[0], r[0], P.c);
+    macros_v(f[0], r[0], u[0], v[0], P.c);
     s_uv[x] = u[0];
     s_uv[nx + x] = v[0];
     advance();
@@ -460,9 +494,7 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const T* __restrict__ fi
                    float& ub, float& vb, float uc, float vc, float* sa, float* sb, int jc) {
         advance();
         if (jc + 2 <= j1) pull(fc);  // prefetch the row after next
-        rb = rf(fb);
-        ub = uf(fb, rb, P.c);
-        vb = vf(fb, rb, P.c);
+        macros_v(fb, rb, ub, vb, P.c);
         sb[x] = ub;
         sb[nx + x] = vb;
         __syncthreads();
@@ -627,22 +659,17 @@ __global__ void __launch_bounds__(1024) lbm_step_tma_kernel(const __grid_constan
     {
         float t[kQ];
         take(0, t);  // halo row j0-1: u,v only
-        const float r = rf(t);
-        uM = uf(t, r, P.c);
-        vM = vf(t, r, P.c);
+        float r;
+        macros_v(t, r, uM, vM, P.c);
     }
     take(1, fA);  // row j0
-    rA = rf(fA);
-    uA = uf(fA, rA, P.c);
-    vA = vf(fA, rA, P.c);
+    macros_v(fA, rA, uA, vA, P.c);
     s_a[x] = uA;
     s_a[nx + x] = vA;
     int ij = j0 * nx;
     for (int jc = j0; jc < j1; jc++) {
         take(jc - j0 + 2, fB);  // row jc+1
-        rB = rf(fB);
-        uB = uf(fB, rB, P.c);
-        vB = vf(fB, rB, P.c);
+        macros_v(fB, rB, uB, vB, P.c);
         s_b[x] = uB;
         s_b[nx + x] = vB;
         consumer_sync(ncons);
@@ -677,11 +704,12 @@ __global__ void macros_kernel(const T* __restrict__ f, float* __restrict__ mac, 
     float fc[kQ];
 #pragma unroll
     for (int q = 0; q < kQ; q++) fc[q] = Store<T>::ld(f + (size_t(m) * kQ + q) * P.nxy + ij, w_q(q));
-    const float r = rf(fc);
+    float r, u, v;
+    macros_v(fc, r, u, v, P.c);
     float* mm = mac + size_t(m) * 3 * P.nxy;
     mm[ij] = r;
-    mm[P.nxy + ij] = uf(fc, r, P.c);
-    mm[2 * P.nxy + ij] = vf(fc, r, P.c);
+    mm[P.nxy + ij] = u;
+    mm[2 * P.nxy + ij] = v;
 }
 
 // Strip height: fill the GPU's resident CTA slots with as few waves as possible,
@@ -817,6 +845,7 @@ int lbm_tma_prepare(int nx) {
 void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s) {
     const Phys& P = c->P;
     const int sq = (P.nx == P.ny) ? P.nx : 0;
+
     const int ty = strip_rows(P, c->use_tma);
     dim3 grid((P.ny + ty - 1) / ty, P.M);
     if (c->use_tma) {

@@ -209,3 +209,4 @@ def test_tma_variant_rejected_where_unsupported():
     with pytest.raises(lbl.LblError) as ei:
         lbl.Ensemble(lbl.config_default("NATURE", 384, 1, lbm_variant=lbl.LBM_TMA))
     assert ei.value.code == -8
+
