@@ -150,34 +150,39 @@ __device__ __forceinline__ V les_omega_v(V ue, V uw, V ve, V vw, V un, V us, V v
 
 // BGK toward feq (lbm.h:31-39, lbm_collision_srt.h:8-16) plus the first-order force
 // with friction (lbm.h:41-70, lbm.cu:142-147): fx = (fx_ - friction/dt u) dt, ...
+// feq_q = rho w_q (1 + 3 uc + 4.5 uc^2 - 1.5 uu0) with uc = e_q.u / c.  Opposite
+// directions q and 8 - q share w and see -uc, so each pair evaluates the even part
+// E = (1 - 1.5 uu0) + 4.5 uc^2 and the odd part O = 3 uc once, and its force terms
+// differ only in sign.
 template <int q, typename V>
-__device__ __forceinline__ void collide_q(V& fq, V rho, V u, V v, V uu0, V nomega, V gx, V gy, const Phys& P) {
-    const V uc0 = edot_s<q>(u, v, P.inv_c);
-    V t = vfma(splat<V>(3.f), uc0, splat<V>(1.f));
-    t = vfma(vmul(splat<V>(4.5f), uc0), uc0, t);
-    t = vfma(splat<V>(-1.5f), uu0, t);
-    const V rw = vmul(rho, splat<V>(w_q(q)));
-    const V feq = vmul(rw, t);
+__device__ __forceinline__ void collide_pair(V& fq, V& fqb, V rw, V u, V v, V c0, V nomega, V gx, V gy,
+                                             const Phys& P) {
+    const V uc = edot_s<q>(u, v, P.inv_c);
+    const V e = vfma(vmul(splat<V>(4.5f), uc), uc, c0);
+    const V o = vmul(splat<V>(3.f), uc);
+    const V feq = vmul(rw, vadd(e, o)), feqb = vmul(rw, vsub(e, o));
     fq = vfma(nomega, vsub(fq, feq), fq);
-    if (q != 4) fq = vfma(edot_s<q>(gx, gy, P.inv_cs2), rw, fq);
+    fqb = vfma(nomega, vsub(fqb, feqb), fqb);
+    const V fe = edot_s<q>(gx, gy, P.inv_cs2);
+    fq = vfma(fe, rw, fq);
+    fqb = vfma(vneg(fe), rw, fqb);
 }
 template <typename V>
 __device__ __forceinline__ void collide_v(V (&f)[kQ], V rho, V u, V v, V omega, float fxc, float fyc,
                                           const Phys& P) {
     const V uu0 = vmul(vfma(u, u, vmul(v, v)), splat<V>(P.inv_c2));
+    const V c0 = vfma(splat<V>(-1.5f), uu0, splat<V>(1.f));
     const V fx = vmul(vfma(splat<V>(-P.fr_dt), u, splat<V>(fxc)), splat<V>(P.dt));
     const V fy = vmul(vfma(splat<V>(-P.fr_dt), v, splat<V>(fyc)), splat<V>(P.dt));
     const V gx = vmul(splat<V>(P.u_ref), fx), gy = vmul(splat<V>(P.u_ref), fy);
     const V nomega = vneg(omega);
-    collide_q<0>(f[0], rho, u, v, uu0, nomega, gx, gy, P);
-    collide_q<1>(f[1], rho, u, v, uu0, nomega, gx, gy, P);
-    collide_q<2>(f[2], rho, u, v, uu0, nomega, gx, gy, P);
-    collide_q<3>(f[3], rho, u, v, uu0, nomega, gx, gy, P);
-    collide_q<4>(f[4], rho, u, v, uu0, nomega, gx, gy, P);
-    collide_q<5>(f[5], rho, u, v, uu0, nomega, gx, gy, P);
-    collide_q<6>(f[6], rho, u, v, uu0, nomega, gx, gy, P);
-    collide_q<7>(f[7], rho, u, v, uu0, nomega, gx, gy, P);
-    collide_q<8>(f[8], rho, u, v, uu0, nomega, gx, gy, P);
+    const V rw_axis = vmul(rho, splat<V>(w_q(1))), rw_diag = vmul(rho, splat<V>(w_q(0)));
+    collide_pair<0>(f[0], f[8], rw_diag, u, v, c0, nomega, gx, gy, P);
+    collide_pair<1>(f[1], f[7], rw_axis, u, v, c0, nomega, gx, gy, P);
+    collide_pair<2>(f[2], f[6], rw_diag, u, v, c0, nomega, gx, gy, P);
+    collide_pair<3>(f[3], f[5], rw_axis, u, v, c0, nomega, gx, gy, P);
+    const V feq4 = vmul(vmul(rho, splat<V>(w_q(4))), c0);  // uc = 0 at rest
+    f[4] = vfma(nomega, vsub(f[4], feq4), f[4]);
 }
 
 // the one-member forms the scalar kernels call
