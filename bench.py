@@ -386,6 +386,62 @@ def profile_cycles(args):
     ens.close()
 
 
+# The batched form: 8 concurrent independent OSSEs of uneven grid and ensemble sizes
+C3_EXPERIMENTS = [(128, 4), (128, 8), (256, 16), (256, 16), (256, 32), (512, 32), (512, 64), (1024, 64)]
+
+
+def run_batch(args):
+    """C3: every experiment is its own context (own stream, cycle graphs, autotuned
+    strip height); their cycles are issued round-robin and run concurrently on the GPU.
+    Device time: each context records events around the timed cycles after a full
+    synchronisation, so all start together; the batch time is the longest span."""
+    global NX, M
+    import lbl
+    T = STEPS_PER_CYCLE
+    K, W = args.steps, args.warmup
+    exps = []
+    for nx, m in C3_EXPERIMENTS:
+        NX, M = nx, m
+        obs, _ = make_observations(lbl, 1)
+        e = lbl.Ensemble(workload_config(lbl))
+        ty, ms_tuned = e.autotune()
+        e.init(0)
+        e.cycle_async(0, None, None, None, T)
+        e.cycle_async(T, *obs[0], T)  # observations resident from here on
+        exps.append({"nx": nx, "M": m, "ens": e, "strip_rows": ty, "ms_per_lbm_launch_tuned": ms_tuned})
+    for c in range(W):
+        for x in exps:
+            x["ens"].cycle_async((c + 2) * T, None, None, None, T)
+    for x in exps:
+        x["ens"].sync()
+    for x in exps:
+        x["ens"].event_record(0)
+    for c in range(K):
+        for x in exps:
+            x["ens"].cycle_async((W + c + 2) * T, None, None, None, T)
+    spans = []
+    for x in exps:
+        x["ens"].event_record(1)
+        spans.append(x["ens"].event_elapsed(0, 1))
+        x["ens"].sync()
+    ms = max(spans)
+    lu = sum(x["M"] * x["nx"] ** 2 for x in exps) * T * K
+    line = {"metric": "experiment DA cycles/s (C3 batch)", "value": len(exps) * K / (ms / 1e3), "unit": "cycles/s",
+            "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded nature runs + Gaussian observation noise)",
+            "config": {"workload": "C3: 8 concurrent DA_LETKF OSSEs, (grid, M) = " +
+                       ", ".join(f"{x['nx']}^2 x {x['M']}" for x in exps) +
+                       ", obs every 4th point, GC radius 4 cells, inflation 1.1, 100 LBM steps + 1 analysis per cycle",
+                       "concurrency": "one context, stream and per-cycle CUDA graph per experiment"},
+            "glups": lu / (ms / 1e3) / 1e9,
+            "experiments": [{"nx": x["nx"], "M": x["M"], "strip_rows": x["strip_rows"],
+                             "ms_per_lbm_launch_tuned": x["ms_per_lbm_launch_tuned"],
+                             "ms_per_cycle_in_batch": spans[i] / K} for i, x in enumerate(exps)]}
+    for x in exps:
+        x["ens"].close()
+    return line
+
+
 def lbm_sweep(args):
     """Stream-collide alone at the given grids (NXxM,...): back-to-back launches on the
     engine's stream, CUDA events, one JSON line per size.  Sizes whose population
@@ -419,8 +475,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="run warmup + steps cycles of the workload and exit (for ncu captures)")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="C1",
-                    help="C1 (the headline, 256^2 x 16) or C2 (512^2 x 64)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["C3"], default="C1",
+                    help="C1 (the headline, 256^2 x 16), C2 (512^2 x 64) or C3 (8 concurrent experiments)")
     ap.add_argument("--storage", choices=["f32", "f16"], default="f32",
                     help="population storage: f32, or the precision form's f16 deviations f - w_q")
     ap.add_argument("--lbm", default=None, metavar="NXxM[,NXxM...]",
@@ -429,12 +485,15 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     global NX, M, WORKLOAD, STORAGE
-    NX, M, WORKLOAD = WORKLOADS[args.workload]
+    NX, M, WORKLOAD = WORKLOADS.get(args.workload, WORKLOADS["C1"])
     STORAGE = 1 if args.storage == "f16" else 0
     if STORAGE:
         WORKLOAD = WORKLOAD.replace("FP32 storage", "FP16 deviation storage").replace(", FP32", ", FP16 deviation storage")
     if args.lbm:
         lbm_sweep(args)
+        return
+    if args.workload == "C3":
+        print(json.dumps(run_batch(args)), flush=True)
         return
     if args.profile:
         profile_cycles(args)

@@ -231,6 +231,13 @@ int lbl_event_elapsed(lbl_ctx* ctx, int slot_a, int slot_b, double* ms);
 int lbl_letkf_analysis_noalloc(const lbl_config* cfg, const float* f_in, float* f_out, float* mac_out,
                                const float* yo_sites, void* stream, int* host_stats, char* err, size_t err_cap);
 
+/* Tile autotuning for this context's grid and ensemble size: times the fused
+ * stream-collide on the rest state for candidate strip heights (rows per CTA) and
+ * keeps the fastest for every later step.  Call between lbl_create and lbl_init (it
+ * overwrites the populations).  *strip_rows / *ms_per_launch (optional) receive
+ * the choice and its time.  No counterpart in the reference. */
+int lbl_autotune(lbl_ctx* ctx, int* strip_rows, double* ms_per_launch);
+
 /* Directory prefix (config::prefix, "io" by default, config.h:287) under which the
  * LETKF matrix dumps go when cfg.write_mat is set: <prefix>/letkf/mat/ens<r>/
  * <label>.float_<rows>_<cols>_<batch>.<t>.h5 (letkf.cu:276-306, cu_matrix.hpp:97-117),

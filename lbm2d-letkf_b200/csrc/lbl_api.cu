@@ -1191,6 +1191,50 @@ int lbl_profile_step(lbl_ctx* ctx, int n, double* ms_per_launch) {
     return LBL_OK;
 }
 
+int lbl_autotune(lbl_ctx* ctx, int* strip_rows_out, double* ms_per_launch) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    if (ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_autotune runs between lbl_create and lbl_init");
+    // time the stream-collide on the rest state for candidate strip heights
+    launch_rest_state(ctx, ctx->stream);
+    LBL_CK(cudaGetLastError());
+    const float* force = ctx->d_force;
+    const int heuristic = lbm_strip_rows(ctx);
+    int best = heuristic;
+    double best_ms = 1e30;
+    // each candidate: the best of three samples of at least ~2 ms of back-to-back launches
+    auto sample = [&](int reps, double* ms_out) -> int {
+        LBL_CK(cudaEventRecord(ctx->ev[8], ctx->stream));
+        for (int k = 0; k < reps; k++) launch_lbm_step(ctx, k & 1, (k & 1) ^ 1, force, nullptr, ctx->stream);
+        LBL_CK(cudaEventRecord(ctx->ev[9], ctx->stream));
+        LBL_CK(cudaEventSynchronize(ctx->ev[9]));
+        LBL_CK(cudaGetLastError());
+        float ms = 0;
+        LBL_CK(cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]));
+        *ms_out = double(ms) / reps;
+        return LBL_OK;
+    };
+    for (int ty : {heuristic, 2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16, 20, 24, 32}) {
+        if (ty > ctx->P.ny) continue;
+        ctx->ty_tuned = ty;
+        double one = 0;
+        LBL_TRY(sample(2, &one));  // warm-up and a first estimate
+        const int reps = int(std::min(200.0, std::max(4.0, 2.0 / std::max(one, 1e-4))));
+        double t = 1e30;
+        for (int k = 0; k < 3; k++) {
+            double m = 0;
+            LBL_TRY(sample(reps, &m));
+            t = std::min(t, m);
+        }
+        if (t < best_ms * 0.99) { best_ms = t; best = ty; }
+    }
+    ctx->ty_tuned = best;
+    LBL_TRY(check_timeout(ctx));
+    if (strip_rows_out) *strip_rows_out = best;
+    if (ms_per_launch) *ms_per_launch = best_ms;
+    return LBL_OK;
+}
+
 int lbl_set_io_prefix(lbl_ctx* ctx, const char* io_prefix) {
     if (!ctx || !io_prefix) return LBL_ERR_ARG;
     ctx->io_prefix = io_prefix;

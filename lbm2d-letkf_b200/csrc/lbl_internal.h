@@ -127,6 +127,7 @@ struct lbl_ctx {
     // TMA descriptors of the two population buffers (input side of a step)
     CUtensorMap tmap[2];
     bool use_tma = false;
+    int ty_tuned = 0;                    // stream-collide strip height chosen by lbl_autotune (0: heuristic)
     int* d_err = nullptr;                // bounded-wait timeout flag of the TMA kernel
 
     // CUDA graphs keyed by (kind, n, parity)
@@ -148,6 +149,10 @@ void launch_ic_velocity(const double* modes /*[4][n]*/, int n_modes, int nx, int
 void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s);
 // one step from population buffer src to dst (FP32 or FP16 storage)
 void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s);
+// strip height of the stream-collide for this grid and ensemble (heuristic)
+int lbm_strip_rows(const lbl_ctx* c);
+// fill both population buffers with the rest state (rho = rho_ref, u = v = 0)
+void launch_rest_state(const lbl_ctx* c, cudaStream_t s);
 // FP16 deviation storage <-> FP32 populations, all members
 void launch_expand(const lbl_ctx* c, const __half* h, float* f, cudaStream_t s);
 void launch_compress(const lbl_ctx* c, const float* f, __half* h, cudaStream_t s);

@@ -851,7 +851,7 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
     const Phys& P = c->P;
     const int sq = (P.nx == P.ny) ? P.nx : 0;
 
-    const int ty = strip_rows(P, c->use_tma);
+    const int ty = c->ty_tuned > 0 ? c->ty_tuned : strip_rows(P, c->use_tma);
     dim3 grid((P.ny + ty - 1) / ty, P.M);
     if (c->use_tma) {
         float* fout = c->f[dst];
@@ -873,6 +873,23 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
         default:
             if (P.nx <= 256) launch_direct<256, 0>(c, grid, ty, src, dst, force, mac_out, s);
             else launch_direct<1024, 0>(c, grid, ty, src, dst, force, mac_out, s);
+    }
+}
+
+int lbm_strip_rows(const lbl_ctx* c) { return strip_rows(c->P, c->use_tma); }
+
+// rest state f = w_q rho_ref in every member of both buffers (FP16 storage: deviation 0)
+__global__ void rest_kernel(float* f, size_t n, int nxy, float rho) {
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x) * blockDim.x)
+        f[e] = w_q_rt(int((e / nxy) % kQ)) * rho;
+}
+void launch_rest_state(const lbl_ctx* c, cudaStream_t s) {
+    const size_t n = size_t(c->P.M) * kQ * c->P.nxy;
+    for (int b = 0; b < 2; b++) {
+        if (c->f16)
+            cudaMemsetAsync(c->h[b], 0, sizeof(__half) * n, s);
+        else
+            rest_kernel<<<4 * 148, 256, 0, s>>>(c->f[b], n, c->P.nxy, float(c->cfg.rho_ref));
     }
 }
 

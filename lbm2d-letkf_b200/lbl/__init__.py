@@ -49,7 +49,7 @@ EXPORTS = (
     "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_timer_csv", "lbl_timer_clear",
     "lbl_timer_transit", "lbl_profile_step", "lbl_get_cycle_phases", "lbl_event_record", "lbl_event_elapsed",
     "lbl_letkf_analysis_noalloc", "lbl_bindiff", "lbl_ensemble_stat", "lbl_energy_spectrum",
-    "lbl_set_io_prefix", "lbl_h5_write_dataset",
+    "lbl_set_io_prefix", "lbl_h5_write_dataset", "lbl_autotune",
 )
 
 
@@ -141,6 +141,7 @@ def load_library() -> ctypes.CDLL:
         "lbl_ensemble_stat": (I, [ctypes.c_char_p, ctypes.c_char_p, I, I, D, ctypes.c_char_p, U]),
         "lbl_energy_spectrum": (I, [F, F, I, I, D]),
         "lbl_set_io_prefix": (I, [P, ctypes.c_char_p]),
+        "lbl_autotune": (I, [P, IP, D]),
         "lbl_h5_write_dataset": (I, [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, P, I]),
     }
     for name, (res, args) in sig.items():
@@ -325,6 +326,12 @@ class Ensemble:
         ms = ctypes.c_double()
         self._check(self.lib.lbl_profile_step(self._h, n, ctypes.byref(ms)), "lbl_profile_step")
         return ms.value
+
+    def autotune(self) -> Tuple[int, float]:
+        """Pick the stream-collide strip height for this grid and ensemble (before init)."""
+        ty, ms = ctypes.c_int(), ctypes.c_double()
+        self._check(self.lib.lbl_autotune(self._h, ctypes.byref(ty), ctypes.byref(ms)), "lbl_autotune")
+        return ty.value, ms.value
 
     def set_io_prefix(self, prefix: str):
         """Directory prefix of the LETKF matrix dumps (cfg.write_mat)."""

@@ -210,3 +210,18 @@ def test_tma_variant_rejected_where_unsupported():
         lbl.Ensemble(lbl.config_default("NATURE", 384, 1, lbm_variant=lbl.LBM_TMA))
     assert ei.value.code == -8
 
+
+
+def test_autotune_changes_speed_not_results():
+    cfg = lbl.config_default("NATURE", 256, 3)
+    a, b = lbl.Ensemble(cfg), lbl.Ensemble(cfg)
+    ty, ms = a.autotune()
+    assert 2 <= ty <= 32 and ms > 0
+    for x in (a, b):
+        x.init(0)
+        x.update(0, 12)
+    for m in range(3):
+        np.testing.assert_array_equal(a.get_f(m), b.get_f(m))  # strip height never changes the arithmetic
+    with pytest.raises(lbl.LblError) as ei:
+        a.autotune()  # only before init
+    assert ei.value.code == -6
