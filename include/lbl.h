@@ -251,6 +251,54 @@ int lbl_set_io_prefix(lbl_ctx* ctx, const char* io_prefix);
  * (is_double), like H5Fcreate + H5LTmake_dataset (cu_matrix.hpp:108-117). */
 int lbl_h5_write_dataset(const char* path, uint64_t d0, uint64_t d1, uint64_t d2, const void* data, int is_double);
 
+/* Learned eddy-viscosity closure.  No counterpart in the reference, whose closure is
+ * the fixed Smagorinsky constant (lbm.cu:42-60).  A 6 -> 32 -> 32 -> 1 MLP (GELU,
+ * softplus output) maps six invariants of the resolved velocity gradient to a
+ * multiplier m >= 0 of the Smagorinsky viscosity, nu_t = m (cs dx)^2 |S|; m = 1 is
+ * plain Smagorinsky.  Parameters: LBL_CLOSURE_PARAMS floats, laid out W1[32][6],
+ * b1[32], W2[32][32], b2[32], W3[32], b3; they are used as BF16 with FP32 sums.
+ * Features (LBL_CLOSURE_FEATURES per cell), with k = dx^2 / nu_ref:
+ * log1p(k|S|), log1p(k|W|), (W:W - S:S)/(W:W + S:S), (S11 + S22)/sqrt(S:S),
+ * dx/dx_ref, asinh(k omega). */
+#define LBL_CLOSURE_PARAMS 1313
+#define LBL_CLOSURE_FEATURES 6
+
+/* Switch the context's stream-collide to the closure (params != NULL) or back to
+ * plain Smagorinsky (params == NULL).  nu_ref, dx_ref: the feature scales of the
+ * training (<= 0: this context's nu and h_ref/255).  Needs nx % 32 == 0, nx <= 1024
+ * and the direct-load stream-collide. */
+int lbl_set_closure(lbl_ctx* ctx, const float* params, double nu_ref, double dx_ref);
+
+/* Training data from the code's own runs: a run of the fine configuration (mode set
+ * to NATURE; every member a seeded random-phase IC) is spun up for `spinup` steps,
+ * then every `spacing` steps, n_snapshots times, each member's (u, v, uu, uv, vv) is
+ * box-filtered over filter x filter cells onto the coarse grid nx/filter.  Each
+ * coarse cell gives one sample: the features of the filtered velocity gradient
+ * (central differences, dx = h_ref/(ny/filter - 1), nu_ref = the fine run's nu,
+ * dx_ref = h_ref/255) and the target multiplier that makes the Smagorinsky stress
+ * match the filtered subgrid stress tau_d in the mean-square sense on that cell,
+ * m* = -(tau_d : S) / (2 S:S (cs dx)^2 |S|), clipped to [0, 8].  features
+ * [n][6], targets [n]; capacity >= n_ens * n_snapshots * (nx/filter)(ny/filter). */
+int lbl_closure_generate(const lbl_config* fine, int filter, int spinup, int n_snapshots, int spacing, int device,
+                         float* features, float* targets, size_t capacity, size_t* n_samples, char* err,
+                         size_t err_cap);
+
+/* Mean-square loss of the closure over n samples and its gradient with respect to
+ * the FP32 parameters (one fused forward/backward launch on the GPU). */
+int lbl_closure_grad(const float* params, const float* features, const float* targets, size_t n, int device,
+                     float* grad, float* loss);
+
+/* Adam training on the GPU: iters steps of `batch` samples drawn with replacement
+ * (seeded), learning rate lr, betas 0.9/0.999.  init (optional) starts from given
+ * parameters, else a seeded Xavier start with m = 1 everywhere.  params receives the
+ * FP32 result; loss_curve (optional, iters floats) the minibatch losses. */
+int lbl_closure_train(const float* features, const float* targets, size_t n, int iters, int batch, float lr,
+                      uint64_t seed, int device, const float* init, float* params, float* loss_curve);
+
+/* The closure's multiplier for n feature rows: path 0 = the tensor-core form used
+ * inside the stream-collide, path 1 = the per-thread FP32 form. */
+int lbl_closure_infer(const float* params, const float* features, size_t n, int path, int device, float* out);
+
 /* Evaluation measures over the files lbl_output writes (host only; no context, no
  * GPU).  err (optional) receives a message of at most err_cap bytes.
  *

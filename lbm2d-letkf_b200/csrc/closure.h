@@ -1,0 +1,244 @@
+// closure.h -- the learned eddy-viscosity closure shared by the stream-collide
+// (inference) and the closure data/training kernels.
+//
+// A 6 -> 32 -> 32 -> 1 MLP (GELU hidden layers, softplus output, 1313 parameters)
+// maps invariants of the resolved velocity gradient to a multiplier m >= 0 of the
+// Smagorinsky viscosity: nu_t = m (Cs dx)^2 |S|, so m = 1 is the plain Smagorinsky
+// closure the model falls back to.
+//
+// Arithmetic contract (the same in training and in the stream-collide): parameters
+// are BF16; the inputs of the two matrix layers (the features and the first hidden
+// activations) are rounded to BF16, as tensor-core operands are; every sum is
+// accumulated in FP32; GELU, the output dot product and softplus run in FP32.
+#pragma once
+#include <cuda_bf16.h>
+#include <cstdint>
+#include <cstring>
+
+namespace lbl {
+
+constexpr int kMlpIn = 6;
+constexpr int kMlpHid = 32;
+// parameter layout: W1[32][6], b1[32], W2[32][32], b2[32], W3[32], b3
+constexpr int kMlpW1 = 0;
+constexpr int kMlpB1 = kMlpW1 + kMlpHid * kMlpIn;
+constexpr int kMlpW2 = kMlpB1 + kMlpHid;
+constexpr int kMlpB2 = kMlpW2 + kMlpHid * kMlpHid;
+constexpr int kMlpW3 = kMlpB2 + kMlpHid;
+constexpr int kMlpB3 = kMlpW3 + kMlpHid;
+constexpr int kMlpParams = kMlpB3 + 1;  // 1313
+
+// Scales of the features: dx of the grid the closure runs on, the molecular
+// viscosity as the reference rate, and the reference grid spacing of the training.
+struct ClosureScales {
+    float dx, nu_ref, dx_ref;
+};
+
+// The six inputs from the velocity gradient (ux = du/dx, uy = du/dy, ...):
+//   x0 = log(1 + dx^2 |S| / nu_ref),  |S| = sqrt(2 S:S)
+//   x1 = log(1 + dx^2 |W| / nu_ref),  |W| = sqrt(2 W:W)
+//   x2 = (W:W - S:S) / (W:W + S:S)    strain / rotation balance
+//   x3 = (S11 + S22) / sqrt(S:S)      divergence relative to strain
+//   x4 = dx / dx_ref                  grid scale
+//   x5 = asinh(dx^2 omega / nu_ref)   signed vorticity, omega = vx - uy
+// Returns |S|.
+__host__ __device__ inline float closure_features(float ux, float uy, float vx, float vy, const ClosureScales& c,
+                                                  float* x) {
+    const float s11 = ux, s22 = vy, s12 = 0.5f * (uy + vx), w12 = 0.5f * (uy - vx);
+    const float ss = s11 * s11 + 2.f * s12 * s12 + s22 * s22;
+    const float ww = 2.f * w12 * w12;
+    const float smag = sqrtf(2.f * ss), wmag = sqrtf(2.f * ww);
+    const float k = c.dx * c.dx / c.nu_ref;
+    x[0] = log1pf(k * smag);
+    x[1] = log1pf(k * wmag);
+    x[2] = (ww - ss) / (ww + ss + 1e-30f);
+    x[3] = (s11 + s22) / sqrtf(ss + 1e-30f);
+    x[4] = c.dx / c.dx_ref;
+    x[5] = asinhf(k * (vx - uy));
+    return smag;
+}
+
+// GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))
+constexpr float kGeluK = 0.7978845608f, kGeluC = 0.044715f;
+__host__ __device__ inline float mlp_gelu(float x) {
+    const float t = tanhf(kGeluK * (x + kGeluC * x * x * x));
+    return 0.5f * x * (1.f + t);
+}
+__host__ __device__ inline float mlp_softplus(float z) { return z > 20.f ? z : log1pf(expf(z)); }
+__host__ __device__ inline float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// forward pass under the contract above (one cell): the Smagorinsky multiplier
+__device__ inline float mlp_forward(const __nv_bfloat16* __restrict__ p, const float* x_in) {
+    float x[kMlpIn], a1[kMlpHid];
+#pragma unroll
+    for (int k = 0; k < kMlpIn; k++) x[k] = bf16_round(x_in[k]);
+#pragma unroll 4
+    for (int i = 0; i < kMlpHid; i++) {
+        float h = __bfloat162float(p[kMlpB1 + i]);
+#pragma unroll
+        for (int k = 0; k < kMlpIn; k++) h = fmaf(__bfloat162float(p[kMlpW1 + i * kMlpIn + k]), x[k], h);
+        a1[i] = bf16_round(mlp_gelu(h));
+    }
+    float z = __bfloat162float(p[kMlpB3]);
+    for (int i = 0; i < kMlpHid; i++) {
+        float h = __bfloat162float(p[kMlpB2 + i]);
+#pragma unroll
+        for (int j = 0; j < kMlpHid; j++) h = fmaf(__bfloat162float(p[kMlpW2 + i * kMlpHid + j]), a1[j], h);
+        z = fmaf(__bfloat162float(p[kMlpW3 + i]), mlp_gelu(h), z);
+    }
+    return mlp_softplus(z);
+}
+
+// ---------------------------------------------------------------------------
+// Warp-cooperative inference on the tensor cores (mma.sync m16n8k16, BF16 in,
+// FP32 accumulate): the 32 lanes of a warp hold 32 cells, the warp evaluates the
+// network for all of them at once and returns each lane its own multiplier.
+//
+// The parameters are prepared once (closure_pack) in the fragment order of the
+// m16n8k16 operands, so that lane t reads its share with vector loads:
+//   u32 B1[32][4]   layer-1 B fragments (k = feature, n = hidden), one per n-tile
+//   u32 B2[32][16]  layer-2 B fragments, [n-tile][k-step][2]
+//   f32 C[32][24]   b1, b2, W3 at the accumulator columns of lane t: [n-tile][2] each
+//   f32 b3
+// ---------------------------------------------------------------------------
+constexpr int kPackB1 = 0;             // u32 offset of B1
+constexpr int kPackB2 = 32 * 4;        // u32 offset of B2
+constexpr int kPackC = kPackB2 + 32 * 16;  // f32 offset of the per-lane constants
+constexpr int kPackB3 = kPackC + 32 * 24;
+constexpr int kPackWords = kPackB3 + 4;    // 1412 words = 5648 B
+constexpr int kStageWords = 128;           // per-warp feature staging (32 lanes x 4 words)
+
+// round-to-nearest-even BF16 bits of a finite float (host side of the packing)
+inline uint32_t bf16_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return (u + 0x7FFFu + ((u >> 16) & 1u)) >> 16;
+}
+inline float bf16_value(float f) {
+    const uint32_t u = bf16_bits(f) << 16;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+// FP32 parameters (layout above) -> the fragment-ordered BF16 pack
+inline void closure_pack(const float* w, uint32_t* out) {
+    auto pk = [&](int lo, int hi) { return bf16_bits(w[lo]) | (bf16_bits(w[hi]) << 16); };
+    float* cf = reinterpret_cast<float*>(out);
+    for (int t = 0; t < 32; t++) {
+        const int g = t >> 2, c = t & 3;
+        for (int nt = 0; nt < 4; nt++) {
+            const int n = 8 * nt + g;  // hidden unit = the fragment's n column
+            out[kPackB1 + t * 4 + nt] = (2 * c < kMlpIn) ? pk(kMlpW1 + n * kMlpIn + 2 * c, kMlpW1 + n * kMlpIn + 2 * c + 1) : 0u;
+            for (int ks = 0; ks < 2; ks++) {
+                const int k0 = kMlpW2 + n * kMlpHid + 16 * ks + 2 * c;
+                out[kPackB2 + t * 16 + (nt * 2 + ks) * 2 + 0] = pk(k0, k0 + 1);
+                out[kPackB2 + t * 16 + (nt * 2 + ks) * 2 + 1] = pk(k0 + 8, k0 + 9);
+            }
+            for (int e = 0; e < 2; e++) {
+                const int col = 8 * nt + 2 * c + e;  // accumulator column of lane t
+                cf[kPackC + t * 24 + nt * 2 + e] = bf16_value(w[kMlpB1 + col]);
+                cf[kPackC + t * 24 + 8 + nt * 2 + e] = bf16_value(w[kMlpB2 + col]);
+                cf[kPackC + t * 24 + 16 + nt * 2 + e] = bf16_value(w[kMlpW3 + col]);
+            }
+        }
+    }
+    cf[kPackB3] = bf16_value(w[kMlpB3]);
+    out[kPackB3 + 1] = out[kPackB3 + 2] = out[kPackB3 + 3] = 0u;
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // .x (lo) is the low half
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+// MUFU tanh (PTX tanh.approx.f32, about 2^-11 relative error)
+__device__ __forceinline__ float tanh_mufu(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float gelu_mufu(float x) {
+    const float t = tanh_mufu(x * fmaf(kGeluK * kGeluC, x * x, kGeluK));
+    const float hx = 0.5f * x;
+    return fmaf(hx, t, hx);
+}
+// D += A (16x16, row) * B (16x8, col), BF16 operands, FP32 accumulators
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                               uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// The warp's 32 lanes each bring the features of one cell; every lane gets back its
+// cell's multiplier.  Rows of the m16 tiles are cells: tile mt row r = lane 16 mt + r.
+// pk: closure_pack output (shared or global memory, 16-byte aligned); stage: this
+// warp's kStageWords words of shared memory.  All 32 lanes must call it together.
+__device__ __forceinline__ float mlp_forward_warp(const uint32_t* __restrict__ pk, uint32_t* __restrict__ stage,
+                                                  const float* x) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+    __syncwarp();
+    reinterpret_cast<uint4*>(stage)[lane] =
+        make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]), pack_bf16x2(x[4], x[5]), 0u);
+    __syncwarp();
+    uint32_t xa[2][2];
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+        xa[mt][0] = stage[(16 * mt + g) * 4 + c];
+        xa[mt][1] = stage[(16 * mt + g + 8) * 4 + c];
+    }
+    const uint4 w1 = reinterpret_cast<const uint4*>(pk + kPackB1)[lane];
+    const uint32_t w1f[4] = {w1.x, w1.y, w1.z, w1.w};
+    const float4* cv = reinterpret_cast<const float4*>(pk + kPackC + lane * 24);
+    const float4 b1a = cv[0], b1b = cv[1], b2a = cv[2], b2b = cv[3], w3a = cv[4], w3b = cv[5];
+    const float b1[8] = {b1a.x, b1a.y, b1a.z, b1a.w, b1b.x, b1b.y, b1b.z, b1b.w};
+    const float b2[8] = {b2a.x, b2a.y, b2a.z, b2a.w, b2b.x, b2b.y, b2b.z, b2b.w};
+    const float w3[8] = {w3a.x, w3a.y, w3a.z, w3a.w, w3b.x, w3b.y, w3b.z, w3b.w};
+    // layer 1 (K = 6 of 16), GELU, BF16: the accumulators of n-tiles 2ks, 2ks+1 are
+    // the A fragment of layer 2's k-step ks
+    uint32_t a2[2][2][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            float h[4] = {b1[2 * nt], b1[2 * nt + 1], b1[2 * nt], b1[2 * nt + 1]};
+            mma_bf16_16816(h, xa[mt][0], xa[mt][1], 0u, 0u, w1f[nt], 0u);
+            a2[mt][nt >> 1][2 * (nt & 1) + 0] = pack_bf16x2(gelu_mufu(h[0]), gelu_mufu(h[1]));
+            a2[mt][nt >> 1][2 * (nt & 1) + 1] = pack_bf16x2(gelu_mufu(h[2]), gelu_mufu(h[3]));
+        }
+    // layer 2, GELU, and the output dot product of each row
+    float z[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+    const uint4* w2v = reinterpret_cast<const uint4*>(pk + kPackB2 + lane * 16);
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++) {
+        const uint4 w2 = w2v[nt];  // {ks0 b0, ks0 b1, ks1 b0, ks1 b1}
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++) {
+            float o[4] = {b2[2 * nt], b2[2 * nt + 1], b2[2 * nt], b2[2 * nt + 1]};
+            mma_bf16_16816(o, a2[mt][0][0], a2[mt][0][1], a2[mt][0][2], a2[mt][0][3], w2.x, w2.y);
+            mma_bf16_16816(o, a2[mt][1][0], a2[mt][1][1], a2[mt][1][2], a2[mt][1][3], w2.z, w2.w);
+            z[mt][0] = fmaf(gelu_mufu(o[0]), w3[2 * nt], z[mt][0]);
+            z[mt][0] = fmaf(gelu_mufu(o[1]), w3[2 * nt + 1], z[mt][0]);
+            z[mt][1] = fmaf(gelu_mufu(o[2]), w3[2 * nt], z[mt][1]);
+            z[mt][1] = fmaf(gelu_mufu(o[3]), w3[2 * nt + 1], z[mt][1]);
+        }
+    }
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int hh = 0; hh < 2; hh++) {
+            z[mt][hh] += __shfl_xor_sync(0xffffffffu, z[mt][hh], 1);
+            z[mt][hh] += __shfl_xor_sync(0xffffffffu, z[mt][hh], 2);
+        }
+    // lane 4 g + (2 mt + hh) of quad g offers row g + 8 hh of tile mt
+    const float offer = (c == 0) ? z[0][0] : (c == 1) ? z[0][1] : (c == 2) ? z[1][0] : z[1][1];
+    const int r = lane & 15;
+    const float zz = __shfl_sync(0xffffffffu, offer, 4 * (r & 7) + 2 * (lane >> 4) + (r >> 3));
+    return mlp_softplus(zz + reinterpret_cast<const float*>(pk)[kPackB3]);
+}
+#endif
+
+}  // namespace lbl

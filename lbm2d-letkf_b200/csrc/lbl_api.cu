@@ -584,6 +584,7 @@ void destroy_impl(lbl_ctx* ctx) {
     cudaFree(ctx->d_modes); cudaFree(ctx->d_amps); cudaFree(ctx->d_pool); cudaFree(ctx->d_force); cudaFree(ctx->d_sched);
     cudaFree(ctx->d_wtab); cudaFree(ctx->d_yo); cudaFree(ctx->d_dY); cudaFree(ctx->d_dyo);
     cudaFree(ctx->d_stats); cudaFree(ctx->d_red); cudaFree(ctx->d_tmp); cudaFree(ctx->d_err); cudaFree(ctx->d_dump);
+    cudaFree(ctx->d_closure);
     for (int b = 0; b < 2; b++) {
         if (ctx->h_yo[b]) cudaFreeHost(ctx->h_yo[b]);
         if (ctx->h_sched[b]) cudaFreeHost(ctx->h_sched[b]);

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/lbl.h"
+#include "closure.h"
 
 namespace lbl {
 
@@ -130,6 +131,11 @@ struct lbl_ctx {
     int ty_tuned = 0;                    // stream-collide strip height chosen by lbl_autotune (0: heuristic)
     int* d_err = nullptr;                // bounded-wait timeout flag of the TMA kernel
 
+    // learned closure (closure.h): fragment-ordered BF16 parameters, feature scales
+    uint32_t* d_closure = nullptr;       // [kPackWords]
+    bool closure = false;
+    lbl::ClosureScales closure_sc{};
+
     // CUDA graphs keyed by (kind, n, parity)
     std::map<long long, cudaGraphExec_t> graphs;
 
@@ -156,6 +162,8 @@ void launch_rest_state(const lbl_ctx* c, cudaStream_t s);
 // FP16 deviation storage <-> FP32 populations, all members
 void launch_expand(const lbl_ctx* c, const __half* h, float* f, cudaStream_t s);
 void launch_compress(const lbl_ctx* c, const float* f, __half* h, cudaStream_t s);
+// dynamic shared memory of the learned-closure stream-collide
+size_t closure_step_smem(int nx);
 int lbm_tma_prepare(int nx);
 bool lbm_tma_supported(int nx);
 void launch_macros(const lbl_ctx* c, int buf, float* mac, cudaStream_t s);

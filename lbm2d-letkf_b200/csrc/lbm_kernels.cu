@@ -195,6 +195,22 @@ __device__ __forceinline__ float les_omega(float ue, float uw, float ve, float v
     return les_omega_v<float>(ue, uw, ve, vw, un, us, vn, vs, P);
 }
 
+// Learned closure: the same central differences as les_omega_v give the features,
+// the warp's tensor cores evaluate the MLP for its 32 cells, and the multiplier m
+// scales the Smagorinsky eddy viscosity: nu_t = m cs^2 dx^2 |S|.
+__device__ __forceinline__ float closure_omega(float ue, float uw, float ve, float vw, float un, float us, float vn,
+                                               float vs, const Phys& P, const ClosureScales& csc,
+                                               const uint32_t* pack, uint32_t* stage) {
+    const float ux = (ue - uw) * P.inv_two_dx, uy = (un - us) * P.inv_two_dx;
+    const float vx = (ve - vw) * P.inv_two_dx, vy = (vn - vs) * P.inv_two_dx;
+    float feat[kMlpIn];
+    const float smag = closure_features(ux, uy, vx, vy, csc, feat);
+    const float m = mlp_forward_warp(pack, stage, feat);
+    const float nus = m * float(P.les_k * double(smag));
+    const float tau = float(fma(double(P.nu + nus), P.tau_k, 0.5));
+    return __frcp_rn(tau);
+}
+
 // ---------------------------------------------------------------------------
 // initial velocity from the stream-function modes (data.cu:76-110).  The sum is
 // accumulated in a float that receives each FP64 term, exactly like `real utmp`.
@@ -442,13 +458,20 @@ __global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __res
 // NX > 0 fixes the (square) grid at compile time so that plane and row offsets are
 // immediates; NX = 0 reads nx, ny from P.
 // ---------------------------------------------------------------------------
-template <bool WRITE_MAC, int MAXT, int NX, typename T>
+template <bool WRITE_MAC, int MAXT, int NX, typename T, bool CL = false>
 __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const T* __restrict__ fin, T* __restrict__ fout,
                                                         const float* __restrict__ force,
-                                                        float* __restrict__ mac, Phys P, int TY) {
-    extern __shared__ float s_uv[];  // [3][2][nx]
+                                                        float* __restrict__ mac, Phys P, int TY,
+                                                        const uint32_t* __restrict__ cpack, ClosureScales csc) {
+    extern __shared__ float s_uv[];  // [3][2][nx]; CL: + packed closure + per-warp staging
     const int nx = NX ? NX : P.nx, ny = NX ? NX : P.ny, nxy = NX ? NX * NX : P.nxy;
     const int x = threadIdx.x;
+    uint32_t* s_pack = reinterpret_cast<uint32_t*>(s_uv + 6 * nx);
+    uint32_t* s_stage = s_pack + kPackWords + (x >> 5) * kStageWords;
+    if (CL) {
+        for (int k = x; k < kPackWords; k += nx) s_pack[k] = cpack[k];
+        // made visible by the barrier of the first row
+    }
     const int m = blockIdx.y;
     const int j0 = blockIdx.x * TY;
     const int j1 = min(j0 + TY, ny);
@@ -503,7 +526,11 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const T* __restrict__ fi
         sb[x] = ub;
         sb[nx + x] = vb;
         __syncthreads();
-        const float omega = les_omega(sa[xp], sa[xm], sa[nx + xp], sa[nx + xm], ub, uc, vb, vc, P);
+        float omega;
+        if constexpr (CL)
+            omega = closure_omega(sa[xp], sa[xm], sa[nx + xp], sa[nx + xm], ub, uc, vb, vc, P, csc, s_pack, s_stage);
+        else
+            omega = les_omega(sa[xp], sa[xm], sa[nx + xp], sa[nx + xm], ub, uc, vb, vc, P);
         collide(fa, ra, ua, va, omega, Fx[ij], Fy[ij], P);
 #pragma unroll
         for (int q = 0; q < kQ; q++) Store<T>::st(fo + q * nxy + ij, fa[q], w_q(q));
@@ -826,9 +853,31 @@ void launch_direct_t(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout,
     const Phys& P = c->P;
     const size_t sm = sizeof(float) * 6 * P.nx;
     if (mac_out)
-        lbm_step_kernel<true, MAXT, NX, T><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty);
+        lbm_step_kernel<true, MAXT, NX, T><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty, nullptr, {});
     else
-        lbm_step_kernel<false, MAXT, NX, T><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty);
+        lbm_step_kernel<false, MAXT, NX, T><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty, nullptr, {});
+}
+
+// learned-closure variant (nx % 32 == 0 and nx <= 1024, checked by lbl_set_closure)
+template <int MAXT, int NX, typename T>
+void launch_closure_t(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout, const float* force,
+                      float* mac_out, cudaStream_t s) {
+    const Phys& P = c->P;
+    const size_t sm = closure_step_smem(P.nx);
+    if (mac_out)
+        lbm_step_kernel<true, MAXT, NX, T, true>
+            <<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty, c->d_closure, c->closure_sc);
+    else
+        lbm_step_kernel<false, MAXT, NX, T, true>
+            <<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty, c->d_closure, c->closure_sc);
+}
+template <int MAXT, int NX>
+void launch_closure(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
+                    cudaStream_t s) {
+    if (c->f16)
+        launch_closure_t<MAXT, NX, __half>(c, grid, ty, c->h[src], c->h[dst], force, mac_out, s);
+    else
+        launch_closure_t<MAXT, NX, float>(c, grid, ty, c->f[src], c->f[dst], force, mac_out, s);
 }
 
 template <int MAXT, int NX>
@@ -864,6 +913,12 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
         }
         return;
     }
+    if (c->closure) {
+        if (sq == 256) launch_closure<256, 256>(c, grid, ty, src, dst, force, mac_out, s);
+        else if (P.nx <= 256) launch_closure<256, 0>(c, grid, ty, src, dst, force, mac_out, s);
+        else launch_closure<1024, 0>(c, grid, ty, src, dst, force, mac_out, s);
+        return;
+    }
     switch (sq) {
         case 64: launch_direct<256, 64>(c, grid, ty, src, dst, force, mac_out, s); break;
         case 128: launch_direct<256, 128>(c, grid, ty, src, dst, force, mac_out, s); break;
@@ -877,6 +932,10 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
 }
 
 int lbm_strip_rows(const lbl_ctx* c) { return strip_rows(c->P, c->use_tma); }
+
+size_t closure_step_smem(int nx) {
+    return sizeof(float) * 6 * nx + sizeof(uint32_t) * (kPackWords + size_t(nx / 32) * kStageWords);
+}
 
 // rest state f = w_q rho_ref in every member of both buffers (FP16 storage: deviation 0)
 __global__ void rest_kernel(float* f, size_t n, int nxy, float rho) {

@@ -49,8 +49,10 @@ EXPORTS = (
     "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_timer_csv", "lbl_timer_clear",
     "lbl_timer_transit", "lbl_profile_step", "lbl_get_cycle_phases", "lbl_event_record", "lbl_event_elapsed",
     "lbl_letkf_analysis_noalloc", "lbl_bindiff", "lbl_ensemble_stat", "lbl_energy_spectrum",
-    "lbl_set_io_prefix", "lbl_h5_write_dataset", "lbl_autotune",
+    "lbl_set_io_prefix", "lbl_h5_write_dataset", "lbl_autotune", "lbl_set_closure", "lbl_closure_generate",
+    "lbl_closure_grad", "lbl_closure_train", "lbl_closure_infer",
 )
+CLOSURE_PARAMS, CLOSURE_FEATURES = 1313, 6
 
 
 class LblError(RuntimeError):
@@ -128,6 +130,11 @@ def load_library() -> ctypes.CDLL:
         "lbl_get_letkf_stats": (I, [P, IP, IP, IP, IP]),
         "lbl_get_diagnostics": (I, [P, I, D, D, D]),
         "lbl_rmse_uv": (I, [P, F, F, D]),
+        "lbl_set_closure": (I, [P, F, ctypes.c_double, ctypes.c_double]),
+        "lbl_closure_generate": (I, [CP, I, I, I, I, I, F, F, U, ctypes.POINTER(U), ctypes.c_char_p, U]),
+        "lbl_closure_grad": (I, [F, F, F, U, I, F, F]),
+        "lbl_closure_train": (I, [F, F, U, I, I, ctypes.c_float, ctypes.c_uint64, I, F, F, F]),
+        "lbl_closure_infer": (I, [F, F, U, I, I, F]),
         "lbl_timer_csv": (I, [P, I, ctypes.c_char_p, U]),
         "lbl_timer_clear": (I, [P, I]),
         "lbl_timer_transit": (I, [P, I, ctypes.c_char_p]),
@@ -333,6 +340,18 @@ class Ensemble:
         self._check(self.lib.lbl_autotune(self._h, ctypes.byref(ty), ctypes.byref(ms)), "lbl_autotune")
         return ty.value, ms.value
 
+    def set_closure(self, params=None, nu_ref: float = 0.0, dx_ref: float = 0.0):
+        """Learned eddy-viscosity closure in the stream-collide (params: 1313 floats), or
+        plain Smagorinsky again (params None).  nu_ref, dx_ref: the training's feature
+        scales (0: this run's nu and h_ref/255)."""
+        if params is None:
+            self._check(self.lib.lbl_set_closure(self._h, None, 0.0, 0.0), "lbl_set_closure")
+            return
+        w = np.ascontiguousarray(params, dtype=np.float32)
+        if w.size != CLOSURE_PARAMS:
+            raise ValueError(f"closure parameters: {w.size} values, expected {CLOSURE_PARAMS}")
+        self._check(self.lib.lbl_set_closure(self._h, _fp(w), float(nu_ref), float(dx_ref)), "lbl_set_closure")
+
     def set_io_prefix(self, prefix: str):
         """Directory prefix of the LETKF matrix dumps (cfg.write_mat)."""
         self._check(self.lib.lbl_set_io_prefix(self._h, prefix.encode()), "lbl_set_io_prefix")
@@ -423,3 +442,65 @@ def energy_spectrum(u, v) -> np.ndarray:
     if rc != 0:
         raise LblError(rc, "lbl_energy_spectrum")
     return ek
+
+
+# ---- learned closure: data, training, inference (no counterpart in the reference) ------
+
+def closure_generate(fine: Config, filter: int, spinup: int, n_snapshots: int, spacing: int,
+                     device: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    """(features [n][6], targets [n]) from box-filtered runs of the fine configuration."""
+    lib = load_library()
+    nc = (fine.nx // filter) * (fine.ny // filter) * fine.n_ens * n_snapshots
+    feat = np.empty((nc, CLOSURE_FEATURES), np.float32)
+    tgt = np.empty(nc, np.float32)
+    n = ctypes.c_size_t()
+    err = ctypes.create_string_buffer(512)
+    cfg = fine.copy()
+    rc = lib.lbl_closure_generate(ctypes.byref(cfg), filter, spinup, n_snapshots, spacing, device, _fp(feat),
+                                  _fp(tgt), nc, ctypes.byref(n), err, 512)
+    if rc != 0:
+        raise LblError(rc, err.value.decode())
+    return feat[: n.value], tgt[: n.value]
+
+
+def closure_grad(params, features, targets, device: int = 0) -> Tuple[float, np.ndarray]:
+    """Mean-square loss and its gradient (the GPU's fused forward/backward)."""
+    lib = load_library()
+    w = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.ascontiguousarray(features, dtype=np.float32)
+    t = np.ascontiguousarray(targets, dtype=np.float32)
+    g = np.empty(CLOSURE_PARAMS, np.float32)
+    loss = ctypes.c_float()
+    rc = lib.lbl_closure_grad(_fp(w), _fp(x), _fp(t), t.size, device, _fp(g), ctypes.byref(loss))
+    if rc != 0:
+        raise LblError(rc, "lbl_closure_grad")
+    return float(loss.value), g
+
+
+def closure_train(features, targets, iters: int, batch: int = 8192, lr: float = 1e-3, seed: int = 1,
+                  device: int = 0, init=None) -> Tuple[np.ndarray, np.ndarray]:
+    """Adam on the GPU; returns (parameters, minibatch loss curve)."""
+    lib = load_library()
+    x = np.ascontiguousarray(features, dtype=np.float32)
+    t = np.ascontiguousarray(targets, dtype=np.float32)
+    w = np.empty(CLOSURE_PARAMS, np.float32)
+    curve = np.empty(iters, np.float32)
+    w0 = None if init is None else np.ascontiguousarray(init, dtype=np.float32)
+    rc = lib.lbl_closure_train(_fp(x), _fp(t), t.size, iters, batch, lr, seed, device,
+                               None if w0 is None else _fp(w0), _fp(w), _fp(curve))
+    if rc != 0:
+        raise LblError(rc, "lbl_closure_train")
+    return w, curve
+
+
+def closure_infer(params, features, path: int = 0, device: int = 0) -> np.ndarray:
+    """Multipliers for feature rows: path 0 = the tensor-core form of the stream-collide,
+    path 1 = the per-thread FP32 form."""
+    lib = load_library()
+    w = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.ascontiguousarray(features, dtype=np.float32)
+    out = np.empty(x.shape[0], np.float32)
+    rc = lib.lbl_closure_infer(_fp(w), _fp(x), x.shape[0], path, device, _fp(out))
+    if rc != 0:
+        raise LblError(rc, "lbl_closure_infer")
+    return out

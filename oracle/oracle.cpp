@@ -111,9 +111,55 @@ struct orc_ctx {
     bool obs_engine_started = false;
     std::mt19937 baseline_rng;       // normals for baseline timing runs only
     int max_sweeps_seen = 0;
+    // learned closure (orc_set_closure): BF16-rounded parameters, feature scales
+    std::vector<double> cl_w;
+    double cl_nu_ref = 0, cl_dx_ref = 0;
 };
 
 namespace {
+
+// ---------------------------------------------------------------------------
+// learned closure: the 6-32-32-1 MLP of the engine's closure (parameter layout
+// W1[32][6], b1[32], W2[32][32], b2[32], W3[32], b3), evaluated in FP64 under the
+// engine's operand contract: BF16 parameters, BF16 features and BF16 first-layer
+// activations.  No counterpart in the reference (its closure is lbm.cu:42-60).
+// ---------------------------------------------------------------------------
+double bf16_round(double x) {
+    float f = float(x);
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u = ((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16) << 16;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+double gelu(double x) { return 0.5 * x * (1 + std::tanh(0.7978845608028654 * (x + 0.044715 * x * x * x))); }
+
+// w: BF16-rounded parameters; x: the six features
+double mlp_multiplier(const double* w, const double* x) {
+    double xb[6], a1[32];
+    for (int i = 0; i < 6; i++) xb[i] = bf16_round(x[i]);
+    for (int i = 0; i < 32; i++) {
+        double h = w[192 + i];
+        for (int j = 0; j < 6; j++) h += w[i * 6 + j] * xb[j];
+        a1[i] = bf16_round(gelu(h));
+    }
+    double z = w[1312];
+    for (int i = 0; i < 32; i++) {
+        double h = w[1248 + i];
+        for (int j = 0; j < 32; j++) h += w[224 + i * 32 + j] * a1[j];
+        z += w[1280 + i] * gelu(h);
+    }
+    return z > 20 ? z : std::log1p(std::exp(z));
+}
+
+double closure_multiplier(const orc_ctx* o, double ux, double uy, double vx, double vy, double dx) {
+    const double s12 = 0.5 * (uy + vx), w12 = 0.5 * (uy - vx);
+    const double ss = ux * ux + 2 * s12 * s12 + vy * vy, ww = 2 * w12 * w12;
+    const double k = dx * dx / o->cl_nu_ref;
+    const double x[6] = {std::log1p(k * std::sqrt(2 * ss)), std::log1p(k * std::sqrt(2 * ww)), (ww - ss) / (ww + ss + 1e-30),
+                         (ux + vy) / std::sqrt(ss + 1e-30), dx / o->cl_dx_ref, std::asinh(k * (vx - uy))};
+    return mlp_multiplier(o->cl_w.data(), x);
+}
 
 // ---------------------------------------------------------------------------
 // initial condition: src/data.cu:25-141 (reference spectrum) and the K4EXP variant
@@ -416,7 +462,8 @@ int orc_step_noforce(orc_ctx* o) {
                 const double vx = (vm[ije] - vm[ijw]) / (2 * d.dx), vy = (vm[ijn] - vm[ijs]) / (2 * d.dx);
                 const double s01 = 0.5 * (uy + vx);
                 const double ss = std::sqrt(2 * (ux * ux + 2 * s01 * s01 + vy * vy));
-                const double nus = d.cs * d.cs * d.dx * d.dx * ss;
+                double nus = d.cs * d.cs * d.dx * d.dx * ss;
+                if (!o->cl_w.empty()) nus *= closure_multiplier(o, ux, uy, vx, vy, d.dx);
                 const double nut = d.nu + nus;
                 const double tau = 0.5 + 3. * nut / d.c / d.c / d.dt;
                 const double omega = 1. / tau;
@@ -722,6 +769,25 @@ int orc_assimilate_rows(orc_ctx* o, const float* ro, const float* uo, const floa
 }
 
 int orc_max_sweeps(orc_ctx* o) { return o->max_sweeps_seen; }
+
+// the multiplier of n feature rows x [n][6] (FP64 under the BF16 operand contract)
+int orc_closure_forward(const float* params, const double* x, int n, double* out) {
+    std::vector<double> w(1313);
+    for (int k = 0; k < 1313; k++) w[k] = bf16_round(params[k]);
+    for (int i = 0; i < n; i++) out[i] = mlp_multiplier(w.data(), x + size_t(i) * 6);
+    return 0;
+}
+
+// learned closure in the steps (params: 1313 floats, NULL = plain Smagorinsky);
+// nu_ref, dx_ref <= 0 take this run's nu and h_ref/255 like lbl_set_closure
+int orc_set_closure(orc_ctx* o, const float* params, double nu_ref, double dx_ref) {
+    if (!params) { o->cl_w.clear(); return 0; }
+    o->cl_w.resize(1313);
+    for (int k = 0; k < 1313; k++) o->cl_w[k] = bf16_round(params[k]);
+    o->cl_nu_ref = nu_ref > 0 ? nu_ref : double(float(o->d.nu));
+    o->cl_dx_ref = dx_ref > 0 ? dx_ref : o->cfg.h_ref / 255.0;
+    return 0;
+}
 
 // DA_NUDGING (nudging.cu:40-143): f <- alpha feq(rho_o, u_o, v_o) + (1 - alpha) f for every
 // member, in FP64.  ro, uo, vo are full fields (NaN off the p-lattice, never read);

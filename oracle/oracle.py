@@ -53,6 +53,8 @@ def load():
         "orc_assimilate_rows": (I, [P, F, F, F, D, I, I]),
         "orc_max_sweeps": (I, [P]),
         "orc_nudge": (I, [P, F, F, F]),
+        "orc_set_closure": (I, [P, F, ctypes.c_double, ctypes.c_double]),
+        "orc_closure_forward": (I, [F, D, I, D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -94,6 +96,15 @@ def force_modes(cfg):
     kx, ky, amp = (np.empty(128, np.float32) for _ in range(3))
     n = lib.orc_force_modes(ctypes.byref(cfg), _f(kx), _f(ky), _f(amp), 128)
     return kx[:n].copy(), ky[:n].copy(), amp[:n].copy()
+
+
+def closure_forward(params, x):
+    """The C++ oracle's closure multiplier for feature rows x [n][6]."""
+    lib = load()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty(x.shape[0], np.float64)
+    lib.orc_closure_forward(_f(_f32(params)), _d(x), x.shape[0], _d(out))
+    return out
 
 
 def vorticity(cfg, u, v):
@@ -174,6 +185,12 @@ class Oracle:
 
     def assimilate_rows(self, rho_o, u_o, v_o, j0: int, j1: int):
         return self.lib.orc_assimilate_rows(self.h, _f(_f32(rho_o)), _f(_f32(u_o)), _f(_f32(v_o)), None, j0, j1)
+
+    def set_closure(self, params=None, nu_ref: float = 0.0, dx_ref: float = 0.0):
+        """Learned eddy-viscosity multiplier in the steps (1313 parameters; None = plain
+        Smagorinsky), FP64 under the engine's BF16 operand contract."""
+        w = None if params is None else _f32(params)
+        return self.lib.orc_set_closure(self.h, None if w is None else _f(w), float(nu_ref), float(dx_ref))
 
     def nudge(self, rho_o, u_o, v_o):
         """DA_NUDGING (nudging.cu:40-143) of every member, FP64."""
