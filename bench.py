@@ -442,6 +442,13 @@ def run_batch(args):
     return line
 
 
+def closure_params():
+    """(params, nu_ref, dx_ref) of the trained closure shipped with the package."""
+    from lbl import closure
+    w, meta = closure.load_params()
+    return w, meta["nu_ref"], meta["dx_ref"]
+
+
 def lbm_sweep(args):
     """Stream-collide alone at the given grids (NXxM,...): back-to-back launches on the
     engine's stream, CUDA events, one JSON line per size.  Sizes whose population
@@ -451,6 +458,8 @@ def lbm_sweep(args):
         nx, m = (int(v) for v in spec.lower().split("x"))
         e = lbl.Ensemble(lbl.config_default("NATURE", nx, m, storage=STORAGE))
         e.init(0)
+        if args.closure:
+            e.set_closure(*closure_params())
         e.update(0, 2)
         e.profile_step(max(3, args.warmup))
         ms = e.profile_step(max(1, args.steps))
@@ -459,6 +468,7 @@ def lbm_sweep(args):
         gbs = bytes_launch / (ms * 1e-3) / 1e9
         print(json.dumps({"lbm_stream_collide": {
             "nx": nx, "ny": nx, "members": m, "storage": "f16 deviations" if STORAGE else "f32",
+            "closure": "mlp" if args.closure else "smagorinsky",
             "launches": args.steps, "ms_per_launch": ms,
             "glups": m * nx * nx / (ms * 1e-3) / 1e9, "algorithmic_bytes_per_launch": bytes_launch,
             "population_buffer_mb": bytes_launch / 2 / 1e6, "achieved_gbs": gbs, "peak_gbs": peak,
@@ -481,6 +491,8 @@ def main():
                     help="population storage: f32, or the precision form's f16 deviations f - w_q")
     ap.add_argument("--lbm", default=None, metavar="NXxM[,NXxM...]",
                     help="time the stream-collide alone at these grids and exit")
+    ap.add_argument("--closure", action="store_true",
+                    help="with --lbm: the learned-closure stream-collide (trained parameters of the package)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -8,8 +8,8 @@
 //   lbl_closure_grad      loss and gradient over a sample set (fused forward/backward)
 //   lbl_closure_train     Adam on random minibatches with the same fused kernel
 //
-// The network keeps FP32 master parameters and computes with their BF16 copies,
-// accumulating in FP32 (the precision of the inference inside the stream-collide).
+// The network keeps FP32 master parameters and computes with their BF16 copies under
+// the operand contract of closure.h (FP16 matrix operands, FP32 sums).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(32 * kTrainWarps) mlp_grad_kernel(const __nv_b
     extern __shared__ float smem[];
     float* p = smem;                                             // parameters as float
     Stage* st = reinterpret_cast<Stage*>(smem + ((kMlpParams + 3) & ~3));
-    for (int k = threadIdx.x; k < kMlpParams; k += blockDim.x) p[k] = __bfloat162float(pw[k]);
+    for (int k = threadIdx.x; k < kMlpParams; k += blockDim.x) p[k] = param_value(pw, k);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Stage& S = st[warp];
@@ -140,14 +140,14 @@ __global__ void __launch_bounds__(32 * kTrainWarps) mlp_grad_kernel(const __nv_b
         if (valid) sample = idx_seed ? size_t(hash32(idx_seed * 0x9E3779B97F4A7C15ull + uint64_t(s)) % n) : size_t(s);
         float x[kMlpIn], h1[kMlpHid], a1[kMlpHid], h2[kMlpHid];
 #pragma unroll
-        for (int k = 0; k < kMlpIn; k++) x[k] = valid ? bf16_round(feat[sample * kMlpIn + k]) : 0.f;
+        for (int k = 0; k < kMlpIn; k++) x[k] = valid ? f16_round(feat[sample * kMlpIn + k]) : 0.f;
 #pragma unroll
         for (int i = 0; i < kMlpHid; i++) {
             float h = p[kMlpB1 + i];
 #pragma unroll
             for (int k = 0; k < kMlpIn; k++) h = fmaf(p[kMlpW1 + i * kMlpIn + k], x[k], h);
             h1[i] = h;
-            a1[i] = bf16_round(mlp_gelu(h));  // the layer-2 operand (gradient passes straight through)
+            a1[i] = f16_round(mlp_gelu(h));  // the layer-2 operand (gradient passes straight through)
         }
         float z = p[kMlpB3];
 #pragma unroll 4
@@ -431,8 +431,8 @@ int lbl_set_closure(lbl_ctx* ctx, const float* params, double nu_ref, double dx_
     if (!ctx) return LBL_ERR_ARG;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return LBL_ERR_CUDA;
     if (params) {
-        if (ctx->P.nx % 32 != 0 || ctx->P.nx > 1024) {
-            ctx->err = "the learned closure needs nx a multiple of 32 and at most 1024";
+        if (ctx->P.nx % 32 != 0) {  // whole warps of cells
+            ctx->err = "the learned closure needs nx a multiple of 32";
             return LBL_ERR_UNSUPPORTED;
         }
         if (ctx->use_tma) {

@@ -7,11 +7,15 @@
 // closure the model falls back to.
 //
 // Arithmetic contract (the same in training and in the stream-collide): parameters
-// are BF16; the inputs of the two matrix layers (the features and the first hidden
-// activations) are rounded to BF16, as tensor-core operands are; every sum is
-// accumulated in FP32; GELU, the output dot product and softplus run in FP32.
+// are BF16 values.  The two matrix layers run on FP16 tensor-core operands: their
+// weights are those BF16 values carried in FP16 (exact for |w| >= 2^-14), and their
+// inputs -- the features and the first hidden activations -- are rounded to FP16.
+// Every sum is accumulated in FP32; the output dot product and softplus run in FP32.
+// GELU is FP32 (tanhf) in training and in the per-thread form; the stream-collide
+// evaluates it on pairs in FP16 arithmetic with the MUFU tanh (about 1e-3 relative).
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cstdint>
 #include <cstring>
 
@@ -65,39 +69,44 @@ __host__ __device__ inline float mlp_gelu(float x) {
     return 0.5f * x * (1.f + t);
 }
 __host__ __device__ inline float mlp_softplus(float z) { return z > 20.f ? z : log1pf(expf(z)); }
-__host__ __device__ inline float bf16_round(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+__host__ __device__ inline float f16_round(float x) { return __half2float(__float2half_rn(x)); }
+// a parameter as the network uses it: BF16, and for the matrix weights also FP16
+__host__ __device__ inline float param_value(const __nv_bfloat16* p, int k) {
+    const float w = __bfloat162float(p[k]);
+    return (k < kMlpB1 || (k >= kMlpW2 && k < kMlpB2)) ? f16_round(w) : w;
+}
 
 // forward pass under the contract above (one cell): the Smagorinsky multiplier
 __device__ inline float mlp_forward(const __nv_bfloat16* __restrict__ p, const float* x_in) {
     float x[kMlpIn], a1[kMlpHid];
 #pragma unroll
-    for (int k = 0; k < kMlpIn; k++) x[k] = bf16_round(x_in[k]);
+    for (int k = 0; k < kMlpIn; k++) x[k] = f16_round(x_in[k]);
 #pragma unroll 4
     for (int i = 0; i < kMlpHid; i++) {
-        float h = __bfloat162float(p[kMlpB1 + i]);
+        float h = param_value(p, kMlpB1 + i);
 #pragma unroll
-        for (int k = 0; k < kMlpIn; k++) h = fmaf(__bfloat162float(p[kMlpW1 + i * kMlpIn + k]), x[k], h);
-        a1[i] = bf16_round(mlp_gelu(h));
+        for (int k = 0; k < kMlpIn; k++) h = fmaf(param_value(p, kMlpW1 + i * kMlpIn + k), x[k], h);
+        a1[i] = f16_round(mlp_gelu(h));
     }
-    float z = __bfloat162float(p[kMlpB3]);
+    float z = param_value(p, kMlpB3);
     for (int i = 0; i < kMlpHid; i++) {
-        float h = __bfloat162float(p[kMlpB2 + i]);
+        float h = param_value(p, kMlpB2 + i);
 #pragma unroll
-        for (int j = 0; j < kMlpHid; j++) h = fmaf(__bfloat162float(p[kMlpW2 + i * kMlpHid + j]), a1[j], h);
-        z = fmaf(__bfloat162float(p[kMlpW3 + i]), mlp_gelu(h), z);
+        for (int j = 0; j < kMlpHid; j++) h = fmaf(param_value(p, kMlpW2 + i * kMlpHid + j), a1[j], h);
+        z = fmaf(param_value(p, kMlpW3 + i), mlp_gelu(h), z);
     }
     return mlp_softplus(z);
 }
 
 // ---------------------------------------------------------------------------
-// Warp-cooperative inference on the tensor cores (mma.sync m16n8k16, BF16 in,
+// Warp-cooperative inference on the tensor cores (mma.sync m16n8k16, FP16 in,
 // FP32 accumulate): the 32 lanes of a warp hold 32 cells, the warp evaluates the
 // network for all of them at once and returns each lane its own multiplier.
 //
 // The parameters are prepared once (closure_pack) in the fragment order of the
 // m16n8k16 operands, so that lane t reads its share with vector loads:
-//   u32 B1[32][4]   layer-1 B fragments (k = feature, n = hidden), one per n-tile
-//   u32 B2[32][16]  layer-2 B fragments, [n-tile][k-step][2]
+//   u32 B1[32][4]   layer-1 B fragments (k = feature, n = hidden), one per n-tile, FP16x2
+//   u32 B2[32][16]  layer-2 B fragments, [n-tile][k-step][2], FP16x2
 //   f32 C[32][24]   b1, b2, W3 at the accumulator columns of lane t: [n-tile][2] each
 //   f32 b3
 // ---------------------------------------------------------------------------
@@ -108,22 +117,26 @@ constexpr int kPackB3 = kPackC + 32 * 24;
 constexpr int kPackWords = kPackB3 + 4;    // 1412 words = 5648 B
 constexpr int kStageWords = 128;           // per-warp feature staging (32 lanes x 4 words)
 
-// round-to-nearest-even BF16 bits of a finite float (host side of the packing)
-inline uint32_t bf16_bits(float f) {
+// round-to-nearest-even BF16 value of a finite float (host side of the packing)
+inline float bf16_value(float f) {
     uint32_t u;
     std::memcpy(&u, &f, 4);
-    return (u + 0x7FFFu + ((u >> 16) & 1u)) >> 16;
-}
-inline float bf16_value(float f) {
-    const uint32_t u = bf16_bits(f) << 16;
+    u = ((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16) << 16;
     float r;
     std::memcpy(&r, &u, 4);
     return r;
 }
+// FP16 bits of the BF16 value of f (a matrix weight as the tensor cores take it)
+inline uint32_t weight_bits(float f) {
+    const __half h = __float2half_rn(bf16_value(f));
+    uint16_t b;
+    std::memcpy(&b, &h, 2);
+    return b;
+}
 
-// FP32 parameters (layout above) -> the fragment-ordered BF16 pack
+// FP32 parameters (layout above) -> the fragment-ordered pack
 inline void closure_pack(const float* w, uint32_t* out) {
-    auto pk = [&](int lo, int hi) { return bf16_bits(w[lo]) | (bf16_bits(w[hi]) << 16); };
+    auto pk = [&](int lo, int hi) { return weight_bits(w[lo]) | (weight_bits(w[hi]) << 16); };
     float* cf = reinterpret_cast<float*>(out);
     for (int t = 0; t < 32; t++) {
         const int g = t >> 2, c = t & 3;
@@ -148,26 +161,29 @@ inline void closure_pack(const float* w, uint32_t* out) {
 }
 
 #ifdef __CUDACC__
-__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
-    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // .x (lo) is the low half
+__device__ __forceinline__ uint32_t pack_f16x2(float lo, float hi) {
+    const __half2 v = __floats2half2_rn(lo, hi);  // .x (lo) is the low half
     return *reinterpret_cast<const uint32_t*>(&v);
 }
-// MUFU tanh (PTX tanh.approx.f32, about 2^-11 relative error)
-__device__ __forceinline__ float tanh_mufu(float x) {
-    float y;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
+__device__ __forceinline__ __half2 as_h2(uint32_t u) { return *reinterpret_cast<const __half2*>(&u); }
+__device__ __forceinline__ uint32_t as_u32(__half2 h) { return *reinterpret_cast<const uint32_t*>(&h); }
+// GELU of a pair in FP16 arithmetic, MUFU tanh (PTX tanh.approx.f16x2).  Past
+// |x| = 256, x^2 overflows to inf, tanh gives +-1 and the result is x or 0, the
+// function's own limits.
+__device__ __forceinline__ uint32_t gelu_f16x2(uint32_t xu) {
+    const __half2 x = as_h2(xu);
+    const __half2 inner = __hfma2(__hmul2(x, x), __float2half2_rn(kGeluK * kGeluC), __float2half2_rn(kGeluK));
+    const uint32_t yu = as_u32(__hmul2(x, inner));
+    uint32_t tu;
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(tu) : "r"(yu));
+    const __half2 hx = __hmul2(x, __float2half2_rn(0.5f));
+    return as_u32(__hfma2(hx, as_h2(tu), hx));
 }
-__device__ __forceinline__ float gelu_mufu(float x) {
-    const float t = tanh_mufu(x * fmaf(kGeluK * kGeluC, x * x, kGeluK));
-    const float hx = 0.5f * x;
-    return fmaf(hx, t, hx);
-}
-// D += A (16x16, row) * B (16x8, col), BF16 operands, FP32 accumulators
-__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                               uint32_t b0, uint32_t b1) {
+// D += A (16x16, row) * B (16x8, col), FP16 operands, FP32 accumulators
+__device__ __forceinline__ void mma_f16_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                              uint32_t b0, uint32_t b1) {
     asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
         "{%0,%1,%2,%3};"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
@@ -182,7 +198,7 @@ __device__ __forceinline__ float mlp_forward_warp(const uint32_t* __restrict__ p
     const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
     __syncwarp();
     reinterpret_cast<uint4*>(stage)[lane] =
-        make_uint4(pack_bf16x2(x[0], x[1]), pack_bf16x2(x[2], x[3]), pack_bf16x2(x[4], x[5]), 0u);
+        make_uint4(pack_f16x2(x[0], x[1]), pack_f16x2(x[2], x[3]), pack_f16x2(x[4], x[5]), 0u);
     __syncwarp();
     uint32_t xa[2][2];
 #pragma unroll
@@ -197,19 +213,19 @@ __device__ __forceinline__ float mlp_forward_warp(const uint32_t* __restrict__ p
     const float b1[8] = {b1a.x, b1a.y, b1a.z, b1a.w, b1b.x, b1b.y, b1b.z, b1b.w};
     const float b2[8] = {b2a.x, b2a.y, b2a.z, b2a.w, b2b.x, b2b.y, b2b.z, b2b.w};
     const float w3[8] = {w3a.x, w3a.y, w3a.z, w3a.w, w3b.x, w3b.y, w3b.z, w3b.w};
-    // layer 1 (K = 6 of 16), GELU, BF16: the accumulators of n-tiles 2ks, 2ks+1 are
-    // the A fragment of layer 2's k-step ks
+    // layer 1 (K = 6 of 16) and GELU in FP16 pairs: the accumulators of n-tiles 2ks,
+    // 2ks+1 are the A fragment of layer 2's k-step ks
     uint32_t a2[2][2][4];
 #pragma unroll
     for (int mt = 0; mt < 2; mt++)
 #pragma unroll
         for (int nt = 0; nt < 4; nt++) {
             float h[4] = {b1[2 * nt], b1[2 * nt + 1], b1[2 * nt], b1[2 * nt + 1]};
-            mma_bf16_16816(h, xa[mt][0], xa[mt][1], 0u, 0u, w1f[nt], 0u);
-            a2[mt][nt >> 1][2 * (nt & 1) + 0] = pack_bf16x2(gelu_mufu(h[0]), gelu_mufu(h[1]));
-            a2[mt][nt >> 1][2 * (nt & 1) + 1] = pack_bf16x2(gelu_mufu(h[2]), gelu_mufu(h[3]));
+            mma_f16_16816(h, xa[mt][0], xa[mt][1], 0u, 0u, w1f[nt], 0u);
+            a2[mt][nt >> 1][2 * (nt & 1) + 0] = gelu_f16x2(pack_f16x2(h[0], h[1]));
+            a2[mt][nt >> 1][2 * (nt & 1) + 1] = gelu_f16x2(pack_f16x2(h[2], h[3]));
         }
-    // layer 2, GELU, and the output dot product of each row
+    // layer 2, GELU, and the output dot product of each row (FP32)
     float z[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
     const uint4* w2v = reinterpret_cast<const uint4*>(pk + kPackB2 + lane * 16);
 #pragma unroll
@@ -218,12 +234,12 @@ __device__ __forceinline__ float mlp_forward_warp(const uint32_t* __restrict__ p
 #pragma unroll
         for (int mt = 0; mt < 2; mt++) {
             float o[4] = {b2[2 * nt], b2[2 * nt + 1], b2[2 * nt], b2[2 * nt + 1]};
-            mma_bf16_16816(o, a2[mt][0][0], a2[mt][0][1], a2[mt][0][2], a2[mt][0][3], w2.x, w2.y);
-            mma_bf16_16816(o, a2[mt][1][0], a2[mt][1][1], a2[mt][1][2], a2[mt][1][3], w2.z, w2.w);
-            z[mt][0] = fmaf(gelu_mufu(o[0]), w3[2 * nt], z[mt][0]);
-            z[mt][0] = fmaf(gelu_mufu(o[1]), w3[2 * nt + 1], z[mt][0]);
-            z[mt][1] = fmaf(gelu_mufu(o[2]), w3[2 * nt], z[mt][1]);
-            z[mt][1] = fmaf(gelu_mufu(o[3]), w3[2 * nt + 1], z[mt][1]);
+            mma_f16_16816(o, a2[mt][0][0], a2[mt][0][1], a2[mt][0][2], a2[mt][0][3], w2.x, w2.y);
+            mma_f16_16816(o, a2[mt][1][0], a2[mt][1][1], a2[mt][1][2], a2[mt][1][3], w2.z, w2.w);
+            const float2 g0 = __half22float2(as_h2(gelu_f16x2(pack_f16x2(o[0], o[1]))));
+            const float2 g1 = __half22float2(as_h2(gelu_f16x2(pack_f16x2(o[2], o[3]))));
+            z[mt][0] = fmaf(g0.x, w3[2 * nt], fmaf(g0.y, w3[2 * nt + 1], z[mt][0]));
+            z[mt][1] = fmaf(g1.x, w3[2 * nt], fmaf(g1.y, w3[2 * nt + 1], z[mt][1]));
         }
     }
 #pragma unroll

@@ -142,8 +142,13 @@ int validate(const lbl_config& c, std::string& err) {
     if (c.storage == LBL_STORAGE_F16 && c.lbm_variant == LBL_LBM_TMA) {
         err = "the TMA stream-collide reads FP32 populations only"; return LBL_ERR_UNSUPPORTED;
     }
-    if (c.nx < 32 || c.ny < 8 || c.nx > 1024 || c.nx % 32 != 0) {
-        err = "nx must be a multiple of 32 in [32, 1024] and ny >= 8"; return LBL_ERR_ARG;
+    if (c.nx < 32 || c.ny < 8 || c.nx % 32 != 0 || cluster_chunks(c.nx) == 0) {
+        err = "nx must be a multiple of 32 up to 1024, or a multiple of 256 up to 8192 with nx/256 <= 8, "
+              "nx/512 <= 8 or nx/1024 <= 8 (rows split over a cluster), and ny >= 8";
+        return LBL_ERR_ARG;
+    }
+    if (c.nx > 1024 && c.mode != LBL_MODE_NATURE && c.mode != LBL_MODE_OBSERVE) {
+        err = "grids wider than 1024 run NATURE and OBSERVE in this build"; return LBL_ERR_UNSUPPORTED;
     }
     if (c.n_ens < 1) { err = "n_ens must be >= 1"; return LBL_ERR_ARG; }
     if (c.iiter < 1 || c.ioprune < 1 || c.daprune < 1) { err = "iiter/ioprune/daprune must be >= 1"; return LBL_ERR_ARG; }

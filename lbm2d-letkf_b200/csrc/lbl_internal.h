@@ -162,8 +162,11 @@ void launch_rest_state(const lbl_ctx* c, cudaStream_t s);
 // FP16 deviation storage <-> FP32 populations, all members
 void launch_expand(const lbl_ctx* c, const __half* h, float* f, cudaStream_t s);
 void launch_compress(const lbl_ctx* c, const float* f, __half* h, cudaStream_t s);
-// dynamic shared memory of the learned-closure stream-collide
+// dynamic shared memory of the learned-closure stream-collide for rows of nx columns
 size_t closure_step_smem(int nx);
+// CTAs per row of the stream-collide: 1 up to 1024 columns, else a cluster of up to
+// 8 CTAs of 1024, 512 or 256 columns; 0 = unsupported width
+int cluster_chunks(int nx);
 int lbm_tma_prepare(int nx);
 bool lbm_tma_supported(int nx);
 void launch_macros(const lbl_ctx* c, int buf, float* mac, cudaStream_t s);

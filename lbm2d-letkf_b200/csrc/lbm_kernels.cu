@@ -12,6 +12,8 @@
 //   lbm_step_kernel     fused pull streaming + macros + Smagorinsky + BGK + force
 //                       (lbm.cu:24-160, lbm.h:31-109, lbm_collision_srt.h:8-16)
 //   macros_kernel       rho,u,v moments of f (lbm.h:72-109)
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 
@@ -458,19 +460,33 @@ __global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __res
 // NX > 0 fixes the (square) grid at compile time so that plane and row offsets are
 // immediates; NX = 0 reads nx, ny from P.
 // ---------------------------------------------------------------------------
-template <bool WRITE_MAC, int MAXT, int NX, typename T, bool CL = false>
+template <bool WRITE_MAC, int MAXT, int NX, typename T, bool CL = false, bool CLU = false>
 __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const T* __restrict__ fin, T* __restrict__ fout,
                                                         const float* __restrict__ force,
                                                         float* __restrict__ mac, Phys P, int TY,
                                                         const uint32_t* __restrict__ cpack, ClosureScales csc) {
-    extern __shared__ float s_uv[];  // [3][2][nx]; CL: + packed closure + per-warp staging
+    // CLU: rows wider than one CTA.  The cluster's CTAs (blockIdx.z = chunk) each take
+    // blockDim.x columns of the same strip and read the (u, v) of the neighbour
+    // columns across a chunk edge from the neighbour CTA's ring (distributed shared
+    // memory); the per-row barrier becomes a cluster barrier.
+    extern __shared__ float s_uv[];  // [3][2][W]; CL: + packed closure + per-warp staging
     const int nx = NX ? NX : P.nx, ny = NX ? NX : P.ny, nxy = NX ? NX * NX : P.nxy;
-    const int x = threadIdx.x;
-    uint32_t* s_pack = reinterpret_cast<uint32_t*>(s_uv + 6 * nx);
-    uint32_t* s_stage = s_pack + kPackWords + (x >> 5) * kStageWords;
+    const int W = CLU ? int(blockDim.x) : nx;  // columns of this CTA
+    const int xl = threadIdx.x;
+    const int x = CLU ? int(blockIdx.z) * W + xl : xl;
+    uint32_t* s_pack = reinterpret_cast<uint32_t*>(s_uv + 6 * W);
+    uint32_t* s_stage = s_pack + kPackWords + (xl >> 5) * kStageWords;
     if (CL) {
-        for (int k = x; k < kPackWords; k += nx) s_pack[k] = cpack[k];
+        for (int k = xl; k < kPackWords; k += W) s_pack[k] = cpack[k];
         // made visible by the barrier of the first row
+    }
+    // ring columns of the x-1 / x+1 neighbours and the cluster ranks that hold them
+    int lxm = xl == 0 ? W - 1 : xl - 1, lxp = xl == W - 1 ? 0 : xl + 1;
+    unsigned rank_m = 0, rank_p = 0;
+    if (CLU) {
+        const unsigned C = gridDim.z, r = blockIdx.z;
+        rank_m = xl == 0 ? (r + C - 1) % C : r;
+        rank_p = xl == W - 1 ? (r + 1) % C : r;
     }
     const int m = blockIdx.y;
     const int j0 = blockIdx.x * TY;
@@ -512,8 +528,8 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const T* __restrict__ fi
     advance();
     pull(f[0]);  // row j0
     macros_v(f[0], r[0], u[0], v[0], P.c);
-    s_uv[x] = u[0];
-    s_uv[nx + x] = v[0];
+    s_uv[xl] = u[0];
+    s_uv[W + xl] = v[0];
     advance();
     pull(f[1]);  // row j0+1
     int ij = j0 * nx;
@@ -523,14 +539,23 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const T* __restrict__ fi
         advance();
         if (jc + 2 <= j1) pull(fc);  // prefetch the row after next
         macros_v(fb, rb, ub, vb, P.c);
-        sb[x] = ub;
-        sb[nx + x] = vb;
-        __syncthreads();
+        sb[xl] = ub;
+        sb[W + xl] = vb;
+        const float* am = sa;
+        const float* ap = sa;
+        if constexpr (CLU) {
+            cooperative_groups::this_cluster().sync();
+            am = cooperative_groups::this_cluster().map_shared_rank(sa, rank_m);
+            ap = cooperative_groups::this_cluster().map_shared_rank(sa, rank_p);
+        } else {
+            __syncthreads();
+        }
         float omega;
         if constexpr (CL)
-            omega = closure_omega(sa[xp], sa[xm], sa[nx + xp], sa[nx + xm], ub, uc, vb, vc, P, csc, s_pack, s_stage);
+            omega = closure_omega(ap[lxp], am[lxm], ap[W + lxp], am[W + lxm], ub, uc, vb, vc, P, csc, s_pack,
+                                  s_stage);
         else
-            omega = les_omega(sa[xp], sa[xm], sa[nx + xp], sa[nx + xm], ub, uc, vb, vc, P);
+            omega = les_omega(ap[lxp], am[lxm], ap[W + lxp], am[W + lxm], ub, uc, vb, vc, P);
         collide(fa, ra, ua, va, omega, Fx[ij], Fy[ij], P);
 #pragma unroll
         for (int q = 0; q < kQ; q++) Store<T>::st(fo + q * nxy + ij, fa[q], w_q(q));
@@ -543,13 +568,15 @@ __global__ void __launch_bounds__(MAXT) lbm_step_kernel(const T* __restrict__ fi
         ij += nx;
     };
     float* s0 = s_uv;
-    float* s1 = s_uv + 2 * nx;
-    float* s2 = s_uv + 4 * nx;
+    float* s1 = s_uv + 2 * W;
+    float* s2 = s_uv + 4 * W;
     for (int jc = j0; jc < j1; jc += 3) {
         row(f[0], f[1], f[2], r[0], u[0], v[0], r[1], u[1], v[1], u[2], v[2], s0, s1, jc);
         if (jc + 1 < j1) row(f[1], f[2], f[0], r[1], u[1], v[1], r[2], u[2], v[2], u[0], v[0], s1, s2, jc + 1);
         if (jc + 2 < j1) row(f[2], f[0], f[1], r[2], u[2], v[2], r[0], u[0], v[0], u[1], v[1], s2, s0, jc + 2);
     }
+    // the neighbours may still read this CTA's ring: leave together
+    if constexpr (CLU) cooperative_groups::this_cluster().sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -761,15 +788,17 @@ int strip_rows(const Phys& P, bool tma) {
         else if (P.nx <= 256)
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 256, 0, float>, P.nx,
                                                           sizeof(float) * 6 * P.nx);
-        else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 1024, 0, float>, P.nx,
-                                                          sizeof(float) * 6 * P.nx);
+        else {
+            const int w = P.nx / cluster_chunks(P.nx);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 1024, 0, float>, w,
+                                                          sizeof(float) * 6 * w);
+        }
         slots[t] = std::max(1, per_sm) * sms;
     }
     int best = 4;
     double best_cost = 1e30;
     for (int ty = 2; ty <= 32; ty++) {
-        const long long strips = (long long)P.M * ((P.ny + ty - 1) / ty);
+        const long long strips = (long long)P.M * ((P.ny + ty - 1) / ty) * cluster_chunks(P.nx);
         const long long waves = (strips + slots[t] - 1) / slots[t];
         const double cost = double(waves) * (ty + 1.0);
         if (cost < best_cost - 1e-9) { best_cost = cost; best = ty; }
@@ -858,6 +887,46 @@ void launch_direct_t(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout,
         lbm_step_kernel<false, MAXT, NX, T><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty, nullptr, {});
 }
 
+// rows wider than 1024 columns: clusters of cluster_chunks(nx) CTAs per strip
+template <bool CL, typename T, int NX>
+void launch_cluster_t(const lbl_ctx* c, int strips, int ty, const T* fin, T* fout, const float* force,
+                      float* mac_out, cudaStream_t s) {
+    const Phys& P = c->P;
+    const int C = cluster_chunks(P.nx), W = P.nx / C;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(strips, P.M, C);
+    lc.blockDim = dim3(W);
+    lc.dynamicSmemBytes = CL ? closure_step_smem(W) : sizeof(float) * 6 * W;
+    lc.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 1;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = C;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    const uint32_t* pk = CL ? c->d_closure : nullptr;
+    const ClosureScales sc = CL ? c->closure_sc : ClosureScales{};
+    if (mac_out)
+        cudaLaunchKernelEx(&lc, lbm_step_kernel<true, 1024, NX, T, CL, true>, fin, fout, force, mac_out, P, ty, pk,
+                           sc);
+    else
+        cudaLaunchKernelEx(&lc, lbm_step_kernel<false, 1024, NX, T, CL, true>, fin, fout, force,
+                           static_cast<float*>(nullptr), P, ty, pk, sc);
+}
+template <bool CL>
+void launch_cluster(const lbl_ctx* c, int strips, int ty, int src, int dst, const float* force, float* mac_out,
+                    cudaStream_t s) {
+    const bool sq2048 = c->P.nx == 2048 && c->P.ny == 2048;
+    if (c->f16) {
+        if (sq2048) launch_cluster_t<CL, __half, 2048>(c, strips, ty, c->h[src], c->h[dst], force, mac_out, s);
+        else launch_cluster_t<CL, __half, 0>(c, strips, ty, c->h[src], c->h[dst], force, mac_out, s);
+    } else {
+        if (sq2048) launch_cluster_t<CL, float, 2048>(c, strips, ty, c->f[src], c->f[dst], force, mac_out, s);
+        else launch_cluster_t<CL, float, 0>(c, strips, ty, c->f[src], c->f[dst], force, mac_out, s);
+    }
+}
+
 // learned-closure variant (nx % 32 == 0 and nx <= 1024, checked by lbl_set_closure)
 template <int MAXT, int NX, typename T>
 void launch_closure_t(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout, const float* force,
@@ -902,6 +971,11 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
 
     const int ty = c->ty_tuned > 0 ? c->ty_tuned : strip_rows(P, c->use_tma);
     dim3 grid((P.ny + ty - 1) / ty, P.M);
+    if (P.nx > 1024) {
+        if (c->closure) launch_cluster<true>(c, int(grid.x), ty, src, dst, force, mac_out, s);
+        else launch_cluster<false>(c, int(grid.x), ty, src, dst, force, mac_out, s);
+        return;
+    }
     if (c->use_tma) {
         float* fout = c->f[dst];
         switch (sq) {
@@ -932,6 +1006,13 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
 }
 
 int lbm_strip_rows(const lbl_ctx* c) { return strip_rows(c->P, c->use_tma); }
+
+int cluster_chunks(int nx) {
+    if (nx <= 1024) return 1;
+    for (int w : {1024, 512, 256})
+        if (nx % w == 0 && nx / w <= 8) return nx / w;
+    return 0;
+}
 
 size_t closure_step_smem(int nx) {
     return sizeof(float) * 6 * nx + sizeof(uint32_t) * (kPackWords + size_t(nx / 32) * kStageWords);

@@ -7,7 +7,8 @@ Smagorinsky term of lbm.cu:42-60, restated in oracle.cpp); this module pins the
 engine's closure kernels against the mathematics they implement:
   * features / targets  -> lbl_closure_generate's filter and sample kernels
   * forward             -> the stream-collide's tensor-core inference and the
-                           per-thread form (lbl_closure_infer)
+                           per-thread form (lbl_closure_infer), under the engine's
+                           operand contract (BF16 parameters, FP16 matrix operands)
   * loss_and_grad       -> the fused forward/backward training kernel
 The gradient itself is pinned against central finite differences in FP64.
 Only tests/ use this module.
@@ -34,6 +35,20 @@ def bf16(x) -> np.ndarray:
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+def f16(x) -> np.ndarray:
+    """Round to the nearest FP16 (ties to even), returned as float64."""
+    return np.asarray(x, dtype=np.float64).astype(np.float16).astype(np.float64)
+
+
+def contract_params(params) -> np.ndarray:
+    """Parameters as the engine uses them: BF16 values, the matrix weights W1, W2
+    carried in FP16."""
+    p = bf16(params)
+    p[W1:B1] = f16(p[W1:B1])
+    p[W2:B2] = f16(p[W2:B2])
+    return p
+
+
 def unpack(p):
     p = np.asarray(p, dtype=np.float64)
     return (p[W1:B1].reshape(N_HID, N_IN), p[B1:W2], p[W2:B2].reshape(N_HID, N_HID), p[B2:W3], p[W3:B3], p[B3])
@@ -56,28 +71,28 @@ def sigmoid(z):
     return 1.0 / (1.0 + np.exp(-z))
 
 
-def forward(params, x, bf16_operands: bool = True):
-    """Multiplier m for feature rows x [n][6].  bf16_operands applies the engine's
-    arithmetic contract: BF16 parameters, BF16 features and first-layer activations
-    as matrix operands; everything else in FP64 here."""
-    p = bf16(params) if bf16_operands else np.asarray(params, np.float64)
+def forward(params, x, contract: bool = True):
+    """Multiplier m for feature rows x [n][6].  contract applies the engine's
+    arithmetic contract: BF16 parameter values, FP16 matrix operands (weights,
+    features, first-layer activations); everything else in FP64 here."""
+    p = contract_params(params) if contract else np.asarray(params, np.float64)
     w1, b1, w2, b2, w3, b3 = unpack(p)
-    x = bf16(x) if bf16_operands else np.asarray(x, np.float64)
+    x = f16(x) if contract else np.asarray(x, np.float64)
     h1 = x @ w1.T + b1
     a1 = gelu(h1)
-    a1q = bf16(a1) if bf16_operands else a1
+    a1q = f16(a1) if contract else a1
     h2 = a1q @ w2.T + b2
     a2 = gelu(h2)
     z = a2 @ w3 + b3
     return softplus(z), (x, h1, a1q, h2, a2, z)
 
 
-def loss_and_grad(params, x, t, bf16_operands: bool = True):
+def loss_and_grad(params, x, t, contract: bool = True):
     """Mean-square loss over the rows and its gradient with respect to the
-    parameters (BF16 roundings pass the gradient straight through)."""
-    p = bf16(params) if bf16_operands else np.asarray(params, np.float64)
+    parameters (the contract's roundings pass the gradient straight through)."""
+    p = contract_params(params) if contract else np.asarray(params, np.float64)
     w1, b1, w2, b2, w3, b3 = unpack(p)
-    m, (xq, h1, a1q, h2, a2, z) = forward(params, x, bf16_operands)
+    m, (xq, h1, a1q, h2, a2, z) = forward(params, x, contract)
     n = len(t)
     err = m - np.asarray(t, np.float64)
     loss = float(np.mean(err * err))

@@ -121,8 +121,8 @@ namespace {
 // ---------------------------------------------------------------------------
 // learned closure: the 6-32-32-1 MLP of the engine's closure (parameter layout
 // W1[32][6], b1[32], W2[32][32], b2[32], W3[32], b3), evaluated in FP64 under the
-// engine's operand contract: BF16 parameters, BF16 features and BF16 first-layer
-// activations.  No counterpart in the reference (its closure is lbm.cu:42-60).
+// engine's operand contract: BF16 parameter values, FP16 matrix operands (the
+// weights W1, W2, the features and the first-layer activations).  No counterpart in the reference (its closure is lbm.cu:42-60).
 // ---------------------------------------------------------------------------
 double bf16_round(double x) {
     float f = float(x);
@@ -132,16 +132,34 @@ double bf16_round(double x) {
     std::memcpy(&f, &u, 4);
     return f;
 }
+// nearest FP16 value (ties to even), subnormals included, inf past 65520
+double f16_round(double x) {
+    if (x == 0 || !std::isfinite(x)) return x;
+    const double a = std::fabs(x);
+    if (a >= 65520.0) return std::copysign(INFINITY, x);
+    int e;
+    std::frexp(a, &e);  // a in [2^(e-1), 2^e)
+    const double ulp = std::ldexp(1.0, std::max(e - 11, -24));
+    return std::copysign(std::nearbyint(a / ulp) * ulp, x);
+}
 double gelu(double x) { return 0.5 * x * (1 + std::tanh(0.7978845608028654 * (x + 0.044715 * x * x * x))); }
 
-// w: BF16-rounded parameters; x: the six features
+// BF16 values of the parameters, W1 (0..191) and W2 (224..1247) also FP16
+void contract_params(const float* params, double* w) {
+    for (int k = 0; k < 1313; k++) {
+        w[k] = bf16_round(params[k]);
+        if (k < 192 || (k >= 224 && k < 1248)) w[k] = f16_round(w[k]);
+    }
+}
+
+// w: contract_params output; x: the six features
 double mlp_multiplier(const double* w, const double* x) {
     double xb[6], a1[32];
-    for (int i = 0; i < 6; i++) xb[i] = bf16_round(x[i]);
+    for (int i = 0; i < 6; i++) xb[i] = f16_round(x[i]);
     for (int i = 0; i < 32; i++) {
         double h = w[192 + i];
         for (int j = 0; j < 6; j++) h += w[i * 6 + j] * xb[j];
-        a1[i] = bf16_round(gelu(h));
+        a1[i] = f16_round(gelu(h));
     }
     double z = w[1312];
     for (int i = 0; i < 32; i++) {
@@ -773,7 +791,7 @@ int orc_max_sweeps(orc_ctx* o) { return o->max_sweeps_seen; }
 // the multiplier of n feature rows x [n][6] (FP64 under the BF16 operand contract)
 int orc_closure_forward(const float* params, const double* x, int n, double* out) {
     std::vector<double> w(1313);
-    for (int k = 0; k < 1313; k++) w[k] = bf16_round(params[k]);
+    contract_params(params, w.data());
     for (int i = 0; i < n; i++) out[i] = mlp_multiplier(w.data(), x + size_t(i) * 6);
     return 0;
 }
@@ -783,7 +801,7 @@ int orc_closure_forward(const float* params, const double* x, int n, double* out
 int orc_set_closure(orc_ctx* o, const float* params, double nu_ref, double dx_ref) {
     if (!params) { o->cl_w.clear(); return 0; }
     o->cl_w.resize(1313);
-    for (int k = 0; k < 1313; k++) o->cl_w[k] = bf16_round(params[k]);
+    contract_params(params, o->cl_w.data());
     o->cl_nu_ref = nu_ref > 0 ? nu_ref : double(float(o->d.nu));
     o->cl_dx_ref = dx_ref > 0 ? dx_ref : o->cfg.h_ref / 255.0;
     return 0;

@@ -39,7 +39,8 @@ def test_inference_matches_oracle(path):
     err = np.abs(got - want) / (1 + np.abs(want))
     # path 1: FP32 sums and tanhf; path 0: tensor cores and the MUFU tanh (2^-11),
     # whose result flips some BF16 roundings of the first-layer activations
-    tol_max, tol_mean = (1e-4, 1e-5) if path == 1 else (2e-2, 2e-3)
+    # (both: an FP16 rounding of a first-layer activation may flip against FP64)
+    tol_max, tol_mean = (2e-3, 1e-5) if path == 1 else (2e-2, 2e-3)
     assert err.max() < tol_max and err.mean() < tol_mean, (err.max(), err.mean())
 
 
@@ -56,7 +57,7 @@ def test_gradient_matches_oracle():
     x = _features(3000, 22)
     t = np.random.default_rng(23).uniform(0, 4, 3000).astype(np.float32)
     loss, g = lbl.closure_grad(p, x, t)
-    want_loss, want_g = co.loss_and_grad(p, x, t, bf16_operands=True)
+    want_loss, want_g = co.loss_and_grad(p, x, t, contract=True)
     assert loss == pytest.approx(want_loss, rel=1e-5)
     assert np.linalg.norm(g - want_g) < 1e-3 * np.linalg.norm(want_g)
 
@@ -122,12 +123,14 @@ def _lbm_pair(cfg, params, steps):
     return err, off
 
 
-# cs large enough that nu_t is comparable to nu on each grid, so that the network
-# moves the populations well above the FP32-vs-FP64 difference
-@pytest.mark.parametrize("nx,M,cs", [(64, 2, 0.5), (256, 1, 2.0)])
-def test_closure_stream_collide_matches_oracle(nx, M, cs):
+# cs and the output bias large enough that nu_t is comparable to nu on each grid, so
+# that the network moves the populations well above the FP32-vs-FP64 difference
+@pytest.mark.parametrize("nx,M,cs,b3", [(64, 2, 0.5, 0.0), (256, 1, 4.0, 2.0)])
+def test_closure_stream_collide_matches_oracle(nx, M, cs, b3):
     cfg = lbl.config_default("NATURE", nx, M, cs=cs)
-    err, off = _lbm_pair(cfg, _params(31), 10)
+    p = _params(31)
+    p[co.B3] += b3
+    err, off = _lbm_pair(cfg, p, 10)
     assert err < 1e-5, err
     assert off > 20 * err, (off, err)  # the check sees the network, not just Smagorinsky
 
@@ -152,10 +155,15 @@ def test_closure_off_restores_smagorinsky_bitwise():
     assert np.max(np.abs(a.get_f(0) - c.get_f(0))) > 0  # the 3 closure steps left their mark
 
 
-def test_closure_rejects_unsupported_grid():
-    e = lbl.Ensemble(lbl.config_default("NATURE", 48, 1))
+def test_closure_rejects_the_tma_stream_collide():
+    e = lbl.Ensemble(lbl.config_default("NATURE", 64, 1, lbm_variant=lbl.LBM_TMA))
     with pytest.raises(lbl.LblError):
         e.set_closure(_params(1))
+    bad = _params(1)
+    bad[5] = np.nan
+    f = lbl.Ensemble(lbl.config_default("NATURE", 64, 1))
+    with pytest.raises(lbl.LblError):
+        f.set_closure(bad)
 
 
 def test_training_lowers_the_loss_below_smagorinsky():

@@ -205,6 +205,35 @@ def test_stream_collide_variants_agree(nx):
     np.testing.assert_allclose(out[lbl.LBM_TMA][2], ud, rtol=0, atol=1e-4 * np.max(np.abs(ud)))
 
 
+@pytest.mark.parametrize("nx,ny,M,steps", [(2048, 16, 2, 20), (1280, 24, 1, 20), (2048, 2048, 1, 2)])
+def test_wide_rows_match_fp64_oracle(nx, ny, M, steps):
+    """Rows wider than 1024 columns: a cluster of CTAs per strip (2048 = 2 x 1024,
+    1280 = 5 x 256), the (u, v) across a chunk edge read from the neighbour CTA's
+    shared memory."""
+    e = lbl.Ensemble(lbl.config_default("NATURE", nx, M, ny=ny))
+    e.init(0)
+    o = oracle.Oracle(e.cfg)
+    for m in range(M):
+        o.set_f(m, e.get_f(m))
+    for t in range(steps):
+        e.update(t, 1)
+        fx, fy = e.force()
+        o.set_force(fx, fy)
+        o.step_noforce()
+    for m in range(M):
+        fe, fo = e.get_f(m).astype(np.float64), o.get_f(m)
+        assert np.max(np.abs(fe - fo) / np.abs(fo)) < 1e-5
+
+
+def test_wide_rows_limits():
+    with pytest.raises(lbl.LblError) as ei:  # a multiple of 32 that no cluster of <= 8 CTAs splits
+        lbl.Ensemble(lbl.config_default("NATURE", 2080, 1, ny=16))
+    assert ei.value.code == -1
+    with pytest.raises(lbl.LblError) as ei:  # the analysis stays at <= 1024 columns
+        lbl.Ensemble(lbl.config_default("DA_LETKF", 2048, 2, ny=16))
+    assert ei.value.code == -8
+
+
 def test_tma_variant_rejected_where_unsupported():
     with pytest.raises(lbl.LblError) as ei:
         lbl.Ensemble(lbl.config_default("NATURE", 384, 1, lbm_variant=lbl.LBM_TMA))

@@ -18,7 +18,7 @@ def test_gradient_matches_finite_differences():
     p = _params(3).astype(np.float64)
     x = rng.normal(0, 1, (48, 6))
     t = rng.uniform(0, 3, 48)
-    _, g = co.loss_and_grad(p, x, t, bf16_operands=False)
+    _, g = co.loss_and_grad(p, x, t, contract=False)
     eps = 1e-6
     fd = np.empty_like(p)
     for k in range(p.size):
