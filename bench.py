@@ -58,7 +58,12 @@ WORKLOADS = {
     "C2": (512, 64, "DA_LETKF OSSE, M=64 members resident on 1 GPU, 512x512 D2Q9 BGK+Smagorinsky (Cs 0.1, tau 0.51), "
                     "obs (u,v,rho) every 4th point (16384 sites), GC localisation radius 4 cells (75 obs/point), "
                     "inflation 1.1, 100 LBM steps + 1 LETKF analysis per cycle, FP32 storage"),
+    "C4": (256, 16, "DA_LETKF OSSE as C1 (M=16, 256x256, obs every 4th point, GC radius 4, inflation 1.1, 100 steps + "
+                    "1 analysis per cycle, FP32) with the learned closure in the stream-collide: nu_t = m (Cs dx)^2 |S|, "
+                    "m from a 6-32-32-1 GELU/softplus MLP (BF16 parameters, FP16 tensor-core operands, FP32 sums) "
+                    "trained on 4096 8x-box-filtered 2048^2 snapshots; nature run plain Smagorinsky"),
 }
+CLOSURE = False  # the ensemble (and the CPU baselines) use the trained closure (workload C4)
 WORKLOAD = WORKLOADS["C1"][2]
 
 
@@ -84,7 +89,8 @@ def ncu_traffic():
     """DRAM bytes per stream-collide launch from the committed ncu summary, if any."""
     if STORAGE:
         return None
-    path = os.path.join(ROOT, "profiles", f"lbm_step_kernel_{NX}x{NX}_M{M}.md")
+    name = "lbm_step_kernel_closure" if CLOSURE else "lbm_step_kernel"
+    path = os.path.join(ROOT, "profiles", f"{name}_{NX}x{NX}_M{M}.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -168,7 +174,7 @@ def cpu_baseline_sample(lbl, oracle, obs, threads=None):
     4 LBM steps of the whole 16-member ensemble + the analysis of 16 of the 256 rows,
     scaled to a full cycle (25x the steps, 16x the rows)."""
     nthreads = oracle.set_threads(threads or os.cpu_count())
-    o = oracle.Oracle(workload_config(lbl))
+    o = with_closure(oracle.Oracle(workload_config(lbl)))
     o.init(0)
     rng = np.random.default_rng(5)
     o.step(1, rng.normal(0, 0.84, 4 * 29).astype(np.float32))  # warm caches / page in
@@ -224,7 +230,7 @@ def run_engine(args, dist, rank, world, device):
     import oracle
     K, W = args.steps, args.warmup
     obs, truth = make_observations(lbl, W + K + 1)
-    ens = lbl.Ensemble(workload_config(lbl), device=device)
+    ens = with_closure(lbl.Ensemble(workload_config(lbl), device=device))
     ens.init(0)
     T = STEPS_PER_CYCLE
     # first cycle has no analysis (t = 0): bring the ensemble to t = 100
@@ -268,7 +274,7 @@ def run_engine(args, dist, rank, world, device):
     stats = ens.letkf_stats()
 
     # ---- e2e: host observations in, RMSE out, every cycle -----------------------------
-    e2e_ens = lbl.Ensemble(workload_config(lbl), device=device)
+    e2e_ens = with_closure(lbl.Ensemble(workload_config(lbl), device=device))
     e2e_ens.init(0)
     e2e_ens.cycle_async(0, None, None, None, T)
     for c in range(W):
@@ -307,7 +313,7 @@ def run_engine(args, dist, rank, world, device):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f16 storage, f32 compute" if STORAGE else "f32",
+        "dtype": ("f16 storage, f32 compute" if STORAGE else "f32") + ("; closure f16 mma, f32 sums" if CLOSURE else ""),
         "data": "synthetic (seeded nature run + Gaussian observation noise)",
         "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                    "l2": "flushed (256 MB write) between timed cycles, outside the timed intervals",
@@ -339,7 +345,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     nthreads = oracle.set_threads(os.cpu_count())
-    o = oracle.Oracle(workload_config(lbl))
+    o = with_closure(oracle.Oracle(workload_config(lbl)))
     o.init(0)
     rng = np.random.default_rng(9)
     obs_nan = np.full((NX, NX), np.nan, np.float32)
@@ -374,7 +380,7 @@ def profile_cycles(args):
     """The workload's cycles only (no timing, no baseline): a clean launch list for ncu."""
     import lbl
     obs, _ = make_observations(lbl, 1)
-    ens = lbl.Ensemble(workload_config(lbl))
+    ens = with_closure(lbl.Ensemble(workload_config(lbl)))
     ens.init(0)
     T = STEPS_PER_CYCLE
     ens.cycle_async(0, None, None, None, T)
@@ -449,6 +455,14 @@ def closure_params():
     return w, meta["nu_ref"], meta["dx_ref"]
 
 
+def with_closure(obj):
+    """Switch an engine ensemble or an oracle to the trained closure when the workload
+    asks for it."""
+    if CLOSURE:
+        obj.set_closure(*closure_params())
+    return obj
+
+
 def lbm_sweep(args):
     """Stream-collide alone at the given grids (NXxM,...): back-to-back launches on the
     engine's stream, CUDA events, one JSON line per size.  Sizes whose population
@@ -486,7 +500,8 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="run warmup + steps cycles of the workload and exit (for ncu captures)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["C3"], default="C1",
-                    help="C1 (the headline, 256^2 x 16), C2 (512^2 x 64) or C3 (8 concurrent experiments)")
+                    help="C1 (the headline, 256^2 x 16), C2 (512^2 x 64), C3 (8 concurrent experiments) or C4 "
+                         "(C1 with the learned closure)")
     ap.add_argument("--storage", choices=["f32", "f16"], default="f32",
                     help="population storage: f32, or the precision form's f16 deviations f - w_q")
     ap.add_argument("--lbm", default=None, metavar="NXxM[,NXxM...]",
@@ -496,8 +511,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global NX, M, WORKLOAD, STORAGE
+    global NX, M, WORKLOAD, STORAGE, CLOSURE
     NX, M, WORKLOAD = WORKLOADS.get(args.workload, WORKLOADS["C1"])
+    CLOSURE = args.workload == "C4"
     STORAGE = 1 if args.storage == "f16" else 0
     if STORAGE:
         WORKLOAD = WORKLOAD.replace("FP32 storage", "FP16 deviation storage").replace(", FP32", ", FP16 deviation storage")

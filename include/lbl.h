@@ -266,7 +266,8 @@ int lbl_h5_write_dataset(const char* path, uint64_t d0, uint64_t d1, uint64_t d2
 /* Switch the context's stream-collide to the closure (params != NULL) or back to
  * plain Smagorinsky (params == NULL).  nu_ref, dx_ref: the feature scales of the
  * training (<= 0: this context's nu and h_ref/255).  Needs the direct-load
- * stream-collide (lbm_variant AUTO or DIRECT). */
+ * stream-collide (lbm_variant AUTO or DIRECT).  Switching drops a strip height that
+ * lbl_autotune chose and returns to the heuristic's for the kernel now in use. */
 int lbl_set_closure(lbl_ctx* ctx, const float* params, double nu_ref, double dx_ref);
 
 /* Training data from the code's own runs: a run of the fine configuration (mode set

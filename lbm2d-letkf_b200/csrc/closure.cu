@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(32 * kTrainWarps) mlp_grad_kernel(const __nv_b
 #pragma unroll
             for (int j = 0; j < kMlpHid; j++) h = fmaf(p[kMlpW2 + i * kMlpHid + j], a1[j], h);
             h2[i] = h;
-            z = fmaf(p[kMlpW3 + i], mlp_gelu(h), z);
+            z = fmaf(p[kMlpW3 + i], f16_round(mlp_gelu(h)), z);  // the layer-3 operand
         }
         const float y = mlp_softplus(z);
         const float t = valid ? tgt[sample] : 0.f;
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(32 * kTrainWarps) mlp_grad_kernel(const __nv_b
         }
 #pragma unroll
         for (int i = 0; i < kMlpHid; i++) {
-            S.a2[lane][i] = mlp_gelu(h2[i]);
+            S.a2[lane][i] = f16_round(mlp_gelu(h2[i]));
             S.d2[lane][i] = d2[i];
         }
         S.dz[lane] = dz;
@@ -447,8 +447,10 @@ int lbl_set_closure(lbl_ctx* ctx, const float* params, double nu_ref, double dx_
         return LBL_ERR_CUDA;
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
     ctx->graphs.clear();
+    ctx->ty_tuned = 0;  // a strip height tuned for the other variant does not carry over
     if (!params) {
         ctx->closure = false;
+        ctx->ty_default = lbm_strip_rows(ctx);
         return LBL_OK;
     }
     std::vector<uint32_t> pack(kPackWords);
@@ -463,6 +465,7 @@ int lbl_set_closure(lbl_ctx* ctx, const float* params, double nu_ref, double dx_
     ctx->closure_sc.nu_ref = nu_ref > 0 ? float(nu_ref) : ctx->P.nu;
     ctx->closure_sc.dx_ref = dx_ref > 0 ? float(dx_ref) : float(ctx->cfg.h_ref / 255.0);
     ctx->closure = true;
+    ctx->ty_default = lbm_strip_rows(ctx);
     return LBL_OK;
 }
 

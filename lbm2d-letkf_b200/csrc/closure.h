@@ -7,12 +7,13 @@
 // closure the model falls back to.
 //
 // Arithmetic contract (the same in training and in the stream-collide): parameters
-// are BF16 values.  The two matrix layers run on FP16 tensor-core operands: their
-// weights are those BF16 values carried in FP16 (exact for |w| >= 2^-14), and their
-// inputs -- the features and the first hidden activations -- are rounded to FP16.
-// Every sum is accumulated in FP32; the output dot product and softplus run in FP32.
-// GELU is FP32 (tanhf) in training and in the per-thread form; the stream-collide
-// evaluates it on pairs in FP16 arithmetic with the MUFU tanh (about 1e-3 relative).
+// are BF16 values.  The three matrix products run on FP16 tensor-core operands: the
+// weights W1, W2, W3 and the first layer's bias (a weight on a constant input) are
+// those BF16 values carried in FP16 (exact for |w| >= 2^-14), and the inputs -- the
+// features and both hidden activations -- are rounded to FP16.  Every sum is
+// accumulated in FP32; b2, b3 and softplus are FP32.  GELU is FP32 (tanhf) in
+// training and in the per-thread form; the stream-collide evaluates it on pairs in
+// FP16 arithmetic with the MUFU tanh (about 1e-3 relative).
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -62,6 +63,27 @@ __host__ __device__ inline float closure_features(float ux, float uy, float vx, 
     return smag;
 }
 
+#ifdef __CUDACC__
+// The same features with the hardware log / reciprocal / square root (a few ulp;
+// the features are rounded to FP16 before use): the stream-collide's form.
+__device__ __forceinline__ float closure_features_fast(float ux, float uy, float vx, float vy,
+                                                       const ClosureScales& c, float* x) {
+    const float s11 = ux, s22 = vy, s12 = 0.5f * (uy + vx), w12 = 0.5f * (uy - vx);
+    const float ss = fmaf(s11, s11, fmaf(2.f * s12, s12, s22 * s22));
+    const float ww = 2.f * w12 * w12;
+    const float smag = __fsqrt_rn(2.f * ss), wmag = __fsqrt_rn(2.f * ww);
+    const float k = c.dx * c.dx / c.nu_ref;
+    const float y = k * (vx - uy);
+    x[0] = __logf(fmaf(k, smag, 1.f));
+    x[1] = __logf(fmaf(k, wmag, 1.f));
+    x[2] = __fdividef(ww - ss, ww + ss + 1e-30f);
+    x[3] = (s11 + s22) * rsqrtf(ss + 1e-30f);
+    x[4] = c.dx / c.dx_ref;
+    x[5] = copysignf(__logf(fabsf(y) + __fsqrt_rn(fmaf(y, y, 1.f))), y);
+    return smag;
+}
+#endif
+
 // GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))
 constexpr float kGeluK = 0.7978845608f, kGeluC = 0.044715f;
 __host__ __device__ inline float mlp_gelu(float x) {
@@ -70,10 +92,10 @@ __host__ __device__ inline float mlp_gelu(float x) {
 }
 __host__ __device__ inline float mlp_softplus(float z) { return z > 20.f ? z : log1pf(expf(z)); }
 __host__ __device__ inline float f16_round(float x) { return __half2float(__float2half_rn(x)); }
-// a parameter as the network uses it: BF16, and for the matrix weights also FP16
+// a parameter as the network uses it: BF16, and for W1, b1, W2 and W3 also FP16
 __host__ __device__ inline float param_value(const __nv_bfloat16* p, int k) {
     const float w = __bfloat162float(p[k]);
-    return (k < kMlpB1 || (k >= kMlpW2 && k < kMlpB2)) ? f16_round(w) : w;
+    return (k < kMlpB2 || (k >= kMlpW3 && k < kMlpB3)) ? f16_round(w) : w;
 }
 
 // forward pass under the contract above (one cell): the Smagorinsky multiplier
@@ -93,7 +115,7 @@ __device__ inline float mlp_forward(const __nv_bfloat16* __restrict__ p, const f
         float h = param_value(p, kMlpB2 + i);
 #pragma unroll
         for (int j = 0; j < kMlpHid; j++) h = fmaf(param_value(p, kMlpW2 + i * kMlpHid + j), a1[j], h);
-        z = fmaf(param_value(p, kMlpW3 + i), mlp_gelu(h), z);
+        z = fmaf(param_value(p, kMlpW3 + i), f16_round(mlp_gelu(h)), z);
     }
     return mlp_softplus(z);
 }
@@ -105,16 +127,20 @@ __device__ inline float mlp_forward(const __nv_bfloat16* __restrict__ p, const f
 //
 // The parameters are prepared once (closure_pack) in the fragment order of the
 // m16n8k16 operands, so that lane t reads its share with vector loads:
-//   u32 B1[32][4]   layer-1 B fragments (k = feature, n = hidden), one per n-tile, FP16x2
+//   u32 B1[32][4]   layer-1 B fragments (k = feature, n = hidden), one per n-tile, FP16x2;
+//                   k = 6 is a constant 1 input whose weight is b1
 //   u32 B2[32][16]  layer-2 B fragments, [n-tile][k-step][2], FP16x2
-//   f32 C[32][24]   b1, b2, W3 at the accumulator columns of lane t: [n-tile][2] each
+//   u32 B3[32][4]   layer-3 B fragments, [k-step][2]: W3 in all 8 columns, so that
+//                   every lane's accumulators end up holding its rows' outputs
+//   f32 C[32][8]    b2 at the accumulator columns of lane t, [n-tile][2]
 //   f32 b3
 // ---------------------------------------------------------------------------
-constexpr int kPackB1 = 0;             // u32 offset of B1
-constexpr int kPackB2 = 32 * 4;        // u32 offset of B2
-constexpr int kPackC = kPackB2 + 32 * 16;  // f32 offset of the per-lane constants
-constexpr int kPackB3 = kPackC + 32 * 24;
-constexpr int kPackWords = kPackB3 + 4;    // 1412 words = 5648 B
+constexpr int kPackB1 = 0;                   // u32 offset of B1
+constexpr int kPackB2 = 32 * 4;              // u32 offset of B2
+constexpr int kPackB3f = kPackB2 + 32 * 16;  // u32 offset of B3
+constexpr int kPackC = kPackB3f + 32 * 4;    // f32 offset of the per-lane b2
+constexpr int kPackB3 = kPackC + 32 * 8;
+constexpr int kPackWords = kPackB3 + 4;      // 1028 words = 4112 B
 constexpr int kStageWords = 128;           // per-warp feature staging (32 lanes x 4 words)
 
 // round-to-nearest-even BF16 value of a finite float (host side of the packing)
@@ -142,18 +168,20 @@ inline void closure_pack(const float* w, uint32_t* out) {
         const int g = t >> 2, c = t & 3;
         for (int nt = 0; nt < 4; nt++) {
             const int n = 8 * nt + g;  // hidden unit = the fragment's n column
-            out[kPackB1 + t * 4 + nt] = (2 * c < kMlpIn) ? pk(kMlpW1 + n * kMlpIn + 2 * c, kMlpW1 + n * kMlpIn + 2 * c + 1) : 0u;
+            out[kPackB1 + t * 4 + nt] = (2 * c < kMlpIn) ? pk(kMlpW1 + n * kMlpIn + 2 * c, kMlpW1 + n * kMlpIn + 2 * c + 1)
+                                                         : weight_bits(w[kMlpB1 + n]);  // k = 6, 7: (b1, 0)
             for (int ks = 0; ks < 2; ks++) {
                 const int k0 = kMlpW2 + n * kMlpHid + 16 * ks + 2 * c;
                 out[kPackB2 + t * 16 + (nt * 2 + ks) * 2 + 0] = pk(k0, k0 + 1);
                 out[kPackB2 + t * 16 + (nt * 2 + ks) * 2 + 1] = pk(k0 + 8, k0 + 9);
             }
-            for (int e = 0; e < 2; e++) {
-                const int col = 8 * nt + 2 * c + e;  // accumulator column of lane t
-                cf[kPackC + t * 24 + nt * 2 + e] = bf16_value(w[kMlpB1 + col]);
-                cf[kPackC + t * 24 + 8 + nt * 2 + e] = bf16_value(w[kMlpB2 + col]);
-                cf[kPackC + t * 24 + 16 + nt * 2 + e] = bf16_value(w[kMlpW3 + col]);
-            }
+            for (int e = 0; e < 2; e++)  // accumulator column 8 nt + 2 c + e of lane t
+                cf[kPackC + t * 8 + nt * 2 + e] = bf16_value(w[kMlpB2 + 8 * nt + 2 * c + e]);
+        }
+        for (int ks = 0; ks < 2; ks++) {
+            const int k0 = kMlpW3 + 16 * ks + 2 * c;
+            out[kPackB3f + t * 4 + ks * 2 + 0] = pk(k0, k0 + 1);
+            out[kPackB3f + t * 4 + ks * 2 + 1] = pk(k0 + 8, k0 + 9);
         }
     }
     cf[kPackB3] = bf16_value(w[kMlpB3]);
@@ -198,7 +226,7 @@ __device__ __forceinline__ float mlp_forward_warp(const uint32_t* __restrict__ p
     const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
     __syncwarp();
     reinterpret_cast<uint4*>(stage)[lane] =
-        make_uint4(pack_f16x2(x[0], x[1]), pack_f16x2(x[2], x[3]), pack_f16x2(x[4], x[5]), 0u);
+        make_uint4(pack_f16x2(x[0], x[1]), pack_f16x2(x[2], x[3]), pack_f16x2(x[4], x[5]), 0x3C00u /* (1, 0) */);
     __syncwarp();
     uint32_t xa[2][2];
 #pragma unroll
@@ -206,54 +234,52 @@ __device__ __forceinline__ float mlp_forward_warp(const uint32_t* __restrict__ p
         xa[mt][0] = stage[(16 * mt + g) * 4 + c];
         xa[mt][1] = stage[(16 * mt + g + 8) * 4 + c];
     }
-    const uint4 w1 = reinterpret_cast<const uint4*>(pk + kPackB1)[lane];
-    const uint32_t w1f[4] = {w1.x, w1.y, w1.z, w1.w};
-    const float4* cv = reinterpret_cast<const float4*>(pk + kPackC + lane * 24);
-    const float4 b1a = cv[0], b1b = cv[1], b2a = cv[2], b2b = cv[3], w3a = cv[4], w3b = cv[5];
-    const float b1[8] = {b1a.x, b1a.y, b1a.z, b1a.w, b1b.x, b1b.y, b1b.z, b1b.w};
-    const float b2[8] = {b2a.x, b2a.y, b2a.z, b2a.w, b2b.x, b2b.y, b2b.z, b2b.w};
-    const float w3[8] = {w3a.x, w3a.y, w3a.z, w3a.w, w3b.x, w3b.y, w3b.z, w3b.w};
-    // layer 1 (K = 6 of 16) and GELU in FP16 pairs: the accumulators of n-tiles 2ks,
-    // 2ks+1 are the A fragment of layer 2's k-step ks
-    uint32_t a2[2][2][4];
+    const uint4* w1v = reinterpret_cast<const uint4*>(pk + kPackB1);
+    const uint4* w2v = reinterpret_cast<const uint4*>(pk + kPackB2 + lane * 16);
+    const uint4* w3v = reinterpret_cast<const uint4*>(pk + kPackB3f);
+    const float2* b2v = reinterpret_cast<const float2*>(pk + kPackC + lane * 8);
+    const float b3 = reinterpret_cast<const float*>(pk)[kPackB3];
+    float z[2][4];
+    // one m-tile (16 cells) at a time through the three layers keeps few registers live
 #pragma unroll
-    for (int mt = 0; mt < 2; mt++)
+    for (int mt = 0; mt < 2; mt++) {
+        // layer 1 (K = 6 features + the constant 1 of the bias, of 16) and GELU in FP16
+        // pairs: the accumulators of n-tiles 2ks, 2ks+1 are the A fragment of layer 2's
+        // k-step ks
+        const uint4 w1 = w1v[lane];
+        const uint32_t w1f[4] = {w1.x, w1.y, w1.z, w1.w};
+        uint32_t a2[2][4];
 #pragma unroll
         for (int nt = 0; nt < 4; nt++) {
-            float h[4] = {b1[2 * nt], b1[2 * nt + 1], b1[2 * nt], b1[2 * nt + 1]};
+            float h[4] = {0.f, 0.f, 0.f, 0.f};
             mma_f16_16816(h, xa[mt][0], xa[mt][1], 0u, 0u, w1f[nt], 0u);
-            a2[mt][nt >> 1][2 * (nt & 1) + 0] = gelu_f16x2(pack_f16x2(h[0], h[1]));
-            a2[mt][nt >> 1][2 * (nt & 1) + 1] = gelu_f16x2(pack_f16x2(h[2], h[3]));
+            a2[nt >> 1][2 * (nt & 1) + 0] = gelu_f16x2(pack_f16x2(h[0], h[1]));
+            a2[nt >> 1][2 * (nt & 1) + 1] = gelu_f16x2(pack_f16x2(h[2], h[3]));
         }
-    // layer 2, GELU, and the output dot product of each row (FP32)
-    float z[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-    const uint4* w2v = reinterpret_cast<const uint4*>(pk + kPackB2 + lane * 16);
+        // layer 2 and GELU, laid out the same way as the A fragment of layer 3
+        uint32_t a3[2][4];
 #pragma unroll
-    for (int nt = 0; nt < 4; nt++) {
-        const uint4 w2 = w2v[nt];  // {ks0 b0, ks0 b1, ks1 b0, ks1 b1}
-#pragma unroll
-        for (int mt = 0; mt < 2; mt++) {
-            float o[4] = {b2[2 * nt], b2[2 * nt + 1], b2[2 * nt], b2[2 * nt + 1]};
-            mma_f16_16816(o, a2[mt][0][0], a2[mt][0][1], a2[mt][0][2], a2[mt][0][3], w2.x, w2.y);
-            mma_f16_16816(o, a2[mt][1][0], a2[mt][1][1], a2[mt][1][2], a2[mt][1][3], w2.z, w2.w);
-            const float2 g0 = __half22float2(as_h2(gelu_f16x2(pack_f16x2(o[0], o[1]))));
-            const float2 g1 = __half22float2(as_h2(gelu_f16x2(pack_f16x2(o[2], o[3]))));
-            z[mt][0] = fmaf(g0.x, w3[2 * nt], fmaf(g0.y, w3[2 * nt + 1], z[mt][0]));
-            z[mt][1] = fmaf(g1.x, w3[2 * nt], fmaf(g1.y, w3[2 * nt + 1], z[mt][1]));
+        for (int nt = 0; nt < 4; nt++) {
+            const uint4 w2 = w2v[nt];  // {ks0 b0, ks0 b1, ks1 b0, ks1 b1}
+            const float2 b2 = b2v[nt];
+            float o[4] = {b2.x, b2.y, b2.x, b2.y};
+            mma_f16_16816(o, a2[0][0], a2[0][1], a2[0][2], a2[0][3], w2.x, w2.y);
+            mma_f16_16816(o, a2[1][0], a2[1][1], a2[1][2], a2[1][3], w2.z, w2.w);
+            a3[nt >> 1][2 * (nt & 1) + 0] = gelu_f16x2(pack_f16x2(o[0], o[1]));
+            a3[nt >> 1][2 * (nt & 1) + 1] = gelu_f16x2(pack_f16x2(o[2], o[3]));
         }
+        // layer 3: W3 fills every column of B, so each lane's accumulators hold z of
+        // its rows g (z[mt][0]) and g + 8 (z[mt][2]) of the tile
+        const uint4 w3 = w3v[lane];
+        z[mt][0] = z[mt][1] = z[mt][2] = z[mt][3] = b3;
+        mma_f16_16816(z[mt], a3[0][0], a3[0][1], a3[0][2], a3[0][3], w3.x, w3.y);
+        mma_f16_16816(z[mt], a3[1][0], a3[1][1], a3[1][2], a3[1][3], w3.z, w3.w);
     }
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-        for (int hh = 0; hh < 2; hh++) {
-            z[mt][hh] += __shfl_xor_sync(0xffffffffu, z[mt][hh], 1);
-            z[mt][hh] += __shfl_xor_sync(0xffffffffu, z[mt][hh], 2);
-        }
     // lane 4 g + (2 mt + hh) of quad g offers row g + 8 hh of tile mt
-    const float offer = (c == 0) ? z[0][0] : (c == 1) ? z[0][1] : (c == 2) ? z[1][0] : z[1][1];
+    const float offer = (c == 0) ? z[0][0] : (c == 1) ? z[0][2] : (c == 2) ? z[1][0] : z[1][2];
     const int r = lane & 15;
     const float zz = __shfl_sync(0xffffffffu, offer, 4 * (r & 7) + 2 * (lane >> 4) + (r >> 3));
-    return mlp_softplus(zz + reinterpret_cast<const float*>(pk)[kPackB3]);
+    return zz > 20.f ? zz : __logf(1.f + __expf(zz));
 }
 #endif
 

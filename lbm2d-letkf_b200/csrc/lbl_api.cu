@@ -568,6 +568,7 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     }
     if (cfg->lbm_variant == LBL_LBM_TMA && !ctx->use_tma)
         return fail(ctx, LBL_ERR_UNSUPPORTED, "TMA stream-collide unavailable for this grid (nx <= 512) or driver");
+    ctx->ty_default = lbm_strip_rows(ctx);
     for (auto& e : ctx->ev) LBL_CK(cudaEventCreate(&e));
     for (auto& e : ctx->user_ev) LBL_CK(cudaEventCreate(&e));
     ctx->have_events = true;

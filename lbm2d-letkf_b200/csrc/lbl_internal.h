@@ -129,6 +129,7 @@ struct lbl_ctx {
     CUtensorMap tmap[2];
     bool use_tma = false;
     int ty_tuned = 0;                    // stream-collide strip height chosen by lbl_autotune (0: heuristic)
+    int ty_default = 0;                  // the heuristic's strip height for the kernel that runs
     int* d_err = nullptr;                // bounded-wait timeout flag of the TMA kernel
 
     // learned closure (closure.h): fragment-ordered BF16 parameters, feature scales
@@ -155,7 +156,8 @@ void launch_ic_velocity(const double* modes /*[4][n]*/, int n_modes, int nx, int
 void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s);
 // one step from population buffer src to dst (FP32 or FP16 storage)
 void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s);
-// strip height of the stream-collide for this grid and ensemble (heuristic)
+// strip height of the stream-collide for this grid, ensemble and kernel variant
+// (occupancy heuristic); call outside stream capture
 int lbm_strip_rows(const lbl_ctx* c);
 // fill both population buffers with the rest state (rho = rho_ref, u = v = 0)
 void launch_rest_state(const lbl_ctx* c, cudaStream_t s);
@@ -169,6 +171,7 @@ size_t closure_step_smem(int nx);
 int cluster_chunks(int nx);
 int lbm_tma_prepare(int nx);
 bool lbm_tma_supported(int nx);
+size_t lbm_tma_smem(int nx);
 void launch_macros(const lbl_ctx* c, int buf, float* mac, cudaStream_t s);
 
 // ---- kernels (letkf_kernels.cu) ----

@@ -206,7 +206,7 @@ __device__ __forceinline__ float closure_omega(float ue, float uw, float ve, flo
     const float ux = (ue - uw) * P.inv_two_dx, uy = (un - us) * P.inv_two_dx;
     const float vx = (ve - vw) * P.inv_two_dx, vy = (vn - vs) * P.inv_two_dx;
     float feat[kMlpIn];
-    const float smag = closure_features(ux, uy, vx, vy, csc, feat);
+    const float smag = closure_features_fast(ux, uy, vx, vy, csc, feat);
     const float m = mlp_forward_warp(pack, stage, feat);
     const float nus = m * float(P.les_k * double(smag));
     const float tau = float(fma(double(P.nu + nus), P.tau_k, 0.5));
@@ -460,11 +460,11 @@ __global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __res
 // NX > 0 fixes the (square) grid at compile time so that plane and row offsets are
 // immediates; NX = 0 reads nx, ny from P.
 // ---------------------------------------------------------------------------
+// (the closure variant at 256 threads is held to 2 CTAs per SM: 128 registers)
 template <bool WRITE_MAC, int MAXT, int NX, typename T, bool CL = false, bool CLU = false>
-__global__ void __launch_bounds__(MAXT) lbm_step_kernel(const T* __restrict__ fin, T* __restrict__ fout,
-                                                        const float* __restrict__ force,
-                                                        float* __restrict__ mac, Phys P, int TY,
-                                                        const uint32_t* __restrict__ cpack, ClosureScales csc) {
+__global__ void __launch_bounds__(MAXT, (CL && MAXT == 256) ? 2 : 1)
+    lbm_step_kernel(const T* __restrict__ fin, T* __restrict__ fout, const float* __restrict__ force,
+                    float* __restrict__ mac, Phys P, int TY, const uint32_t* __restrict__ cpack, ClosureScales csc) {
     // CLU: rows wider than one CTA.  The cluster's CTAs (blockIdx.z = chunk) each take
     // blockDim.x columns of the same strip and read the (u, v) of the neighbour
     // columns across a chunk edge from the neighbour CTA's ring (distributed shared
@@ -771,35 +771,78 @@ __global__ void macros_kernel(const T* __restrict__ f, float* __restrict__ mac, 
     mm[2 * P.nxy + ij] = v;
 }
 
-// Strip height: fill the GPU's resident CTA slots with as few waves as possible,
-// counting the two halo rows each strip pulls.
-int strip_rows(const Phys& P, bool tma) {
-    static int slots[2] = {0, 0}, slots_nx[2] = {0, 0};
-    const int t = tma ? 1 : 0;
-    if (slots[t] == 0 || slots_nx[t] != P.nx) {
-        slots_nx[t] = P.nx;
-        int dev = 0, sms = 148, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (tma)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_tma_kernel<false, 0>, P.nx + 32,
-                                                          sizeof(float) * (size_t(kStages) * kQ * P.nx + 6 * P.nx) +
-                                                              2 * kStages * sizeof(uint64_t));
-        else if (P.nx <= 256)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 256, 0, float>, P.nx,
-                                                          sizeof(float) * 6 * P.nx);
-        else {
-            const int w = P.nx / cluster_chunks(P.nx);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_step_kernel<false, 1024, 0, float>, w,
-                                                          sizeof(float) * 6 * w);
-        }
-        slots[t] = std::max(1, per_sm) * sms;
+// The kernel launch_lbm_step runs for a context (its WRITE_MAC = false form), with its
+// block size and dynamic shared memory, for the occupancy query of the strip height.
+struct StepKernel {
+    const void* fn;
+    int threads;
+    size_t smem;
+};
+template <typename T>
+StepKernel direct_kernel(const lbl_ctx* c) {
+    const Phys& P = c->P;
+    const int sq = (P.nx == P.ny) ? P.nx : 0;
+    if (P.nx > 1024) {
+        const int w = P.nx / cluster_chunks(P.nx);
+        const size_t sm = c->closure ? closure_step_smem(w) : sizeof(float) * 6 * w;
+        const void* fn = c->closure ? (sq == 2048 ? (const void*)lbm_step_kernel<false, 1024, 2048, T, true, true>
+                                                  : (const void*)lbm_step_kernel<false, 1024, 0, T, true, true>)
+                                    : (sq == 2048 ? (const void*)lbm_step_kernel<false, 1024, 2048, T, false, true>
+                                                  : (const void*)lbm_step_kernel<false, 1024, 0, T, false, true>);
+        return {fn, w, sm};
     }
+    if (c->closure) {
+        const size_t sm = closure_step_smem(P.nx);
+        if (sq == 256) return {(const void*)lbm_step_kernel<false, 256, 256, T, true>, P.nx, sm};
+        if (P.nx <= 256) return {(const void*)lbm_step_kernel<false, 256, 0, T, true>, P.nx, sm};
+        return {(const void*)lbm_step_kernel<false, 1024, 0, T, true>, P.nx, sm};
+    }
+    const size_t sm = sizeof(float) * 6 * P.nx;
+    switch (sq) {
+        case 64: return {(const void*)lbm_step_kernel<false, 256, 64, T>, P.nx, sm};
+        case 128: return {(const void*)lbm_step_kernel<false, 256, 128, T>, P.nx, sm};
+        case 256: return {(const void*)lbm_step_kernel<false, 256, 256, T>, P.nx, sm};
+        case 512: return {(const void*)lbm_step_kernel<false, 1024, 512, T>, P.nx, sm};
+        case 1024: return {(const void*)lbm_step_kernel<false, 1024, 1024, T>, P.nx, sm};
+        default:
+            if (P.nx <= 256) return {(const void*)lbm_step_kernel<false, 256, 0, T>, P.nx, sm};
+            return {(const void*)lbm_step_kernel<false, 1024, 0, T>, P.nx, sm};
+    }
+}
+StepKernel step_kernel(const lbl_ctx* c) {
+    const Phys& P = c->P;
+    if (c->use_tma) {
+        const int sq = (P.nx == P.ny) ? P.nx : 0;
+        const void* fn = sq == 64    ? (const void*)lbm_step_tma_kernel<false, 64>
+                         : sq == 128 ? (const void*)lbm_step_tma_kernel<false, 128>
+                         : sq == 256 ? (const void*)lbm_step_tma_kernel<false, 256>
+                         : sq == 512 ? (const void*)lbm_step_tma_kernel<false, 512>
+                                     : (const void*)lbm_step_tma_kernel<false, 0>;
+        return {fn, P.nx + 32, lbm_tma_smem(P.nx)};
+    }
+    return c->f16 ? direct_kernel<__half>(c) : direct_kernel<float>(c);
+}
+
+// Strip height: fill the GPU's resident CTA slots with as few waves as possible,
+// counting the two halo rows each strip pulls.  Queried outside stream capture (at
+// context creation and when the closure is switched), for the kernel that runs: an
+// occupancy query inside a capture may fail and must not decide the launch shape.
+int strip_rows(const lbl_ctx* c) {
+    const Phys& P = c->P;
+    const StepKernel k = step_kernel(c);
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem) != cudaSuccess) {
+        (void)cudaGetLastError();
+        per_sm = 1;
+    }
+    const long long slots = (long long)std::max(1, per_sm) * sms;
     int best = 4;
     double best_cost = 1e30;
     for (int ty = 2; ty <= 32; ty++) {
         const long long strips = (long long)P.M * ((P.ny + ty - 1) / ty) * cluster_chunks(P.nx);
-        const long long waves = (strips + slots[t] - 1) / slots[t];
+        const long long waves = (strips + slots - 1) / slots;
         const double cost = double(waves) * (ty + 1.0);
         if (cost < best_cost - 1e-9) { best_cost = cost; best = ty; }
     }
@@ -969,7 +1012,7 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
     const Phys& P = c->P;
     const int sq = (P.nx == P.ny) ? P.nx : 0;
 
-    const int ty = c->ty_tuned > 0 ? c->ty_tuned : strip_rows(P, c->use_tma);
+    const int ty = c->ty_tuned > 0 ? c->ty_tuned : (c->ty_default > 0 ? c->ty_default : 4);
     dim3 grid((P.ny + ty - 1) / ty, P.M);
     if (P.nx > 1024) {
         if (c->closure) launch_cluster<true>(c, int(grid.x), ty, src, dst, force, mac_out, s);
@@ -1005,7 +1048,7 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
     }
 }
 
-int lbm_strip_rows(const lbl_ctx* c) { return strip_rows(c->P, c->use_tma); }
+int lbm_strip_rows(const lbl_ctx* c) { return strip_rows(c); }
 
 int cluster_chunks(int nx) {
     if (nx <= 1024) return 1;

@@ -50,13 +50,20 @@ def coarse_config(nx: int = 256, n_ens: int = 16, mode: str = "DA_LETKF", **kw):
 
 def fine_config(coarse, filter: int, members: int):
     """A NATURE run filter times finer with the coarse run's physics: the same domain,
-    forcing, friction, IC spectrum and molecular viscosity (tau follows from nu)."""
+    IC spectrum and molecular viscosity (tau follows from nu), and the same forcing
+    and friction per unit time.  The engine applies both per step (lbm.h:41-70): the
+    random force is drawn afresh every step, so its energy input per unit time goes
+    as fkf^2 dt and fkf scales with sqrt(dt_coarse / dt_fine); the friction removes
+    friction_rate of the velocity per step, so friction_rate scales with dt_fine /
+    dt_coarse."""
     f = lbl.config_default("NATURE", coarse.nx * filter, members)
-    for k in ("cs", "cfl", "rho_ref", "u_ref", "h_ref", "kf", "fkf", "friction_rate", "ic_kind", "ic_amp",
-              "force_seed"):
+    for k in ("cs", "cfl", "rho_ref", "u_ref", "h_ref", "kf", "ic_kind", "ic_amp", "force_seed"):
         setattr(f, k, getattr(coarse, k))
     f.tau = 0.0
     f.nu = phys(coarse)["nu"]
+    ratio = phys(coarse)["dt"] / phys(f)["dt"]
+    f.fkf = coarse.fkf * np.sqrt(ratio)
+    f.friction_rate = coarse.friction_rate / ratio
     return f
 
 
@@ -149,6 +156,115 @@ def train(coarse=None, filter: int = 8, members: int = 64, snapshots: int = 64, 
     return w, rep
 
 
+def spectrum_error(e_run, e_ref, kmax: int) -> float:
+    """Mean |log10(E_run / E_ref)| over shells 1..kmax."""
+    k = np.arange(1, kmax + 1)
+    return float(np.mean(np.abs(np.log10(np.maximum(e_run[k], 1e-300) / np.maximum(e_ref[k], 1e-300)))))
+
+
+def evaluate(params=None, meta=None, filter: int = 8, spinup: int = 20000, cycles: int = 100, members: int = 16,
+             spectrum_every: int = 5, seed: int = 0, device: int = 0, log=print):
+    """The closure against plain Smagorinsky in the coarse configuration, with the
+    box-filtered fine run as the truth (an imperfect-model experiment: neither coarse
+    model represents the truth exactly).
+
+    * analysis RMSE: two DA_LETKF ensembles (members, 256^2) started from the filtered
+      truth plus 10 % random-phase perturbations; every 100 coarse steps both
+      assimilate the same noisy observations of the filtered truth (u, v, rho every
+      4th point, sigma 0.1 / 0.01) and the RMSE of the analysis mean against the
+      filtered truth is recorded;
+    * spectrum: two free coarse runs from the filtered truth; their energy spectra
+      and the filtered truth's, averaged over the run, and the mean |log10| error.
+    Returns the report dict."""
+    if params is None:
+        params, meta = load_params()
+    coarse = coarse_config(n_ens=members)
+    fine = fine_config(coarse, filter, 1)
+    ratio = phys(coarse)["dt"] / phys(fine)["dt"]
+    nat = lbl.Ensemble(fine, device)
+    nat.init(0)
+    nat.update(0, spinup)
+    tf, done_f = spinup, 0
+
+    def truth():
+        r, u, v, _ = nat.get_fields(0)
+        return box(r, filter).astype(np.float32), box(u, filter).astype(np.float32), box(v, filter).astype(np.float32)
+
+    rt, ut, vt = truth()
+    c = phys(coarse)["c"]
+    pert = lbl.Ensemble(lbl.config_default("NATURE", coarse.nx, members, ic_kind=coarse.ic_kind, ic_amp=coarse.ic_amp),
+                        device)
+    pert.init(1000)
+    dvel = [pert.get_fields(m)[1:3] for m in range(members)]
+    pert.close()
+    setups = (("smagorinsky", None), ("mlp", params))
+    da, free = {}, {}
+    for name, w in setups:
+        e = lbl.Ensemble(coarse, device)
+        e.init(0)
+        f1 = lbl.Ensemble(coarse_config(n_ens=1, mode="NATURE"), device)
+        f1.init(0)
+        if w is not None:
+            e.set_closure(w, meta["nu_ref"], meta["dx_ref"])
+            f1.set_closure(w, meta["nu_ref"], meta["dx_ref"])
+        for m in range(members):
+            e.set_f(m, feq_populations(rt, ut + coarse.ens_perturb * dvel[m][0], vt + coarse.ens_perturb * dvel[m][1], c))
+        f1.set_f(0, feq_populations(rt, ut, vt, c))
+        da[name], free[name] = e, f1
+    rng = np.random.default_rng(seed)
+    rmse = {n: [] for n, _ in setups}
+    spec = {n: [] for n in ["truth"] + [n for n, _ in setups]}
+    t0 = time.time()
+    for cyc in range(cycles):
+        n_f = int(round((cyc + 1) * 100 * ratio)) - done_f  # fine steps for 100 coarse steps
+        nat.update(tf, n_f)
+        tf += n_f
+        done_f += n_f
+        rt, ut, vt = truth()
+        ro = rt + rng.normal(0, coarse.obs_error_rho, rt.shape).astype(np.float32)
+        uo = ut + rng.normal(0, coarse.obs_error_u, ut.shape).astype(np.float32)
+        vo = vt + rng.normal(0, coarse.obs_error_u, vt.shape).astype(np.float32)
+        t = cyc * 100
+        for name, _ in setups:
+            da[name].update(t, 100)
+            da[name].assimilate(t + 100, ro, uo, vo)
+            rmse[name].append(da[name].rmse_uv(ut, vt))
+            free[name].update(t, 100)
+        if (cyc + 1) % spectrum_every == 0:
+            spec["truth"].append(lbl.energy_spectrum(ut, vt))
+            for name, _ in setups:
+                _, u, v, _ = free[name].get_fields(0)
+                spec[name].append(lbl.energy_spectrum(u, v))
+    wall = time.time() - t0
+    half = cycles // 2
+    es = {n: np.mean(v, axis=0) for n, v in spec.items()}
+    kq, kh = coarse.nx // 4, coarse.nx // 2 - 1
+    rep = {
+        "cycles": cycles, "members": members, "fine_grid": fine.nx, "filter": filter, "spinup_fine_steps": spinup,
+        "dt_ratio": ratio, "wall_s": wall,
+        "rmse_mean_second_half": {n: float(np.mean(v[half:])) for n, v in rmse.items()},
+        "rmse_final": {n: float(v[-1]) for n, v in rmse.items()},
+        "rmse_series": {n: [float(x) for x in v] for n, v in rmse.items()},
+        f"spectrum_error_k1_to_{kq}": {n: spectrum_error(es[n], es["truth"], kq) for n, _ in setups},
+        f"spectrum_error_k1_to_{kh}": {n: spectrum_error(es[n], es["truth"], kh) for n, _ in setups},
+        "spectra": {n: [float(x) for x in v] for n, v in es.items()},
+    }
+    for d in (da, free):
+        for e in d.values():
+            e.close()
+    nat.close()
+    log(json.dumps({k: v for k, v in rep.items() if k not in ("rmse_series", "spectra")}))
+    return rep
+
+
+def _cli_eval(a):
+    w, meta = load_params(a.params)
+    rep = evaluate(w, meta, filter=meta.get("filter", 8), spinup=a.spinup, cycles=a.cycles, members=a.members)
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(rep, f, indent=1)
+
+
 def _cli_train(a):
     w, rep = train(filter=a.filter, members=a.members, snapshots=a.snapshots, spinup=a.spinup, spacing=a.spacing,
                    iters=tuple(a.iters), lrs=tuple(a.lrs), batch=a.batch, seed=a.seed)
@@ -170,9 +286,17 @@ def main():
     t.add_argument("--batch", type=int, default=65536)
     t.add_argument("--seed", type=int, default=1)
     t.add_argument("--out", default=DEFAULT_PARAMS)
+    e = sub.add_parser("eval", help="closure vs Smagorinsky: analysis RMSE and spectrum against filtered truth")
+    e.add_argument("--params", default=DEFAULT_PARAMS)
+    e.add_argument("--spinup", type=int, default=20000)
+    e.add_argument("--cycles", type=int, default=100)
+    e.add_argument("--members", type=int, default=16)
+    e.add_argument("--out", default=None, help="write the full report (series, spectra) as JSON")
     a = ap.parse_args()
     if a.cmd == "train":
         _cli_train(a)
+    else:
+        _cli_eval(a)
 
 
 if __name__ == "__main__":

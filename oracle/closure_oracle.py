@@ -41,11 +41,11 @@ def f16(x) -> np.ndarray:
 
 
 def contract_params(params) -> np.ndarray:
-    """Parameters as the engine uses them: BF16 values, the matrix weights W1, W2
-    carried in FP16."""
+    """Parameters as the engine uses them: BF16 values, the matrix operands W1, b1
+    (the weight of a constant input), W2 and W3 carried in FP16."""
     p = bf16(params)
-    p[W1:B1] = f16(p[W1:B1])
-    p[W2:B2] = f16(p[W2:B2])
+    p[W1:B2] = f16(p[W1:B2])
+    p[W3:B3] = f16(p[W3:B3])
     return p
 
 
@@ -74,7 +74,7 @@ def sigmoid(z):
 def forward(params, x, contract: bool = True):
     """Multiplier m for feature rows x [n][6].  contract applies the engine's
     arithmetic contract: BF16 parameter values, FP16 matrix operands (weights,
-    features, first-layer activations); everything else in FP64 here."""
+    features, both hidden activations); everything else in FP64 here."""
     p = contract_params(params) if contract else np.asarray(params, np.float64)
     w1, b1, w2, b2, w3, b3 = unpack(p)
     x = f16(x) if contract else np.asarray(x, np.float64)
@@ -83,8 +83,9 @@ def forward(params, x, contract: bool = True):
     a1q = f16(a1) if contract else a1
     h2 = a1q @ w2.T + b2
     a2 = gelu(h2)
-    z = a2 @ w3 + b3
-    return softplus(z), (x, h1, a1q, h2, a2, z)
+    a2q = f16(a2) if contract else a2
+    z = a2q @ w3 + b3
+    return softplus(z), (x, h1, a1q, h2, a2q, z)
 
 
 def loss_and_grad(params, x, t, contract: bool = True):

@@ -122,7 +122,8 @@ namespace {
 // learned closure: the 6-32-32-1 MLP of the engine's closure (parameter layout
 // W1[32][6], b1[32], W2[32][32], b2[32], W3[32], b3), evaluated in FP64 under the
 // engine's operand contract: BF16 parameter values, FP16 matrix operands (the
-// weights W1, W2, the features and the first-layer activations).  No counterpart in the reference (its closure is lbm.cu:42-60).
+// weights W1, W2, W3, the bias b1, the features and both hidden activations).
+// No counterpart in the reference (its closure is lbm.cu:42-60).
 // ---------------------------------------------------------------------------
 double bf16_round(double x) {
     float f = float(x);
@@ -144,11 +145,11 @@ double f16_round(double x) {
 }
 double gelu(double x) { return 0.5 * x * (1 + std::tanh(0.7978845608028654 * (x + 0.044715 * x * x * x))); }
 
-// BF16 values of the parameters, W1 (0..191) and W2 (224..1247) also FP16
+// BF16 values of the parameters, W1, b1, W2 (0..1247) and W3 (1280..1311) also FP16
 void contract_params(const float* params, double* w) {
     for (int k = 0; k < 1313; k++) {
         w[k] = bf16_round(params[k]);
-        if (k < 192 || (k >= 224 && k < 1248)) w[k] = f16_round(w[k]);
+        if (k < 1248 || (k >= 1280 && k < 1312)) w[k] = f16_round(w[k]);
     }
 }
 
@@ -165,7 +166,7 @@ double mlp_multiplier(const double* w, const double* x) {
     for (int i = 0; i < 32; i++) {
         double h = w[1248 + i];
         for (int j = 0; j < 32; j++) h += w[224 + i * 32 + j] * a1[j];
-        z += w[1280 + i] * gelu(h);
+        z += w[1280 + i] * f16_round(gelu(h));
     }
     return z > 20 ? z : std::log1p(std::exp(z));
 }
