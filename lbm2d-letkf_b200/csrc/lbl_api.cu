@@ -246,7 +246,7 @@ void enqueue_steps(lbl_ctx* ctx, int n, int cur, cudaStream_t s, bool force_done
         const int src = (cur + k) & 1, dst = src ^ 1;
         const bool mac = k >= n - 2;
         launch_lbm_step(ctx, src, dst, ctx->d_force + size_t(k) * 2 * ctx->P.nxy,
-                        mac ? ctx->mac[dst] : nullptr, s);
+                        mac ? ctx->mac[dst] : nullptr, s, /*pdl=*/k > 0);
     }
 }
 

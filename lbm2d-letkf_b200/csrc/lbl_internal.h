@@ -155,7 +155,10 @@ void launch_ic_velocity(const double* modes /*[4][n]*/, int n_modes, int nx, int
                         float* u, float* v, cudaStream_t s);
 void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s);
 // one step from population buffer src to dst (FP32 or FP16 storage)
-void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s);
+// pdl: the previous launch on s is the previous step; the launch may then overlap its
+// tail (programmatic dependent launch; the kernel waits for that grid's completion)
+void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s,
+                     bool pdl = false);
 // strip height of the stream-collide for this grid, ensemble and kernel variant
 // (occupancy heuristic); call outside stream capture
 int lbm_strip_rows(const lbl_ctx* c);

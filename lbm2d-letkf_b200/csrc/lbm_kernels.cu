@@ -470,6 +470,12 @@ __global__ void __launch_bounds__(MAXT, (CL && MAXT == 256) ? 2 : 1)
     // columns across a chunk edge from the neighbour CTA's ring (distributed shared
     // memory); the per-row barrier becomes a cluster barrier.
     extern __shared__ float s_uv[];  // [3][2][W]; CL: + packed closure + per-warp staging
+    // Programmatic dependent launch (a no-op for an ordinary launch): the previous
+    // step's grid is complete, its populations written, before any is read or written
+    // here; then the next step's CTAs may start launching into the slots this grid
+    // frees, so the launch gap between steps overlaps this grid's tail.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" :::);
     const int nx = NX ? NX : P.nx, ny = NX ? NX : P.ny, nxy = NX ? NX * NX : P.nxy;
     const int W = CLU ? int(blockDim.x) : nx;  // columns of this CTA
     const int xl = threadIdx.x;
@@ -919,15 +925,35 @@ void launch_tma(const lbl_ctx* c, dim3 grid, int ty, int b, float* fout, const f
         lbm_step_tma_kernel<false, NX><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, nullptr, P, ty, box, c->d_err);
 }
 
+// a stream-collide launch, with programmatic stream serialization when the previous
+// launch on the stream is the previous step (pdl)
+template <typename... KArgs, typename... Args>
+void launch_step(void (*kernel)(KArgs...), dim3 grid, int threads, size_t sm, cudaStream_t s, bool pdl,
+                 Args... args) {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = grid;
+    lc.blockDim = dim3(threads);
+    lc.dynamicSmemBytes = sm;
+    lc.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&lc, kernel, args...);
+}
+
 template <int MAXT, int NX, typename T>
 void launch_direct_t(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout, const float* force,
-                     float* mac_out, cudaStream_t s) {
+                     float* mac_out, cudaStream_t s, bool pdl) {
     const Phys& P = c->P;
     const size_t sm = sizeof(float) * 6 * P.nx;
     if (mac_out)
-        lbm_step_kernel<true, MAXT, NX, T><<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty, nullptr, {});
+        launch_step(lbm_step_kernel<true, MAXT, NX, T>, grid, P.nx, sm, s, pdl, fin, fout, force, mac_out, P, ty,
+                    static_cast<const uint32_t*>(nullptr), ClosureScales{});
     else
-        lbm_step_kernel<false, MAXT, NX, T><<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty, nullptr, {});
+        launch_step(lbm_step_kernel<false, MAXT, NX, T>, grid, P.nx, sm, s, pdl, fin, fout, force,
+                    static_cast<float*>(nullptr), P, ty, static_cast<const uint32_t*>(nullptr), ClosureScales{});
 }
 
 // rows wider than 1024 columns: clusters of cluster_chunks(nx) CTAs per strip
@@ -973,32 +999,33 @@ void launch_cluster(const lbl_ctx* c, int strips, int ty, int src, int dst, cons
 // learned-closure variant (nx % 32 == 0 and nx <= 1024, checked by lbl_set_closure)
 template <int MAXT, int NX, typename T>
 void launch_closure_t(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout, const float* force,
-                      float* mac_out, cudaStream_t s) {
+                      float* mac_out, cudaStream_t s, bool pdl) {
     const Phys& P = c->P;
     const size_t sm = closure_step_smem(P.nx);
+    const uint32_t* pk = c->d_closure;
     if (mac_out)
-        lbm_step_kernel<true, MAXT, NX, T, true>
-            <<<grid, P.nx, sm, s>>>(fin, fout, force, mac_out, P, ty, c->d_closure, c->closure_sc);
+        launch_step(lbm_step_kernel<true, MAXT, NX, T, true>, grid, P.nx, sm, s, pdl, fin, fout, force, mac_out, P,
+                    ty, pk, c->closure_sc);
     else
-        lbm_step_kernel<false, MAXT, NX, T, true>
-            <<<grid, P.nx, sm, s>>>(fin, fout, force, nullptr, P, ty, c->d_closure, c->closure_sc);
+        launch_step(lbm_step_kernel<false, MAXT, NX, T, true>, grid, P.nx, sm, s, pdl, fin, fout, force,
+                    static_cast<float*>(nullptr), P, ty, pk, c->closure_sc);
 }
 template <int MAXT, int NX>
 void launch_closure(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
-                    cudaStream_t s) {
+                    cudaStream_t s, bool pdl) {
     if (c->f16)
-        launch_closure_t<MAXT, NX, __half>(c, grid, ty, c->h[src], c->h[dst], force, mac_out, s);
+        launch_closure_t<MAXT, NX, __half>(c, grid, ty, c->h[src], c->h[dst], force, mac_out, s, pdl);
     else
-        launch_closure_t<MAXT, NX, float>(c, grid, ty, c->f[src], c->f[dst], force, mac_out, s);
+        launch_closure_t<MAXT, NX, float>(c, grid, ty, c->f[src], c->f[dst], force, mac_out, s, pdl);
 }
 
 template <int MAXT, int NX>
 void launch_direct(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
-                   cudaStream_t s) {
+                   cudaStream_t s, bool pdl) {
     if (c->f16)
-        launch_direct_t<MAXT, NX, __half>(c, grid, ty, c->h[src], c->h[dst], force, mac_out, s);
+        launch_direct_t<MAXT, NX, __half>(c, grid, ty, c->h[src], c->h[dst], force, mac_out, s, pdl);
     else
-        launch_direct_t<MAXT, NX, float>(c, grid, ty, c->f[src], c->f[dst], force, mac_out, s);
+        launch_direct_t<MAXT, NX, float>(c, grid, ty, c->f[src], c->f[dst], force, mac_out, s, pdl);
 }
 }  // namespace
 
@@ -1008,7 +1035,8 @@ int lbm_tma_prepare(int nx) {
            tma_prepare_nx<512>(sm);
 }
 
-void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s) {
+void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s,
+                     bool pdl) {
     const Phys& P = c->P;
     const int sq = (P.nx == P.ny) ? P.nx : 0;
 
@@ -1031,20 +1059,20 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
         return;
     }
     if (c->closure) {
-        if (sq == 256) launch_closure<256, 256>(c, grid, ty, src, dst, force, mac_out, s);
-        else if (P.nx <= 256) launch_closure<256, 0>(c, grid, ty, src, dst, force, mac_out, s);
-        else launch_closure<1024, 0>(c, grid, ty, src, dst, force, mac_out, s);
+        if (sq == 256) launch_closure<256, 256>(c, grid, ty, src, dst, force, mac_out, s, pdl);
+        else if (P.nx <= 256) launch_closure<256, 0>(c, grid, ty, src, dst, force, mac_out, s, pdl);
+        else launch_closure<1024, 0>(c, grid, ty, src, dst, force, mac_out, s, pdl);
         return;
     }
     switch (sq) {
-        case 64: launch_direct<256, 64>(c, grid, ty, src, dst, force, mac_out, s); break;
-        case 128: launch_direct<256, 128>(c, grid, ty, src, dst, force, mac_out, s); break;
-        case 256: launch_direct<256, 256>(c, grid, ty, src, dst, force, mac_out, s); break;
-        case 512: launch_direct<1024, 512>(c, grid, ty, src, dst, force, mac_out, s); break;
-        case 1024: launch_direct<1024, 1024>(c, grid, ty, src, dst, force, mac_out, s); break;
+        case 64: launch_direct<256, 64>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        case 128: launch_direct<256, 128>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        case 256: launch_direct<256, 256>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        case 512: launch_direct<1024, 512>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        case 1024: launch_direct<1024, 1024>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
         default:
-            if (P.nx <= 256) launch_direct<256, 0>(c, grid, ty, src, dst, force, mac_out, s);
-            else launch_direct<1024, 0>(c, grid, ty, src, dst, force, mac_out, s);
+            if (P.nx <= 256) launch_direct<256, 0>(c, grid, ty, src, dst, force, mac_out, s, pdl);
+            else launch_direct<1024, 0>(c, grid, ty, src, dst, force, mac_out, s, pdl);
     }
 }
 
