@@ -166,12 +166,21 @@ int lbl_assimilate_files(lbl_ctx* ctx, int t, const char* io_prefix);
  * n_fc forecast steps, launched as one CUDA graph.  NULL observation pointers
  * reuse the observations already resident on the device from the previous call. */
 int lbl_cycle_async(lbl_ctx* ctx, int t, const float* rho_o, const float* u_o, const float* v_o, int n_fc);
-int lbl_sync(lbl_ctx* ctx);
+int lbl_sync(lbl_ctx* ctx);  /* also waits for a pending lbl_output_async writer */
 
 /* output(dat, mpi, t) (io.cu:22-266): writes the reference's .dat files under
  * io_prefix for the mode (calc/, nature/, observed/, ensemble statistics).
- * Gate `t % (iiter*ioprune) == 0` as in the reference. */
+ * Gate `t % (iiter*ioprune) == 0` as in the reference.  The vorticity and the
+ * ensemble statistics are computed on the GPU in the reference's FP32 operation
+ * order (the files match its host loops bit for bit). */
 int lbl_output(lbl_ctx* ctx, int t, const char* io_prefix);
+/* The same output without waiting for the files: the fields are computed and copied
+ * to a pinned staging buffer in stream order, and a host thread writes the files
+ * while later forecasts run.  The next lbl_output / lbl_output_async, lbl_sync,
+ * lbl_get_observed, lbl_assimilate_files or lbl_destroy waits for that writer and
+ * returns its status (LBL_ERR_NAN, LBL_ERR_IO).  (The reference writes synchronously,
+ * io.cu:22-266.) */
+int lbl_output_async(lbl_ctx* ctx, int t, const char* io_prefix);
 
 /* Field access (parity injection and inspection). */
 int lbl_get_f(lbl_ctx* ctx, int member, float* f /* 9*nx*ny */);

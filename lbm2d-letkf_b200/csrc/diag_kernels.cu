@@ -61,7 +61,58 @@ __global__ void rmse_kernel(const float* __restrict__ mac, int nxy, int M, const
     block_add(s, red);
 }
 
+// Output fields of every member and the ensemble statistics, in the reference's
+// FP32 operation order so that the files match its host loops bit for bit
+// (io.cu:61-139): vor = (ve - vw) / (2 dx) - (un - us) / (2 dx) per member; over the
+// members in order, mean_u += u, mean_v += v, mean_w += vor, w2 += (1/M)(vor vor);
+// then means *= 1/M and std = sqrt(w2 - mean_w^2) (all zero for M = 1).  Every
+// operation is an explicitly rounded intrinsic, so nothing is contracted into an FMA.
+// A NaN vorticity sets *nan (io.cu:79-83).
+__global__ void output_fields_kernel(const float* __restrict__ mac, int nx, int ny, int M, float two_dx,
+                                     float* __restrict__ vor, float* __restrict__ stats, int* __restrict__ nan) {
+    const int nxy = nx * ny;
+    const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ij >= nxy) return;
+    const int i = ij % nx, j = ij / nx;
+    const int ie = j * nx + (i + 1) % nx, iw = j * nx + (i - 1 + nx) % nx;
+    const int jn = ((j + 1) % ny) * nx + i, js = ((j - 1 + ny) % ny) * nx + i;
+    const float iv = __fdiv_rn(1.f, float(M));
+    float um = 0.f, vm = 0.f, wm = 0.f, w2 = 0.f;
+    bool bad = false;
+    for (int m = 0; m < M; m++) {
+        const float* u = mac + (size_t(m) * 3 + 1) * nxy;
+        const float* v = mac + (size_t(m) * 3 + 2) * nxy;
+        const float uy = __fdiv_rn(__fsub_rn(u[jn], u[js]), two_dx);
+        const float vx = __fdiv_rn(__fsub_rn(v[ie], v[iw]), two_dx);
+        const float w = __fsub_rn(vx, uy);
+        vor[size_t(m) * nxy + ij] = w;
+        bad |= (w != w);
+        um = __fadd_rn(um, u[ij]);
+        vm = __fadd_rn(vm, v[ij]);
+        wm = __fadd_rn(wm, w);
+        w2 = __fadd_rn(w2, __fmul_rn(iv, __fmul_rn(w, w)));
+    }
+    if (M > 1) {
+        um = __fmul_rn(um, iv);
+        vm = __fmul_rn(vm, iv);
+        wm = __fmul_rn(wm, iv);
+        w2 = __fsqrt_rn(__fsub_rn(w2, __fmul_rn(wm, wm)));
+    } else {
+        um = vm = wm = w2 = 0.f;
+    }
+    stats[ij] = um;
+    stats[nxy + ij] = vm;
+    stats[2 * nxy + ij] = wm;
+    stats[3 * nxy + ij] = w2;
+    if (bad) atomicOr(nan, 1);
+}
+
 }  // namespace
+
+void launch_output_fields(const lbl_ctx* c, const float* mac, float* vor, float* stats, int* nan, cudaStream_t s) {
+    output_fields_kernel<<<(c->P.nxy + 255) / 256, 256, 0, s>>>(mac, c->P.nx, c->P.ny, c->P.M, c->P.two_dx, vor,
+                                                                 stats, nan);
+}
 
 void launch_diag(const lbl_ctx* c, const float* mac, int member, double* red, cudaStream_t s) {
     const int m0 = member < 0 ? 0 : member, m1 = member < 0 ? c->P.M : member + 1;

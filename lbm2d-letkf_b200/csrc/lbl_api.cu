@@ -21,6 +21,8 @@ using namespace lbl;
 
 namespace {
 
+int wait_output(lbl_ctx* ctx);
+
 #define LBL_CK(call)                                                                            \
     do {                                                                                        \
         cudaError_t e_ = (call);                                                                \
@@ -580,6 +582,7 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
 
 void destroy_impl(lbl_ctx* ctx) {
     cudaSetDevice(ctx->device);
+    if (ctx->out_thread.joinable()) ctx->out_thread.join();
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
     ctx->graphs.clear();
@@ -600,6 +603,9 @@ void destroy_impl(lbl_ctx* ctx) {
         for (auto& e : ctx->user_ev) cudaEventDestroy(e);
     }
     if (ctx->obs_engine) obs_engine_free(ctx->obs_engine);
+    cudaFree(ctx->d_outf);
+    if (ctx->h_outf) cudaFreeHost(ctx->h_outf);
+    if (ctx->out_ev) cudaEventDestroy(ctx->out_ev);
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
     if (ctx->side) cudaStreamDestroy(ctx->side);
@@ -792,6 +798,85 @@ int assimilate_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
     return LBL_OK;
 }
 
+// The files of one output (io.cu:22-266) from the staged copy: macros mh [M][3][nxy],
+// vorticity vor [M][nxy], statistics st [4][nxy], NaN flag.  Runs on the writer thread;
+// touches only the staging, the OBSERVE engine and h_obs, which no other call uses
+// while an output is pending.
+int write_output_files(lbl_ctx* ctx, int t, const std::string& pre, std::string& err) {
+    const lbl_config& cfg = ctx->cfg;
+    const int nx = cfg.nx, ny = cfg.ny, M = cfg.n_ens;
+    const size_t nxy = size_t(nx) * ny;
+    const float* mh = ctx->h_outf;
+    const float* vor = mh + size_t(M) * 3 * nxy;
+    const float* st = vor + size_t(M) * nxy;
+    int nan_flag = 0;
+    std::memcpy(&nan_flag, st + 4 * nxy, sizeof(int));
+    if (nan_flag) { err = "nan value detected"; return LBL_ERR_NAN; }  // io.cu:79-83
+    const std::string step = "_step" + to_string_aligned(t / cfg.iiter, 10) + ".dat";
+    auto dname = [&](const std::string& kind, int id) { return pre + "/" + kind + "/ens" + to_string_aligned(id, 4); };
+    auto mkdir = [&](const std::string& d) {
+        if (mkdir_p(d) == 0) return LBL_OK;
+        err = "could not create " + d;
+        return LBL_ERR_IO;
+    };
+    if (cfg.mode == LBL_MODE_DA_LETKF) {                            // ENSEMBLE_STAT (io.cu:88-139)
+        LBL_TRY(mkdir(pre + "/calc"));
+        LBL_TRY(write_dat(pre + "/calc/ens_mean_u" + step, st, nxy, err));
+        LBL_TRY(write_dat(pre + "/calc/ens_mean_v" + step, st + nxy, nxy, err));
+        LBL_TRY(write_dat(pre + "/calc/ens_vor_mean" + step, st + 2 * nxy, nxy, err));
+        LBL_TRY(write_dat(pre + "/calc/ens_vor_std" + step, st + 3 * nxy, nxy, err));
+    }
+    for (int m = 0; m < M; m++) {
+        const int id = m + ctx->ens_offset;
+        const float* r = mh + (size_t(m) * 3 + 0) * nxy;
+        const float* u = mh + (size_t(m) * 3 + 1) * nxy;
+        const float* v = mh + (size_t(m) * 3 + 2) * nxy;
+        const float* w = vor + size_t(m) * nxy;
+        if (cfg.mode != LBL_MODE_OBSERVE) {                          // io.cu:151-157
+            const std::string d = dname("calc", id);
+            LBL_TRY(mkdir(d));
+            LBL_TRY(write_dat(d + "/vor" + step, w, nxy, err));
+            LBL_TRY(write_dat(d + "/rho" + step, r, nxy, err));
+            LBL_TRY(write_dat(d + "/u" + step, u, nxy, err));
+            LBL_TRY(write_dat(d + "/v" + step, v, nxy, err));
+        }
+        if (cfg.mode == LBL_MODE_OBSERVE && id == 0) {               // io.cu:160-246
+            if (!ctx->obs_engine) ctx->obs_engine = obs_engine_new(uint32_t(cfg.obs_seed + id));
+            for (auto& a : ctx->h_obs) a.resize(nxy);
+            observe_host(ctx->obs_engine, nx, ny, cfg.da_xyprune, float(cfg.obs_error_rho), float(cfg.obs_error_u),
+                         r, u, v, ctx->h_obs[0].data(), ctx->h_obs[1].data(), ctx->h_obs[2].data(),
+                         ctx->h_obs[3].data(), ctx->P.dx);
+            const std::string d = dname("observed", id);
+            LBL_TRY(mkdir(d));
+            LBL_TRY(write_dat(d + "/rho" + step, ctx->h_obs[0].data(), nxy, err));
+            LBL_TRY(write_dat(d + "/u" + step, ctx->h_obs[1].data(), nxy, err));
+            LBL_TRY(write_dat(d + "/v" + step, ctx->h_obs[2].data(), nxy, err));
+            LBL_TRY(write_dat(d + "/vor" + step, ctx->h_obs[3].data(), nxy, err));
+        }
+        if ((cfg.mode == LBL_MODE_NATURE || cfg.mode == LBL_MODE_OBSERVE) && id == 0) {  // io.cu:248-258
+            const std::string d = dname("nature", id);
+            LBL_TRY(mkdir(d));
+            LBL_TRY(write_dat(d + "/rho" + step, r, nxy, err));
+            LBL_TRY(write_dat(d + "/u" + step, u, nxy, err));
+            LBL_TRY(write_dat(d + "/v" + step, v, nxy, err));
+            LBL_TRY(write_dat(d + "/vor" + step, w, nxy, err));
+        }
+    }
+    return LBL_OK;
+}
+
+// Waits for the writer of the previous output and returns its status.
+int wait_output(lbl_ctx* ctx) {
+    if (ctx->out_thread.joinable()) ctx->out_thread.join();
+    const int rc = ctx->out_rc;
+    if (rc != LBL_OK) {
+        ctx->err = ctx->out_err;
+        ctx->out_rc = LBL_OK;
+        ctx->out_err.clear();
+    }
+    return rc;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -888,6 +973,7 @@ int lbl_sync(lbl_ctx* ctx) {
     if (!ctx) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
     LBL_CK(cudaStreamSynchronize(ctx->stream));
+    LBL_TRY(wait_output(ctx));
     LBL_TRY(check_timeout(ctx));
     if (ctx->cfg.mode == LBL_MODE_DA_LETKF) LBL_TRY(read_stats(ctx));
     return LBL_OK;
@@ -907,6 +993,7 @@ int lbl_assimilate_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, 
 
 int lbl_assimilate_files(lbl_ctx* ctx, int t, const char* io_prefix) {
     if (!ctx || !io_prefix) return LBL_ERR_ARG;
+    LBL_TRY(wait_output(ctx));  // an OBSERVE output of this context may still be writing the files
     if (!is_da_mode(ctx->cfg.mode)) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate needs mode DA_LETKF or DA_NUDGING");
     if (ctx->cfg.da_dummy) return LBL_OK;                           // DA_DUMMY (main.cu:94)
     if (!da_due(ctx, t)) {
@@ -953,87 +1040,53 @@ int lbl_cycle_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
     return LBL_OK;
 }
 
-int lbl_output(lbl_ctx* ctx, int t, const char* io_prefix) {
+int lbl_output_async(lbl_ctx* ctx, int t, const char* io_prefix) {
     if (!ctx || !io_prefix) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
     const lbl_config& cfg = ctx->cfg;
     if (t % (cfg.iiter * cfg.ioprune) != 0) return LBL_OK;          // io.cu:23
-    const int nx = cfg.nx, ny = cfg.ny, M = cfg.n_ens;
-    const size_t nxy = size_t(nx) * ny;
+    LBL_TRY(wait_output(ctx));                                       // the staging is free again
+    const size_t nxy = size_t(ctx->P.nxy), M = size_t(ctx->P.M);
+    const size_t n_dev = (M + 4) * nxy + 4, n_host = 3 * M * nxy + n_dev;
+    if (!ctx->d_outf) {
+        LBL_CK(cudaMalloc(&ctx->d_outf, sizeof(float) * n_dev));
+        LBL_CK(cudaMallocHost(&ctx->h_outf, sizeof(float) * n_host));
+        LBL_CK(cudaEventCreateWithFlags(&ctx->out_ev, cudaEventDisableTiming));
+    }
+    int* d_nan = reinterpret_cast<int*>(ctx->d_outf + (M + 4) * nxy);
+    LBL_CK(cudaMemsetAsync(d_nan, 0, sizeof(int), ctx->stream));
+    launch_output_fields(ctx, ctx->mac[ctx->cur], ctx->d_outf, ctx->d_outf + M * nxy, d_nan, ctx->stream);
+    LBL_CK(cudaGetLastError());
+    LBL_CK(cudaMemcpyAsync(ctx->h_outf, ctx->mac[ctx->cur], sizeof(float) * 3 * M * nxy, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    LBL_CK(cudaMemcpyAsync(ctx->h_outf + 3 * M * nxy, ctx->d_outf, sizeof(float) * n_dev, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    LBL_CK(cudaEventRecord(ctx->out_ev, ctx->stream));
     const std::string pre(io_prefix);
-    const std::string step = "_step" + to_string_aligned(t / cfg.iiter, 10) + ".dat";
-    std::vector<float> mh(size_t(M) * 3 * nxy);
-    LBL_CK(cudaStreamSynchronize(ctx->stream));
-    LBL_CK(cudaMemcpy(mh.data(), ctx->mac[ctx->cur], sizeof(float) * mh.size(), cudaMemcpyDeviceToHost));
-    std::vector<float> vor(size_t(M) * nxy);
-    for (int m = 0; m < M; m++) {
-        const float* u = mh.data() + (size_t(m) * 3 + 1) * nxy;
-        const float* v = mh.data() + (size_t(m) * 3 + 2) * nxy;
-        vorticity_host(nx, ny, ctx->P.dx, u, v, vor.data() + size_t(m) * nxy);
-        for (size_t ij = 0; ij < nxy; ij++)
-            if (std::isnan(vor[size_t(m) * nxy + ij])) return fail(ctx, LBL_ERR_NAN, "nan value detected");  // io.cu:79-83
-    }
-    auto dname = [&](const std::string& kind, int id) { return pre + "/" + kind + "/ens" + to_string_aligned(id, 4); };
-    if (cfg.mode == LBL_MODE_DA_LETKF) {                            // ENSEMBLE_STAT (io.cu:88-139)
-        std::vector<float> um(nxy, 0.f), vm(nxy, 0.f), wm(nxy, 0.f), w2(nxy, 0.f), ws(nxy, 0.f);
-        if (M > 1) {
-            const float iv = float(1) / M;
-            for (int m = 0; m < M; m++)
-                for (size_t ij = 0; ij < nxy; ij++) {
-                    wm[ij] += vor[size_t(m) * nxy + ij];
-                    um[ij] += mh[(size_t(m) * 3 + 1) * nxy + ij];
-                    vm[ij] += mh[(size_t(m) * 3 + 2) * nxy + ij];
-                    const float a = vor[size_t(m) * nxy + ij];
-                    w2[ij] += iv * (a * a);
-                }
-            for (size_t ij = 0; ij < nxy; ij++) {
-                wm[ij] *= iv; um[ij] *= iv; vm[ij] *= iv;
-                ws[ij] = std::sqrt(w2[ij] - wm[ij] * wm[ij]);
+    try {
+        ctx->out_thread = std::thread([ctx, t, pre]() {
+            std::string err;
+            int rc = LBL_OK;
+            cudaSetDevice(ctx->device);
+            const cudaError_t e = cudaEventSynchronize(ctx->out_ev);
+            if (e != cudaSuccess) {
+                rc = LBL_ERR_CUDA;
+                err = std::string("output staging copy: ") + cudaGetErrorString(e);
+            } else {
+                rc = write_output_files(ctx, t, pre, err);
             }
-        }
-        if (mkdir_p(pre + "/calc") != 0) return fail(ctx, LBL_ERR_IO, "could not create " + pre + "/calc");
-        LBL_TRY(write_dat(pre + "/calc/ens_mean_u" + step, um.data(), nxy, ctx->err));
-        LBL_TRY(write_dat(pre + "/calc/ens_mean_v" + step, vm.data(), nxy, ctx->err));
-        LBL_TRY(write_dat(pre + "/calc/ens_vor_mean" + step, wm.data(), nxy, ctx->err));
-        LBL_TRY(write_dat(pre + "/calc/ens_vor_std" + step, ws.data(), nxy, ctx->err));
-    }
-    for (int m = 0; m < M; m++) {
-        const int id = m + ctx->ens_offset;
-        const float* r = mh.data() + (size_t(m) * 3 + 0) * nxy;
-        const float* u = mh.data() + (size_t(m) * 3 + 1) * nxy;
-        const float* v = mh.data() + (size_t(m) * 3 + 2) * nxy;
-        const float* w = vor.data() + size_t(m) * nxy;
-        if (cfg.mode != LBL_MODE_OBSERVE) {                          // io.cu:151-157
-            const std::string d = dname("calc", id);
-            if (mkdir_p(d) != 0) return fail(ctx, LBL_ERR_IO, "could not create " + d);
-            LBL_TRY(write_dat(d + "/vor" + step, w, nxy, ctx->err));
-            LBL_TRY(write_dat(d + "/rho" + step, r, nxy, ctx->err));
-            LBL_TRY(write_dat(d + "/u" + step, u, nxy, ctx->err));
-            LBL_TRY(write_dat(d + "/v" + step, v, nxy, ctx->err));
-        }
-        if (cfg.mode == LBL_MODE_OBSERVE && id == 0) {               // io.cu:160-246
-            if (!ctx->obs_engine) ctx->obs_engine = obs_engine_new(uint32_t(cfg.obs_seed + id));
-            for (auto& a : ctx->h_obs) a.resize(nxy);
-            observe_host(ctx->obs_engine, nx, ny, cfg.da_xyprune, float(cfg.obs_error_rho), float(cfg.obs_error_u),
-                         r, u, v, ctx->h_obs[0].data(), ctx->h_obs[1].data(), ctx->h_obs[2].data(),
-                         ctx->h_obs[3].data(), ctx->P.dx);
-            const std::string d = dname("observed", id);
-            if (mkdir_p(d) != 0) return fail(ctx, LBL_ERR_IO, "could not create " + d);
-            LBL_TRY(write_dat(d + "/rho" + step, ctx->h_obs[0].data(), nxy, ctx->err));
-            LBL_TRY(write_dat(d + "/u" + step, ctx->h_obs[1].data(), nxy, ctx->err));
-            LBL_TRY(write_dat(d + "/v" + step, ctx->h_obs[2].data(), nxy, ctx->err));
-            LBL_TRY(write_dat(d + "/vor" + step, ctx->h_obs[3].data(), nxy, ctx->err));
-        }
-        if ((cfg.mode == LBL_MODE_NATURE || cfg.mode == LBL_MODE_OBSERVE) && id == 0) {  // io.cu:248-258
-            const std::string d = dname("nature", id);
-            if (mkdir_p(d) != 0) return fail(ctx, LBL_ERR_IO, "could not create " + d);
-            LBL_TRY(write_dat(d + "/rho" + step, r, nxy, ctx->err));
-            LBL_TRY(write_dat(d + "/u" + step, u, nxy, ctx->err));
-            LBL_TRY(write_dat(d + "/v" + step, v, nxy, ctx->err));
-            LBL_TRY(write_dat(d + "/vor" + step, w, nxy, ctx->err));
-        }
+            ctx->out_err = err;
+            ctx->out_rc = rc;
+        });
+    } catch (const std::exception& ex) {
+        return fail(ctx, LBL_ERR_NOMEM, std::string("could not start the output writer: ") + ex.what());
     }
     return LBL_OK;
+}
+
+int lbl_output(lbl_ctx* ctx, int t, const char* io_prefix) {
+    LBL_TRY(lbl_output_async(ctx, t, io_prefix));
+    return wait_output(ctx);
 }
 
 int lbl_get_f(lbl_ctx* ctx, int member, float* f) {
@@ -1128,6 +1181,7 @@ int lbl_get_force_state(lbl_ctx* ctx, float* randoms, float* kx, float* ky, floa
 
 int lbl_get_observed(lbl_ctx* ctx, float* rho_o, float* u_o, float* v_o, float* vor_o) {
     if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(wait_output(ctx));
     if (ctx->h_obs[0].empty()) return fail(ctx, LBL_ERR_STATE, "no observation generated yet (OBSERVE output)");
     const size_t n = sizeof(float) * ctx->P.nxy;
     if (rho_o) std::memcpy(rho_o, ctx->h_obs[0].data(), n);

@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lbl.h"
@@ -132,6 +133,15 @@ struct lbl_ctx {
     int ty_default = 0;                  // the heuristic's strip height for the kernel that runs
     int* d_err = nullptr;                // bounded-wait timeout flag of the TMA kernel
 
+    // asynchronous output (lbl_output_async): vorticity and ensemble statistics on the
+    // device, one pinned staging copy, and a writer thread for the files
+    float* d_outf = nullptr;             // [M][nxy] vorticity, [4][nxy] statistics, 1 int NaN flag
+    float* h_outf = nullptr;             // pinned: [M][3][nxy] macros, then the above
+    cudaEvent_t out_ev = nullptr;        // the staging copy is complete
+    std::thread out_thread;
+    int out_rc = 0;                      // the writer's status and message
+    std::string out_err;
+
     // learned closure (closure.h): fragment-ordered BF16 parameters, feature scales
     uint32_t* d_closure = nullptr;       // [kPackWords]
     bool closure = false;
@@ -216,6 +226,9 @@ void launch_analysis_args(const AnalysisArgs& a, cudaStream_t s);
 
 // ---- kernels (diag_kernels.cu) ----
 void launch_diag(const lbl_ctx* c, const float* mac, int member, double* red, cudaStream_t s);
+// per-member vorticity [M][nxy] and ensemble statistics [4][nxy] (mean u, mean v,
+// mean vor, std vor) in the reference's FP32 order; *nan |= 1 on a NaN vorticity
+void launch_output_fields(const lbl_ctx* c, const float* mac, float* vor, float* stats, int* nan, cudaStream_t s);
 void launch_rmse(const lbl_ctx* c, const float* mac, const float* ut, const float* vt, double* red,
                  cudaStream_t s);
 

@@ -131,13 +131,14 @@ int main(int argc, char** argv) {
             lbl_timer_transit(ctx, T, "_sync.DA");
         }
         lbl_timer_transit(ctx, T, "output");
-        check(ctx, lbl_output(ctx, t, prefix.c_str()), "output");
+        check(ctx, lbl_output_async(ctx, t, prefix.c_str()), "output");  // files written beside the next steps
         lbl_timer_transit(ctx, T, "_sync.output");
         lbl_timer_transit(ctx, T, "forecast");
         check(ctx, lbl_update(ctx, t, cfg.iiter), "forecast");
         lbl_timer_transit(ctx, T, "_sync.forecast");
     }
     lbl_timer_transit(ctx, T, "_ignored");
+    check(ctx, lbl_sync(ctx), "output");  // the last files are written and their status known
 
     const std::string main_csv = timer_text(ctx, T);
     const double fc = timer_get(main_csv, "forecast"), out = timer_get(main_csv, "output"), t_da = timer_get(main_csv, "DA");

@@ -44,7 +44,7 @@ STORAGE_F32, STORAGE_F16 = 0, 1
 EXPORTS = (
     "lbl_config_default", "lbl_create", "lbl_destroy", "lbl_last_error", "lbl_version", "lbl_init",
     "lbl_update", "lbl_update_async", "lbl_assimilate", "lbl_assimilate_async", "lbl_assimilate_files",
-    "lbl_cycle_async", "lbl_sync", "lbl_output", "lbl_get_f", "lbl_set_f", "lbl_get_fields",
+    "lbl_cycle_async", "lbl_sync", "lbl_output", "lbl_output_async", "lbl_get_f", "lbl_set_f", "lbl_get_fields",
     "lbl_get_ens_stats", "lbl_get_force", "lbl_get_force_state", "lbl_get_observed",
     "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_timer_csv", "lbl_timer_clear",
     "lbl_timer_transit", "lbl_profile_step", "lbl_get_cycle_phases", "lbl_event_record", "lbl_event_elapsed",
@@ -120,6 +120,7 @@ def load_library() -> ctypes.CDLL:
         "lbl_cycle_async": (I, [P, I, F, F, F, I]),
         "lbl_sync": (I, [P]),
         "lbl_output": (I, [P, I, ctypes.c_char_p]),
+        "lbl_output_async": (I, [P, I, ctypes.c_char_p]),
         "lbl_get_f": (I, [P, I, F]),
         "lbl_set_f": (I, [P, I, F]),
         "lbl_get_fields": (I, [P, I, F, F, F, F]),
@@ -257,8 +258,11 @@ class Ensemble:
     def sync(self):
         self._check(self.lib.lbl_sync(self._h), "lbl_sync")
 
-    def output(self, t: int, io_prefix: str = "io"):
-        self._check(self.lib.lbl_output(self._h, t, io_prefix.encode()), "lbl_output")
+    def output(self, t: int, io_prefix: str = "io", sync: bool = True):
+        """The reference's output files; sync=False leaves the file writing to a host
+        thread (lbl_output_async) that the next output or sync() waits for."""
+        fn = self.lib.lbl_output if sync else self.lib.lbl_output_async
+        self._check(fn(self._h, t, io_prefix.encode()), "lbl_output")
 
     # -- accessors --------------------------------------------------------------
     def get_f(self, member: int) -> np.ndarray:

@@ -77,6 +77,59 @@ def test_da_output_with_ensemble_statistics(tmp_path):
     np.testing.assert_allclose(um, us.mean(0), rtol=1e-5, atol=1e-9)
 
 
+def _stats_like_reference(us, vs, ws):
+    """io.cu:88-139 in FP32, members summed in order, one rounding per operation."""
+    M = len(us)
+    iv = np.float32(1) / np.float32(M)
+    um, vm, wm, w2 = (np.zeros_like(us[0]) for _ in range(4))
+    for m in range(M):
+        um = um + us[m]
+        vm = vm + vs[m]
+        wm = wm + ws[m]
+        w2 = w2 + iv * (ws[m] * ws[m])
+    um, vm, wm = um * iv, vm * iv, wm * iv
+    with np.errstate(invalid="ignore"):
+        sd = np.sqrt(w2 - wm * wm)
+    return um, vm, wm, sd
+
+
+def test_ensemble_statistics_bit_exact_and_async_output(tmp_path):
+    """The device vorticity and statistics equal the reference's FP32 host loops bit
+    for bit; the asynchronous output writes the same files as the synchronous one."""
+    cfg = lbl.config_default("DA_LETKF", 64, 5, ioprune=1)
+    e = lbl.Ensemble(cfg)
+    e.init(0)
+    e.update(0, 3 * cfg.iiter)
+    a, b = str(tmp_path / "a"), str(tmp_path / "b")
+    e.output(3 * cfg.iiter, a)
+    e.output(3 * cfg.iiter, b, sync=False)
+    e.sync()
+    fields = [e.get_fields(k) for k in range(5)]
+    us, vs = [f[1] for f in fields], [f[2] for f in fields]
+    ws = [oracle.vorticity(cfg, f[1], f[2]) for f in fields]
+    want = _stats_like_reference(us, vs, ws)
+    step = "_step0000000003.dat"
+    for name, w in zip(("ens_mean_u", "ens_mean_v", "ens_vor_mean", "ens_vor_std"), want):
+        np.testing.assert_array_equal(read(f"{a}/calc/{name}{step}"), w.reshape(-1))
+    for rel in [f"calc/{n}{step}" for n in ("ens_mean_u", "ens_mean_v", "ens_vor_mean", "ens_vor_std")] + \
+               [f"calc/ens{k:04d}/{v}{step}" for k in range(5) for v in ("rho", "u", "v", "vor")]:
+        assert open(f"{a}/{rel}", "rb").read() == open(f"{b}/{rel}", "rb").read(), rel
+
+
+def test_async_output_reports_nan_at_the_next_wait(tmp_path):
+    cfg = lbl.config_default("NATURE", 64, 1, ioprune=1)
+    e = lbl.Ensemble(cfg)
+    e.init(0)
+    f = e.get_f(0)
+    f[:, 10, 10] = np.nan
+    e.set_f(0, f)
+    e.output(0, str(tmp_path / "io"), sync=False)  # returns at once; the writer finds the NaN
+    with pytest.raises(lbl.LblError) as ei:
+        e.sync()
+    assert ei.value.code == -5
+    e.sync()  # the status was reported once
+
+
 def test_driver_observe_then_letkf(tmp_path):
     """lbl_run replays main.cu: OBSERVE writes io/observed, DA_LETKF reads it."""
     exe = os.path.join(PKG, "lbl_run")
