@@ -68,13 +68,15 @@ WORKLOAD = WORKLOADS["C1"][2]
 
 
 STORAGE = 0  # lbl_config.storage of the ensemble (the nature run stays FP32)
+GRAM = 0     # lbl_config.gram of the ensemble: 0 FP32, 1 BF16 tensor cores (32 < M <= 64)
 
 
 def workload_config(lbl, mode="DA_LETKF", n_ens=None):
     return lbl.config_default(
         mode, NX, M if n_ens is None else n_ens, da_xyprune=P_OBS, letkf_rloc_len=1, letkf_covinf=1.1, obs_error_u=0.1,
-        obs_error_rho=0.01, daprune=5, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP, ic_amp=1.0,
-        ens_init=lbl.ENS_PERTURBED, ens_perturb=0.1, storage=STORAGE if mode != "NATURE" else 0)
+        obs_error_rho=0.01, iiter=20, daprune=5, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP, ic_amp=1.0,
+        ens_init=lbl.ENS_PERTURBED, ens_perturb=0.1, storage=STORAGE if mode != "NATURE" else 0,
+        gram=GRAM if mode == "DA_LETKF" else 0)
 
 
 def measured_peak():
@@ -504,6 +506,8 @@ def main():
                          "(C1 with the learned closure)")
     ap.add_argument("--storage", choices=["f32", "f16"], default="f32",
                     help="population storage: f32, or the precision form's f16 deviations f - w_q")
+    ap.add_argument("--gram", choices=["f32", "bf16"], default="f32",
+                    help="the analysis Gram: FP32, or the precision form's BF16 tensor cores (M > 32, i.e. C2)")
     ap.add_argument("--lbm", default=None, metavar="NXxM[,NXxM...]",
                     help="time the stream-collide alone at these grids and exit")
     ap.add_argument("--closure", action="store_true",
@@ -511,10 +515,13 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global NX, M, WORKLOAD, STORAGE, CLOSURE
+    global NX, M, WORKLOAD, STORAGE, CLOSURE, GRAM
     NX, M, WORKLOAD = WORKLOADS.get(args.workload, WORKLOADS["C1"])
     CLOSURE = args.workload == "C4"
     STORAGE = 1 if args.storage == "f16" else 0
+    GRAM = 1 if args.gram == "bf16" else 0
+    if GRAM:
+        WORKLOAD += "; Gram on BF16 tensor cores with FP32 sums"
     if STORAGE:
         WORKLOAD = WORKLOAD.replace("FP32 storage", "FP16 deviation storage").replace(", FP32", ", FP16 deviation storage")
     if args.lbm:

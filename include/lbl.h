@@ -57,6 +57,8 @@ extern "C" {
 #define LBL_LBM_TMA    2    /* rows streamed into shared memory by the TMA unit  */
 
 /* population storage (lbl_config.storage) */
+#define LBL_GRAM_F32  0  /* Gram dY^T R^-1 dY in FP32 (the reference's arithmetic)                       */
+#define LBL_GRAM_BF16 1  /* precision form: BF16 operands on the tensor cores, FP32 sums; 32 < M <= 64   */
 #define LBL_STORAGE_F32 0    /* FP32 populations (the reference's `real`)                   */
 #define LBL_STORAGE_F16 1    /* FP16 deviations f - w_q from the lattice weights, FP32 collide */
 
@@ -118,7 +120,7 @@ typedef struct lbl_config {
     int32_t da_dummy;        /* DA_DUMMY (config.h:71-74): a DA run without analyses (main.cu:94) */
     int32_t da_quadra;       /* DA_QUADRA (config.h:63-65): nudge only x < nx/2 (odd), y < ny/2 (>= 2) */
     int32_t da_obs_ruv;      /* 1: DA_OBS_RUV, rho observed (config.h:44); 0: DA_OBS_UV, model rho */
-    int32_t reserved0;       /* must be 0                                                 */
+    int32_t gram;            /* LBL_GRAM_*: the analysis Gram in FP32 or on BF16 tensor cores */
     double da_nud_rate;      /* DA_NUD_RATE, nudging weight alpha, 0.1 (config.h:67-69)   */
     int32_t storage;         /* LBL_STORAGE_* (the precision form stores FP16 deviations)  */
     int32_t reserved1;       /* must be 0                                                 */
@@ -163,8 +165,9 @@ int lbl_assimilate_async(lbl_ctx* ctx, int t, const float* rho_o, const float* u
 int lbl_assimilate_files(lbl_ctx* ctx, int t, const char* io_prefix);
 
 /* One forecast-and-assimilate cycle: analysis at t (if due) followed by
- * n_fc forecast steps, launched as one CUDA graph.  NULL observation pointers
- * reuse the observations already resident on the device from the previous call. */
+ * n_fc forecast steps, launched as one CUDA graph.  Given observations become the
+ * resident ones (also when the DA gate skips this call's analysis); NULL observation
+ * pointers reuse them, and a due analysis with none given yet is LBL_ERR_STATE. */
 int lbl_cycle_async(lbl_ctx* ctx, int t, const float* rho_o, const float* u_o, const float* v_o, int n_fc);
 int lbl_sync(lbl_ctx* ctx);  /* also waits for a pending lbl_output_async writer */
 

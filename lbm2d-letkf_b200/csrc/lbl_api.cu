@@ -139,7 +139,12 @@ int validate(const lbl_config& c, std::string& err) {
     if (c.mode == LBL_MODE_DA_NUDGING && !(c.da_nud_rate >= 0 && c.da_nud_rate <= 1)) {
         err = "DA_NUD_RATE must lie in [0, 1]"; return LBL_ERR_ARG;
     }
-    if (c.reserved0 != 0 || c.reserved1 != 0) { err = "reserved fields must be 0"; return LBL_ERR_ARG; }
+    if (c.reserved1 != 0) { err = "reserved fields must be 0"; return LBL_ERR_ARG; }
+    if (c.gram != LBL_GRAM_F32 && c.gram != LBL_GRAM_BF16) { err = "unknown gram"; return LBL_ERR_ARG; }
+    if (c.gram == LBL_GRAM_BF16 && (c.mode != LBL_MODE_DA_LETKF || c.n_ens <= 32 || c.write_mat)) {
+        err = "the BF16 tensor-core Gram serves the wide analysis (DA_LETKF, 32 < n_ens <= 64, no matrix dumps)";
+        return LBL_ERR_UNSUPPORTED;
+    }
     if (c.storage != LBL_STORAGE_F32 && c.storage != LBL_STORAGE_F16) { err = "unknown storage"; return LBL_ERR_ARG; }
     if (c.storage == LBL_STORAGE_F16 && c.lbm_variant == LBL_LBM_TMA) {
         err = "the TMA stream-collide reads FP32 populations only"; return LBL_ERR_UNSUPPORTED;
@@ -237,6 +242,7 @@ int upload_obs(lbl_ctx* ctx, const float* ro, const float* uo, const float* vo) 
     const size_t ns = size_t(ctx->G.nsx) * ctx->G.nsy;
     LBL_CK(cudaMemcpyAsync(ctx->d_yo, ctx->h_yo[b], sizeof(float) * 3 * ns, cudaMemcpyHostToDevice, ctx->stream));
     LBL_CK(cudaEventRecord(ctx->ev[6 + b], ctx->stream));
+    ctx->have_obs = true;
     return LBL_OK;
 }
 
@@ -1031,7 +1037,11 @@ int lbl_cycle_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
         LBL_TRY(assimilate_impl(ctx, t, ro, uo, vo, true));
         return lbl_cycle_async(ctx, -1, nullptr, nullptr, nullptr, n_fc);
     }
-    if (due && ro && uo && vo) LBL_TRY(upload_obs(ctx, ro, uo, vo));  // NULL: resident observations
+    // given observations become the resident ones even when this call assimilates
+    // nothing; NULL reuses them and needs some to have been given before
+    if (ro && uo && vo && is_da_mode(ctx->cfg.mode)) LBL_TRY(upload_obs(ctx, ro, uo, vo));
+    if (due && !ctx->have_obs)
+        return fail(ctx, LBL_ERR_STATE, "lbl_cycle_async: an analysis is due and no observations were given yet");
     if (n_fc > 0) LBL_TRY(schedule_force(ctx, n_fc));
     LBL_TRY(launch_graph(ctx, due ? 1 : 0, n_fc));
     if (due && ctx->cfg.mode == LBL_MODE_DA_LETKF) ctx->cur ^= 1;

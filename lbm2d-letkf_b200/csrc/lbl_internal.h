@@ -108,6 +108,7 @@ struct lbl_ctx {
     // LETKF
     int* d_wtab = nullptr;               // int4 [p*p][nobs] window entries + int [p*p] counts
     float* d_yo = nullptr;               // [3][nsites] observations at sites (u, v, rho)
+    bool have_obs = false;               // d_yo holds observations given by the caller
     float* h_yo[2] = {nullptr, nullptr}; // pinned staging of the above, alternating
     int yo_buf = 0;
     float* d_dY = nullptr;               // [3][nsites][M] H(x)-mean at sites

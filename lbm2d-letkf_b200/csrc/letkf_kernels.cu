@@ -480,6 +480,24 @@ __device__ __forceinline__ int sa_chunk(int hb, int c4) { return hb * kHalf + 4 
 // sum of the two halves of a column (adjacent lanes)
 __device__ __forceinline__ float pair_sum(float v) { return v + __shfl_xor_sync(0xffffffffu, v, 1); }
 
+// BF16 tensor-core Gram (TC): the point's weighted window C = sqrt(w) dY (one row per
+// member, one column per weight-table entry) is staged as BF16 in sA, kCStride
+// entries per row (the padding spreads a quarter warp's fragment loads over all 32
+// banks), and Q - diag = C C^T is formed by mma.sync m16n8k16 with FP32 accumulators,
+// warp w taking rows [16 w, 16 w + 16).  Entries are taken kGramChunk at a time.
+constexpr int kGramChunk = 80;  // entries per staged chunk (5 k-steps)
+constexpr int kCStride = 88;    // BF16 elements per staged row
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                               uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+template <bool TC>
 __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const float* __restrict__ fin,
                                                                      float* __restrict__ fout, float* __restrict__ mac,
                                                                      const float* __restrict__ dY,
@@ -575,7 +593,68 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
 #pragma unroll
         for (int l = 0; l < kHalf; l++) qv[l] = 0.f;
         float ck = 0.f;
-        for (int o = 0; o < cnt; o++) {
+        if constexpr (TC) {
+            __nv_bfloat16* sCb = reinterpret_cast<__nv_bfloat16*>(sA);
+            const int g = lane >> 2, c4 = lane & 3;
+            float acc[8][4];
+#pragma unroll
+            for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+            float ckp = 0.f;
+            for (int ob = 0; ob < cnt; ob += kGramChunk) {
+                // stage: thread (k, h) fills entries [ob + 40 h, ob + 40 h + 40) of row k
+                for (int o2 = kGramChunk / 2 * h; o2 < kGramChunk / 2 * (h + 1); o2 += 2) {
+                    float v2[2];
+#pragma unroll
+                    for (int u = 0; u < 2; u++) {
+                        const int o = ob + o2 + u;
+                        float val = 0.f;
+                        if (o < cnt) {
+                            const int4 e = ent[o];
+                            const float wv = __int_as_float(e.w);
+                            const float y = sW[e.x * kWide + k];
+                            ckp = fmaf(wv * y, sDyo[e.x], ckp);
+                            val = sqrtf(wv) * y;
+                        }
+                        v2[u] = val;
+                    }
+                    *reinterpret_cast<__nv_bfloat162*>(sCb + k * kCStride + o2) = __floats2bfloat162_rn(v2[0], v2[1]);
+                }
+                __syncthreads();
+                const __nv_bfloat16* ra = sCb + (16 * warp + g) * kCStride + 2 * c4;
+#pragma unroll
+                for (int ks = 0; ks < kGramChunk / 16; ks++) {
+                    const uint32_t a0 = *reinterpret_cast<const uint32_t*>(ra + 16 * ks);
+                    const uint32_t a1 = *reinterpret_cast<const uint32_t*>(ra + 8 * kCStride + 16 * ks);
+                    const uint32_t a2 = *reinterpret_cast<const uint32_t*>(ra + 16 * ks + 8);
+                    const uint32_t a3 = *reinterpret_cast<const uint32_t*>(ra + 8 * kCStride + 16 * ks + 8);
+#pragma unroll
+                    for (int nt = 0; nt < 8; nt++) {
+                        const __nv_bfloat16* rb = sCb + (8 * nt + g) * kCStride + 16 * ks + 2 * c4;
+                        mma_bf16_16816(acc[nt], a0, a1, a2, a3, *reinterpret_cast<const uint32_t*>(rb),
+                                       *reinterpret_cast<const uint32_t*>(rb + 8));
+                    }
+                }
+                __syncthreads();  // the staging is read: the next chunk, or Q, may overwrite it
+            }
+            ck = pair_sum(ckp);
+            // Q into the half-column layout of sA: element (row, col) = Q[col][row] by symmetry
+#pragma unroll
+            for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int row = 16 * warp + g + 8 * (e >> 1), col = 8 * nt + 2 * c4 + (e & 1);
+                    const float d = (row == col && row < M) ? A.diag : 0.f;
+                    sA[sa_chunk(2 * row + (col >> 5), (col & 31) >> 2) + (col & 3)] = acc[nt][e] + d;
+                }
+            __syncthreads();
+#pragma unroll
+            for (int l = 0; l < kHalf; l += 4) {
+                const float4 q4 = *reinterpret_cast<const float4*>(sA + sa_chunk(2 * k + h, l >> 2));
+                qv[l] = q4.x; qv[l + 1] = q4.y; qv[l + 2] = q4.z; qv[l + 3] = q4.w;
+            }
+            __syncthreads();  // the warm start below rewrites sA
+        }
+        for (int o = 0; !TC && o < cnt; o++) {
             const int4 e = ent[o];
             const float* row = sW + e.x * kWide;
             const float ek = __int_as_float(e.w) * row[k];
@@ -589,9 +668,11 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                 qv[l + 3] = fmaf(ek, r4.w, qv[l + 3]);
             }
         }
+        if (!TC) {
 #pragma unroll
-        for (int l = 0; l < kHalf; l++)
-            if (r0 + l == k && k < M) qv[l] += A.diag;
+            for (int l = 0; l < kHalf; l++)
+                if (r0 + l == k && k < M) qv[l] += A.diag;
+        }
 
         // 4. warm start A = Q V_prev: Q's columns go through sA
         if (idx > 0) {
@@ -852,7 +933,8 @@ int analysis_prepare() {
     rc |= int(cudaFuncSetAttribute(analysis_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
     rc |= int(cudaFuncSetAttribute(analysis_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
     rc |= int(cudaFuncSetAttribute(analysis_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    rc |= int(cudaFuncSetAttribute(analysis_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_wide_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    rc |= int(cudaFuncSetAttribute(analysis_wide_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
     return rc;
 }
 
@@ -892,9 +974,15 @@ void launch_analysis_dump(const lbl_ctx* c, const float* fin, float* buf, int j0
 void launch_analysis_wide(const lbl_ctx* c, const float* fin, float* fout, float* mac, cudaStream_t s) {
     const AnaParams A = make_params(c);
     const int tiles = ((A.nx + kCW - 1) / kCW) * ((A.ny + kCH - 1) / kCH);
-    analysis_wide_kernel<<<tiles, kWideThreads, analysis_smem_bytes(A.M, A.n_pat_max), s>>>(
-        fin, fout, mac, c->d_dY, c->d_dyo, reinterpret_cast<const int4*>(c->d_wtab),
-        c->d_wtab + size_t(4) * c->G.p * c->G.p * c->G.nobs, c->d_stats, A);
+    const size_t sm = analysis_smem_bytes(A.M, A.n_pat_max);
+    const int4* wt = reinterpret_cast<const int4*>(c->d_wtab);
+    const int* wc = c->d_wtab + size_t(4) * c->G.p * c->G.p * c->G.nobs;
+    if (c->cfg.gram == LBL_GRAM_BF16)
+        analysis_wide_kernel<true><<<tiles, kWideThreads, sm, s>>>(fin, fout, mac, c->d_dY, c->d_dyo, wt, wc,
+                                                                    c->d_stats, A);
+    else
+        analysis_wide_kernel<false><<<tiles, kWideThreads, sm, s>>>(fin, fout, mac, c->d_dY, c->d_dyo, wt, wc,
+                                                                     c->d_stats, A);
 }
 
 void launch_analysis(const lbl_ctx* c, const float* fin, float* fout, float* mac, cudaStream_t s) {

@@ -39,6 +39,7 @@ ERRORS = {
 }
 LBM_AUTO, LBM_DIRECT, LBM_TMA = 0, 1, 2
 STORAGE_F32, STORAGE_F16 = 0, 1
+GRAM_F32, GRAM_BF16 = 0, 1
 
 # names of the exported C functions (must match include/lbl.h)
 EXPORTS = (
@@ -78,7 +79,7 @@ class Config(ctypes.Structure):
         ("ic_amp", ctypes.c_double), ("ens_perturb", ctypes.c_double), ("jacobi_tol", ctypes.c_double),
         ("force_seed", ctypes.c_uint64), ("obs_seed", ctypes.c_uint64),
         ("da_dummy", ctypes.c_int32), ("da_quadra", ctypes.c_int32), ("da_obs_ruv", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32), ("da_nud_rate", ctypes.c_double),
+        ("gram", ctypes.c_int32), ("da_nud_rate", ctypes.c_double),
         ("storage", ctypes.c_int32), ("reserved1", ctypes.c_int32),
     ]
 

@@ -73,6 +73,40 @@ def test_analysis_matches_oracle(nx, M, p, L, beta):
     assert np.max(np.abs(np.stack([e.get_f(m) for m in range(M)]) - fa) / np.abs(fa)) < 1e-5
 
 
+@pytest.mark.parametrize("M,p,L", [(64, 4, 1), (48, 2, 0), (40, 4, 2)])
+def test_bf16_gram_precision_form(M, p, L):
+    """The precision form's Gram (BF16 operands on the tensor cores, FP32 sums) against
+    the FP64 oracle: the analysis increments move by the BF16 rounding of the weighted
+    window (2^-9 relative), so the bound is 1e-2 of the largest increment instead of 1e-3;
+    and it is a different computation from the FP32 Gram."""
+    cfg, e, obs, _, _ = make_case(64, M, p, L, 1.1, gram=lbl.GRAM_BF16)
+    F = [e.get_f(m) for m in range(M)]
+    o = oracle.Oracle(cfg)
+    for m in range(M):
+        o.set_f(m, F[m])
+    e.assimilate(cfg.iiter, *obs)
+    o.assimilate(*obs)
+    st = e.letkf_stats()
+    assert st["nan"] == 0 and st["n_noconv"] == 0, st
+    inc_e = np.stack([e.get_f(m).astype(np.float64) - F[m] for m in range(M)])
+    inc_o = np.stack([o.get_f(m) - F[m] for m in range(M)])
+    scale = np.max(np.abs(inc_o))
+    err = np.max(np.abs(inc_e - inc_o)) / scale
+    print(f"BF16 Gram M={M} p={p} L={L}: increment error {err:.2e} of the largest increment")
+    assert scale > 1e-6 and err < 1e-2
+    cfg32, e32, _, _, _ = make_case(64, M, p, L, 1.1)
+    e32.assimilate(cfg32.iiter, *obs)
+    inc_32 = np.stack([e32.get_f(m).astype(np.float64) - F[m] for m in range(M)])
+    assert np.max(np.abs(inc_e - inc_32)) > 0
+
+
+def test_bf16_gram_limits():
+    for kw in (dict(mode="DA_LETKF", M=16), dict(mode="NATURE", M=64)):
+        with pytest.raises(lbl.LblError) as ei:
+            lbl.Ensemble(lbl.config_default(kw["mode"], 64, kw["M"], gram=lbl.GRAM_BF16))
+        assert ei.value.code == -8
+
+
 def moments(f):
     ex = np.array([(q % 3) - 1 for q in range(9)], float)
     ey = np.array([(q // 3) - 1 for q in range(9)], float)
