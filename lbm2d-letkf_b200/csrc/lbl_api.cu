@@ -1285,7 +1285,7 @@ int lbl_autotune(lbl_ctx* ctx, int* strip_rows_out, double* ms_per_launch) {
         *ms_out = double(ms) / reps;
         return LBL_OK;
     };
-    for (int ty : {heuristic, 2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16, 20, 24, 32}) {
+    for (int ty : {heuristic, 2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16, 20, 24, 32, 40, 48, 64}) {
         if (ty > ctx->P.ny) continue;
         ctx->ty_tuned = ty;
         double one = 0;

@@ -846,7 +846,7 @@ int strip_rows(const lbl_ctx* c) {
     const long long slots = (long long)std::max(1, per_sm) * sms;
     int best = 4;
     double best_cost = 1e30;
-    for (int ty = 2; ty <= 32; ty++) {
+    for (int ty = 2; ty <= 64; ty++) {
         const long long strips = (long long)P.M * ((P.ny + ty - 1) / ty) * cluster_chunks(P.nx);
         const long long waves = (strips + slots - 1) / slots;
         const double cost = double(waves) * (ty + 1.0);
