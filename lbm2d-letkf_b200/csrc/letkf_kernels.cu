@@ -287,9 +287,17 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         //    off-diagonal |g|/sqrt(a b) stayed below sqrt(tol) ends the iteration:
         //    convergence is quadratic, so that sweep's rotations leave about tol, the
         //    relative off-diagonal norm at which the reference's syevj stops.
+        //    Rotations are applied with a lazy column scale: column k is sc * qv, so a
+        //    rotation cs a + sn b becomes qv += (sn / cs)(sc_b / sc) pq_b, sc *= cs: one
+        //    FMA per element instead of a multiply and an FMA.  The scale is folded back
+        //    into qv at the start of every sweep.
         int sweeps = 0;
         bool converged = false;
+        float sc = 1.f;
         for (int sw = 0; sw < A.max_sweeps; sw++) {
+#pragma unroll
+            for (int l = 0; l < MP; l++) qv[l] *= sc;
+            sc = 1.f;
             float a0 = 0.f, a1 = 0.f;
 #pragma unroll
             for (int l = 0; l < MP; l += 2) { a0 = fmaf(qv[l], qv[l], a0); a1 = fmaf(qv[l + 1], qv[l + 1], a1); }
@@ -301,10 +309,11 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
                 float pq[MP];
 #pragma unroll
                 for (int l = 0; l < MP; l++) pq[l] = __shfl_xor_sync(0xffffffffu, qv[l], rr);
+                const float sp = __shfl_xor_sync(0xffffffffu, sc, rr);
                 float g0 = 0.f, g1 = 0.f;
 #pragma unroll
                 for (int l = 0; l < MP; l += 2) { g0 = fmaf(qv[l], pq[l], g0); g1 = fmaf(qv[l + 1], pq[l + 1], g1); }
-                const float g = g0 + g1;
+                const float g = (g0 + g1) * (sc * sp);
                 const float b = __shfl_xor_sync(0xffffffffu, a, rr);
                 const bool low = k < (k ^ rr);
                 const float alo = low ? a : b, ahi = low ? b : a;
@@ -316,9 +325,11 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
                     const float zeta = __fdividef(ahi - alo, 2.f * g);
                     const float t = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.f)));
                     const float cs = rsqrtf(fmaf(t, t, 1.f));
-                    const float sn = low ? -(cs * t) : cs * t;  // low: cs a - sn b; high: sn a + cs b
+                    // low: cs a - sn b; high: sn a + cs b (sn = cs t), with the scales
+                    const float rho = (low ? -t : t) * __fdividef(sp, sc);
 #pragma unroll
-                    for (int l = 0; l < MP; l++) qv[l] = fmaf(sn, pq[l], cs * qv[l]);
+                    for (int l = 0; l < MP; l++) qv[l] = fmaf(rho, pq[l], qv[l]);
+                    sc *= cs;
                     a = low ? a - t * g : a + t * g;
                 }
                 rot |= doit;
@@ -337,6 +348,8 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
 
         // 6. eigenpair of column k: lambda_k = |a_k|, v_k = a_k / lambda_k (padding
         //    columns are zero and keep the unit vector); transform (letkf_solver.h:288-316)
+#pragma unroll
+        for (int l = 0; l < MP; l++) qv[l] *= sc;
         float lam = 0.f;
         {
             float n0 = 0.f, n1 = 0.f;
@@ -696,10 +709,16 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
             __syncthreads();  // sA is the Jacobi exchange next
         }
 
-        // 5. one-sided Jacobi on the columns of A (see analysis_kernel)
+        // 5. one-sided Jacobi on the columns of A, lazily scaled (see analysis_kernel);
+        //    a column's scale is published beside its squared norm
         int sweeps = 0;
         bool converged = false;
+        float sc = 1.f;
+        float* sSc = sS;  // [64] column scales during the Jacobi (sS is written after it)
         for (int sw = 0; sw < A.max_sweeps; sw++) {
+#pragma unroll
+            for (int l = 0; l < kHalf; l++) qv[l] *= sc;
+            sc = 1.f;
             float a0 = 0.f, a1 = 0.f;
 #pragma unroll
             for (int l = 0; l < kHalf; l += 2) { a0 = fmaf(qv[l], qv[l], a0); a1 = fmaf(qv[l + 1], qv[l + 1], a1); }
@@ -715,7 +734,10 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                             make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
                     dirty = false;
                 }
-                if (h == 0) sN[k] = a;
+                if (h == 0) {
+                    sN[k] = a;
+                    sSc[k] = sc;
+                }
                 __syncthreads();
                 float pq[kHalf];
 #pragma unroll
@@ -724,11 +746,12 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                     pq[l] = p4.x; pq[l + 1] = p4.y; pq[l + 2] = p4.z; pq[l + 3] = p4.w;
                 }
                 const float b = sN[pk];
+                const float sp = sSc[pk];
                 __syncthreads();  // the partner's half is in registers: sA may change
                 float g0 = 0.f, g1 = 0.f;
 #pragma unroll
                 for (int l = 0; l < kHalf; l += 2) { g0 = fmaf(qv[l], pq[l], g0); g1 = fmaf(qv[l + 1], pq[l + 1], g1); }
-                const float g = pair_sum(g0 + g1);
+                const float g = pair_sum(g0 + g1) * (sc * sp);
                 const bool low = k < pk;
                 const float alo = low ? a : b, ahi = low ? b : a;
                 const float nrm = sqrtf(alo * ahi);
@@ -738,9 +761,10 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                     const float zeta = __fdividef(ahi - alo, 2.f * g);
                     const float tt = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.f)));
                     const float cs = rsqrtf(fmaf(tt, tt, 1.f));
-                    const float sn = low ? -(cs * tt) : cs * tt;
+                    const float rho = (low ? -tt : tt) * __fdividef(sp, sc);
 #pragma unroll
-                    for (int l = 0; l < kHalf; l++) qv[l] = fmaf(sn, pq[l], cs * qv[l]);
+                    for (int l = 0; l < kHalf; l++) qv[l] = fmaf(rho, pq[l], qv[l]);
+                    sc *= cs;
                     a = low ? a - tt * g : a + tt * g;
                     dirty = true;
                 }
@@ -760,6 +784,8 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
         }
 
         // 6. eigenpair of column k and the transform (letkf_solver.h:288-316)
+#pragma unroll
+        for (int l = 0; l < kHalf; l++) qv[l] *= sc;
         float lam = 0.f;
         {
             float n0 = 0.f, n1 = 0.f;
