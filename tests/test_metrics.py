@@ -91,6 +91,20 @@ def test_energy_spectrum_matches_notebook():
         np.testing.assert_allclose(lbl.energy_spectrum(u, v), notebook_spectrum(u, v), rtol=1e-9, atol=1e-14)
 
 
+def test_longrun_fixture_measure_is_the_notebook_spectrum():
+    """The statistics in tests/golden/ref_longrun_id0.npz use this spectrum."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_longrun as ml
+    rng = np.random.default_rng(7)
+    u, v = rng.standard_normal((2, 32, 32)).astype(np.float32)
+    np.testing.assert_allclose(ml.spectrum(u, v), notebook_spectrum(u, v), rtol=1e-12, atol=1e-15)
+    from conftest import golden
+    g = golden("ref_longrun_id0.npz")
+    assert g["spectra"].shape == (len(g["steps"]), 129) and np.all(g["energy"] > 0) and np.all(g["enstrophy"] > 0)
+
+
 def test_cli_tools_keep_the_reference_formats(tmp_path):
     make_run(str(tmp_path), M=3, steps=(0, 10))
     out = subprocess.run([os.path.join(PKG, "lbl_ensemble_stat"), f"{tmp_path}/nature", f"{tmp_path}/calc", "10"],
