@@ -20,6 +20,11 @@
 #include "closure.h"
 #include "lbl_internal.h"
 
+#define CLOSURE_CK(call)                              \
+    do {                                              \
+        if ((call) != cudaSuccess) return LBL_ERR_CUDA; \
+    } while (0)
+
 namespace lbl {
 namespace {
 
@@ -351,24 +356,24 @@ int lbl_closure_grad(const float* params, const float* features, const float* ta
         cudaMalloc(&f.p, sizeof(float) * kMlpIn * n) != cudaSuccess || cudaMalloc(&t.p, sizeof(float) * n) != cudaSuccess ||
         cudaMalloc(&g.p, sizeof(float) * kMlpParams) != cudaSuccess || cudaMalloc(&l.p, sizeof(float)) != cudaSuccess)
         return LBL_ERR_CUDA;
-    cudaMemcpy(w.p, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice);
-    cudaMemcpy(f.p, features, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice);
-    cudaMemcpy(t.p, targets, sizeof(float) * n, cudaMemcpyHostToDevice);
-    cudaMemset(g.p, 0, sizeof(float) * kMlpParams);
-    cudaMemset(l.p, 0, sizeof(float));
+    CLOSURE_CK(cudaMemcpy(w.p, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice));
+    CLOSURE_CK(cudaMemcpy(f.p, features, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice));
+    CLOSURE_CK(cudaMemcpy(t.p, targets, sizeof(float) * n, cudaMemcpyHostToDevice));
+    CLOSURE_CK(cudaMemset(g.p, 0, sizeof(float) * kMlpParams));
+    CLOSURE_CK(cudaMemset(l.p, 0, sizeof(float)));
     to_bf16_kernel<<<(kMlpParams + 255) / 256, 256>>>(static_cast<float*>(w.p), static_cast<__nv_bfloat16*>(wb.p),
                                                       kMlpParams);
-    cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(grad_smem()));
+    CLOSURE_CK(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(grad_smem())));
     const int blocks = int(std::min<size_t>(148 * 4, (n + 32 * kTrainWarps - 1) / (32 * kTrainWarps)));
     mlp_grad_kernel<<<blocks, 32 * kTrainWarps, grad_smem()>>>(static_cast<__nv_bfloat16*>(wb.p),
                                                                 static_cast<float*>(f.p), static_cast<float*>(t.p), n,
                                                                 int(n), 0, static_cast<float*>(g.p),
                                                                 static_cast<float*>(l.p));
     if (cudaDeviceSynchronize() != cudaSuccess) return LBL_ERR_CUDA;
-    cudaMemcpy(grad, g.p, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost);
+    CLOSURE_CK(cudaMemcpy(grad, g.p, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost));
     if (loss) {
         float ls = 0;
-        cudaMemcpy(&ls, l.p, sizeof(float), cudaMemcpyDeviceToHost);
+        CLOSURE_CK(cudaMemcpy(&ls, l.p, sizeof(float), cudaMemcpyDeviceToHost));
         *loss = ls / float(n);
     }
     return cudaGetLastError() == cudaSuccess ? LBL_OK : LBL_ERR_CUDA;
@@ -390,20 +395,20 @@ int lbl_closure_train(const float* features, const float* targets, size_t n, int
         cudaMalloc(&v.p, sizeof(float) * kMlpParams) != cudaSuccess ||
         cudaMalloc(&l.p, sizeof(float) * iters) != cudaSuccess)
         return LBL_ERR_CUDA;
-    cudaMemcpy(w.p, w0.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice);
-    cudaMemcpy(f.p, features, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice);
-    cudaMemcpy(t.p, targets, sizeof(float) * n, cudaMemcpyHostToDevice);
-    cudaMemset(m.p, 0, sizeof(float) * kMlpParams);
-    cudaMemset(v.p, 0, sizeof(float) * kMlpParams);
-    cudaMemset(l.p, 0, sizeof(float) * iters);
+    CLOSURE_CK(cudaMemcpy(w.p, w0.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice));
+    CLOSURE_CK(cudaMemcpy(f.p, features, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice));
+    CLOSURE_CK(cudaMemcpy(t.p, targets, sizeof(float) * n, cudaMemcpyHostToDevice));
+    CLOSURE_CK(cudaMemset(m.p, 0, sizeof(float) * kMlpParams));
+    CLOSURE_CK(cudaMemset(v.p, 0, sizeof(float) * kMlpParams));
+    CLOSURE_CK(cudaMemset(l.p, 0, sizeof(float) * iters));
     to_bf16_kernel<<<(kMlpParams + 255) / 256, 256>>>(static_cast<float*>(w.p), static_cast<__nv_bfloat16*>(wb.p),
                                                       kMlpParams);
-    cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(grad_smem()));
+    CLOSURE_CK(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(grad_smem())));
     const int blocks = int(std::min<int>(148 * 4, (batch + 32 * kTrainWarps - 1) / (32 * kTrainWarps)));
     const float b1 = 0.9f, b2 = 0.999f;
     double p1 = 1, p2 = 1;
     for (int it = 0; it < iters; it++) {
-        cudaMemsetAsync(g.p, 0, sizeof(float) * kMlpParams);
+        CLOSURE_CK(cudaMemsetAsync(g.p, 0, sizeof(float) * kMlpParams));
         mlp_grad_kernel<<<blocks, 32 * kTrainWarps, grad_smem()>>>(
             static_cast<__nv_bfloat16*>(wb.p), static_cast<float*>(f.p), static_cast<float*>(t.p), n, batch,
             seed * 1000003ull + uint64_t(it) + 1, static_cast<float*>(g.p), static_cast<float*>(l.p) + it);
@@ -415,9 +420,9 @@ int lbl_closure_train(const float* features, const float* targets, size_t n, int
                                                        float(1 - p1), float(1 - p2));
     }
     if (cudaDeviceSynchronize() != cudaSuccess || cudaGetLastError() != cudaSuccess) return LBL_ERR_CUDA;
-    cudaMemcpy(params, w.p, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost);
+    CLOSURE_CK(cudaMemcpy(params, w.p, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost));
     if (loss_curve) {
-        cudaMemcpy(loss_curve, l.p, sizeof(float) * iters, cudaMemcpyDeviceToHost);
+        CLOSURE_CK(cudaMemcpy(loss_curve, l.p, sizeof(float) * iters, cudaMemcpyDeviceToHost));
         for (int it = 0; it < iters; it++) loss_curve[it] /= float(batch);
     }
     return LBL_OK;
@@ -480,9 +485,9 @@ int lbl_closure_infer(const float* params, const float* features, size_t n, int 
         cudaMalloc(&pk.p, sizeof(uint32_t) * kPackWords) != cudaSuccess ||
         cudaMalloc(&f.p, sizeof(float) * kMlpIn * n) != cudaSuccess || cudaMalloc(&o.p, sizeof(float) * n) != cudaSuccess)
         return LBL_ERR_CUDA;
-    cudaMemcpy(w.p, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice);
-    cudaMemcpy(pk.p, pack.data(), sizeof(uint32_t) * kPackWords, cudaMemcpyHostToDevice);
-    cudaMemcpy(f.p, features, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice);
+    CLOSURE_CK(cudaMemcpy(w.p, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice));
+    CLOSURE_CK(cudaMemcpy(pk.p, pack.data(), sizeof(uint32_t) * kPackWords, cudaMemcpyHostToDevice));
+    CLOSURE_CK(cudaMemcpy(f.p, features, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice));
     to_bf16_kernel<<<(kMlpParams + 255) / 256, 256>>>(static_cast<float*>(w.p), static_cast<__nv_bfloat16*>(wb.p),
                                                       kMlpParams);
     closure_infer_kernel<<<int((n + 127) / 128), 128>>>(static_cast<uint32_t*>(pk.p),

@@ -235,11 +235,12 @@ def test_long_run_statistics_match_reference():
         assert abs(mine[k0:k1].sum() / ref[k0:k1].sum() - 1) < 2e-3, (k0, k1)
 
 
-@pytest.mark.parametrize("nx,ny,M,steps", [(2048, 16, 2, 20), (1280, 24, 1, 20), (2048, 2048, 1, 2)])
+@pytest.mark.parametrize("nx,ny,M,steps", [(2048, 16, 2, 20), (1280, 24, 1, 20), (1536, 16, 1, 10), (8192, 8, 1, 10),
+                                           (2048, 2048, 1, 2)])
 def test_wide_rows_match_fp64_oracle(nx, ny, M, steps):
     """Rows wider than 1024 columns: a cluster of CTAs per strip (2048 = 2 x 1024,
-    1280 = 5 x 256), the (u, v) across a chunk edge read from the neighbour CTA's
-    shared memory."""
+    1280 = 5 x 256, 1536 = 3 x 512, 8192 = 8 x 1024: the widest), the (u, v) across a
+    chunk edge read from the neighbour CTA's shared memory."""
     e = lbl.Ensemble(lbl.config_default("NATURE", nx, M, ny=ny))
     e.init(0)
     o = oracle.Oracle(e.cfg)
