@@ -398,11 +398,80 @@ def profile_cycles(args):
 C3_EXPERIMENTS = [(128, 4), (128, 8), (256, 16), (256, 16), (256, 32), (512, 32), (512, 64), (1024, 64)]
 
 
+def run_batch_graph(args):
+    """C3 as one batch (lbl_batch): per cycle one CUDA graph with every experiment's
+    analysis and forcing on parallel branches, then each of the 100 steps as one
+    launch of the batched persistent stream-collide over all 8 experiments.  The strip
+    height is picked by timing candidate heights on two cycles each.  Device time:
+    events on the first context's stream, which follows the batch's graphs."""
+    global NX, M
+    import lbl
+    T = STEPS_PER_CYCLE
+    K, W = args.steps, args.warmup
+    ens, obs = [], []
+    for nx, m in C3_EXPERIMENTS:
+        NX, M = nx, m
+        o, _ = make_observations(lbl, 1)
+        e = lbl.Ensemble(workload_config(lbl))
+        e.init(0)
+        ens.append(e)
+        obs.append(o[0])
+    t = 0
+    tuning = {}
+    for sr in (8, 12, 16, 24, 32):
+        b = lbl.Batch(ens, sr)
+        b.cycle_async(t, obs, T)
+        t += T
+        for _ in range(2):  # both buffer parities have their graphs
+            b.cycle_async(t, None, T)
+            t += T
+        b.sync()
+        ens[0].event_record(0)
+        for _ in range(2):
+            b.cycle_async(t, None, T)
+            t += T
+        ens[0].event_record(1)
+        b.sync()
+        tuning[sr] = ens[0].event_elapsed(0, 1) / 2
+        b.close()
+    best = min(tuning, key=tuning.get)
+    b = lbl.Batch(ens, best)
+    b.cycle_async(t, obs, T)
+    t += T
+    for _ in range(W):
+        b.cycle_async(t, None, T)
+        t += T
+    b.sync()
+    ens[0].event_record(0)
+    for _ in range(K):
+        b.cycle_async(t, None, T)
+        t += T
+    ens[0].event_record(1)
+    b.sync()
+    ms = ens[0].event_elapsed(0, 1)
+    lu = sum(m * nx ** 2 for nx, m in C3_EXPERIMENTS) * T * K
+    line = {"metric": "experiment DA cycles/s (C3 batch)", "value": len(ens) * K / (ms / 1e3), "unit": "cycles/s",
+            "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded nature runs + Gaussian observation noise)",
+            "config": {"workload": "C3: 8 DA_LETKF OSSEs in one batch, (grid, M) = " +
+                       ", ".join(f"{nx}^2 x {m}" for nx, m in C3_EXPERIMENTS) +
+                       ", obs every 4th point, GC radius 4 cells, inflation 1.1, 100 LBM steps + 1 analysis per cycle",
+                       "concurrency": "one graph per batch cycle: analyses and forcing on parallel branches, one "
+                                      "batched persistent stream-collide launch per step for all experiments"},
+            "glups": lu / (ms / 1e3) / 1e9,
+            "strip_rows": best, "autotune_ms_per_cycle": tuning, "gpu_launches": K * (T + 1 + 3 * len(ens))}
+    b.close()
+    for e in ens:
+        e.close()
+    return line
+
+
 def run_batch(args):
-    """C3: every experiment is its own context (own stream, cycle graphs, autotuned
-    strip height); their cycles are issued round-robin and run concurrently on the GPU.
-    Device time: each context records events around the timed cycles after a full
-    synchronisation, so all start together; the batch time is the longest span."""
+    """C3 as concurrent contexts: every experiment is its own context (own stream,
+    cycle graphs, autotuned strip height); their cycles are issued round-robin and run
+    concurrently on the GPU.  Device time: each context records events around the
+    timed cycles after a full synchronisation, so all start together; the batch time
+    is the longest span."""
     global NX, M
     import lbl
     T = STEPS_PER_CYCLE
@@ -506,6 +575,8 @@ def main():
                          "(C1 with the learned closure)")
     ap.add_argument("--storage", choices=["f32", "f16"], default="f32",
                     help="population storage: f32, or the precision form's f16 deviations f - w_q")
+    ap.add_argument("--c3", choices=["batch", "contexts"], default="batch",
+                    help="C3 as one batch with a batched persistent stream-collide, or as concurrent contexts")
     ap.add_argument("--gram", choices=["f32", "bf16"], default="f32",
                     help="the analysis Gram: FP32, or the precision form's BF16 tensor cores (M > 32, i.e. C2)")
     ap.add_argument("--lbm", default=None, metavar="NXxM[,NXxM...]",
@@ -528,7 +599,7 @@ def main():
         lbm_sweep(args)
         return
     if args.workload == "C3":
-        print(json.dumps(run_batch(args)), flush=True)
+        print(json.dumps(run_batch_graph(args) if args.c3 == "batch" else run_batch(args)), flush=True)
         return
     if args.profile:
         profile_cycles(args)

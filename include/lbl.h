@@ -312,6 +312,28 @@ int lbl_closure_train(const float* features, const float* targets, size_t n, int
  * inside the stream-collide, path 1 = the per-thread FP32 form. */
 int lbl_closure_infer(const float* params, const float* features, size_t n, int path, int device, float* out);
 
+/* Batches: several contexts (independent experiments of any grid and ensemble size)
+ * cycled together.  No counterpart in the reference, which runs one experiment per
+ * MPI job.  Each batch cycle is one CUDA graph: every context's analysis (when its
+ * DA gate is due) and forcing chunk on parallel branches, then n_fc steps of all
+ * the experiments, each step one launch of a persistent kernel whose CTAs take
+ * (experiment, member, strip, 128-column chunk) items from a counter, tallest
+ * strips first.  The populations match the contexts' own lbl_cycle_async bit for
+ * bit.  The contexts must be initialised, on one device, with FP32 storage, the
+ * direct stream-collide, no closure and nx % 128 == 0; strip_rows <= 0 takes 16.
+ * While a batch is in use, its contexts take no other cycle or update calls;
+ * accessors (lbl_get_f, lbl_rmse_uv, ...) wait for the batch's last graph.
+ * Observation arrays are per context in the order given to lbl_batch_create (NULL
+ * array or entry: reuse that context's resident observations).  n_fc is at most
+ * the smallest forcing buffer of the batch. */
+typedef struct lbl_batch lbl_batch;
+int lbl_batch_create(lbl_ctx* const* ctxs, int n, int strip_rows, lbl_batch** out);
+const char* lbl_batch_last_error(const lbl_batch* b);  /* never NULL */
+int lbl_batch_cycle_async(lbl_batch* b, int t, const float* const* rho_o, const float* const* u_o,
+                          const float* const* v_o, int n_fc);
+int lbl_batch_sync(lbl_batch* b);
+int lbl_batch_destroy(lbl_batch* b);
+
 /* Evaluation measures over the files lbl_output writes (host only; no context, no
  * GPU).  err (optional) receives a message of at most err_cap bytes.
  *

@@ -1373,3 +1373,267 @@ int lbl_timer_transit(lbl_ctx* ctx, int which, const char* tag) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches: several contexts cycled together, their forecasts stepped by one batched
+// persistent launch per step (lbm_batch_step_kernel), their analyses and forcing
+// on parallel branches of one CUDA graph per cycle.
+// ---------------------------------------------------------------------------
+struct lbl_batch {
+    std::vector<lbl_ctx*> ctx;         // in item order (tallest strips first)
+    std::vector<int> order;            // caller's index of each
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork_ev = nullptr, done_ev = nullptr;
+    std::vector<cudaEvent_t> ready_ev, join_ev;
+    bool launched = false;
+    std::vector<BatchExp> exps;        // host copy of the table (cur set per graph)
+    BatchExp* d_exps = nullptr;        // one device table per cur pattern, keyed in tables
+    std::map<int, BatchExp*> tables;
+    int* d_counter = nullptr;          // [kMaxBatchSteps] work counters, one per step
+    int total = 0, grid = 0;
+    int max_steps = 0;
+    std::map<long long, cudaGraphExec_t> graphs;
+    std::string err;
+};
+
+namespace {
+
+int batch_fail(lbl_batch* b, int code, const std::string& msg) {
+    b->err = msg;
+    return code;
+}
+
+#define BATCH_CK(call)                                                                            \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return batch_fail(b, LBL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+void batch_free(lbl_batch* b) {
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto& g : b->graphs) cudaGraphExecDestroy(g.second);
+    for (auto& t : b->tables) cudaFree(t.second);
+    cudaFree(b->d_counter);
+    for (auto e : b->ready_ev) cudaEventDestroy(e);
+    for (auto e : b->join_ev) cudaEventDestroy(e);
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+    if (b->done_ev) cudaEventDestroy(b->done_ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+// the device table of this cur pattern
+int batch_table(lbl_batch* b, int cur_mask, BatchExp** out) {
+    auto it = b->tables.find(cur_mask);
+    if (it == b->tables.end()) {
+        std::vector<BatchExp> t = b->exps;
+        for (size_t e = 0; e < t.size(); e++) t[e].cur = (cur_mask >> e) & 1;
+        BatchExp* d = nullptr;
+        BATCH_CK(cudaMalloc(&d, sizeof(BatchExp) * t.size()));
+        BATCH_CK(cudaMemcpy(d, t.data(), sizeof(BatchExp) * t.size(), cudaMemcpyHostToDevice));
+        it = b->tables.emplace(cur_mask, d).first;
+    }
+    *out = it->second;
+    return LBL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbl_batch_create(lbl_ctx* const* ctxs, int n, int strip_rows, lbl_batch** out) {
+    if (!ctxs || !out || n < 1 || n > kMaxBatch || strip_rows < 0) return LBL_ERR_ARG;
+    *out = nullptr;
+    auto* b = new (std::nothrow) lbl_batch();
+    if (!b) return LBL_ERR_NOMEM;
+    std::vector<lbl_ctx*> v(ctxs, ctxs + n);
+    int rc = LBL_OK;
+    for (lbl_ctx* c : v) {
+        if (!c || !c->initialised) { rc = LBL_ERR_STATE; b->err = "every context must exist and be initialised"; break; }
+        if (c->device != v[0]->device) { rc = LBL_ERR_ARG; b->err = "the contexts of a batch share one device"; break; }
+        if (c->f16 || c->use_tma || c->closure || c->P.nx % kBatchW != 0) {
+            rc = LBL_ERR_UNSUPPORTED;
+            b->err = "batched steps need FP32 storage, the direct stream-collide, no closure and nx a multiple of 128";
+            break;
+        }
+    }
+    for (size_t i = 0; rc == LBL_OK && i < v.size(); i++)
+        for (size_t j = i + 1; j < v.size(); j++)
+            if (v[i] == v[j]) { rc = LBL_ERR_ARG; b->err = "a context appears twice"; }
+    if (rc != LBL_OK) {
+        *out = b;  // for lbl_batch_last_error; the caller destroys it
+        return rc;
+    }
+    b->device = v[0]->device;
+    cudaSetDevice(b->device);
+    auto ty_of = [&](const lbl_ctx* c) { return std::max(2, std::min(strip_rows > 0 ? strip_rows : 16, c->P.ny)); };
+    std::vector<int> order(v.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = int(i);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return ty_of(v[a]) > ty_of(v[c]); });
+    for (int i : order) b->ctx.push_back(v[i]);
+    b->order = order;
+    v = b->ctx;
+    int item = 0;
+    b->max_steps = 1 << 30;
+    for (lbl_ctx* c : v) {
+        BatchExp e{};
+        e.f[0] = c->f[0];
+        e.f[1] = c->f[1];
+        e.mac[0] = c->mac[0];
+        e.mac[1] = c->mac[1];
+        e.force = c->d_force;
+        e.P = c->P;
+        e.ty = ty_of(c);
+        e.strips = (c->P.ny + e.ty - 1) / e.ty;
+        e.chunks = c->P.nx / kBatchW;
+        e.item0 = item;
+        item += c->P.M * e.strips * e.chunks;
+        b->exps.push_back(e);
+        b->max_steps = std::min(b->max_steps, c->force_cap);
+    }
+    b->total = item;
+    auto done = [&](int code, const std::string& msg) {
+        b->err = msg;
+        *out = b;
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->done_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc(&b->d_counter, sizeof(int) * b->max_steps) != cudaSuccess)
+        return done(LBL_ERR_CUDA, "batch resources");
+    b->ready_ev.resize(v.size());
+    b->join_ev.resize(v.size());
+    for (size_t e = 0; e < v.size(); e++)
+        if (cudaEventCreateWithFlags(&b->ready_ev[e], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->join_ev[e], cudaEventDisableTiming) != cudaSuccess)
+            return done(LBL_ERR_CUDA, "batch events");
+    b->grid = std::min(b->total, batch_step_slots());
+    *out = b;
+    return LBL_OK;
+}
+
+const char* lbl_batch_last_error(const lbl_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int lbl_batch_destroy(lbl_batch* b) {
+    if (!b) return LBL_OK;
+    batch_free(b);
+    delete b;
+    return LBL_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// One batch graph: the due analyses and every forcing chunk beside each other, then
+// n_fc batched steps.  t < 0: a forecast-only continuation (no analysis, no uploads).
+int batch_launch(lbl_batch* b, int t, const float* const* rho_o, const float* const* u_o, const float* const* v_o,
+                 int n_fc) {
+    const int n = int(b->ctx.size());
+    int due_mask = 0, cur_mask = 0, after_mask = 0;
+    for (int e = 0; e < n; e++) {
+        lbl_ctx* ctx = b->ctx[e];
+        // the previous batch graph read this context's schedule and observations
+        if (b->launched) BATCH_CK(cudaStreamWaitEvent(ctx->stream, b->done_ev, 0));
+        const bool due = t > 0 && is_da_mode(ctx->cfg.mode) && !ctx->cfg.da_dummy && da_due(ctx, t);
+        const int ui = b->order[e];  // the caller's index
+        const float* ro = rho_o ? rho_o[ui] : nullptr;
+        const float* uo = u_o ? u_o[ui] : nullptr;
+        const float* vo = v_o ? v_o[ui] : nullptr;
+        if (t >= 0 && ro && uo && vo && is_da_mode(ctx->cfg.mode)) {
+            const int rc = upload_obs(ctx, ro, uo, vo);
+            if (rc != LBL_OK) return batch_fail(b, rc, ctx->err);
+        }
+        if (due && !ctx->have_obs) return batch_fail(b, LBL_ERR_STATE, "an analysis is due and no observations were given yet");
+        const int rc = schedule_force(ctx, n_fc);
+        if (rc != LBL_OK) return batch_fail(b, rc, ctx->err);
+        BATCH_CK(cudaEventRecord(b->ready_ev[e], ctx->stream));
+        const int cur = ctx->cur & 1;
+        if (due) due_mask |= 1 << e;
+        cur_mask |= cur << e;
+        after_mask |= ((due && ctx->cfg.mode == LBL_MODE_DA_LETKF) ? cur ^ 1 : cur) << e;
+    }
+    for (int e = 0; e < n; e++) BATCH_CK(cudaStreamWaitEvent(b->stream, b->ready_ev[e], 0));
+    const long long key = ((long long)due_mask << 40) | ((long long)n_fc << 20) | cur_mask;
+    auto it = b->graphs.find(key);
+    if (it == b->graphs.end()) {
+        BatchExp* table = nullptr;
+        LBL_TRY(batch_table(b, after_mask, &table));  // allocates: before the capture
+        for (lbl_ctx* ctx : b->ctx) BATCH_CK(cudaStreamSynchronize(ctx->stream));
+        BATCH_CK(cudaStreamSynchronize(b->stream));
+        cudaGraph_t g = nullptr;
+        BATCH_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        cudaEventRecord(b->fork_ev, b->stream);
+        for (int e = 0; e < n; e++) {
+            lbl_ctx* ctx = b->ctx[e];
+            cudaStreamWaitEvent(ctx->stream, b->fork_ev, 0);
+            cudaStreamWaitEvent(ctx->side, b->fork_ev, 0);
+            launch_force_chunk(ctx, n_fc, 0, ctx->side);  // beside the analysis
+            cudaEventRecord(ctx->join_ev, ctx->side);
+            if ((due_mask >> e) & 1) enqueue_analysis(ctx, (cur_mask >> e) & 1, ctx->stream);
+            cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0);
+            cudaEventRecord(b->join_ev[e], ctx->stream);
+            cudaStreamWaitEvent(b->stream, b->join_ev[e], 0);
+        }
+        cudaMemsetAsync(b->d_counter, 0, sizeof(int) * n_fc, b->stream);
+        for (int k = 0; k < n_fc; k++)
+            launch_batch_step(table, n, b->total, k, b->d_counter, b->grid, k >= n_fc - 2, k > 0, b->stream);
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+        if (le != cudaSuccess || ee != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return batch_fail(b, LBL_ERR_CUDA, std::string("batch graph capture failed: ") +
+                                                   cudaGetErrorString(le != cudaSuccess ? le : ee));
+        }
+        cudaGraphExec_t ge;
+        const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) return batch_fail(b, LBL_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ie));
+        it = b->graphs.emplace(key, ge).first;
+    }
+    BATCH_CK(cudaGraphLaunch(it->second, b->stream));
+    BATCH_CK(cudaEventRecord(b->done_ev, b->stream));
+    b->launched = true;
+    for (int e = 0; e < n; e++) {
+        lbl_ctx* ctx = b->ctx[e];
+        ctx->cur = ((after_mask >> e) & 1) ^ (n_fc & 1);
+        ctx->last_force_slot = n_fc - 1;
+        ctx->phases = 0;
+        // later calls on the context run after the batch's graph
+        BATCH_CK(cudaStreamWaitEvent(ctx->stream, b->done_ev, 0));
+    }
+    return LBL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbl_batch_cycle_async(lbl_batch* b, int t, const float* const* rho_o, const float* const* u_o,
+                          const float* const* v_o, int n_fc) {
+    if (!b) return LBL_ERR_ARG;
+    if (n_fc < 1) return batch_fail(b, LBL_ERR_ARG, "n_fc must be >= 1");
+    BATCH_CK(cudaSetDevice(b->device));
+    // more steps than the smallest forcing buffer: the cycle graph takes the first
+    // max_steps, forecast-only graphs the rest
+    const int first = std::min(n_fc, b->max_steps);
+    LBL_TRY(batch_launch(b, t < 0 ? 0 : t, rho_o, u_o, v_o, first));
+    for (int done = first; done < n_fc; done += b->max_steps)
+        LBL_TRY(batch_launch(b, -1, nullptr, nullptr, nullptr, std::min(b->max_steps, n_fc - done)));
+    return LBL_OK;
+}
+
+int lbl_batch_sync(lbl_batch* b) {
+    if (!b) return LBL_ERR_ARG;
+    BATCH_CK(cudaSetDevice(b->device));
+    BATCH_CK(cudaStreamSynchronize(b->stream));
+    for (lbl_ctx* ctx : b->ctx) {
+        const int rc = lbl_sync(ctx);
+        if (rc != LBL_OK) return batch_fail(b, rc, ctx->err);
+    }
+    return LBL_OK;
+}
+
+}  // extern "C"

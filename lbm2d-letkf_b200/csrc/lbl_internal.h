@@ -188,6 +188,24 @@ bool lbm_tma_supported(int nx);
 size_t lbm_tma_smem(int nx);
 void launch_macros(const lbl_ctx* c, int buf, float* mac, cudaStream_t s);
 
+// Batched persistent stream-collide (lbl_batch_*): one launch steps every experiment
+// of a batch; work items are (experiment, member, strip, kBatchW-column chunk)
+constexpr int kBatchW = 128;
+constexpr int kMaxBatch = 16;
+struct BatchExp {
+    float* f[2];           // population buffers (FP32)
+    float* mac[2];         // macro buffers
+    const float* force;    // forcing chunk, [step][2][nxy]
+    Phys P;
+    int ty, strips, chunks, item0;  // strip height, strips per member, chunks per row, first item
+    int cur;               // buffer read by step 0 of the launched sequence
+};
+// step `step` of every experiment (exps: device table sorted by item0, counter[step]
+// zeroed before); mac: write the macros (the last two steps of a forecast)
+void launch_batch_step(const BatchExp* exps, int n_exp, int total, int step, int* counter, int grid, bool mac,
+                       bool pdl, cudaStream_t s);
+int batch_step_slots();  // resident CTAs of the batched kernel on the current device
+
 // ---- kernels (letkf_kernels.cu) ----
 void launch_obs_ensemble(const lbl_ctx* c, const float* f, cudaStream_t s);
 void launch_nudging(const lbl_ctx* c, int buf, const float* mac, cudaStream_t s);

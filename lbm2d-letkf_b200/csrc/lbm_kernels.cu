@@ -586,6 +586,136 @@ __global__ void __launch_bounds__(MAXT, (CL && MAXT == 256) ? 2 : 1)
 }
 
 // ---------------------------------------------------------------------------
+// Batched persistent stream-collide: one launch steps every experiment of a batch
+// (own grid, members, buffers, forcing and strip height).  The work items are
+// (experiment, member, strip, 128-column chunk); a grid sized to the GPU's resident
+// CTA slots takes them from an atomic counter, largest strips first, so uneven
+// experiments share one launch per step.  The arithmetic is lbm_step_kernel's.  A
+// chunk of a row wider than 128 columns gets the (u, v) of its two edge neighbours
+// from its edge threads, which pull and reduce those columns themselves (prefetched
+// one row ahead, like the populations); a 128-column row wraps inside the CTA.
+// ---------------------------------------------------------------------------
+template <bool WRITE_MAC>
+__global__ void __launch_bounds__(kBatchW, 8) lbm_batch_step_kernel(const BatchExp* __restrict__ exps, int n_exp,
+                                                                int total, int step, int* __restrict__ counter) {
+    __shared__ float s_uv[3][2][kBatchW + 2];  // per row slot: u, v with a halo column on each side
+    __shared__ int s_item;
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" :::);
+    const int xl = threadIdx.x;
+    for (;;) {
+        __syncthreads();  // the previous item's ring is no longer read
+        if (xl == 0) s_item = atomicAdd(counter + step, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= total) break;
+        int e = 0;
+        while (e + 1 < n_exp && item >= exps[e + 1].item0) e++;
+        const BatchExp& E = exps[e];
+        const Phys P = E.P;
+        const int nx = P.nx, ny = P.ny, nxy = P.nxy, TY = E.ty;
+        const int local = item - E.item0;
+        const int chunk = local % E.chunks, rest = local / E.chunks;
+        const int strip = rest % E.strips, m = rest / E.strips;
+        const int x0 = chunk * kBatchW, x = x0 + xl;
+        const bool whole = E.chunks == 1;
+        // ring slots of the x -1 / x +1 neighbours; edge threads of a chunked row also
+        // carry the halo column beside them (hx, at ring slot hs)
+        const int lidx = (whole && xl == 0) ? kBatchW : xl;
+        const int ridx = (whole && xl == kBatchW - 1) ? 1 : xl + 2;
+        const int hx = whole ? -1
+                             : (xl == 0 ? (x0 == 0 ? nx - 1 : x0 - 1)
+                                        : (xl == kBatchW - 1 ? (x0 + kBatchW == nx ? 0 : x0 + kBatchW) : -1));
+        const int hs = xl == 0 ? 0 : kBatchW + 1;
+        const int hxm = hx <= 0 ? nx - 1 : hx - 1, hxp = hx == nx - 1 ? 0 : hx + 1;
+        const int src = (E.cur + step) & 1;
+        const float* __restrict__ fm = E.f[src] + size_t(m) * kQ * nxy;
+        float* __restrict__ fo = E.f[src ^ 1] + size_t(m) * kQ * nxy + x;
+        float* __restrict__ mac = E.mac[src ^ 1];
+        const float* __restrict__ force = E.force + size_t(step) * 2 * nxy;
+        const int j0 = strip * TY;
+        const int j1 = min(j0 + TY, ny);
+        const int xm = (x == 0) ? nx - 1 : x - 1;
+        const int xp = (x == nx - 1) ? 0 : x + 1;
+        const float* __restrict__ Fx = force + x;
+        const float* __restrict__ Fy = force + nxy + x;
+        auto wrap_row = [&](int r) { return (r < 0 ? r + ny : (r >= ny ? r - ny : r)) * nx; };
+        int o_m = wrap_row(j0 - 2), o_0 = wrap_row(j0 - 1), o_p = wrap_row(j0);
+        auto advance = [&]() {
+            o_m = o_0;
+            o_0 = o_p;
+            o_p = (o_p + nx == nxy) ? 0 : o_p + nx;
+        };
+        auto pull_at = [&](float (&fc)[kQ], int c, int cm, int cp) {
+#pragma unroll
+            for (int q = 0; q < kQ; q++) {
+                const int col = ex_q(q) == -1 ? cp : (ex_q(q) == 0 ? c : cm);
+                const int row = ey_q(q) == -1 ? o_p : (ey_q(q) == 0 ? o_0 : o_m);
+                fc[q] = Store<float>::ld(fm + q * nxy + row + col, w_q(q));
+            }
+        };
+        float hreg[kQ];  // the halo column's pulled populations, one row ahead
+        auto pull = [&](float (&fc)[kQ]) {
+            pull_at(fc, x, xm, xp);
+            if (hx >= 0) pull_at(hreg, hx, hxm, hxp);
+        };
+        auto halo = [&](float* sb) {  // the halo column's (u, v) for the row in hreg
+            if (hx >= 0) {
+                float hr, hu, hv;
+                macros_v(hreg, hr, hu, hv, P.c);
+                sb[hs] = hu;
+                sb[kBatchW + 2 + hs] = hv;
+            }
+        };
+        float f[3][kQ], r[3], u[3], v[3];
+        {  // halo row below the strip: only its u,v (own column) are needed
+            pull_at(f[2], x, xm, xp);
+            float rr;
+            macros_v(f[2], rr, u[2], v[2], P.c);
+        }
+        float* s0 = &s_uv[0][0][0];
+        float* s1 = &s_uv[1][0][0];
+        float* s2 = &s_uv[2][0][0];
+        advance();
+        pull(f[0]);  // row j0 (and its halo)
+        macros_v(f[0], r[0], u[0], v[0], P.c);
+        s0[xl + 1] = u[0];
+        s0[kBatchW + 2 + xl + 1] = v[0];
+        halo(s0);
+        advance();
+        pull(f[1]);  // row j0+1
+        int ij = j0 * nx;
+        auto row = [&](float (&fa)[kQ], float (&fb)[kQ], float (&fc)[kQ], float& ra, float& ua, float& va,
+                       float& rb, float& ub, float& vb, float uc, float vc, float* sa, float* sb, int jc) {
+            advance();
+            halo(sb);  // row B's halo, pulled one row ago, before hreg takes row C's
+            if (jc + 2 <= j1) pull(fc);
+            macros_v(fb, rb, ub, vb, P.c);
+            sb[xl + 1] = ub;
+            sb[kBatchW + 2 + xl + 1] = vb;
+            __syncthreads();
+            const float omega = les_omega(sa[ridx], sa[lidx], sa[kBatchW + 2 + ridx], sa[kBatchW + 2 + lidx], ub, uc, vb,
+                                          vc, P);
+            collide(fa, ra, ua, va, omega, Fx[ij], Fy[ij], P);
+#pragma unroll
+            for (int q = 0; q < kQ; q++) Store<float>::st(fo + q * nxy + ij, fa[q], w_q(q));
+            if (WRITE_MAC) {
+                float* mm = mac + size_t(m) * 3 * nxy + x;
+                mm[ij] = ra;
+                mm[nxy + ij] = ua;
+                mm[2 * nxy + ij] = va;
+            }
+            ij += nx;
+        };
+        for (int jc = j0; jc < j1; jc += 3) {
+            row(f[0], f[1], f[2], r[0], u[0], v[0], r[1], u[1], v[1], u[2], v[2], s0, s1, jc);
+            if (jc + 1 < j1) row(f[1], f[2], f[0], r[1], u[1], v[1], r[2], u[2], v[2], u[0], v[0], s1, s2, jc + 1);
+            if (jc + 2 < j1) row(f[2], f[0], f[1], r[2], u[2], v[2], r[0], u[0], v[0], u[1], v[1], s2, s0, jc + 2);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // TMA-fed stream-collide (same arithmetic as lbm_step_kernel).  A producer warp
 // streams, for every pulled row jj of the strip (j0-1 .. j1), the nine source rows
 // f_q(:, jj - ey_q) into one stage of a shared-memory ring with
@@ -1077,6 +1207,25 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
 }
 
 int lbm_strip_rows(const lbl_ctx* c) { return strip_rows(c); }
+
+void launch_batch_step(const BatchExp* exps, int n_exp, int total, int step, int* counter, int grid, bool mac,
+                       bool pdl, cudaStream_t s) {
+    if (mac)
+        launch_step(lbm_batch_step_kernel<true>, dim3(grid), kBatchW, 0, s, pdl, exps, n_exp, total, step, counter);
+    else
+        launch_step(lbm_batch_step_kernel<false>, dim3(grid), kBatchW, 0, s, pdl, exps, n_exp, total, step, counter);
+}
+
+int batch_step_slots() {
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_batch_step_kernel<false>, kBatchW, 0) != cudaSuccess) {
+        (void)cudaGetLastError();
+        per_sm = 1;
+    }
+    return std::max(1, per_sm) * sms;
+}
 
 int cluster_chunks(int nx) {
     if (nx <= 1024) return 1;

@@ -51,7 +51,8 @@ EXPORTS = (
     "lbl_timer_transit", "lbl_profile_step", "lbl_get_cycle_phases", "lbl_event_record", "lbl_event_elapsed",
     "lbl_letkf_analysis_noalloc", "lbl_bindiff", "lbl_ensemble_stat", "lbl_energy_spectrum",
     "lbl_set_io_prefix", "lbl_h5_write_dataset", "lbl_autotune", "lbl_set_closure", "lbl_closure_generate",
-    "lbl_closure_grad", "lbl_closure_train", "lbl_closure_infer",
+    "lbl_closure_grad", "lbl_closure_train", "lbl_closure_infer", "lbl_batch_create", "lbl_batch_last_error",
+    "lbl_batch_cycle_async", "lbl_batch_sync", "lbl_batch_destroy",
 )
 CLOSURE_PARAMS, CLOSURE_FEATURES = 1313, 6
 
@@ -137,6 +138,11 @@ def load_library() -> ctypes.CDLL:
         "lbl_closure_grad": (I, [F, F, F, U, I, F, F]),
         "lbl_closure_train": (I, [F, F, U, I, I, ctypes.c_float, ctypes.c_uint64, I, F, F, F]),
         "lbl_closure_infer": (I, [F, F, U, I, I, F]),
+        "lbl_batch_create": (I, [ctypes.POINTER(P), I, I, ctypes.POINTER(P)]),
+        "lbl_batch_last_error": (ctypes.c_char_p, [P]),
+        "lbl_batch_cycle_async": (I, [P, I, ctypes.POINTER(F), ctypes.POINTER(F), ctypes.POINTER(F), I]),
+        "lbl_batch_sync": (I, [P]),
+        "lbl_batch_destroy": (I, [P]),
         "lbl_timer_csv": (I, [P, I, ctypes.c_char_p, U]),
         "lbl_timer_clear": (I, [P, I]),
         "lbl_timer_transit": (I, [P, I, ctypes.c_char_p]),
@@ -509,3 +515,58 @@ def closure_infer(params, features, path: int = 0, device: int = 0) -> np.ndarra
     if rc != 0:
         raise LblError(rc, "lbl_closure_infer")
     return out
+
+
+class Batch:
+    """Several ensembles cycled together: per cycle one CUDA graph with every
+    experiment's analysis and forcing beside each other and one batched persistent
+    stream-collide launch per step for all of them (lbl_batch_*)."""
+
+    def __init__(self, ensembles, strip_rows: int = 0):
+        self.lib = load_library()
+        self.members = list(ensembles)
+        arr = (ctypes.c_void_p * len(self.members))(*[e._h.value for e in self.members])
+        h = ctypes.c_void_p()
+        rc = self.lib.lbl_batch_create(arr, len(self.members), strip_rows, ctypes.byref(h))
+        self._h = h
+        if rc != 0:
+            msg = self.lib.lbl_batch_last_error(h).decode() if h.value else "lbl_batch_create"
+            if h.value:
+                self.lib.lbl_batch_destroy(h)
+            self._h = ctypes.c_void_p()
+            raise LblError(rc, msg)
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise LblError(rc, f"{what}: {self.lib.lbl_batch_last_error(self._h).decode()}")
+
+    def cycle_async(self, t: int, observations=None, n_fc: int = 100):
+        """observations: None, or one (rho, u, v) tuple (or None) per ensemble."""
+        n = len(self.members)
+        if observations is None:
+            self._check(self.lib.lbl_batch_cycle_async(self._h, t, None, None, None, n_fc), "lbl_batch_cycle_async")
+            return
+        keep = []
+        ptrs = [(ctypes.POINTER(ctypes.c_float) * n)() for _ in range(3)]
+        for i, (ens, obs) in enumerate(zip(self.members, observations)):
+            if obs is None:
+                continue
+            for k, a in enumerate(obs):
+                a = _f32(a, ens.nxy)
+                keep.append(a)
+                ptrs[k][i] = _fp(a)
+        self._check(self.lib.lbl_batch_cycle_async(self._h, t, *ptrs, n_fc), "lbl_batch_cycle_async")
+
+    def sync(self):
+        self._check(self.lib.lbl_batch_sync(self._h), "lbl_batch_sync")
+
+    def close(self):
+        if self._h and self._h.value:
+            self.lib.lbl_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
