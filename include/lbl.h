@@ -321,8 +321,9 @@ int lbl_closure_infer(const float* params, const float* features, size_t n, int 
  * strips first.  The populations match the contexts' own lbl_cycle_async bit for
  * bit.  The contexts must be initialised, on one device, with FP32 storage, the
  * direct stream-collide, no closure and nx % 128 == 0; strip_rows <= 0 takes 16.
- * While a batch is in use, its contexts take no other cycle or update calls;
- * accessors (lbl_get_f, lbl_rmse_uv, ...) wait for the batch's last graph.
+ * While a batch is in use, its contexts take no other cycle or update calls and
+ * must outlive it (destroy the batch first); accessors (lbl_get_f, lbl_rmse_uv, ...)
+ * wait for the batch's last graph.
  * Observation arrays are per context in the order given to lbl_batch_create (NULL
  * array or entry: reuse that context's resident observations).  n_fc is at most
  * the smallest forcing buffer of the batch. */
