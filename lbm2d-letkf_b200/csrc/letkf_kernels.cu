@@ -122,6 +122,9 @@ __device__ __forceinline__ float group_sum(float v) {
 // bits (sigma^-2 x Gaspari-Cohn), only w > 0, per pattern (i mod p, j mod p).
 // ---------------------------------------------------------------------------
 constexpr int kCW = 4, kCH = 2;  // chain tile (points in x, points in y)
+// the wide analysis walks taller tiles: fewer cold starts, and its many waves hide
+// the longer CTAs (C2: 60.2 ms against 62.8 ms for 4 x 2; C1's kernel is fastest at 4 x 2)
+constexpr int kWCW = 4, kWCH = 4;
 
 // DUMP = true recomputes the tiles that cover the rows of D and, instead of writing
 // the analysis, writes every intermediate matrix of those rows (need_save_mat).
@@ -470,7 +473,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
 
 // ---------------------------------------------------------------------------
 // The local analysis for 32 < M <= 64 (the C2 ensembles; the reference runs them
-// through EigenG-Batched).  One CTA of 128 threads walks one CW x CH tile of points;
+// through EigenG-Batched).  One CTA of 128 threads walks one kWCW x kWCH tile of points;
 // thread t owns rows [32h, 32h + 32) (h = t & 1) of member column k = t >> 1, and
 // the two halves of a column combine their partial dot products with one shuffle.
 // The algorithm is the one above; the Jacobi's partner columns go through a 64 x 64
@@ -539,19 +542,19 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
     float* sXbar = sN + kWide;           // [12]       ensemble mean
     float* sV = sXbar + 12;              // [64][64]   eigenvectors, V[l][k] at sV[l*64 + k]
 
-    const int tiles_x = (A.nx + kCW - 1) / kCW;
+    const int tiles_x = (A.nx + kWCW - 1) / kWCW;
     const int tile = blockIdx.x;
-    const int x0 = (tile % tiles_x) * kCW;
-    const int y0 = (A.tile_y0 + tile / tiles_x) * kCH;
+    const int x0 = (tile % tiles_x) * kWCW;
+    const int y0 = (A.tile_y0 + tile / tiles_x) * kWCH;
 
     for (int l = 0; l < kHalf; l++) sV[(r0 + l) * kWide + k] = (r0 + l == k) ? 1.f : 0.f;
     int cached_bi = -1, cached_bj = -1;
     int max_sweeps = 0, noconv = 0, total_sweeps = 0;
     bool bad = false;
 
-    for (int idx = 0; idx < kCW * kCH; idx++) {
-        const int rr_ = idx / kCW;
-        const int cc = (rr_ & 1) ? (kCW - 1 - idx % kCW) : (idx % kCW);
+    for (int idx = 0; idx < kWCW * kWCH; idx++) {
+        const int rr_ = idx / kWCW;
+        const int cc = (rr_ & 1) ? (kWCW - 1 - idx % kWCW) : (idx % kWCW);
         const int i = x0 + cc, j = y0 + rr_;
         const bool active = (i < A.nx) && (j < A.ny);  // uniform within the CTA
         if (!active) continue;
@@ -999,7 +1002,7 @@ void launch_analysis_dump(const lbl_ctx* c, const float* fin, float* buf, int j0
 
 void launch_analysis_wide(const lbl_ctx* c, const float* fin, float* fout, float* mac, cudaStream_t s) {
     const AnaParams A = make_params(c);
-    const int tiles = ((A.nx + kCW - 1) / kCW) * ((A.ny + kCH - 1) / kCH);
+    const int tiles = ((A.nx + kWCW - 1) / kWCW) * ((A.ny + kWCH - 1) / kWCH);
     const size_t sm = analysis_smem_bytes(A.M, A.n_pat_max);
     const int4* wt = reinterpret_cast<const int4*>(c->d_wtab);
     const int* wc = c->d_wtab + size_t(4) * c->G.p * c->G.p * c->G.nobs;
