@@ -25,7 +25,13 @@ One bench "step" = one DA cycle = the LETKF analysis + 100 LBM steps.
 
 `--impl reference` times the reference's path on the host cores.  The reference
 has no CPU implementation (its only backend is CUDA + MPI + cuBLAS/cuSOLVER), so
-its arm is the FP64 OpenMP restatement of the reference's path in oracle/.
+its arm is the FP64 OpenMP restatement of the reference's path in oracle/.  Where
+the reference's own LBM build (oracle/_ref/ref_lbm: its src/lbm.cu and src/data.cu
+compiled unmodified) is present and a GPU is visible, the line also carries
+`reference_build`: that build's forecast run as M processes sharing the GPU, one
+per member as the reference's one-MPI-rank-per-member runs do, and the cycles/s
+bound it implies (forecast only: the reference's LETKF needs MPI and HDF5 and is
+not built, so its real cycle is slower still).
 
 Multi-GPU: replicas only (one independent experiment per GPU, no collective on
 the data path); `value` is the cycles of all ranks / the slowest rank's time.
@@ -340,6 +346,78 @@ def run_engine(args, dist, rank, world, device):
     return line
 
 
+def reference_build_forecast(n_proc, nsteps, warmup=50):
+    """The reference's own LBM (oracle/_ref/ref_lbm) run as n_proc processes sharing
+    the GPU, one ensemble member each, started together after their warm-up.
+    Returns the forecast rate, or {"unavailable": why}."""
+    import tempfile
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_lbm")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_lbm not built (it needs the reference sources at build time)"}
+    with tempfile.TemporaryDirectory() as tmp:
+        go = os.path.join(tmp, "go")
+        ready = [os.path.join(tmp, f"ready{k}") for k in range(n_proc)]
+        procs = [subprocess.Popen([exe, "time", str(k), str(nsteps), str(warmup), ready[k], go],
+                                  stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True) for k in range(n_proc)]
+
+        def stop(why):
+            for p in procs:
+                if p.poll() is None:
+                    p.kill()
+            for p in procs:
+                p.wait()
+            return {"unavailable": why}
+
+        deadline = time.time() + 240
+        while not all(os.path.exists(r) for r in ready):
+            done = [p for p in procs if p.poll() is not None]
+            if done:
+                err = done[0].stderr.read().strip().splitlines()
+                return stop(f"ref_lbm exited {done[0].returncode}: {err[-1] if err else ''}")
+            if time.time() > deadline:
+                return stop("ref_lbm processes not ready within 240 s")
+            time.sleep(0.005)
+        open(go, "w").close()
+        spans = []
+        for p in procs:
+            try:
+                out, err = p.communicate(timeout=240)
+            except subprocess.TimeoutExpired:
+                return stop("ref_lbm timed steps did not end within 240 s")
+            rec = [ln.split() for ln in out.splitlines() if ln.startswith("ref_lbm_time")]
+            if p.returncode != 0 or not rec:
+                return stop(f"ref_lbm exited {p.returncode}: {err.strip()[-200:]}")
+            spans.append((int(rec[0][3]), int(rec[0][4])))
+    t0 = min(a for a, _ in spans)
+    t1 = max(b for _, b in spans)
+    sec = (t1 - t0) * 1e-9
+    nxy = 256 * 256  # the reference's compiled default grid
+    return {"processes": n_proc, "steps_per_process": nsteps, "seconds": sec,
+            "ms_per_100_steps": 1e3 * sec * 100 / nsteps, "forecast_glups": n_proc * nxy * nsteps / sec * 1e-9}
+
+
+def reference_build_line(args):
+    """`reference_build` of the reference arm's JSON line (see the module docstring)."""
+    nsteps = min(2000, max(200, 20 * args.steps))
+    solo = reference_build_forecast(1, nsteps)
+    if "unavailable" in solo:
+        return solo
+    shared = reference_build_forecast(M, nsteps)
+    if "unavailable" in shared:
+        return shared
+    # the better of the two ways to run M members: M processes sharing the GPU, or
+    # one process M times over (the single-process time x M, no context switches)
+    best = min(shared["ms_per_100_steps"], solo["ms_per_100_steps"] * M)
+    return {"kind": "the reference's src/lbm.cu + src/data.cu compiled unmodified (sm_100a, its nvcc flags), "
+                    "its update() per step: forcing, streaming + macros, LES, collision",
+            "grid": "256x256 (its compiled default; the cost per step does not depend on the flow)",
+            "members": M, "shared": shared, "single_process": solo,
+            "forecast_ms_per_cycle": best,
+            "cycles_per_s_upper_bound": 1e3 / best,
+            "note": "forecast only: the reference's LETKF analysis (MPI, HDF5, cuSOLVER) is not built here, "
+                    "so its cycles/s is below this bound"}
+
+
 def run_reference(args, rank, world):
     """The reference's path on the host cores: FP64 OpenMP restatement (oracle/)."""
     import lbl
@@ -375,7 +453,9 @@ def run_reference(args, rank, world):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "backend": "FP64 OpenMP CPU restatement of the reference path"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_build": reference_build_line(args) if NX == 256 and not CLOSURE else
+            {"unavailable": "the reference build runs its compiled 256x256 plain-Smagorinsky default only"}}
 
 
 def profile_cycles(args):

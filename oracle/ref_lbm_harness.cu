@@ -9,12 +9,24 @@
 // pin the CPU oracle and the CUDA engine against the reference itself.
 //
 // usage: ref_lbm <out_dir> <ensemble_id> <nsteps> <dump_step>[,<dump_step>...]
+//        ref_lbm time <ensemble_id> <nsteps> <warmup> [<ready_file> <go_file>]
+//
+// The `time` form runs `warmup` untimed steps, then (when given the two files)
+// creates <ready_file> and waits, at most 300 s, for <go_file> to appear, so that
+// several such processes sharing one GPU start their timed steps together, as the
+// reference's one-rank-per-member runs do.  It prints
+//   ref_lbm_time <ensemble_id> <nsteps> <t0_ns> <t1_ns>
+// with CLOCK_REALTIME stamps around the timed steps (the end after a device sync).
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <ctime>
 #include <set>
 #include <sstream>
 #include <string>
 #include <vector>
+
+#include <unistd.h>
 
 #include <cuda_runtime.h>
 
@@ -43,7 +55,41 @@ static void dump_state(data& dat, const std::string& dir, int step) {
     dump(pre + "cursor.i32", &cursor, sizeof(int));
 }
 
+static long long now_ns() {
+    timespec ts;
+    clock_gettime(CLOCK_REALTIME, &ts);
+    return ts.tv_sec * 1000000000LL + ts.tv_nsec;
+}
+
+static int time_steps(int argc, char** argv) {
+    const int id = std::atoi(argv[2]);
+    const int nsteps = std::atoi(argv[3]);
+    const int warmup = std::atoi(argv[4]);
+    auto dat = data(id);
+    for (int s = 0; s < warmup; s++) update(dat, s);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) { std::fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(e)); return 1; }
+    if (argc >= 7) {
+        std::FILE* fp = std::fopen(argv[5], "w");
+        if (!fp) { std::fprintf(stderr, "cannot write %s\n", argv[5]); return 1; }
+        std::fclose(fp);
+        const long long limit = now_ns() + 300LL * 1000000000LL;
+        while (access(argv[6], F_OK) != 0) {
+            if (now_ns() > limit) { std::fprintf(stderr, "ref_lbm: no start signal within 300 s\n"); return 3; }
+            usleep(100);
+        }
+    }
+    const long long t0 = now_ns();
+    for (int s = warmup; s < warmup + nsteps; s++) update(dat, s);
+    e = cudaDeviceSynchronize();
+    const long long t1 = now_ns();
+    if (e != cudaSuccess) { std::fprintf(stderr, "CUDA error: %s\n", cudaGetErrorString(e)); return 1; }
+    std::printf("ref_lbm_time %d %d %lld %lld\n", id, nsteps, t0, t1);
+    return 0;
+}
+
 int main(int argc, char** argv) {
+    if (argc >= 5 && std::strcmp(argv[1], "time") == 0) return time_steps(argc, argv);
     if (argc < 5) { std::fprintf(stderr, "usage: %s out_dir ensemble_id nsteps dumps\n", argv[0]); return 2; }
     const std::string dir = argv[1];
     const int id = std::atoi(argv[2]);
