@@ -489,10 +489,13 @@ __device__ __forceinline__ float warp_sum(float v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
-// float offset of 16-byte chunk c4 (rows 4 c4 .. 4 c4 + 3) of half column hb in the exchange
-// matrix: chunks are XOR-swizzled by hb so that the eight threads of a quarter warp,
-// which touch eight different half columns at the same chunk, hit eight bank groups
-__device__ __forceinline__ int sa_chunk(int hb, int c4) { return hb * kHalf + 4 * (c4 ^ (hb & 7)); }
+// floats per half column in the exchange matrix: 32 rows and 4 of padding.  The eight
+// threads of a quarter warp touch eight half columns with indices in one aligned group
+// of eight at the same chunk; a stride of 36 = 4 (mod 32) puts those in eight different
+// bank groups, and a thread's eight chunks sit at fixed offsets from one base address.
+constexpr int kHS = kHalf + 4;
+// float offset of 16-byte chunk c4 (rows 4 c4 .. 4 c4 + 3) of half column hb
+__device__ __forceinline__ int sa_chunk(int hb, int c4) { return hb * kHS + 4 * c4; }
 // sum of the two halves of a column (adjacent lanes)
 __device__ __forceinline__ float pair_sum(float v) { return v + __shfl_xor_sync(0xffffffffu, v, 1); }
 
@@ -532,22 +535,24 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
     const int nobs_pad = (nobs + 3) & ~3;
     float* sW = smem;                    // [nobs][64] window dY (unweighted)
     float* sDyo = sW + nobs * kWide;     // [nobs]     window innovations (padded to 4)
-    float* sA = sDyo + nobs_pad;         // [128][32]  half columns: Q, the Jacobi exchange, then V (swizzled)
-    float* sDX = sA + kWide * kWide;     // [9][64]    dX, then D = dX V in place
+    float* sA = sDyo + nobs_pad;         // [128][kHS] half columns: Q, the Jacobi exchange, then V
+    float* sDX = sA + 2 * kWide * kHS;   // [9][64]    dX, then D = dX V in place
     float* sS = sDX + kQ * kWide;        // [64]       sqrt(M-1)/sqrt(lambda)
     float* sY = sS + kWide;              // [64]       Lambda^-1 V^T c
     float* sN = sY + kWide;              // [64]       squared column norms of A (Jacobi rounds), and
     float* sC = sN;                      //            c = dY^T R^-1 dyo (transform), and
     float* sRed = sN;                    //            per-warp partial sums [4][12] (between those)
     float* sXbar = sN + kWide;           // [12]       ensemble mean
-    float* sV = sXbar + 12;              // [64][64]   eigenvectors, V[l][k] at sV[l*64 + k]
 
     const int tiles_x = (A.nx + kWCW - 1) / kWCW;
     const int tile = blockIdx.x;
     const int x0 = (tile % tiles_x) * kWCW;
     const int y0 = (A.tile_y0 + tile / tiles_x) * kWCH;
 
-    for (int l = 0; l < kHalf; l++) sV[(r0 + l) * kWide + k] = (r0 + l == k) ? 1.f : 0.f;
+    // rows [r0, r0 + 32) of eigenvector k, carried from point to point in registers
+    float vv[kHalf];
+#pragma unroll
+    for (int l = 0; l < kHalf; l++) vv[l] = (r0 + l == k) ? 1.f : 0.f;
     int cached_bi = -1, cached_bj = -1;
     int max_sweeps = 0, noconv = 0, total_sweeps = 0;
     bool bad = false;
@@ -690,7 +695,10 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                 if (r0 + l == k && k < M) qv[l] += A.diag;
         }
 
-        // 4. warm start A = Q V_prev: Q's columns go through sA
+        // 4. warm start A = Q V_prev: Q's columns go through sA.  Column k of V_prev is in
+        //    the registers of the column's two threads: V[32h + c][k] here, V[32(1-h) + c][k]
+        //    one lane over; they meet Q's columns 32h + c (half column 65h + 2c of sA) and
+        //    32(1-h) + c (half column 64 - 63h + 2c).
         if (idx > 0) {
 #pragma unroll
             for (int l = 0; l < kHalf; l += 4)
@@ -698,15 +706,20 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
             __syncthreads();
 #pragma unroll
             for (int l = 0; l < kHalf; l++) qv[l] = 0.f;
-            for (int c = 0; c < kWide; c++) {
-                const float vc = sV[c * kWide + k];
+            const float* qo = sA + sa_chunk(65 * h, 0);
+            const float* qt = sA + sa_chunk(64 - 63 * h, 0);
+#pragma unroll
+            for (int c = 0; c < kHalf; c++) {
+                const float vo = vv[c];
+                const float vt = __shfl_xor_sync(0xffffffffu, vo, 1);
 #pragma unroll
                 for (int l = 0; l < kHalf; l += 4) {
-                    const float4 q4 = *reinterpret_cast<const float4*>(sA + sa_chunk(2 * c + h, l >> 2));
-                    qv[l + 0] = fmaf(q4.x, vc, qv[l + 0]);
-                    qv[l + 1] = fmaf(q4.y, vc, qv[l + 1]);
-                    qv[l + 2] = fmaf(q4.z, vc, qv[l + 2]);
-                    qv[l + 3] = fmaf(q4.w, vc, qv[l + 3]);
+                    const float4 a4 = *reinterpret_cast<const float4*>(qo + 2 * c * kHS + l);
+                    const float4 b4 = *reinterpret_cast<const float4*>(qt + 2 * c * kHS + l);
+                    qv[l + 0] = fmaf(b4.x, vt, fmaf(a4.x, vo, qv[l + 0]));
+                    qv[l + 1] = fmaf(b4.y, vt, fmaf(a4.y, vo, qv[l + 1]));
+                    qv[l + 2] = fmaf(b4.z, vt, fmaf(a4.z, vo, qv[l + 2]));
+                    qv[l + 3] = fmaf(b4.w, vt, fmaf(a4.w, vo, qv[l + 3]));
                 }
             }
             __syncthreads();  // sA is the Jacobi exchange next
@@ -805,9 +818,9 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                 for (int l = 0; l < kHalf; l++) qv[l] = (r0 + l == k) ? 1.f : 0.f;
             }
         }
-        // qv holds rows [r0, r0 + 32) of v_k: into sV (row-major) and sA (column-major)
+        // qv holds rows [r0, r0 + 32) of v_k: kept for the next warm start, and into sA
 #pragma unroll
-        for (int l = 0; l < kHalf; l++) sV[(r0 + l) * kWide + k] = qv[l];
+        for (int l = 0; l < kHalf; l++) vv[l] = qv[l];
 #pragma unroll
         for (int l = 0; l < kHalf; l += 4)
             *reinterpret_cast<float4*>(sA + sa_chunk(2 * k + h, l >> 2)) = make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
@@ -943,7 +956,7 @@ int analysis_supported(int M) { return M >= 2 && M <= kMaxAnalysisMembers; }
 // dynamic shared memory of one analysis CTA (4 warps) for M members and a window of nobs slots
 size_t analysis_smem_bytes(int M, int nobs) {
     if (M > 32)  // analysis_wide_kernel: one 64-thread CTA
-        return sizeof(float) * (size_t(nobs) * kWide + ((nobs + 3) & ~3) + 2 * kWide * kWide + kQ * kWide + 3 * kWide +
+        return sizeof(float) * (size_t(nobs) * kWide + ((nobs + 3) & ~3) + 2 * kWide * kHS + kQ * kWide + 3 * kWide +
                                 12);
     const int mp = pad_pow2(M);
     const int per_grp = nobs * mp + ((nobs + 3) & ~3) + mp * mp + kQ * mp + 2 * mp + 12;
