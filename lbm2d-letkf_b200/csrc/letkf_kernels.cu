@@ -123,8 +123,9 @@ __device__ __forceinline__ float group_sum(float v) {
 // ---------------------------------------------------------------------------
 constexpr int kCW = 4, kCH = 2;  // chain tile (points in x, points in y)
 // the wide analysis walks taller tiles: fewer cold starts, and its many waves hide
-// the longer CTAs (C2: 60.2 ms against 62.8 ms for 4 x 2; C1's kernel is fastest at 4 x 2)
-constexpr int kWCW = 4, kWCH = 4;
+// the longer CTAs (512^2, M = 64: 58.7 ms at 4 x 8, 59.3 at 4 x 4, 62.8 at 4 x 2;
+// C1's kernel is fastest at 4 x 2)
+constexpr int kWCW = 4, kWCH = 8;
 
 // DUMP = true recomputes the tiles that cover the rows of D and, instead of writing
 // the analysis, writes every intermediate matrix of those rows (need_save_mat).
