@@ -495,6 +495,11 @@ __device__ __forceinline__ float warp_sum(float v) {
 // of eight at the same chunk; a stride of 36 = 4 (mod 32) puts those in eight different
 // bank groups, and a thread's eight chunks sit at fixed offsets from one base address.
 constexpr int kHS = kHalf + 4;
+// Arrays indexed by member (window rows, dX, the per-column scalars) put the upper half
+// 4 floats further on, so that a column's two threads, which read element m and m + 32
+// together, hit different bank groups: member m sits at hx(m) of a kHP-float row.
+constexpr int kHP = kWide + 4;
+__device__ __forceinline__ int hx(int m) { return m + 4 * (m >> 5); }
 // float offset of 16-byte chunk c4 (rows 4 c4 .. 4 c4 + 3) of half column hb
 __device__ __forceinline__ int sa_chunk(int hb, int c4) { return hb * kHS + 4 * c4; }
 // sum of the two halves of a column (adjacent lanes)
@@ -534,16 +539,16 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
     const int nobs = A.n_pat_max;
     const int nox2 = nobs / 3;
     const int nobs_pad = (nobs + 3) & ~3;
-    float* sW = smem;                    // [nobs][64] window dY (unweighted)
-    float* sDyo = sW + nobs * kWide;     // [nobs]     window innovations (padded to 4)
-    float* sA = sDyo + nobs_pad;         // [128][kHS] half columns: Q, the Jacobi exchange, then V
-    float* sDX = sA + 2 * kWide * kHS;   // [9][64]    dX, then D = dX V in place
-    float* sS = sDX + kQ * kWide;        // [64]       sqrt(M-1)/sqrt(lambda)
-    float* sY = sS + kWide;              // [64]       Lambda^-1 V^T c
-    float* sN = sY + kWide;              // [64]       squared column norms of A (Jacobi rounds), and
-    float* sC = sN;                      //            c = dY^T R^-1 dyo (transform), and
-    float* sRed = sN;                    //            per-warp partial sums [4][12] (between those)
-    float* sXbar = sN + kWide;           // [12]       ensemble mean
+    float* sW = smem;                    // [nobs][kHP] window dY (unweighted), member m at hx(m)
+    float* sDyo = sW + nobs * kHP;       // [nobs]      window innovations (padded to 4)
+    float* sA = sDyo + nobs_pad;         // [128][kHS]  half columns: Q, the Jacobi exchange, then V
+    float* sDX = sA + 2 * kWide * kHS;   // [9][kHP]    dX, then D = dX V in place
+    float* sS = sDX + kQ * kHP;          // [kHP]       sqrt(M-1)/sqrt(lambda)
+    float* sY = sS + kHP;                // [kHP]       Lambda^-1 V^T c
+    float* sN = sY + kHP;                // [kHP]       squared column norms of A (Jacobi rounds), and
+    float* sC = sN;                      //             c = dY^T R^-1 dyo (transform), and
+    float* sRed = sN;                    //             per-warp partial sums [4][12] (between those)
+    float* sXbar = sN + kHP;             // [12]        ensemble mean
 
     const int tiles_x = (A.nx + kWCW - 1) / kWCW;
     const int tile = blockIdx.x;
@@ -580,7 +585,7 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
 #pragma unroll
                 for (int q = 0; q < kQ; q++) {
                     const float xb = (sRed[q] + sRed[12 + q] + sRed[24 + q] + sRed[36 + q]) / float(M);
-                    sDX[q * kWide + k] = real_k ? xq[q] - xb : 0.f;
+                    sDX[q * kHP + hx(k)] = real_k ? xq[q] - xb : 0.f;
                     if (k == 0) sXbar[q] = xb;
                 }
         }
@@ -597,7 +602,7 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                     const int site = si + A.nsx * sj;
                     for (int var = h; var < 3; var += 2) {
                         const int sl = a + A.nox * b + var * nox2;
-                        sW[sl * kWide + k] = real_k ? __ldg(dY + (size_t(var) * A.nsites + site) * M + k) : 0.f;
+                        sW[sl * kHP + hx(k)] = real_k ? __ldg(dY + (size_t(var) * A.nsites + site) * M + k) : 0.f;
                         if (k == 0) sDyo[sl] = __ldg(dyo + size_t(var) * A.nsites + site);
                     }
                 }
@@ -633,7 +638,7 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                         if (o < cnt) {
                             const int4 e = ent[o];
                             const float wv = __int_as_float(e.w);
-                            const float y = sW[e.x * kWide + k];
+                            const float y = sW[e.x * kHP + hx(k)];
                             ckp = fmaf(wv * y, sDyo[e.x], ckp);
                             val = sqrtf(wv) * y;
                         }
@@ -678,12 +683,12 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
         }
         for (int o = 0; !TC && o < cnt; o++) {
             const int4 e = ent[o];
-            const float* row = sW + e.x * kWide;
-            const float ek = __int_as_float(e.w) * row[k];
+            const float* row = sW + e.x * kHP;
+            const float ek = __int_as_float(e.w) * row[hx(k)];
             ck = fmaf(ek, sDyo[e.x], ck);
 #pragma unroll
             for (int l = 0; l < kHalf; l += 4) {
-                const float4 r4 = *reinterpret_cast<const float4*>(row + r0 + l);
+                const float4 r4 = *reinterpret_cast<const float4*>(row + hx(r0) + l);
                 qv[l + 0] = fmaf(ek, r4.x, qv[l + 0]);
                 qv[l + 1] = fmaf(ek, r4.y, qv[l + 1]);
                 qv[l + 2] = fmaf(ek, r4.z, qv[l + 2]);
@@ -825,37 +830,39 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
 #pragma unroll
         for (int l = 0; l < kHalf; l += 4)
             *reinterpret_cast<float4*>(sA + sa_chunk(2 * k + h, l >> 2)) = make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
-        if (h == 0) sC[k] = ck;
+        if (h == 0) sC[hx(k)] = ck;
         __syncthreads();
         float vc = 0.f;  // (V^T c)_k
 #pragma unroll
-        for (int l = 0; l < kHalf; l++) vc = fmaf(qv[l], sC[r0 + l], vc);
+        for (int l = 0; l < kHalf; l++) vc = fmaf(qv[l], sC[hx(r0) + l], vc);
         vc = pair_sum(vc);
         float dsum[kQ];
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
             float d = 0.f;
 #pragma unroll
-            for (int l = 0; l < kHalf; l++) d = fmaf(sDX[q * kWide + r0 + l], qv[l], d);
+            for (int l = 0; l < kHalf; l++) d = fmaf(sDX[q * kHP + hx(r0) + l], qv[l], d);
             dsum[q] = pair_sum(d);
         }
         __syncthreads();  // every thread has read dX before D overwrites it
         if (h == 0) {
-            sY[k] = real_k ? vc / lam : 0.f;
-            sS[k] = real_k ? A.sqrt_m1 / sqrtf(lam) : 0.f;
+            sY[hx(k)] = real_k ? vc / lam : 0.f;
+            sS[hx(k)] = real_k ? A.sqrt_m1 / sqrtf(lam) : 0.f;
 #pragma unroll
-            for (int q = 0; q < kQ; q++) sDX[q * kWide + k] = dsum[q];
+            for (int q = 0; q < kQ; q++) sDX[q * kHP + hx(k)] = dsum[q];
         }
         __syncthreads();
-        // Xa_k = xbar + sum_jj D[:, jj] z_jj, z_jj = sS[jj] V[k][jj] + sY[jj]; halves split jj
+        // Xa_k = xbar + sum_jj D[:, jj] z_jj, z_jj = sS[jj] V[k][jj] + sY[jj]; halves split jj,
+        // the upper half one step out of phase (its V reads then fall in other bank groups)
         float acc[kQ];
 #pragma unroll
         for (int q = 0; q < kQ; q++) acc[q] = 0.f;
 #pragma unroll 4
-        for (int jj = r0; jj < r0 + kHalf; jj++) {
-            const float z = fmaf(sS[jj], sA[sa_chunk(2 * jj + (k >> 5), (k & 31) >> 2) + (k & 3)], sY[jj]);
+        for (int ii = 0; ii < kHalf; ii++) {
+            const int jj = r0 + ((ii + h) & (kHalf - 1));
+            const float z = fmaf(sS[hx(jj)], sA[sa_chunk(2 * jj + (k >> 5), (k & 31) >> 2) + (k & 3)], sY[hx(jj)]);
 #pragma unroll
-            for (int q = 0; q < kQ; q++) acc[q] = fmaf(sDX[q * kWide + jj], z, acc[q]);
+            for (int q = 0; q < kQ; q++) acc[q] = fmaf(sDX[q * kHP + hx(jj)], z, acc[q]);
         }
 #pragma unroll
         for (int q = 0; q < kQ; q++) acc[q] = pair_sum(acc[q]);
@@ -957,8 +964,7 @@ int analysis_supported(int M) { return M >= 2 && M <= kMaxAnalysisMembers; }
 // dynamic shared memory of one analysis CTA (4 warps) for M members and a window of nobs slots
 size_t analysis_smem_bytes(int M, int nobs) {
     if (M > 32)  // analysis_wide_kernel: one 64-thread CTA
-        return sizeof(float) * (size_t(nobs) * kWide + ((nobs + 3) & ~3) + 2 * kWide * kHS + kQ * kWide + 3 * kWide +
-                                12);
+        return sizeof(float) * (size_t(nobs) * kHP + ((nobs + 3) & ~3) + 2 * kWide * kHS + kQ * kHP + 3 * kHP + 12);
     const int mp = pad_pow2(M);
     const int per_grp = nobs * mp + ((nobs + 3) & ~3) + mp * mp + kQ * mp + 2 * mp + 12;
     return sizeof(float) * size_t(per_grp) * 4 * (32 / mp);
