@@ -105,6 +105,14 @@ __global__ void obs_ensemble_kernel(const float* __restrict__ f, const float* __
     }
 }
 
+// square root for the Jacobi rotation angle: t only picks the angle, and cs = (1 + t^2)^-1/2
+// makes the rotation orthogonal for any t, so the hardware approximation serves
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 template <int MP>
 __device__ __forceinline__ float group_sum(float v) {
 #pragma unroll
@@ -297,6 +305,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         //    into qv at the start of every sweep.
         int sweeps = 0;
         bool converged = false;
+        const float tol2 = A.tol * A.tol, stop2 = A.stop * A.stop;  // the tests below compare squares
         float sc = 1.f;
         for (int sw = 0; sw < A.max_sweeps; sw++) {
 #pragma unroll
@@ -307,7 +316,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
             for (int l = 0; l < MP; l += 2) { a0 = fmaf(qv[l], qv[l], a0); a1 = fmaf(qv[l + 1], qv[l + 1], a1); }
             float a = a0 + a1;
             bool rot = false;
-            float worst = 0.f;  // largest |g| / sqrt(a b) of the sweep
+            float worst = 0.f;  // largest g^2 / (a b) of the sweep
 #pragma unroll 1
             for (int rr = 1; rr < MP; rr++) {
                 float pq[MP];
@@ -321,13 +330,14 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
                 const float b = __shfl_xor_sync(0xffffffffu, a, rr);
                 const bool low = k < (k ^ rr);
                 const float alo = low ? a : b, ahi = low ? b : a;
-                const float nrm = sqrtf(alo * ahi);
-                const bool doit = fabsf(g) > A.tol * nrm;
+                // |g| > tol sqrt(alo ahi), on squares
+                const float p2 = alo * ahi, g2 = g * g;
+                const bool doit = g2 > tol2 * p2;
                 if (doit) {
                     // any exact rotation converges; cs^2 + sn^2 = 1 keeps the columns' span
-                    worst = fmaxf(worst, __fdividef(fabsf(g), nrm));
+                    worst = fmaxf(worst, __fdividef(g2, p2));
                     const float zeta = __fdividef(ahi - alo, 2.f * g);
-                    const float t = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.f)));
+                    const float t = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrt_approx(fmaf(zeta, zeta, 1.f)));
                     const float cs = rsqrtf(fmaf(t, t, 1.f));
                     // low: cs a - sn b; high: sn a + cs b (sn = cs t), with the scales
                     const float rho = (low ? -t : t) * __fdividef(sp, sc);
@@ -341,7 +351,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
             // group max of the sweep's relative off-diagonal
 #pragma unroll
             for (int o = MP / 2; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
-            const bool done = !rot || worst < A.stop;
+            const bool done = !rot || worst < stop2;
             const unsigned ballot = __ballot_sync(0xffffffffu, !done && active);
             if (!converged) {
                 sweeps = sw + 1;
@@ -735,6 +745,7 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
         //    a column's scale is published beside its squared norm
         int sweeps = 0;
         bool converged = false;
+        const float tol2 = A.tol * A.tol, stop2 = A.stop * A.stop;  // the tests below compare squares
         float sc = 1.f;
         float* sSc = sS;  // [64] column scales during the Jacobi (sS is written after it)
         for (int sw = 0; sw < A.max_sweeps; sw++) {
@@ -746,7 +757,7 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
             for (int l = 0; l < kHalf; l += 2) { a0 = fmaf(qv[l], qv[l], a0); a1 = fmaf(qv[l + 1], qv[l + 1], a1); }
             float a = pair_sum(a0 + a1);
             bool rot = false, dirty = true;
-            float worst = 0.f;
+            float worst = 0.f;  // largest g^2 / (a b) of the sweep
             for (int rr = 1; rr < kWide; rr++) {
                 const int pk = k ^ rr;
                 if (dirty) {
@@ -776,12 +787,13 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                 const float g = pair_sum(g0 + g1) * (sc * sp);
                 const bool low = k < pk;
                 const float alo = low ? a : b, ahi = low ? b : a;
-                const float nrm = sqrtf(alo * ahi);
-                const bool doit = fabsf(g) > A.tol * nrm;
+                // |g| > tol sqrt(alo ahi), on squares
+                const float p2 = alo * ahi, g2 = g * g;
+                const bool doit = g2 > tol2 * p2;
                 if (doit) {
-                    worst = fmaxf(worst, __fdividef(fabsf(g), nrm));
+                    worst = fmaxf(worst, __fdividef(g2, p2));
                     const float zeta = __fdividef(ahi - alo, 2.f * g);
-                    const float tt = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.f)));
+                    const float tt = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrt_approx(fmaf(zeta, zeta, 1.f)));
                     const float cs = rsqrtf(fmaf(tt, tt, 1.f));
                     const float rho = (low ? -tt : tt) * __fdividef(sp, sc);
 #pragma unroll
@@ -800,7 +812,7 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
             const int any_rot = __syncthreads_or(rot ? 1 : 0);
             wmax = fmaxf(fmaxf(sRed[0], sRed[12]), fmaxf(sRed[24], sRed[36]));
             sweeps = sw + 1;
-            const bool done = !any_rot || wmax < A.stop;
+            const bool done = !any_rot || wmax < stop2;
             __syncthreads();
             if (done) { converged = true; break; }
         }
