@@ -336,8 +336,10 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
                 if (doit) {
                     // any exact rotation converges; cs^2 + sn^2 = 1 keeps the columns' span
                     worst = fmaxf(worst, __fdividef(g2, p2));
-                    const float zeta = __fdividef(ahi - alo, 2.f * g);
-                    const float t = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrt_approx(fmaf(zeta, zeta, 1.f)));
+                    // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = d / e, multiplied through by |e|:
+                    // one reciprocal on the critical path instead of two
+                    const float d = ahi - alo, e = 2.f * g;
+                    const float t = __fdividef(copysignf(fabsf(e), d * e), fabsf(d) + sqrt_approx(fmaf(d, d, e * e)));
                     const float cs = rsqrtf(fmaf(t, t, 1.f));
                     // low: cs a - sn b; high: sn a + cs b (sn = cs t), with the scales
                     const float rho = (low ? -t : t) * __fdividef(sp, sc);
@@ -792,8 +794,9 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                 const bool doit = g2 > tol2 * p2;
                 if (doit) {
                     worst = fmaxf(worst, __fdividef(g2, p2));
-                    const float zeta = __fdividef(ahi - alo, 2.f * g);
-                    const float tt = __fdividef(copysignf(1.f, zeta), fabsf(zeta) + sqrt_approx(fmaf(zeta, zeta, 1.f)));
+                    // tt = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = d / e, multiplied through by |e|
+                    const float d = ahi - alo, e = 2.f * g;
+                    const float tt = __fdividef(copysignf(fabsf(e), d * e), fabsf(d) + sqrt_approx(fmaf(d, d, e * e)));
                     const float cs = rsqrtf(fmaf(tt, tt, 1.f));
                     const float rho = (low ? -tt : tt) * __fdividef(sp, sc);
 #pragma unroll
