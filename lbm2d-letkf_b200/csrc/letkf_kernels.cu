@@ -487,11 +487,10 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
 // ---------------------------------------------------------------------------
 // The local analysis for 32 < M <= 64 (the C2 ensembles; the reference runs them
 // through EigenG-Batched).  One CTA of 128 threads walks one kWCW x kWCH tile of points;
-// thread t owns rows [32h, 32h + 32) (h = t & 1) of member column k = t >> 1, and
-// the two halves of a column combine their partial dot products with one shuffle.
-// The algorithm is the one above; the Jacobi's partner columns go through a 64 x 64
-// shared exchange matrix: each round a thread publishes its half column (when it
-// changed) and reads its partner's half once, with a barrier on each side.
+// thread t owns rows [32h, 32h + 32) (h = t & 1) of member column k = t >> 1 for the
+// Gram, the warm start and the transform; the two halves of a column combine their
+// partial sums with one shuffle.  The algorithm is the one above, except that the
+// Jacobi hands whole column pairs between quads of threads through shared memory (step 5).
 // ---------------------------------------------------------------------------
 constexpr int kWide = 64;             // member columns
 constexpr int kHalf = 32;             // rows per thread
@@ -516,6 +515,23 @@ __device__ __forceinline__ int hx(int m) { return m + 4 * (m >> 5); }
 __device__ __forceinline__ int sa_chunk(int hb, int c4) { return hb * kHS + 4 * c4; }
 // sum of the two halves of a column (adjacent lanes)
 __device__ __forceinline__ float pair_sum(float v) { return v + __shfl_xor_sync(0xffffffffu, v, 1); }
+// sum over a quad of lanes (4s .. 4s + 3); every lane of the quad gets the same value
+__device__ __forceinline__ float quad_sum(float v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    return v + __shfl_xor_sync(0xffffffffu, v, 2);
+}
+// 16 consecutive floats of shared memory (16-byte aligned) to registers and back
+__device__ __forceinline__ void wide_load16(float (&x)[16], const float* p) {
+#pragma unroll
+    for (int m = 0; m < 16; m += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p + m);
+        x[m] = v.x; x[m + 1] = v.y; x[m + 2] = v.z; x[m + 3] = v.w;
+    }
+}
+__device__ __forceinline__ void wide_store16(float* p, const float (&x)[16]) {
+#pragma unroll
+    for (int m = 0; m < 16; m += 4) *reinterpret_cast<float4*>(p + m) = make_float4(x[m], x[m + 1], x[m + 2], x[m + 3]);
+}
 
 // BF16 tensor-core Gram (TC): the point's weighted window C = sqrt(w) dY (one row per
 // member, one column per weight-table entry) is staged as BF16 in sA, kCStride
@@ -743,82 +759,139 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
             __syncthreads();  // sA is the Jacobi exchange next
         }
 
-        // 5. one-sided Jacobi on the columns of A, lazily scaled (see analysis_kernel);
-        //    a column's scale is published beside its squared norm
+        // 5. one-sided Jacobi on the columns of A, lazily scaled (see analysis_kernel), with
+        //    the columns handed between thread quads.  Quad s (threads 4s .. 4s + 3, thread r
+        //    holding rows [16 r, 16 r + 16)) rotates one column pair per round: a thread
+        //    holds 16 rows of both columns, and the pair's dot product is one quad reduction.
+        //    The pairs follow a recursive block ordering: at level L = 0..5 the columns form
+        //    blocks of 2H (H = 32 >> L), each split into a fixed half and a shifting half; for
+        //    H rounds fixed column i of a block meets shifting column (i + j) mod H, and
+        //    between rounds every shifting column moves to the quad below.  The levels cover
+        //    every pair once in 32 + 16 + 8 + 4 + 2 + 1 = 63 rounds.  Every column has a home
+        //    slot in sA (its two half columns): the quad that hands a column on writes it
+        //    there, only if it changed since it was last written, and the next owner reads it
+        //    after one barrier.  Per round a pair reads one column and writes at most one.
         int sweeps = 0;
         bool converged = false;
         const float tol2 = A.tol * A.tol, stop2 = A.stop * A.stop;  // the tests below compare squares
-        float sc = 1.f;
         float* sSc = sS;  // [64] column scales during the Jacobi (sS is written after it)
-        for (int sw = 0; sw < A.max_sweeps; sw++) {
 #pragma unroll
-            for (int l = 0; l < kHalf; l++) qv[l] *= sc;
-            sc = 1.f;
-            float a0 = 0.f, a1 = 0.f;
+        for (int l = 0; l < kHalf; l += 4)
+            *reinterpret_cast<float4*>(sA + sa_chunk(2 * k + h, l >> 2)) = make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
+        if (h == 0) sSc[k] = 1.f;
+        __syncthreads();
+        {
+            const int s = t >> 2, r = t & 3;
+            const int hoff = (r >> 1) * kHS + 16 * (r & 1);  // rows [16 r, 16 r + 16) of a home slot
+            float xa[16], xb[16];
+            float sa = 1.f, sb = 1.f, na = 0.f, nb = 0.f;
+            for (int sw = 0; sw < A.max_sweeps; sw++) {
+                bool big = false;  // some rotated pair's relative off-diagonal reached sqrt(tol)
+                for (int L = 0; L < 6; L++) {
+                    const int H = 32 >> L;
+                    const int b = s >> (5 - L), i = s & (H - 1);
+                    const int ca = 2 * H * b + i;
+                    int cb = 2 * H * b + H + i;
+                    wide_load16(xa, sA + 2 * ca * kHS + hoff);
+                    wide_load16(xb, sA + 2 * cb * kHS + hoff);
+                    sa = sSc[ca];
+                    sb = sSc[cb];
+                    bool dirty_a = false, dirty_b = false;
+                    if (L == 0) {  // fold the scales in and recompute the norms once per sweep
+                        float pa = 0.f, pb = 0.f;
 #pragma unroll
-            for (int l = 0; l < kHalf; l += 2) { a0 = fmaf(qv[l], qv[l], a0); a1 = fmaf(qv[l + 1], qv[l + 1], a1); }
-            float a = pair_sum(a0 + a1);
-            bool rot = false, dirty = true;
-            float worst = 0.f;  // largest g^2 / (a b) of the sweep
-            for (int rr = 1; rr < kWide; rr++) {
-                const int pk = k ^ rr;
-                if (dirty) {
+                        for (int l = 0; l < 16; l++) {
+                            xa[l] *= sa;
+                            xb[l] *= sb;
+                            pa = fmaf(xa[l], xa[l], pa);
+                            pb = fmaf(xb[l], xb[l], pb);
+                        }
+                        sa = sb = 1.f;
+                        na = quad_sum(pa);
+                        nb = quad_sum(pb);
+                        dirty_a = dirty_b = true;
+                    } else {
+                        na = sN[ca];
+                        nb = sN[cb];
+                    }
+                    for (int j = 0; j < H; j++) {
+                        float g0 = 0.f, g1 = 0.f;
 #pragma unroll
-                    for (int l = 0; l < kHalf; l += 4)
-                        *reinterpret_cast<float4*>(sA + sa_chunk(2 * k + h, l >> 2)) =
-                            make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
-                    dirty = false;
+                        for (int l = 0; l < 16; l += 2) { g0 = fmaf(xa[l], xb[l], g0); g1 = fmaf(xa[l + 1], xb[l + 1], g1); }
+                        const float g = quad_sum(g0 + g1) * (sa * sb);
+                        const bool alow = ca < cb;
+                        const float alo = alow ? na : nb, ahi = alow ? nb : na;
+                        // |g| > tol sqrt(alo ahi), on squares
+                        const float p2 = alo * ahi, g2 = g * g;
+                        if (g2 > tol2 * p2) {
+                            big |= g2 >= stop2 * p2;
+                            // tt = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = d / e, times |e|
+                            const float d = ahi - alo, e = 2.f * g;
+                            const float tt = __fdividef(copysignf(fabsf(e), d * e), fabsf(d) + sqrt_approx(fmaf(d, d, e * e)));
+                            const float cs = rsqrtf(fmaf(tt, tt, 1.f));
+                            // low column: cs (lo - tt hi); high column: cs (hi + tt lo), with the scales
+                            const float slo = alow ? sa : sb, shi = alow ? sb : sa;
+                            const float rlo = -tt * __fdividef(shi, slo), rhi = tt * __fdividef(slo, shi);
+                            const float ra = alow ? rlo : rhi, rb = alow ? rhi : rlo;
+#pragma unroll
+                            for (int l = 0; l < 16; l++) {
+                                const float a0 = xa[l];
+                                xa[l] = fmaf(ra, xb[l], a0);
+                                xb[l] = fmaf(rb, a0, xb[l]);
+                            }
+                            sa *= cs;
+                            sb *= cs;
+                            const float tg = tt * g;
+                            na = alow ? na - tg : na + tg;
+                            nb = alow ? nb + tg : nb - tg;
+                            dirty_a = dirty_b = true;
+                        }
+                        if (j + 1 < H) {  // hand the shifting column down, take the one from above
+                            if (dirty_b) {
+                                wide_store16(sA + 2 * cb * kHS + hoff, xb);
+                                if (r == 0) {
+                                    sN[cb] = nb;
+                                    sSc[cb] = sb;
+                                }
+                            }
+                            __syncthreads();
+                            cb = 2 * H * b + H + ((i + j + 1) & (H - 1));
+                            wide_load16(xb, sA + 2 * cb * kHS + hoff);
+                            nb = sN[cb];
+                            sb = sSc[cb];
+                            dirty_b = false;
+                        }
+                    }
+                    if (dirty_a) {
+                        wide_store16(sA + 2 * ca * kHS + hoff, xa);
+                        if (r == 0) {
+                            sN[ca] = na;
+                            sSc[ca] = sa;
+                        }
+                    }
+                    if (dirty_b) {
+                        wide_store16(sA + 2 * cb * kHS + hoff, xb);
+                        if (r == 0) {
+                            sN[cb] = nb;
+                            sSc[cb] = sb;
+                        }
+                    }
+                    __syncthreads();
                 }
-                if (h == 0) {
-                    sN[k] = a;
-                    sSc[k] = sc;
+                sweeps = sw + 1;
+                if (!__syncthreads_or(big ? 1 : 0)) {
+                    converged = true;
+                    break;
                 }
-                __syncthreads();
-                float pq[kHalf];
-#pragma unroll
-                for (int l = 0; l < kHalf; l += 4) {
-                    const float4 p4 = *reinterpret_cast<const float4*>(sA + sa_chunk(2 * pk + h, l >> 2));
-                    pq[l] = p4.x; pq[l + 1] = p4.y; pq[l + 2] = p4.z; pq[l + 3] = p4.w;
-                }
-                const float b = sN[pk];
-                const float sp = sSc[pk];
-                __syncthreads();  // the partner's half is in registers: sA may change
-                float g0 = 0.f, g1 = 0.f;
-#pragma unroll
-                for (int l = 0; l < kHalf; l += 2) { g0 = fmaf(qv[l], pq[l], g0); g1 = fmaf(qv[l + 1], pq[l + 1], g1); }
-                const float g = pair_sum(g0 + g1) * (sc * sp);
-                const bool low = k < pk;
-                const float alo = low ? a : b, ahi = low ? b : a;
-                // |g| > tol sqrt(alo ahi), on squares
-                const float p2 = alo * ahi, g2 = g * g;
-                const bool doit = g2 > tol2 * p2;
-                if (doit) {
-                    worst = fmaxf(worst, __fdividef(g2, p2));
-                    // tt = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = d / e, multiplied through by |e|
-                    const float d = ahi - alo, e = 2.f * g;
-                    const float tt = __fdividef(copysignf(fabsf(e), d * e), fabsf(d) + sqrt_approx(fmaf(d, d, e * e)));
-                    const float cs = rsqrtf(fmaf(tt, tt, 1.f));
-                    const float rho = (low ? -tt : tt) * __fdividef(sp, sc);
-#pragma unroll
-                    for (int l = 0; l < kHalf; l++) qv[l] = fmaf(rho, pq[l], qv[l]);
-                    sc *= cs;
-                    a = low ? a - tt * g : a + tt * g;
-                    dirty = true;
-                }
-                rot |= doit;
             }
-            // CTA-wide max of the sweep's relative off-diagonal, and whether any pair rotated
-            float wmax = worst;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
-            if (lane == 0) sRed[warp * 12] = wmax;
-            const int any_rot = __syncthreads_or(rot ? 1 : 0);
-            wmax = fmaxf(fmaxf(sRed[0], sRed[12]), fmaxf(sRed[24], sRed[36]));
-            sweeps = sw + 1;
-            const bool done = !any_rot || wmax < stop2;
-            __syncthreads();
-            if (done) { converged = true; break; }
         }
+        // the columns of A back into the (k, h) half columns
+#pragma unroll
+        for (int l = 0; l < kHalf; l += 4) {
+            const float4 q4 = *reinterpret_cast<const float4*>(sA + sa_chunk(2 * k + h, l >> 2));
+            qv[l] = q4.x; qv[l + 1] = q4.y; qv[l + 2] = q4.z; qv[l + 3] = q4.w;
+        }
+        const float sc = sSc[k];
 
         // 6. eigenpair of column k and the transform (letkf_solver.h:288-316)
 #pragma unroll
