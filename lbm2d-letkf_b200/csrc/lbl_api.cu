@@ -440,7 +440,8 @@ int build_weight_table(lbl_ctx* ctx) {
                         int* e = tab.data() + (size_t(pat) * G.nobs + n) * 4;
                         e[0] = a + G.nox * b + var * G.nox * G.nox;  // window slot (letkf.cu:155, 183-185)
                         e[1] = var;
-                        e[2] = 0;
+                        const float sw = std::sqrt(w);  // correctly rounded, as the device's sqrtf
+                        std::memcpy(&e[2], &sw, sizeof(float));
                         std::memcpy(&e[3], &w, sizeof(float));
                         n++;
                     }

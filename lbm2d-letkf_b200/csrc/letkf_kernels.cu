@@ -126,8 +126,10 @@ __device__ __forceinline__ float group_sum(float v) {
 // order.  The unweighted observation window of the current p x p block is cached
 // in shared memory, and every point's Jacobi starts from the previous point's
 // eigenvectors (A = Q V_prev), which leaves little to rotate.
-// Weight table entry (int4): x = window slot (a + nox*b + var*nox^2), w = weight
-// bits (sigma^-2 x Gaspari-Cohn), only w > 0, per pattern (i mod p, j mod p).
+// Weight table entry (int4): x = window slot (a + nox*b + var*nox^2), y = variable,
+// z = sqrt(w) bits (the tensor-core Gram's row weight; zero in tables that serve only
+// analysis_kernel), w = weight bits (sigma^-2 x Gaspari-Cohn), only w > 0, per pattern
+// (i mod p, j mod p).
 // ---------------------------------------------------------------------------
 constexpr int kCW = 4, kCH = 2;  // chain tile (points in x, points in y)
 // the wide analysis walks taller tiles: fewer cold starts, and its many waves hide
@@ -656,8 +658,11 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
             for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
             float ckp = 0.f;
             for (int ob = 0; ob < cnt; ob += kGramChunk) {
-                // stage: thread (k, h) fills entries [ob + 40 h, ob + 40 h + 40) of row k
-                for (int o2 = kGramChunk / 2 * h; o2 < kGramChunk / 2 * (h + 1); o2 += 2) {
+                // stage: thread (k, h) fills entries [ob + 40 h, ob + 40 h + 40) of row k (unrolled,
+                // so that several weight-table and window loads are in flight at once)
+#pragma unroll 5
+                for (int q2 = 0; q2 < kGramChunk / 4; q2++) {
+                    const int o2 = kGramChunk / 2 * h + 2 * q2;
                     float v2[2];
 #pragma unroll
                     for (int u = 0; u < 2; u++) {
@@ -668,7 +673,7 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                             const float wv = __int_as_float(e.w);
                             const float y = sW[e.x * kHP + hx(k)];
                             ckp = fmaf(wv * y, sDyo[e.x], ckp);
-                            val = sqrtf(wv) * y;
+                            val = __int_as_float(e.z) * y;  // sqrt(w), from the table
                         }
                         v2[u] = val;
                     }
