@@ -553,7 +553,9 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], uint32_t a0, uint3
 }
 
 template <bool TC>
-__global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const float* __restrict__ fin,
+// 5 CTAs per SM for the FP32 Gram (96 registers); the tensor-core Gram keeps 4 (its staging
+// overwrites sA, so it carries the eigenvectors in registers)
+__global__ void __launch_bounds__(kWideThreads, TC ? 4 : 5) analysis_wide_kernel(const float* __restrict__ fin,
                                                                      float* __restrict__ fout, float* __restrict__ mac,
                                                                      const float* __restrict__ dY,
                                                                      const float* __restrict__ dyo,
@@ -585,10 +587,17 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
     const int x0 = (tile % tiles_x) * kWCW;
     const int y0 = (A.tile_y0 + tile / tiles_x) * kWCH;
 
-    // rows [r0, r0 + 32) of eigenvector k, carried from point to point in registers
+    // rows [r0, r0 + 32) of eigenvector k, carried from point to point: in registers for
+    // the tensor-core Gram; for the FP32 Gram in this thread's half column of sA, which
+    // nothing between one point's transform and the next point's warm start rewrites
     float vv[kHalf];
 #pragma unroll
     for (int l = 0; l < kHalf; l++) vv[l] = (r0 + l == k) ? 1.f : 0.f;
+    if constexpr (!TC) {
+#pragma unroll
+        for (int l = 0; l < kHalf; l += 4)
+            *reinterpret_cast<float4*>(sA + sa_chunk(2 * k + h, l >> 2)) = make_float4(vv[l], vv[l + 1], vv[l + 2], vv[l + 3]);
+    }
     int cached_bi = -1, cached_bj = -1;
     int max_sweeps = 0, noconv = 0, total_sweeps = 0;
     bool bad = false;
@@ -739,6 +748,13 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
         //    one lane over; they meet Q's columns 32h + c (half column 65h + 2c of sA) and
         //    32(1-h) + c (half column 64 - 63h + 2c).
         if (idx > 0) {
+            if constexpr (!TC) {  // V_prev from this thread's own half column, before Q replaces it
+#pragma unroll
+                for (int l = 0; l < kHalf; l += 4) {
+                    const float4 v4 = *reinterpret_cast<const float4*>(sA + sa_chunk(2 * k + h, l >> 2));
+                    vv[l] = v4.x; vv[l + 1] = v4.y; vv[l + 2] = v4.z; vv[l + 3] = v4.w;
+                }
+            }
 #pragma unroll
             for (int l = 0; l < kHalf; l += 4)
                 *reinterpret_cast<float4*>(sA + sa_chunk(2 * k + h, l >> 2)) = make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
@@ -917,9 +933,12 @@ __global__ void __launch_bounds__(kWideThreads, 4) analysis_wide_kernel(const fl
                 for (int l = 0; l < kHalf; l++) qv[l] = (r0 + l == k) ? 1.f : 0.f;
             }
         }
-        // qv holds rows [r0, r0 + 32) of v_k: kept for the next warm start, and into sA
+        // qv holds rows [r0, r0 + 32) of v_k: into sA (kept there for the next warm start
+        // with the FP32 Gram), and in registers with the tensor-core Gram
+        if constexpr (TC) {
 #pragma unroll
-        for (int l = 0; l < kHalf; l++) vv[l] = qv[l];
+            for (int l = 0; l < kHalf; l++) vv[l] = qv[l];
+        }
 #pragma unroll
         for (int l = 0; l < kHalf; l += 4)
             *reinterpret_cast<float4*>(sA + sa_chunk(2 * k + h, l >> 2)) = make_float4(qv[l], qv[l + 1], qv[l + 2], qv[l + 3]);
