@@ -22,6 +22,8 @@ One bench "step" = one DA cycle = the LETKF analysis + 100 LBM steps.
             lattice update (9 float loads + 9 float stores) x M*nx*ny per launch
             / the average launch time from CUDA events (lbl_profile_step)
   cpu_baseline  the FP64 OpenMP oracle on this host's cores, bounded sample
+  analysis_roofline  the LETKF analysis phase against the nominal FP32 SIMT peak
+            (algorithmic flops of the survey's per-point formulas)
 
 `--impl reference` times the reference's path on the host cores.  The reference
 has no CPU implementation (its only backend is CUDA + MPI + cuBLAS/cuSOLVER), so
@@ -347,6 +349,7 @@ def run_engine(args, dist, rank, world, device):
                      "timed": "forecast phase of the timed cycles (in-graph events), 100 launches per cycle",
                      "ms_per_launch_back_to_back": ms_isolated},
         "phases_ms_per_cycle": {"analysis_with_forcing_beside": ms_ana / K, "forecast": ms_fc / K},
+        "analysis_roofline": analysis_roofline(stats, ms_ana / K),
         "gpu_launches": K * (T + 3),
         "letkf": stats,
         "clocks": clk.summary(),
@@ -428,6 +431,24 @@ def reference_build_line(args):
             "cycles_per_s_upper_bound": 1e3 / best,
             "note": "forecast only: the reference's LETKF analysis (MPI, HDF5, cuSOLVER) is not built here, "
                     "so its cycles/s is below this bound"}
+
+
+def analysis_roofline(stats, ms_phase):
+    """The LETKF analysis against the FP32 SIMT peak: algorithmic flops per grid point
+    (Gram 2 n_obs M^2, transform 2*9*M^2 + 4 M^3, Jacobi 18 M M(M-1)/2 per sweep at the
+    measured mean sweeps) over the analysis phase of the timed cycles, which also holds
+    the observation operator and the forcing chunk beside it, so the fraction is a floor.
+    The peak is nominal (148 SMs x 128 FP32 lanes x 2 flops x 1965 MHz): the measured
+    peaks cover HBM and BF16 tensor cores only."""
+    n_obs = 75  # 25 sites x 3 variables at LETKF_RLOC_LEN = 1, p = 4
+    sweeps = float(stats.get("mean_sweeps") or 0.0)
+    per_point = 2 * n_obs * M * M + 2 * 9 * M * M + 4 * M ** 3 + 18 * M * M * (M - 1) / 2 * sweeps
+    flops = per_point * NX * NX
+    achieved = flops / (ms_phase * 1e-3) / 1e12
+    peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    return {"bound": "fp32 simt", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_kind": "nominal", "flops_per_point": per_point, "mean_sweeps": sweeps,
+            "timed": "analysis phase of the timed cycles (observation operator + analysis, forcing beside it)"}
 
 
 def run_reference(args, rank, world):
