@@ -460,9 +460,10 @@ __global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __res
 // NX > 0 fixes the (square) grid at compile time so that plane and row offsets are
 // immediates; NX = 0 reads nx, ny from P.
 // ---------------------------------------------------------------------------
-// (the closure variant at 256 threads is held to 2 CTAs per SM: 128 registers)
+// (256 threads: the plain kernel is held to 4 CTAs per SM, 64 registers, the closure variant
+// to 2, 128 registers)
 template <bool WRITE_MAC, int MAXT, int NX, typename T, bool CL = false, bool CLU = false>
-__global__ void __launch_bounds__(MAXT, (CL && MAXT == 256) ? 2 : 1)
+__global__ void __launch_bounds__(MAXT, MAXT == 256 ? (CL ? 2 : 4) : 1)
     lbm_step_kernel(const T* __restrict__ fin, T* __restrict__ fout, const float* __restrict__ force,
                     float* __restrict__ mac, Phys P, int TY, const uint32_t* __restrict__ cpack, ClosureScales csc) {
     // CLU: rows wider than one CTA.  The cluster's CTAs (blockIdx.z = chunk) each take
