@@ -361,12 +361,13 @@ def run_engine(args, dist, rank, world, device):
     return line
 
 
-def reference_build_forecast(n_proc, nsteps, warmup=50):
-    """The reference's own LBM (oracle/_ref/ref_lbm) run as n_proc processes sharing
-    the GPU, one ensemble member each, started together after their warm-up.
-    Returns the forecast rate, or {"unavailable": why}."""
+def reference_build_forecast(n_proc, nsteps, warmup=50, exe=None):
+    """The reference's own LBM (oracle/_ref/ref_lbm, or `exe` speaking its `time`
+    protocol) run as n_proc processes sharing the GPU, one ensemble member each,
+    started together after their warm-up.  Returns the forecast rate, or
+    {"unavailable": why}."""
     import tempfile
-    exe = os.path.join(ROOT, "oracle", "_ref", "ref_lbm")
+    exe = exe or os.path.join(ROOT, "oracle", "_ref", "ref_lbm")
     if not os.path.exists(exe):
         return {"unavailable": "oracle/_ref/ref_lbm not built (it needs the reference sources at build time)"}
     with tempfile.TemporaryDirectory() as tmp:

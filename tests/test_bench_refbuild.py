@@ -1,0 +1,59 @@
+"""The host side of bench.py's reference-build timing (`reference_build` of the
+`--impl reference` line), on the CPU: a stand-in executable that speaks the `time`
+protocol of oracle/ref_lbm_harness.cu (create the ready file, wait for the go file,
+print `ref_lbm_time <id> <nsteps> <t0_ns> <t1_ns>`) replaces the reference build, so
+the start barrier, the parsing and the aggregation are checked without a GPU."""
+import os
+import stat
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+FAKE = """#!{py}
+import os, sys, time
+_, mode, ident, nsteps, warmup, ready, go = sys.argv
+open(ready, "w").close()
+t_end = time.time() + 30
+while not os.path.exists(go):
+    if time.time() > t_end:
+        sys.exit(3)
+    time.sleep(0.001)
+t0 = time.time_ns()
+time.sleep({step_s} * int(nsteps))
+t1 = time.time_ns()
+print("ref_lbm_time", ident, nsteps, t0, t1)
+sys.exit({rc})
+"""
+
+
+def _fake(tmp_path, step_s=0.0002, rc=0):
+    path = tmp_path / "fake_ref_lbm"
+    path.write_text(FAKE.format(py=sys.executable, step_s=step_s, rc=rc))
+    path.chmod(path.stat().st_mode | stat.S_IXUSR)
+    return str(path)
+
+
+def test_processes_start_together_and_rates_aggregate(tmp_path):
+    exe = _fake(tmp_path)
+    r = bench.reference_build_forecast(4, 100, exe=exe)
+    assert "unavailable" not in r, r
+    assert r["processes"] == 4 and r["steps_per_process"] == 100
+    # 4 processes x 100 steps of >= 0.2 ms each, run side by side: the span covers one process at least
+    assert r["seconds"] >= 0.02
+    assert r["ms_per_100_steps"] == pytest.approx(1e3 * r["seconds"], rel=1e-9)
+    assert r["forecast_glups"] == pytest.approx(4 * 256 * 256 * 100 / r["seconds"] * 1e-9, rel=1e-9)
+
+
+def test_a_failing_process_makes_the_line_unavailable(tmp_path):
+    r = bench.reference_build_forecast(2, 10, exe=_fake(tmp_path, rc=1))
+    assert "unavailable" in r and "exited 1" in r["unavailable"]
+
+
+def test_a_missing_build_is_reported(tmp_path):
+    r = bench.reference_build_forecast(1, 10, exe=str(tmp_path / "nothing_here"))
+    assert "unavailable" in r
