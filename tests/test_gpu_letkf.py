@@ -45,6 +45,8 @@ CASES = [  # nx, M, p, L, beta
     (64, 64, 4, 1, 1.1),   # 32 < M <= 64: the 64-thread analysis kernel (C2's ensemble size)
     (64, 48, 4, 1, 1.1),
     (64, 40, 2, 0, 1.05),
+    (64, 33, 4, 1, 1.1),   # 31 zero padding columns in the quad-owned Jacobi
+    (96, 64, 4, 1, 1.1),   # 24 x 12 tiles of 4 x 8 points
 ]
 
 
