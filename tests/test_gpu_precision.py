@@ -1,4 +1,4 @@
-"""The precision form: populations stored as FP16 deviations
+"""The precision form (the 512^2 x 64 workload's storage): populations stored as FP16 deviations
 f - w_q with the collide, the forcing and the analysis in FP32.  Its error is
 stated against the FP32 engine, which the other tests pin to the reference."""
 import numpy as np
