@@ -503,10 +503,13 @@ __device__ __forceinline__ float warp_sum(float v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
-// floats per half column in the exchange matrix: 32 rows and 4 of padding.  The eight
-// threads of a quarter warp touch eight half columns with indices in one aligned group
-// of eight at the same chunk; a stride of 36 = 4 (mod 32) puts those in eight different
-// bank groups, and a thread's eight chunks sit at fixed offsets from one base address.
+// floats per half column in the exchange matrix sA: 32 rows and 4 of padding, so that
+// a stride of 36 = 4 (mod 32) spreads a quarter warp's 16-byte accesses over the bank
+// groups.  The (k, h) threads touch eight consecutive half columns at the same chunk
+// (eight groups); in the Jacobi a quad's threads read 16-row quarters of one column
+// (half columns 2c, 2c + 1 at offsets 0 and 16: groups 2c + {0, 4, 1, 5} mod 8) and the
+// two quads of a quarter warp read columns one apart (the other four groups).  A
+// thread's chunks sit at fixed offsets from one base address.
 constexpr int kHS = kHalf + 4;
 // Arrays indexed by member (window rows, dX, the per-column scalars) put the upper half
 // 4 floats further on, so that a column's two threads, which read element m and m + 32
@@ -573,7 +576,7 @@ __global__ void __launch_bounds__(kWideThreads, TC ? 4 : 5) analysis_wide_kernel
     const int nobs_pad = (nobs + 3) & ~3;
     float* sW = smem;                    // [nobs][kHP] window dY (unweighted), member m at hx(m)
     float* sDyo = sW + nobs * kHP;       // [nobs]      window innovations (padded to 4)
-    float* sA = sDyo + nobs_pad;         // [128][kHS]  half columns: Q, the Jacobi exchange, then V
+    float* sA = sDyo + nobs_pad;         // [128][kHS]  half columns: Q, the Jacobi's home slots, then V
     float* sDX = sA + 2 * kWide * kHS;   // [9][kHP]    dX, then D = dX V in place
     float* sS = sDX + kQ * kHP;          // [kHP]       sqrt(M-1)/sqrt(lambda)
     float* sY = sS + kHP;                // [kHP]       Lambda^-1 V^T c
@@ -777,7 +780,7 @@ __global__ void __launch_bounds__(kWideThreads, TC ? 4 : 5) analysis_wide_kernel
                     qv[l + 3] = fmaf(b4.w, vt, fmaf(a4.w, vo, qv[l + 3]));
                 }
             }
-            __syncthreads();  // sA is the Jacobi exchange next
+            __syncthreads();  // sA holds the Jacobi's home slots next
         }
 
         // 5. one-sided Jacobi on the columns of A, lazily scaled (see analysis_kernel), with
