@@ -57,3 +57,19 @@ def test_a_failing_process_makes_the_line_unavailable(tmp_path):
 def test_a_missing_build_is_reported(tmp_path):
     r = bench.reference_build_forecast(1, 10, exe=str(tmp_path / "nothing_here"))
     assert "unavailable" in r
+
+
+def test_analysis_roofline_counts_the_survey_flops():
+    """analysis_roofline: Gram 2 n_obs M^2 + transform 2*9*M^2 + 4 M^3 + Jacobi 18 M M(M-1)/2
+    per sweep, per grid point, over the phase time, against 148 x 128 x 2 x 1.965 GHz."""
+    nx, m = bench.NX, bench.M
+    try:
+        bench.NX, bench.M = 256, 16
+        r = bench.analysis_roofline({"mean_sweeps": 3.0}, 1.0)
+        per_point = 2 * 75 * 256 + 2 * 9 * 256 + 4 * 4096 + 18 * 16 * 16 * 15 / 2 * 3.0
+        assert r["flops_per_point"] == pytest.approx(per_point)
+        assert r["achieved"] == pytest.approx(per_point * 256 * 256 / 1e-3 / 1e12)
+        assert r["peak"] == pytest.approx(148 * 128 * 2 * 1.965e9 / 1e12)
+        assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
+    finally:
+        bench.NX, bench.M = nx, m
