@@ -64,6 +64,12 @@ __host__ __device__ inline float closure_features(float ux, float uy, float vx, 
 }
 
 #ifdef __CUDACC__
+// the hardware's approximate square root (sqrt.approx.f32)
+__device__ __forceinline__ float closure_sqrt(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 // The same features with the hardware log / reciprocal / square root (a few ulp;
 // the features are rounded to FP16 before use): the stream-collide's form.
 __device__ __forceinline__ float closure_features_fast(float ux, float uy, float vx, float vy,
@@ -71,7 +77,7 @@ __device__ __forceinline__ float closure_features_fast(float ux, float uy, float
     const float s11 = ux, s22 = vy, s12 = 0.5f * (uy + vx), w12 = 0.5f * (uy - vx);
     const float ss = fmaf(s11, s11, fmaf(2.f * s12, s12, s22 * s22));
     const float ww = 2.f * w12 * w12;
-    const float smag = __fsqrt_rn(2.f * ss), wmag = __fsqrt_rn(2.f * ww);
+    const float smag = closure_sqrt(2.f * ss), wmag = closure_sqrt(2.f * ww);
     const float k = c.dx * c.dx / c.nu_ref;
     const float y = k * (vx - uy);
     x[0] = __logf(fmaf(k, smag, 1.f));
@@ -79,7 +85,7 @@ __device__ __forceinline__ float closure_features_fast(float ux, float uy, float
     x[2] = __fdividef(ww - ss, ww + ss + 1e-30f);
     x[3] = (s11 + s22) * rsqrtf(ss + 1e-30f);
     x[4] = c.dx / c.dx_ref;
-    x[5] = copysignf(__logf(fabsf(y) + __fsqrt_rn(fmaf(y, y, 1.f))), y);
+    x[5] = copysignf(__logf(fabsf(y) + closure_sqrt(fmaf(y, y, 1.f))), y);
     return smag;
 }
 #endif
