@@ -232,14 +232,20 @@ int lbl_event_elapsed(lbl_ctx* ctx, int slot_a, int slot_b, double* ms);
  * populations f_out and macros mac_out [M][3][ny][nx] (rho, u and, unless
  * compat_stale_v, v), and the observations at the sites yo_sites
  * [3][ny/p][nx/p] (u, v, rho; site (si, sj) is grid point (si*p, sj*p)).  The
- * analysis scratch lives in one static device array of 8 MiB that every GPU
- * loading liblbl holds until exit; configurations needing more are rejected with
- * LBL_ERR_UNSUPPORTED.  All calls share that array: calls that overlap on the GPU
- * race and must be serialised.  The first call on a device looks the array up
- * (cudaGetSymbolAddress) and must come before any stream capture.  stream is a
- * cudaStream_t (NULL = legacy default stream); with host_stats (int[4]: max
- * sweeps, non-converged points, NaN flag, sweep total) the call waits for the
- * stream.  err (optional) receives a message of at most err_cap bytes. */
+ * analysis scratch lives in one static device array of 8 MiB; configurations
+ * needing more are rejected with LBL_ERR_UNSUPPORTED.  CUDA loads that array
+ * lazily: the first call on a device takes the 8 MiB (and the module holding it)
+ * from the device, so make it during set-up, before a memory budget is fixed; the
+ * device then holds it until exit.  The first call on a device also looks the
+ * array up (cudaGetSymbolAddress) and must come before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialised.  Every call only enqueues kernels and a memset on `stream` (a
+ * cudaStream_t, NULL = legacy default stream): the window weight table is rebuilt
+ * on the device and the counters cleared each time, with no host memory involved.
+ * host_stats (int[4]: max sweeps, non-converged points, NaN flag, sweep total) is
+ * optional; given, the call waits for the stream and returns LBL_ERR_NAN on a NaN
+ * in the analysis.  Without it the call does not wait and cannot report a NaN.
+ * err (optional) receives a message of at most err_cap bytes. */
 int lbl_letkf_analysis_noalloc(const lbl_config* cfg, const float* f_in, float* f_out, float* mac_out,
                                const float* yo_sites, void* stream, int* host_stats, char* err, size_t err_cap);
 

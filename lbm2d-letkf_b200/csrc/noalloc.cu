@@ -10,21 +10,26 @@
 // The analysis needs scratch memory beyond its inputs and outputs: the
 // observation-space ensemble at the sites (dY, dyo), the window weight table and
 // four counters.  Here that scratch is one file-scope __device__ array of fixed
-// size, kNoAllocScratchBytes (8 MiB).  Every GPU that loads liblbl holds it until
-// the process exits.  All calls share the array and it keeps the last call's
-// contents; the counters are cleared on every call.  Two calls that overlap on
-// the GPU (different streams, or different host threads) race on it: serialise
-// them.
+// size, kNoAllocScratchBytes (8 MiB).  CUDA loads the module that holds it lazily,
+// so the first call on a device is the one that takes those 8 MiB (plus the
+// module) from the device: make it during the caller's set-up, before a memory
+// budget is fixed.  From then on the device holds the array until the process
+// exits.  All calls share the array and it keeps the last call's contents; every
+// call rebuilds the weight table on the device and clears the counters, so a call
+// reads nothing an earlier call left.  Two calls that overlap on the GPU (different
+// streams, or different host threads) race on it: serialise them.
 //
 // Set-up: the first call on a device, with that device current, looks up the
 // device address of the array (cudaGetSymbolAddress) and opts the analysis kernel
 // in to its shared-memory size.  Make that first call before any stream capture.
+// Every call enqueues only kernels and a memset on the caller's stream; it waits
+// for the stream only when host_stats is given, and only then can it report a NaN
+// in the analysis (LBL_ERR_NAN).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
-#include <vector>
 
 #include "lbl_internal.h"
 
@@ -66,11 +71,60 @@ int scratch_for_current_device(float** out) {
     return LBL_OK;
 }
 
-double gc_weight(double d) {  // Gaspari-Cohn, letkf.cu:104-109
+// Gaspari-Cohn weight (letkf.cu:104-109) as IEEE double operations in the source
+// order of the host table builder (lbl_api.cu), so the device-built table below is
+// bit-identical to the one lbl_create uploads: no contraction into FMAs.
+__device__ double gc_weight_rn(double d) {
     if (d <= 0) return 1.0;
-    if (d <= 1) return -d * d * d * d * d / 4. + d * d * d * d / 2. + d * d * d * 5. / 8. - d * d * 5. / 3. + 1;
-    if (d <= 2) return d * d * d * d * d / 12. - d * d * d * d / 2. + d * d * d * 5. / 8. + d * d * 5. / 3. - d * 5 + 4 - 2. / 3. / d;
+    const double d2 = __dmul_rn(d, d), d3 = __dmul_rn(d2, d), d4 = __dmul_rn(d3, d), d5 = __dmul_rn(d4, d);
+    const double t3 = __ddiv_rn(__dmul_rn(d3, 5.), 8.), t4 = __ddiv_rn(__dmul_rn(d2, 5.), 3.);
+    if (d <= 1) {
+        const double nd5 = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(-d, d), d), d), d);
+        double s = __dadd_rn(__ddiv_rn(nd5, 4.), __ddiv_rn(d4, 2.));
+        s = __dadd_rn(s, t3);
+        s = __dsub_rn(s, t4);
+        return __dadd_rn(s, 1.);
+    }
+    if (d <= 2) {
+        double s = __dsub_rn(__ddiv_rn(d5, 12.), __ddiv_rn(d4, 2.));
+        s = __dadd_rn(s, t3);
+        s = __dadd_rn(s, t4);
+        s = __dsub_rn(s, __dmul_rn(d, 5.));
+        s = __dadd_rn(s, 4.);
+        return __dsub_rn(s, __ddiv_rn(2. / 3., d));
+    }
     return 0.0;
+}
+
+// The window weight table (set_rR, letkf.cu:75-114), built on the device on every
+// call so that no host memory is involved: one thread per pattern (i mod p, j mod p)
+// lists the window slots with weight > 0, {slot, var, sqrt(w) bits, w bits}, then
+// the pattern's count at tab[4 p^2 nobs + pattern].
+__global__ void noalloc_weight_table_kernel(int p, int nox, int nl, int off, double dloc, double sig_u,
+                                            double sig_rho, int nobs, int* tab) {
+    const int pat = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pat >= p * p) return;
+    const int pi = pat % p, pj = pat / p;
+    int n = 0;
+    for (int b = 0; b < nox; b++)
+        for (int a = 0; a < nox; a++) {
+            const int di = pi - (a - (nl - off)) * p, dj = pj - (b - (nl - off)) * p;
+            if (abs(di) > nl * p || abs(dj) > nl * p) continue;
+            const double g =
+                p > 1 ? gc_weight_rn(__ddiv_rn(__dsqrt_rn(double(di * di + dj * dj)), __dadd_rn(dloc, 1e-6))) : 1.0;
+            for (int var = 0; var < 3; var++) {
+                const double sig = var == 2 ? sig_rho : sig_u;
+                const float w = __double2float_rn(__ddiv_rn(g, __dmul_rn(sig, sig)));
+                if (!(w > 0.f)) continue;
+                int* e = tab + (size_t(pat) * nobs + n) * 4;
+                e[0] = a + nox * b + var * nox * nox;
+                e[1] = var;
+                e[2] = __float_as_int(__fsqrt_rn(w));
+                e[3] = __float_as_int(w);
+                n++;
+            }
+        }
+    tab[size_t(4) * p * p * nobs + pat] = n;
 }
 
 }  // namespace
@@ -144,38 +198,14 @@ int analysis_noalloc_impl(const lbl_config* cfg, const float* f_in, float* f_out
     int* tab = reinterpret_cast<int*>(dyo + n_dyo);
     int* stats = reinterpret_cast<int*>(dyo + n_dyo + n_tab);
 
-    // the window weight table (set_rR, letkf.cu:75-114): entries with weight > 0 per
-    // pattern (i mod p, j mod p), {slot, var, 0, weight bits}, then the counts
-    std::vector<int> h(size_t(4) * p * p * nobs + size_t(p) * p, 0);
-    int* cnt = h.data() + size_t(4) * p * p * nobs;
-    for (int pj = 0; pj < p; pj++)
-        for (int pi = 0; pi < p; pi++) {
-            const int pat = pi + p * pj;
-            int n = 0;
-            for (int b = 0; b < nox; b++)
-                for (int a = 0; a < nox; a++) {
-                    const int di = pi - (a - (nl - off)) * p, dj = pj - (b - (nl - off)) * p;
-                    if (std::abs(di) > nl * p || std::abs(dj) > nl * p) continue;
-                    const double g = p > 1 ? gc_weight(std::sqrt(double(di * di + dj * dj)) / (dloc + 1e-6)) : 1.0;
-                    for (int var = 0; var < 3; var++) {
-                        const double sig = var == 2 ? c.obs_error_rho : c.obs_error_u;
-                        const float w = float(g / (sig * sig));
-                        if (!(w > 0.f)) continue;
-                        int* e = h.data() + (size_t(pat) * nobs + n) * 4;
-                        e[0] = a + nox * b + var * nox * nox;
-                        e[1] = var;
-                        e[2] = 0;
-                        std::memcpy(&e[3], &w, sizeof(float));
-                        n++;
-                    }
-                }
-            cnt[pat] = n;
-        }
-
+    // every call: the weight table for this configuration, then cleared counters;
+    // kernels and a memset only, all on `stream`, no host memory involved
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemcpyAsync(tab, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, s);
+    noalloc_weight_table_kernel<<<(p * p + 127) / 128, 128, 0, s>>>(p, nox, nl, off, dloc, c.obs_error_u,
+                                                                     c.obs_error_rho, nobs, tab);
+    cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemsetAsync(stats, 0, sizeof(int) * 4, s);
-    if (e != cudaSuccess) return noalloc_fail(LBL_ERR_CUDA, std::string("scratch upload: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return noalloc_fail(LBL_ERR_CUDA, std::string("scratch set-up: ") + cudaGetErrorString(e));
 
     lbl::AnalysisArgs a{};
     a.f_in = f_in; a.f_out = f_out; a.mac_out = mac_out; a.yo = yo_sites;
