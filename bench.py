@@ -25,15 +25,24 @@ One bench "step" = one DA cycle = the LETKF analysis + 100 LBM steps.
   analysis_roofline  the LETKF analysis phase against the nominal FP32 SIMT peak
             (algorithmic flops of the survey's per-point formulas)
 
+  roofline_hbm, c2_cycles_per_s, c4_cycles_per_s  (default C1 line on one GPU)
+            two side legs timed the same way: C2 (512^2 x 64, 604 MB population
+            buffers, so the stream-collide launches inside its cycles are
+            HBM-bound) and C4 (C1 with the learned closure)
+
 `--impl reference` times the reference's path on the host cores.  The reference
 has no CPU implementation (its only backend is CUDA + MPI + cuBLAS/cuSOLVER), so
-its arm is the FP64 OpenMP restatement of the reference's path in oracle/.  Where
-the reference's own LBM build (oracle/_ref/ref_lbm: its src/lbm.cu and src/data.cu
-compiled unmodified) is present and a GPU is visible, the line also carries
-`reference_build`: that build's forecast run as M processes sharing the GPU, one
-per member as the reference's one-MPI-rank-per-member runs do, and the cycles/s
-bound it implies (forecast only: the reference's LETKF needs MPI and HDF5 and is
-not built, so its real cycle is slower still).
+its arm is the FP64 OpenMP restatement of the reference's path in oracle/,
+configured by the oracle's own restatement of config.h (the product library is
+never loaded in that arm).  One step of that arm is exactly 1/M of a cycle's
+work (one member's 100 LBM steps + the analysis of ny/M rows), so the K steps'
+wall time is what the line reports.  Where the reference's own LBM build
+(oracle/_ref/ref_lbm: its src/lbm.cu and src/data.cu compiled unmodified) is
+present and a GPU is visible, the line also carries `reference_build`: that
+build's forecast run as M processes sharing the GPU, one per member as the
+reference's one-MPI-rank-per-member runs do, and the cycles/s bound it implies
+(`reference_build_bound_cycles_per_s`; forecast only: the reference's LETKF
+needs MPI and HDF5 and is not built, so its real cycle is slower still).
 
 Multi-GPU: replicas only (one independent experiment per GPU, no collective on
 the data path); `value` is the cycles of all ranks / the slowest rank's time.
@@ -79,11 +88,13 @@ STORAGE = 0  # lbl_config.storage of the ensemble (the nature run stays FP32)
 GRAM = 0     # lbl_config.gram of the ensemble: 0 FP32, 1 BF16 tensor cores (32 < M <= 64)
 
 
-def workload_config(lbl, mode="DA_LETKF", n_ens=None):
-    return lbl.config_default(
+def workload_config(lib, mode="DA_LETKF", n_ens=None):
+    """The workload's lbl_config; `lib` is the product package (lbl) or, for the CPU
+    reference arm, the oracle module, which has its own restatement of config.h."""
+    return lib.config_default(
         mode, NX, M if n_ens is None else n_ens, da_xyprune=P_OBS, letkf_rloc_len=1, letkf_covinf=1.1, obs_error_u=0.1,
-        obs_error_rho=0.01, iiter=20, daprune=5, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP, ic_amp=1.0,
-        ens_init=lbl.ENS_PERTURBED, ens_perturb=0.1, storage=STORAGE if mode != "NATURE" else 0,
+        obs_error_rho=0.01, iiter=20, daprune=5, cs=0.1, tau=0.51, ic_kind=lib.IC_K4EXP, ic_amp=1.0,
+        ens_init=lib.ENS_PERTURBED, ens_perturb=0.1, storage=STORAGE if mode != "NATURE" else 0,
         gram=GRAM if mode == "DA_LETKF" else 0)
 
 
@@ -95,12 +106,15 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
+def ncu_traffic(nx=None, m=None, closure=None):
     """DRAM bytes per stream-collide launch from the committed ncu summary, if any."""
     if STORAGE:
         return None
-    name = "lbm_step_kernel_closure" if CLOSURE else "lbm_step_kernel"
-    path = os.path.join(ROOT, "profiles", f"{name}_{NX}x{NX}_M{M}.md")
+    nx = NX if nx is None else nx
+    m = M if m is None else m
+    closure = CLOSURE if closure is None else closure
+    name = "lbm_step_kernel_closure" if closure else "lbm_step_kernel"
+    path = os.path.join(ROOT, "profiles", f"{name}_{nx}x{nx}_M{m}.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -179,12 +193,12 @@ def make_observations(lbl, n_cycles, seed=2024):
     return obs, truth
 
 
-def cpu_baseline_sample(lbl, oracle, obs, threads=None):
+def cpu_baseline_sample(oracle, obs, threads=None):
     """Oracle (FP64, OpenMP, this host's cores) on a bounded sample of one cycle:
     4 LBM steps of the whole 16-member ensemble + the analysis of 16 of the 256 rows,
     scaled to a full cycle (25x the steps, 16x the rows)."""
     nthreads = oracle.set_threads(threads or os.cpu_count())
-    o = with_closure(oracle.Oracle(workload_config(lbl)))
+    o = with_closure(oracle.Oracle(workload_config(oracle)))
     o.init(0)
     rng = np.random.default_rng(5)
     o.step(1, rng.normal(0, 0.84, 4 * 29).astype(np.float32))  # warm caches / page in
@@ -347,18 +361,86 @@ def run_engine(args, dist, rank, world, device):
                      "traffic": traffic, "kernel": "lbm_step_kernel", "ms_per_launch": ms_step,
                      "algorithmic_bytes_per_launch": bytes_per_launch, "peak_kind": peak_kind,
                      "timed": "forecast phase of the timed cycles (in-graph events), 100 launches per cycle",
-                     "ms_per_launch_back_to_back": ms_isolated},
+                     "ms_per_launch_back_to_back": ms_isolated,
+                     "regime": ("L2-resident: the two population buffers (%.1f MB each) fit in the 126 MB L2, so this "
+                                "is an L2-fed figure; roofline_hbm is the HBM-bound one" % (bytes_per_launch / 2e6))
+                     if bytes_per_launch / 2 < 100e6 else "HBM-bound (population buffers larger than L2)"},
         "phases_ms_per_cycle": {"analysis_with_forcing_beside": ms_ana / K, "forecast": ms_fc / K},
         "analysis_roofline": analysis_roofline(stats, ms_ana / K),
         "gpu_launches": K * (T + 3),
         "letkf": stats,
         "clocks": clk.summary(),
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(lbl, oracle, obs[0])
     ens.close()
     e2e_ens.close()
+    if world == 1 and not args.no_side_legs and args.workload == "C1" and not STORAGE and not GRAM:
+        c2 = side_leg(lbl, "C2", device, flush_l2)
+        c4 = side_leg(lbl, "C4", device, flush_l2)
+        line["c2_cycles_per_s"] = c2["cycles_per_s"]
+        line["c4_cycles_per_s"] = c4["cycles_per_s"]
+        line["c4_over_c1"] = c4["cycles_per_s"] / value
+        line["roofline_hbm"] = c2.pop("roofline")
+        line["c2"] = c2
+        line["c4"] = c4
+        line["gpu_launches"] += c2["gpu_launches"] + c4["gpu_launches"]
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(oracle, obs[0])
     return line
+
+
+def side_leg(lbl, name, device, flush_l2, K=10, W=3):
+    """One of the other single-GPU workloads, timed like the headline (CUDA events on
+    the engine's stream around each cycle, L2 flushed between cycles, observations
+    resident): C2 (512^2 x 64, whose 604 MB population buffers make the stream-collide
+    HBM-bound; its in-cycle launches give roofline_hbm) or C4 (C1 with the learned
+    closure).  Returns cycles/s, phases and, for C2, the stream-collide roofline."""
+    global NX, M, CLOSURE, WORKLOAD
+    saved = (NX, M, CLOSURE, WORKLOAD)
+    NX, M, WORKLOAD = WORKLOADS[name]
+    CLOSURE = name == "C4"
+    T = STEPS_PER_CYCLE
+    try:
+        obs, _ = make_observations(lbl, 1)
+        ens = with_closure(lbl.Ensemble(workload_config(lbl), device=device))
+        ens.init(0)
+        ens.cycle_async(0, None, None, None, T)
+        ens.cycle_async(T, *obs[0], T)
+        for c in range(1, W):
+            ens.cycle_async((c + 1) * T, None, None, None, T)
+        ens.sync()
+        ms = ms_ana = ms_fc = 0.0
+        with ClockSampler(device) as clk:
+            for c in range(K):
+                flush_l2()
+                ens.event_record(0)
+                ens.cycle_async((W + c + 1) * T, None, None, None, T)
+                ens.event_record(1)
+                ms += ens.event_elapsed(0, 1)
+                a, f = ens.cycle_phases()
+                ms_ana += a
+                ms_fc += f
+        ens.sync()
+        stats = ens.letkf_stats()
+        out = {"workload": WORKLOAD, "cycles_per_s": K / (ms / 1e3), "ms_per_cycle": ms / K, "cycles": K,
+               "warmup": W, "phases_ms_per_cycle": {"analysis_with_forcing_beside": ms_ana / K,
+                                                    "forecast": ms_fc / K},
+               "glups": M * NX * NX * T * K / (ms / 1e3) / 1e9, "letkf": stats, "clocks": clk.summary(),
+               "gpu_launches": K * (T + 3)}
+        if name == "C2":
+            ms_step = ms_fc / (K * T)
+            bpl = 72.0 * M * NX * NX
+            achieved = bpl / (ms_step * 1e-3) / 1e9
+            peak, peak_kind = measured_peak()
+            out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                               "frac": achieved / peak, "traffic": ncu_traffic(NX, M, False),
+                               "kernel": "lbm_step_kernel", "grid": f"{NX}x{NX}", "members": M,
+                               "ms_per_launch": ms_step, "algorithmic_bytes_per_launch": bpl, "peak_kind": peak_kind,
+                               "timed": "forecast phase of the C2 cycles (in-graph events), 100 launches per cycle",
+                               "regime": "HBM-bound: two 604 MB population buffers, far larger than the 126 MB L2"}
+        ens.close()
+        return out
+    finally:
+        NX, M, CLOSURE, WORKLOAD = saved
 
 
 def reference_build_forecast(n_proc, nsteps, warmup=50, exe=None):
@@ -453,43 +535,68 @@ def analysis_roofline(stats, ms_phase):
 
 
 def run_reference(args, rank, world):
-    """The reference's path on the host cores: FP64 OpenMP restatement (oracle/)."""
-    import lbl
+    """The reference's path on the host cores: the FP64 OpenMP restatement (oracle/),
+    configured by the oracle's own copy of config.h (no product library is loaded).
+
+    One step is exactly 1/M of a DA cycle's work: 100 LBM steps of one member (each
+    member's forecast costs the same) plus the LETKF analysis of ny/M of the grid rows
+    of the whole M-member ensemble, the row slice moving on each step, so that M steps
+    make one whole cycle.  value = (K/M) cycles over the K timed steps' wall time."""
     import oracle
     if rank != 0:
         return None
+    T = STEPS_PER_CYCLE
     nthreads = oracle.set_threads(os.cpu_count())
-    o = with_closure(oracle.Oracle(workload_config(lbl)))
-    o.init(0)
+    fc = with_closure(oracle.Oracle(workload_config(oracle, n_ens=1)))   # one member's forecast
+    fc.init(0)
+    da = with_closure(oracle.Oracle(workload_config(oracle)))            # the ensemble the analysis reads
+    da.init(0)
     rng = np.random.default_rng(9)
     obs_nan = np.full((NX, NX), np.nan, np.float32)
     ro, uo, vo = obs_nan.copy(), obs_nan.copy(), obs_nan.copy()
     ro[::P_OBS, ::P_OBS] = 1.0 + 0.01 * rng.standard_normal((NX // P_OBS, NX // P_OBS))
     uo[::P_OBS, ::P_OBS] = rng.standard_normal((NX // P_OBS, NX // P_OBS))
     vo[::P_OBS, ::P_OBS] = rng.standard_normal((NX // P_OBS, NX // P_OBS))
+    rows = NX // M
+    n_modes = 29  # forcing modes at kf = 4
 
-    def one():
+    def one(k):
+        j0 = (k % M) * rows
         t0 = time.perf_counter()
-        o.step(2, rng.normal(0, 0.84, 4 * 29 * 2).astype(np.float32))
-        t1 = time.perf_counter()
-        o.assimilate_rows(ro, uo, vo, 0, 8)
-        t2 = time.perf_counter()
-        return 50 * (t1 - t0) + 32 * (t2 - t1)  # scaled to 100 steps + 256 rows
+        fc.step(T, rng.normal(0, 0.84, 4 * n_modes * T).astype(np.float32))
+        da.assimilate_rows(ro, uo, vo, j0, j0 + rows)
+        return time.perf_counter() - t0
 
-    for _ in range(args.warmup):
-        one()
-    est = [one() for _ in range(args.steps)]
-    value = len(est) / sum(est)
-    o.close()
-    sample = "2 LBM steps of 16x256^2 + LETKF of 8/256 rows per step, scaled x50 / x32 to one cycle"
-    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "backend": "FP64 OpenMP CPU restatement of the reference path"},
+    for k in range(args.warmup):
+        one(k)
+    sec = [one(args.warmup + k) for k in range(args.steps)]
+    total = sum(sec)
+    value = (args.steps / M) / total
+    fc.close()
+    da.close()
+    sample = (f"one step = 1/{M} of a cycle: {T} LBM steps of 1 of the {M} members + the LETKF analysis of "
+              f"{rows} of the {NX} rows (moving slice; {M} steps = one whole cycle)")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "backend": "FP64 OpenMP CPU restatement of the reference path "
+                                                        "(the reference has no CPU implementation)",
+                       "step": sample},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "reference_build": reference_build_line(args) if NX == 256 and not CLOSURE else
-            {"unavailable": "the reference build runs its compiled 256x256 plain-Smagorinsky default only"}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if NX == 256 and not CLOSURE:
+        rb = reference_build_line(args)
+        line["reference_build"] = rb
+        if "cycles_per_s_upper_bound" in rb:
+            line["reference_build_bound_cycles_per_s"] = rb["cycles_per_s_upper_bound"]
+            line["reference_build_bound_kind"] = (
+                "forecast-only upper bound on the reference build's DA cycles/s on this GPU: its own LBM "
+                "(src/lbm.cu + src/data.cu, unmodified) for the 16 members x 100 steps; its analysis would only "
+                "add time. Engine cycles/s divided by this number is a lower bound on the speed-up")
+    else:
+        line["reference_build"] = {"unavailable": "the reference build runs its compiled 256x256 "
+                                                  "plain-Smagorinsky default only"}
+    return line
 
 
 def profile_cycles(args):
@@ -634,10 +741,11 @@ def run_batch(args):
 
 
 def closure_params():
-    """(params, nu_ref, dx_ref) of the trained closure shipped with the package."""
-    from lbl import closure
-    w, meta = closure.load_params()
-    return w, meta["nu_ref"], meta["dx_ref"]
+    """(params, nu_ref, dx_ref) of the trained closure shipped with the package, read
+    with numpy (the CPU reference arm must not import the product)."""
+    with np.load(os.path.join(ROOT, "lbm2d-letkf_b200", "lbl", "closure_c4.npz")) as z:
+        meta = json.loads(str(z["meta"]))
+        return z["params"].astype(np.float32), meta["nu_ref"], meta["dx_ref"]
 
 
 def with_closure(obj):
@@ -682,6 +790,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-side-legs", action="store_true",
+                    help="skip the C2 (HBM roofline) and C4 (learned closure) legs of the default C1 line")
     ap.add_argument("--profile", action="store_true",
                     help="run warmup + steps cycles of the workload and exit (for ncu captures)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["C3"], default="C1",

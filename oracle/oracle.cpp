@@ -268,6 +268,50 @@ void ic_member_uv(const lbl_config& cfg, int seed, std::vector<float>& u, std::v
 
 extern "C" {
 
+// The reference's defaults for a run mode at grid nx = 64*SCALER (src/config.h with
+// LES and FORCE_TURB on), so that code timing the oracle needs nothing from the
+// product library.  OBS_ERROR_* have no default in the reference (config.h:195
+// #error); they take run/jserr:146-147's values.
+int orc_config_default(lbl_config* c, int mode, int nx, int n_ens) {
+    if (!c) return LBL_ERR_ARG;
+    std::memset(c, 0, sizeof(*c));
+    const int scaler = nx / 64;
+    c->abi_version = LBL_ABI_VERSION;
+    c->mode = mode;
+    c->nx = nx; c->ny = nx;                               // config.h:88-89, 133-134
+    c->n_ens = n_ens;                                     // mpiexec -np M
+    c->iiter = 5 * (scaler > 0 ? scaler : 1);             // config.h:136
+    c->ioprune = 10;                                      // config.h:90-92
+    c->daprune = 10;                                      // config.h:55-57
+    c->da_xyprune = 1;                                    // config.h:59-61
+    c->iter_main = c->iiter * 2000;                       // config.h:144
+    c->spinup = 100000 * c->iiter;                        // config.h:139
+    c->ic_kind = LBL_IC_REFERENCE;                        // data.cu:53-120
+    c->ens_init = LBL_ENS_INDEPENDENT;                    // data.cu:31-35
+    c->compat_stale_v = 1;                                // letkf.cu:340-355
+    c->jacobi_max_sweeps = 100;                           // cu_matrix_eigensolver_wrapper.hpp:193
+    c->letkf_covinf = 1.0;                                // config.h:48-50
+    c->obs_error_rho = 0.01;                              // run/jserr:146-147
+    c->obs_error_u = 0.1;
+    c->cs = 0.2;                                          // lbm.cu:59
+    c->nu = 1e-4;                                         // config.h:157
+    c->cfl = 0.05;                                        // config.h:153
+    c->rho_ref = 1;                                       // config.h:156
+    c->u_ref = 1;                                         // config.h:182
+    c->h_ref = 2 * M_PI;                                  // config.h:158
+    c->kf = 4;                                            // config.h:161
+    c->fkf = 5.6;                                         // config.h:171
+    c->friction_rate = 5e-4;                              // config.h:180
+    c->ic_amp = 0.01;                                     // data.cu:53
+    c->ens_perturb = 0.1;
+    c->jacobi_tol = 1e-6;                                 // cu_matrix_eigensolver_wrapper.hpp:192
+    c->force_seed = 1991;                                 // data.cu:294
+    c->obs_seed = 334;                                    // io.cu:321
+    c->da_obs_ruv = 1;                                    // config.h:44
+    c->da_nud_rate = 0.1;                                 // config.h:67-69
+    return LBL_OK;
+}
+
 int orc_set_threads(int n) {
 #ifdef _OPENMP
     if (n > 0) omp_set_num_threads(n);

@@ -19,6 +19,54 @@ Q = 9
 
 _lib = None
 
+MODES = {"NATURE": 0, "OBSERVE": 1, "DA_LETKF": 2, "DA_NUDGING": 3}
+IC_K4EXP = 1
+ENS_PERTURBED = 1
+
+
+class Config(ctypes.Structure):
+    """lbl_config of include/lbl.h (the C struct the oracle reads), so that callers of the
+    oracle need nothing from the product package."""
+
+    _fields_ = [
+        ("abi_version", ctypes.c_int32), ("mode", ctypes.c_int32), ("nx", ctypes.c_int32),
+        ("ny", ctypes.c_int32), ("n_ens", ctypes.c_int32), ("iiter", ctypes.c_int32),
+        ("ioprune", ctypes.c_int32), ("daprune", ctypes.c_int32), ("da_xyprune", ctypes.c_int32),
+        ("letkf_rloc_len", ctypes.c_int32), ("iter_main", ctypes.c_int32), ("spinup", ctypes.c_int32),
+        ("ic_kind", ctypes.c_int32), ("ens_init", ctypes.c_int32), ("compat_stale_v", ctypes.c_int32),
+        ("jacobi_max_sweeps", ctypes.c_int32), ("write_mat", ctypes.c_int32), ("lbm_variant", ctypes.c_int32),
+        ("letkf_covinf", ctypes.c_double), ("obs_error_rho", ctypes.c_double), ("obs_error_u", ctypes.c_double),
+        ("cs", ctypes.c_double), ("nu", ctypes.c_double), ("tau", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("rho_ref", ctypes.c_double), ("u_ref", ctypes.c_double), ("h_ref", ctypes.c_double),
+        ("kf", ctypes.c_double), ("fkf", ctypes.c_double), ("friction_rate", ctypes.c_double),
+        ("ic_amp", ctypes.c_double), ("ens_perturb", ctypes.c_double), ("jacobi_tol", ctypes.c_double),
+        ("force_seed", ctypes.c_uint64), ("obs_seed", ctypes.c_uint64),
+        ("da_dummy", ctypes.c_int32), ("da_quadra", ctypes.c_int32), ("da_obs_ruv", ctypes.c_int32),
+        ("gram", ctypes.c_int32), ("da_nud_rate", ctypes.c_double),
+        ("storage", ctypes.c_int32), ("reserved1", ctypes.c_int32),
+    ]
+
+    def copy(self) -> "Config":
+        c = Config()
+        ctypes.pointer(c)[0] = self
+        return c
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def config_default(mode="NATURE", nx: int = 256, n_ens: int = 1, **overrides) -> Config:
+    """The reference's config.h defaults (orc_config_default) with lbl_config overrides."""
+    c = Config()
+    m = MODES[mode] if isinstance(mode, str) else int(mode)
+    if load().orc_config_default(ctypes.byref(c), m, nx, n_ens) != 0:
+        raise ValueError("orc_config_default")
+    for k, v in overrides.items():
+        if not hasattr(c, k):
+            raise KeyError(f"unknown config field {k}")
+        setattr(c, k, v)
+    return c
+
 
 def load():
     global _lib
@@ -33,6 +81,7 @@ def load():
     IP = ctypes.POINTER(ctypes.c_int)
     sig = {
         "orc_set_threads": (I, [I]),
+        "orc_config_default": (I, [P, I, I, I]),
         "orc_create": (P, [P]),
         "orc_destroy": (None, [P]),
         "orc_ic_fields": (I, [P, I, F, F, F, F]),

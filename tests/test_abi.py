@@ -71,3 +71,17 @@ def test_config_overrides_and_unknown_key():
 
 def test_version_string():
     assert "sm_100a" in lbl.version()
+
+
+def test_oracle_config_mirror_matches_the_product():
+    """The oracle's own lbl_config mirror and config.h defaults (used by the CPU
+    reference arm, which must not load liblbl) equal the product's field for field."""
+    import oracle
+    assert [f for f, _ in oracle.Config._fields_] == [f for f, _ in lbl.Config._fields_]
+    assert ctypes.sizeof(oracle.Config) == ctypes.sizeof(lbl.Config)
+    for f, _ in lbl.Config._fields_:
+        assert getattr(oracle.Config, f).offset == getattr(lbl.Config, f).offset, f
+    for mode, nx, m in (("NATURE", 256, 1), ("OBSERVE", 128, 1), ("DA_LETKF", 512, 64), ("DA_NUDGING", 64, 4)):
+        a = oracle.config_default(mode, nx, m, cs=0.1, tau=0.51).as_dict()
+        b = lbl.config_default(mode, nx, m, cs=0.1, tau=0.51).as_dict()
+        assert a == b, (mode, nx, m)
