@@ -132,6 +132,20 @@ __device__ __forceinline__ float group_sum(float v) {
 // (i mod p, j mod p).
 // ---------------------------------------------------------------------------
 constexpr int kCW = 4, kCH = 2;  // chain tile (points in x, points in y)
+
+// The Jacobi ends after a sweep whose largest rotated relative off-diagonal stayed below
+// sqrt(tol), counting on quadratic convergence to bring the sweep's rotations down to tol.
+// That holds while every late rotation is small.  A pair of (nearly) equal column norms
+// turns by up to 45 degrees even for a tiny off-diagonal (the products of other pairs'
+// residues suffice once they pass tol), which remixes residues the sweep had already
+// removed and makes convergence linear: with p = 1 (three observations, a 13-fold
+// eigenvalue (M-1)/beta at M = 16) the increments then kept errors of about sqrt(tol)
+// (8e-4 of the largest increment against the reference's solver).  A sweep with a turn
+// wider than atan(kWideTurn) therefore never ends the iteration.  Measured against the
+// FP64 oracle at 256^2 x 16 (C1's observation settings): 4.3e-4 of the largest increment
+// without the rule, 5.2e-5 at 0.3, 1.0e-5 at 0.1 (3.0 -> 3.5 mean sweeps); at 512^2 x 64,
+// 6.2e-4, 7.6e-5 and 2.8e-5 (2.4 -> 4.6 mean sweeps).
+constexpr float kWideTurn = 0.1f;
 // the wide analysis walks taller tiles: fewer cold starts, and its many waves hide
 // the longer CTAs (512^2, M = 64: 58.7 ms at 4 x 8, 59.3 at 4 x 4, 62.8 at 4 x 2;
 // C1's kernel is fastest at 4 x 2)
@@ -342,6 +356,9 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
                     // one reciprocal on the critical path instead of two
                     const float d = ahi - alo, e = 2.f * g;
                     const float t = __fdividef(copysignf(fabsf(e), d * e), fabsf(d) + sqrt_approx(fmaf(d, d, e * e)));
+                    // a wide turn of a (nearly) degenerate pair remixes what the sweep's other
+                    // rotations removed, so this sweep cannot rely on quadratic convergence
+                    if (fabsf(t) > kWideTurn) worst = fmaxf(worst, stop2);
                     const float cs = rsqrtf(fmaf(t, t, 1.f));
                     // low: cs a - sn b; high: sn a + cs b (sn = cs t), with the scales
                     const float rho = (low ? -t : t) * __fdividef(sp, sc);
@@ -848,10 +865,11 @@ __global__ void __launch_bounds__(kWideThreads, TC ? 4 : 5) analysis_wide_kernel
                         // |g| > tol sqrt(alo ahi), on squares
                         const float p2 = alo * ahi, g2 = g * g;
                         if (g2 > tol2 * p2) {
-                            big |= g2 >= stop2 * p2;
                             // tt = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = d / e, times |e|
                             const float d = ahi - alo, e = 2.f * g;
                             const float tt = __fdividef(copysignf(fabsf(e), d * e), fabsf(d) + sqrt_approx(fmaf(d, d, e * e)));
+                            // a wide turn of a (nearly) degenerate pair also rules out the quadratic stop
+                            big |= g2 >= stop2 * p2 || fabsf(tt) > kWideTurn;
                             const float cs = rsqrtf(fmaf(tt, tt, 1.f));
                             // low column: cs (lo - tt hi); high column: cs (hi + tt lo), with the scales
                             const float slo = alow ? sa : sb, shi = alow ? sb : sa;
