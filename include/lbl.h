@@ -249,6 +249,18 @@ int lbl_event_elapsed(lbl_ctx* ctx, int slot_a, int slot_b, double* ms);
 int lbl_letkf_analysis_noalloc(const lbl_config* cfg, const float* f_in, float* f_out, float* mac_out,
                                const float* yo_sites, void* stream, int* host_stats, char* err, size_t err_cap);
 
+/* Fault injection for tests of the failure paths.  No counterpart in the reference,
+ * whose failures abort the MPI job (main.cu:152-155).  what = LBL_INJECT_TMA_STALL:
+ * from the next stream-collide on, the TMA-fed kernel's producer issues no bulk copy and
+ * every bounded wait polls at most `value` (1 .. 2^20) times, so the consumers' waits run
+ * out with nothing in flight, no population is written and the call (or the next
+ * lbl_sync) returns LBL_ERR_TIMEOUT; the context stays usable (re-run lbl_init).
+ * what = LBL_INJECT_NONE clears it.  Waits for the context's work and drops its captured
+ * graphs.  Nothing here faults or hangs a GPU. */
+#define LBL_INJECT_NONE      0
+#define LBL_INJECT_TMA_STALL 1
+int lbl_inject(lbl_ctx* ctx, int what, int value);
+
 /* Tile autotuning for this context's grid and ensemble size: times the fused
  * stream-collide on the rest state for candidate strip heights (rows per CTA) and
  * keeps the fastest for every later step.  Call between lbl_create and lbl_init (it

@@ -23,11 +23,17 @@ namespace {
 
 int wait_output(lbl_ctx* ctx);
 
+// a failed allocation is LBL_ERR_NOMEM; it is not sticky, so the runtime's last-error
+// slot is cleared for the calls that follow
 #define LBL_CK(call)                                                                            \
     do {                                                                                        \
         cudaError_t e_ = (call);                                                                \
         if (e_ != cudaSuccess) {                                                                \
             ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                      \
+            if (e_ == cudaErrorMemoryAllocation) {                                              \
+                cudaGetLastError();                                                             \
+                return LBL_ERR_NOMEM;                                                           \
+            }                                                                                   \
             return LBL_ERR_CUDA;                                                                \
         }                                                                                       \
     } while (0)
@@ -983,6 +989,21 @@ int lbl_sync(lbl_ctx* ctx) {
     LBL_TRY(wait_output(ctx));
     LBL_TRY(check_timeout(ctx));
     if (ctx->cfg.mode == LBL_MODE_DA_LETKF) LBL_TRY(read_stats(ctx));
+    return LBL_OK;
+}
+
+int lbl_inject(lbl_ctx* ctx, int what, int value) {
+    if (!ctx) return LBL_ERR_ARG;
+    if (what != LBL_INJECT_NONE && what != LBL_INJECT_TMA_STALL) return fail(ctx, LBL_ERR_ARG, "unknown injection");
+    if (what == LBL_INJECT_TMA_STALL && (value < 1 || value > (1 << 20)))
+        return fail(ctx, LBL_ERR_ARG, "LBL_INJECT_TMA_STALL takes a poll limit in [1, 2^20]");
+    LBL_TRY(set_device(ctx));
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    LBL_CK(cudaStreamSynchronize(ctx->side));
+    // the stream-collide's parameters are baked into the captured graphs
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
+    ctx->graphs.clear();
+    ctx->inject_tma_stall = what == LBL_INJECT_TMA_STALL ? value : 0;
     return LBL_OK;
 }
 

@@ -133,6 +133,7 @@ struct lbl_ctx {
     int ty_tuned = 0;                    // stream-collide strip height chosen by lbl_autotune (0: heuristic)
     int ty_default = 0;                  // the heuristic's strip height for the kernel that runs
     int* d_err = nullptr;                // bounded-wait timeout flag of the TMA kernel
+    int inject_tma_stall = 0;            // lbl_inject: > 0 = TMA producer issues nothing, waits poll this often
 
     // asynchronous output (lbl_output_async): vorticity and ensemble statistics on the
     // device, one pinned staging copy, and a writer thread for the files

@@ -754,8 +754,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 // bounded wait; false (and *err set) when the limit is reached
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
-    for (long long it = 0; it < kWaitLimit; it++)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code, long long limit) {
+    for (long long it = 0; it < limit; it++)
         if (mbar_try_wait(bar, parity)) return true;
     atomicCAS(err, 0, code);
     return false;
@@ -776,7 +776,7 @@ __global__ void __launch_bounds__(1024) lbm_step_tma_kernel(const __grid_constan
                                                             float* __restrict__ fout,
                                                             const float* __restrict__ force,
                                                             float* __restrict__ mac, Phys P, int TY, int box,
-                                                            int* __restrict__ err) {
+                                                            int* __restrict__ err, int stall) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int nx = NX ? NX : P.nx, ny = NX ? NX : P.ny, nxy = NX ? NX * NX : P.nxy;
     const int ncons = nx;  // consumer threads, one column each
@@ -800,14 +800,18 @@ __global__ void __launch_bounds__(1024) lbm_step_tma_kernel(const __grid_constan
     }
     __syncthreads();
 
+    // stall > 0 (fault injection, lbl_inject): the producer issues no copy and every wait
+    // polls at most `stall` times, so the consumers' first waits give up with nothing in flight
+    const long long limit = stall > 0 ? stall : kWaitLimit;
     if (warp == nwarps_c) {  // ---------------- producer warp ----------------
         if ((threadIdx.x & 31) == 0) {
             bool ok = true;
             int issued = 0;
             const uint32_t bytes = uint32_t(kQ) * nx * sizeof(float);
-            for (int i = 0; i < nrows && ok; i++) {
+            const int rows = stall > 0 ? 0 : nrows;
+            for (int i = 0; i < rows && ok; i++) {
                 const int s = i % kStages;
-                if (i >= kStages) ok = mbar_wait(&empty[s], ((i / kStages) - 1) & 1, err, 1);
+                if (i >= kStages) ok = mbar_wait(&empty[s], ((i / kStages) - 1) & 1, err, 1, limit);
                 if (!ok) break;
                 issued = i + 1;
                 mbar_expect_tx(&full[s], bytes);
@@ -822,7 +826,8 @@ __global__ void __launch_bounds__(1024) lbm_step_tma_kernel(const __grid_constan
                 }
             }
             // drain: never leave the CTA with a bulk copy still writing shared memory
-            for (int i = max(0, issued - kStages); i < issued; i++) mbar_wait(&full[i % kStages], (i / kStages) & 1, err, 2);
+            for (int i = max(0, issued - kStages); i < issued; i++)
+                mbar_wait(&full[i % kStages], (i / kStages) & 1, err, 2, limit);
         }
         return;
     }
@@ -837,7 +842,7 @@ __global__ void __launch_bounds__(1024) lbm_step_tma_kernel(const __grid_constan
     bool good = true;
     auto take = [&](int i, float (&fc)[kQ]) {  // pulled populations of ring row i
         const int s = i % kStages;
-        if (good) good = mbar_wait(&full[s], (i / kStages) & 1, err, 3);
+        if (good) good = mbar_wait(&full[s], (i / kStages) & 1, err, 3, limit);
         const float* st = ring + size_t(s) * kQ * nx;
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
@@ -1051,9 +1056,11 @@ void launch_tma(const lbl_ctx* c, dim3 grid, int ty, int b, float* fout, const f
     const size_t sm = lbm_tma_smem(P.nx);
     const int box = P.nx < 256 ? P.nx : 256;
     if (mac_out)
-        lbm_step_tma_kernel<true, NX><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, mac_out, P, ty, box, c->d_err);
+        lbm_step_tma_kernel<true, NX><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, mac_out, P, ty, box, c->d_err,
+                                                                   c->inject_tma_stall);
     else
-        lbm_step_tma_kernel<false, NX><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, nullptr, P, ty, box, c->d_err);
+        lbm_step_tma_kernel<false, NX><<<grid, P.nx + 32, sm, s>>>(c->tmap[b], fout, force, nullptr, P, ty, box, c->d_err,
+                                                                    c->inject_tma_stall);
 }
 
 // a stream-collide launch, with programmatic stream serialization when the previous

@@ -19,7 +19,7 @@ import letkf_ref_cases as lc
 
 pytestmark = pytest.mark.gpu
 
-REF_TOL = 1e-3       # increments, as a fraction of the largest increment
+REF_TOL = 1e-4       # increments, as a fraction of the largest increment (measured 7e-6..3e-5)
 CHECKSUM_TOL = 1e-3  # whole-field increment checksums, relative
 
 

@@ -18,7 +18,7 @@ from conftest import golden
 import letkf_ref_cases as lc
 import oracle
 
-REF_TOL = 1e-3        # increments: FP32 cuBLAS/cuSOLVER (tol 1e-6) against FP64
+REF_TOL = 1e-4        # increments: FP32 cuBLAS/cuSOLVER (tol 1e-6) against FP64 (measured 3e-6..2.5e-5)
 LAMBDA_TOL = 1e-4     # eigenvalues of Q, relative
 CHECKSUM_TOL = 1e-3   # sum, sum of squares and weighted sum of the whole increment field, relative
 
