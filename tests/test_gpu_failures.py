@@ -73,7 +73,8 @@ def test_allocation_failure_returns_nomem_without_leak():
         lbl.Ensemble(cfg)
     assert ei.value.code == ERR_NOMEM, ei.value
     torch.cuda.synchronize()
-    assert torch.cuda.mem_get_info(0)[0] == free0, "allocations of the failed context were not returned"
+    # (a context released just before may return a few MiB late, so free memory may grow)
+    assert torch.cuda.mem_get_info(0)[0] >= free0, "allocations of the failed context were not returned"
     # the failure is not sticky: a normal context works afterwards
     e = lbl.Ensemble(lbl.config_default("NATURE", 64, 2))
     e.init(0)
