@@ -3,7 +3,9 @@ src/lbm.cu + src/data.cu compiled unmodified) run for 10,000 steps of the NATURE
 at its defaults (256x256, ensemble id 0), condensed into the statistics that a
 chaotic run can be compared on:
 
-  ref_longrun_id0.npz
+  ref_longrun_id0.npz      the reference's defaults (Cs 0.2, nu 1e-4)
+  ref_longrun_c0_id0.npz   --ref oracle/_ref/ref_lbm_c0 --name ref_longrun_c0_id0.npz: the same
+                           build with Cs 0.1 and tau 0.51 (oracle/make_ref_c0.sh)
     steps        the sampled steps (every 500 from 2000 to 10000)
     spectra      [len(steps)][129] energy spectrum E(k) of (u, v) at each sample, the
                  shell sum of postprocess/fourier.ipynb cell 2 (numpy FFT here)
@@ -55,6 +57,7 @@ def main():
     root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     ap.add_argument("--ref", default=os.path.join(root, "oracle", "_ref", "ref_lbm"))
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
+    ap.add_argument("--name", default="ref_longrun_id0.npz")
     a = ap.parse_args()
     if not os.path.exists(a.ref):
         sys.exit(f"missing {a.ref}: build it with `make -C oracle ref` where the reference is mounted")
@@ -69,7 +72,7 @@ def main():
             spectra.append(e)
             energy.append(en)
             enstrophy.append(z)
-    path = os.path.join(a.out, "ref_longrun_id0.npz")
+    path = os.path.join(a.out, a.name)
     np.savez_compressed(path, steps=np.array(STEPS), spectra=np.array(spectra), energy=np.array(energy),
                         enstrophy=np.array(enstrophy))
     print("wrote", path, os.path.getsize(path), "bytes")
