@@ -801,8 +801,9 @@ def main():
                     help="population storage: f32, or the precision form's f16 deviations f - w_q")
     ap.add_argument("--c3", choices=["batch", "contexts"], default="batch",
                     help="C3 as one batch with a batched persistent stream-collide, or as concurrent contexts")
-    ap.add_argument("--gram", choices=["f32", "bf16"], default="f32",
-                    help="the analysis Gram: FP32, or the precision form's BF16 tensor cores (M > 32, i.e. C2)")
+    ap.add_argument("--gram", choices=["f32", "bf16", "tf32x3"], default="f32",
+                    help="the analysis Gram: FP32 SIMT, the precision form's BF16 mma.sync (M > 32, i.e. C2), or "
+                         "the tcgen05 tensor-core block Gram with FP32 accuracy (3 x TF32)")
     ap.add_argument("--lbm", default=None, metavar="NXxM[,NXxM...]",
                     help="time the stream-collide alone at these grids and exit")
     ap.add_argument("--closure", action="store_true",
@@ -814,9 +815,11 @@ def main():
     NX, M, WORKLOAD = WORKLOADS.get(args.workload, WORKLOADS["C1"])
     CLOSURE = args.workload == "C4"
     STORAGE = 1 if args.storage == "f16" else 0
-    GRAM = 1 if args.gram == "bf16" else 0
-    if GRAM:
+    GRAM = {"f32": 0, "bf16": 1, "tf32x3": 2}[args.gram]
+    if GRAM == 1:
         WORKLOAD += "; Gram on BF16 tensor cores with FP32 sums"
+    elif GRAM == 2:
+        WORKLOAD += "; Gram on the tcgen05 tensor cores (TF32 split in two terms, FP32 sums)"
     if STORAGE:
         WORKLOAD = WORKLOAD.replace("FP32 storage", "FP16 deviation storage").replace(", FP32", ", FP16 deviation storage")
     if args.lbm:

@@ -59,6 +59,9 @@ extern "C" {
 /* population storage (lbl_config.storage) */
 #define LBL_GRAM_F32  0  /* Gram dY^T R^-1 dY in FP32 (the reference's arithmetic)                       */
 #define LBL_GRAM_BF16 1  /* precision form: BF16 operands on the tensor cores, FP32 sums; 32 < M <= 64   */
+#define LBL_GRAM_TF32X3 2 /* the Gram of every p x p block on the tcgen05 tensor cores, FP32-accurate:      */
+                          /* operands split into two TF32 terms, three MMAs, FP32 sums; M <= 64 and p*p a   */
+                          /* multiple of 128/MP (MP = 16, 32, 64 members padded), e.g. p = 4             */
 #define LBL_STORAGE_F32 0    /* FP32 populations (the reference's `real`)                   */
 #define LBL_STORAGE_F16 1    /* FP16 deviations f - w_q from the lattice weights, FP32 collide */
 

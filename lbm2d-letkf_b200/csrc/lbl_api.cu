@@ -146,7 +146,17 @@ int validate(const lbl_config& c, std::string& err) {
         err = "DA_NUD_RATE must lie in [0, 1]"; return LBL_ERR_ARG;
     }
     if (c.reserved1 != 0) { err = "reserved fields must be 0"; return LBL_ERR_ARG; }
-    if (c.gram != LBL_GRAM_F32 && c.gram != LBL_GRAM_BF16) { err = "unknown gram"; return LBL_ERR_ARG; }
+    if (c.gram != LBL_GRAM_F32 && c.gram != LBL_GRAM_BF16 && c.gram != LBL_GRAM_TF32X3) {
+        err = "unknown gram"; return LBL_ERR_ARG;
+    }
+    if (c.gram == LBL_GRAM_TF32X3) {
+        const Geo g = derive_geo(c);
+        if (c.mode != LBL_MODE_DA_LETKF || !gram_tc_supported(c.n_ens, g.p, g.nobs)) {
+            err = "the tensor-core Gram (LBL_GRAM_TF32X3) needs DA_LETKF, n_ens <= 64 and DA_XYPRUNE^2 a multiple of "
+                  "128/MP points (MP = n_ens padded to 16, 32 or 64), e.g. DA_XYPRUNE = 4";
+            return LBL_ERR_UNSUPPORTED;
+        }
+    }
     if (c.gram == LBL_GRAM_BF16 && (c.mode != LBL_MODE_DA_LETKF || c.n_ens <= 32 || c.write_mat)) {
         err = "the BF16 tensor-core Gram serves the wide analysis (DA_LETKF, 32 < n_ens <= 64, no matrix dumps)";
         return LBL_ERR_UNSUPPORTED;
@@ -342,8 +352,9 @@ int check_timeout(lbl_ctx* ctx) {
     LBL_CK(cudaMemcpy(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (h) {
         cudaMemset(ctx->d_err, 0, sizeof(int));
-        return fail(ctx, LBL_ERR_TIMEOUT, "stream-collide: a bounded shared-memory pipeline wait gave up (code " +
-                                              std::to_string(h) + ")");
+        return fail(ctx, LBL_ERR_TIMEOUT, std::string(h == 4 ? "tensor-core Gram: the MMA completion wait"
+                                                               : "stream-collide: a bounded shared-memory pipeline wait") +
+                                              " gave up (code " + std::to_string(h) + ")");
     }
     return LBL_OK;
 }
@@ -456,6 +467,20 @@ int build_weight_table(lbl_ctx* ctx) {
         }
     LBL_CK(cudaMalloc(&ctx->d_wtab, sizeof(int) * tab.size()));
     LBL_CK(cudaMemcpy(ctx->d_wtab, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice));
+    if (cfg.gram == LBL_GRAM_TF32X3) {  // the same weights, dense per pattern, for the tensor-core Gram
+        const int kpad = (G.nobs + 7) & ~7;
+        std::vector<float> dense(size_t(np) * kpad, 0.f);
+        for (int pat = 0; pat < np; pat++)
+            for (int n = 0; n < cnt[pat]; n++) {
+                const int* e = tab.data() + (size_t(pat) * G.nobs + n) * 4;
+                std::memcpy(&dense[size_t(pat) * kpad + e[0]], &e[3], sizeof(float));
+            }
+        LBL_CK(cudaMalloc(&ctx->d_wdense, sizeof(float) * dense.size()));
+        LBL_CK(cudaMemcpy(ctx->d_wdense, dense.data(), sizeof(float) * dense.size(), cudaMemcpyHostToDevice));
+        const int mpq = gram_tc_mp(ctx->P.M);
+        LBL_CK(cudaMalloc(&ctx->d_Q, sizeof(float) * size_t(ctx->P.nxy) * (size_t(mpq) * mpq + mpq)));
+        if (gram_tc_prepare() != 0) return fail(ctx, LBL_ERR_CUDA, "cudaFuncSetAttribute(gram_tc_kernel) failed");
+    }
     return LBL_OK;
 }
 
@@ -605,6 +630,7 @@ void destroy_impl(lbl_ctx* ctx) {
     }
     cudaFree(ctx->d_modes); cudaFree(ctx->d_amps); cudaFree(ctx->d_pool); cudaFree(ctx->d_force); cudaFree(ctx->d_sched);
     cudaFree(ctx->d_wtab); cudaFree(ctx->d_yo); cudaFree(ctx->d_dY); cudaFree(ctx->d_dyo);
+    cudaFree(ctx->d_wdense); cudaFree(ctx->d_Q);
     cudaFree(ctx->d_stats); cudaFree(ctx->d_red); cudaFree(ctx->d_tmp); cudaFree(ctx->d_err); cudaFree(ctx->d_dump);
     cudaFree(ctx->d_closure);
     for (int b = 0; b < 2; b++) {

@@ -107,6 +107,9 @@ struct lbl_ctx {
 
     // LETKF
     int* d_wtab = nullptr;               // int4 [p*p][nobs] window entries + int [p*p] counts
+    float* d_wdense = nullptr;           // LBL_GRAM_TF32X3: [p*p][kpad] slot weights per pattern
+    float* d_Q = nullptr;                // LBL_GRAM_TF32X3: Q - (M-1)/beta I per point, [nxy][mpq][mpq],
+                                         // then c = dY^T R^-1 dyo per point, [nxy][mpq]
     float* d_yo = nullptr;               // [3][nsites] observations at sites (u, v, rho)
     bool have_obs = false;               // d_yo holds observations given by the caller
     float* h_yo[2] = {nullptr, nullptr}; // pinned staging of the above, alternating
@@ -242,6 +245,21 @@ struct AnalysisArgs {
     int max_sweeps, write_v;
 };
 void launch_obs_ensemble_args(const AnalysisArgs& a, cudaStream_t s);
+// ---- the Gram on the tcgen05 tensor cores (gram_tc.cu) ----
+struct GramTcParams {
+    int nx, ny, M, p, nsx, nsy, nsites, nox, nl_off, nobs, kpad;
+};
+// M <= 64, p^2 a multiple of the points per 128-row tile, operands within shared memory
+bool gram_tc_supported(int M, int p, int nobs);
+size_t gram_tc_smem(int M, int p, int nobs);
+int gram_tc_prepare();
+// member padding of the Gram output Qout[point][mpq][mpq]: 16, 32 or 64
+inline int gram_tc_mp(int M) { return M <= 16 ? 16 : (M <= 32 ? 32 : 64); }
+// Qout = Q - (M-1)/beta I and Cout = dY^T R^-1 dyo for every grid point; wdense [p*p][kpad] =
+// the slot weights of each pattern (i mod p, j mod p), zero for absent slots and the padding
+void launch_gram_tc(const GramTcParams& G, const float* dY, const float* dyo, const float* wdense, float* Qout,
+                    float* Cout, int* err, cudaStream_t s);
+
 void launch_analysis_args(const AnalysisArgs& a, cudaStream_t s);
 
 // ---- kernels (diag_kernels.cu) ----

@@ -43,6 +43,9 @@ struct AnaParams {
     float stop;             // sqrt(tol): a sweep whose worst relative off-diagonal is below it ends the
                             // iteration, since the sweep's own rotations leave about stop^2 = tol
     int max_sweeps;
+    const float* qin;       // Q - (M-1)/beta I per point from the tensor-core Gram, or null
+    const float* cin;       // with it, c = dY^T R^-1 dyo per point (cin + n mpq, member k)
+    int mpq;                // its member padding: Q of point n at qin + n mpq^2, row k, column l
     float c;                // lattice speed for the macros
     int write_v;            // 0 reproduces the reference's stale v after analysis
     int tile_y0;            // first tile row (0 for the whole grid)
@@ -228,7 +231,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         // 2. observation window of the point's p x p block (pack_yk/set_yo geometry,
         //    letkf.cu:148-269), gathered once per block from the site ensemble
         const int bi = i / A.p, bj = j / A.p;
-        if (bi != cached_bi || bj != cached_bj) {
+        if ((DUMP || !A.qin) && (bi != cached_bi || bj != cached_bj)) {  // the tensor-core Gram needs no window
             for (int b = 0; b < A.nox; b++) {
                 int sj = (bj + b - A.nl_off) % A.nsy;
                 sj += sj < 0 ? A.nsy : 0;
@@ -263,7 +266,19 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
 #pragma unroll
         for (int l = 0; l < MP; l++) qv[l] = 0.f;
         float ck = 0.f;
-        for (int o = 0; o < cnt; o++) {
+        if (!DUMP && A.qin) {  // Q and c from the tensor-core Gram (gram_tc.cu)
+            ck = real_m ? __ldg(A.cin + size_t(point) * A.mpq + k) : 0.f;
+            const float* qrow = A.qin + (size_t(point) * A.mpq + k) * A.mpq;
+#pragma unroll
+            for (int l = 0; l < MP; l += 4) {
+                const float4 q4 = real_m ? __ldg(reinterpret_cast<const float4*>(qrow + l)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                qv[l] = q4.x;
+                qv[l + 1] = q4.y;
+                qv[l + 2] = q4.z;
+                qv[l + 3] = q4.w;
+            }
+        }
+        for (int o = 0; (DUMP || !A.qin) && o < cnt; o++) {
             const int4 e = ent[o];
             const float* row = sW + e.x * MP;
             const float ek = __int_as_float(e.w) * row[k];
@@ -651,7 +666,7 @@ __global__ void __launch_bounds__(kWideThreads, TC ? 4 : 5) analysis_wide_kernel
 
         // 2. observation window of the point's p x p block, once per block
         const int bi = i / A.p, bj = j / A.p;
-        if (bi != cached_bi || bj != cached_bj) {
+        if ((TC || !A.qin) && (bi != cached_bi || bj != cached_bj)) {  // the tensor-core Gram needs no window
             for (int b = 0; b < A.nox; b++) {
                 int sj = (bj + b - A.nl_off) % A.nsy;
                 sj += sj < 0 ? A.nsy : 0;
@@ -743,7 +758,19 @@ __global__ void __launch_bounds__(kWideThreads, TC ? 4 : 5) analysis_wide_kernel
             }
             __syncthreads();  // the warm start below rewrites sA
         }
-        for (int o = 0; !TC && o < cnt; o++) {
+        if (!TC && A.qin) {  // Q and c from the tensor-core Gram (gram_tc.cu)
+            ck = real_k ? __ldg(A.cin + size_t(point) * A.mpq + k) : 0.f;
+            const float* qrow = A.qin + (size_t(point) * A.mpq + k) * A.mpq + r0;
+#pragma unroll
+            for (int l = 0; l < kHalf; l += 4) {
+                const float4 q4 = real_k ? __ldg(reinterpret_cast<const float4*>(qrow + l)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                qv[l] = q4.x;
+                qv[l + 1] = q4.y;
+                qv[l + 2] = q4.z;
+                qv[l + 3] = q4.w;
+            }
+        }
+        for (int o = 0; !TC && !A.qin && o < cnt; o++) {
             const int4 e = ent[o];
             const float* row = sW + e.x * kHP;
             const float ek = __int_as_float(e.w) * row[hx(k)];
@@ -1045,6 +1072,9 @@ AnaParams make_params(const lbl_ctx* c) {
     A.tol = float(c->cfg.jacobi_tol);
     A.stop = float(std::sqrt(c->cfg.jacobi_tol));
     A.max_sweeps = c->cfg.jacobi_max_sweeps;
+    A.qin = c->cfg.gram == LBL_GRAM_TF32X3 ? c->d_Q : nullptr;
+    A.mpq = gram_tc_mp(c->P.M);
+    A.cin = A.qin ? A.qin + size_t(c->P.nxy) * A.mpq * A.mpq : nullptr;
     A.c = c->P.c;
     A.write_v = c->cfg.compat_stale_v ? 0 : 1;
     A.tile_y0 = 0;
@@ -1168,6 +1198,14 @@ void launch_analysis_wide(const lbl_ctx* c, const float* fin, float* fout, float
 }
 
 void launch_analysis(const lbl_ctx* c, const float* fin, float* fout, float* mac, cudaStream_t s) {
+    if (c->cfg.gram == LBL_GRAM_TF32X3) {  // every point's Q on the tensor cores first
+        GramTcParams G{};
+        G.nx = c->P.nx; G.ny = c->P.ny; G.M = c->P.M; G.p = c->G.p;
+        G.nsx = c->G.nsx; G.nsy = c->G.nsy; G.nsites = c->G.nsx * c->G.nsy;
+        G.nox = c->G.nox; G.nl_off = c->G.nl - c->G.off; G.nobs = c->G.nobs; G.kpad = (c->G.nobs + 7) & ~7;
+        const int mpq = gram_tc_mp(c->P.M);
+        launch_gram_tc(G, c->d_dY, c->d_dyo, c->d_wdense, c->d_Q, c->d_Q + size_t(c->P.nxy) * mpq * mpq, c->d_err, s);
+    }
     if (c->P.M > 32) {
         launch_analysis_wide(c, fin, fout, mac, s);
         return;
@@ -1194,6 +1232,9 @@ AnaParams params_from_args(const AnalysisArgs& a) {
     A.tol = a.tol;
     A.stop = std::sqrt(a.tol);
     A.max_sweeps = a.max_sweeps;
+    A.qin = nullptr;
+    A.cin = nullptr;
+    A.mpq = 16;
     A.c = a.c;
     A.write_v = a.write_v;
     A.tile_y0 = 0;

@@ -39,7 +39,7 @@ ERRORS = {
 }
 LBM_AUTO, LBM_DIRECT, LBM_TMA = 0, 1, 2
 STORAGE_F32, STORAGE_F16 = 0, 1
-GRAM_F32, GRAM_BF16 = 0, 1
+GRAM_F32, GRAM_BF16, GRAM_TF32X3 = 0, 1, 2
 
 # names of the exported C functions (must match include/lbl.h)
 EXPORTS = (

@@ -150,6 +150,44 @@ def test_bf16_gram_precision_form(M, p, L):
     assert np.max(np.abs(inc_e - inc_32)) > 0
 
 
+@pytest.mark.parametrize("nx,M,p,L", [(64, 16, 4, 1), (64, 6, 4, 1), (64, 32, 4, 1), (64, 64, 4, 1), (64, 40, 4, 1),
+                                      (64, 12, 4, 0), (128, 16, 4, 1), (96, 64, 4, 1)])
+def test_tensor_core_gram_matches_oracle(nx, M, p, L):
+    """The Gram on the tcgen05 tensor cores (LBL_GRAM_TF32X3: every operand split into two
+    TF32 terms, three MMAs, FP32 sums) against the FP64 oracle, with the FP32 analysis's
+    bound, and against the SIMT FP32 Gram of the same forecast."""
+    cfg, e, obs, _, _ = make_case(nx, M, p, L, 1.1, gram=lbl.GRAM_TF32X3)
+    F = [e.get_f(m) for m in range(M)]
+    o = oracle.Oracle(cfg)
+    for m in range(M):
+        o.set_f(m, F[m])
+    e.assimilate(cfg.iiter, *obs)
+    o.assimilate(*obs)
+    st = e.letkf_stats()
+    assert st["nan"] == 0 and st["n_noconv"] == 0, st
+    inc_e = np.stack([e.get_f(m).astype(np.float64) - F[m] for m in range(M)])
+    inc_o = np.stack([o.get_f(m) - F[m] for m in range(M)])
+    scale = np.max(np.abs(inc_o))
+    err = np.max(np.abs(inc_e - inc_o)) / scale
+    cfg32, e32, _, _, _ = make_case(nx, M, p, L, 1.1)
+    e32.assimilate(cfg32.iiter, *obs)
+    inc_32 = np.stack([e32.get_f(m).astype(np.float64) - F[m] for m in range(M)])
+    err32 = np.max(np.abs(inc_e - inc_32)) / scale
+    print(f"tcgen05 Gram nx={nx} M={M} p={p} L={L}: increment error {err:.2e} of the largest (vs SIMT Gram {err32:.2e})")
+    assert scale > 1e-6 and err < 1e-3
+
+
+def test_tensor_core_gram_limits():
+    # p^2 not a multiple of the points per tile; not a DA run; a 243-slot window (LETKF_RLOC_LEN = 2)
+    # whose operands do not fit in shared memory
+    for kw in (dict(mode="DA_LETKF", M=16, p=2, L=0), dict(mode="DA_LETKF", M=16, p=1, L=0),
+               dict(mode="NATURE", M=16, p=4, L=1), dict(mode="DA_LETKF", M=16, p=4, L=2)):
+        with pytest.raises(lbl.LblError) as ei:
+            lbl.Ensemble(lbl.config_default(kw["mode"], 64, kw["M"], da_xyprune=kw["p"], letkf_rloc_len=kw["L"],
+                                            gram=lbl.GRAM_TF32X3))
+        assert ei.value.code == -8
+
+
 def test_bf16_gram_limits():
     for kw in (dict(mode="DA_LETKF", M=16), dict(mode="NATURE", M=64)):
         with pytest.raises(lbl.LblError) as ei:

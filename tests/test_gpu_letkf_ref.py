@@ -23,13 +23,15 @@ REF_TOL = 1e-4       # increments, as a fraction of the largest increment (measu
 CHECKSUM_TOL = 1e-3  # whole-field increment checksums, relative
 
 
-@pytest.mark.parametrize("case", list(lc.CASES))
-def test_engine_matches_reference_solver(case):
+@pytest.mark.parametrize("case,gram", [(c, 0) for c in lc.CASES] +
+                         [(c, 2) for c in lc.CASES if lc.CASES[c]["p"] == 4])
+def test_engine_matches_reference_solver(case, gram):
     z = golden(f"ref_letkf_{case}.npz")
     meta = json.loads(str(z["meta"]))
     f, obs = lc.inputs(case)
     assert lc.digest(f, obs) == meta["digest"]
     cfg = lc.config(lbl, case)
+    cfg.gram = gram  # 0: the SIMT FP32 Gram; 2: the tcgen05 tensor-core Gram (LBL_GRAM_TF32X3)
     e = lbl.Ensemble(cfg)
     e.init(0)
     for m in range(cfg.n_ens):
