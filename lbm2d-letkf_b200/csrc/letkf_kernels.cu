@@ -143,11 +143,14 @@ constexpr int kCW = 4, kCH = 2;  // chain tile (points in x, points in y)
 // residues suffice once they pass tol), which remixes residues the sweep had already
 // removed and makes convergence linear: with p = 1 (three observations, a 13-fold
 // eigenvalue (M-1)/beta at M = 16) the increments then kept errors of about sqrt(tol)
-// (8e-4 of the largest increment against the reference's solver).  A sweep with a turn
-// wider than atan(kWideTurn) therefore never ends the iteration.  Measured against the
-// FP64 oracle at 256^2 x 16 (C1's observation settings): 4.3e-4 of the largest increment
-// without the rule, 5.2e-5 at 0.3, 1.0e-5 at 0.1 (3.0 -> 3.5 mean sweeps); at 512^2 x 64,
-// 6.2e-4, 7.6e-5 and 2.8e-5 (2.4 -> 4.6 mean sweeps).
+// (8e-4 of the largest increment against the reference's solver).  So a sweep that meets
+// the quadratic stop but turned some pair wider than atan(kWideTurn) is followed by one
+// cleanup sweep in which such turns are skipped: the nearly degenerate pairs are already
+// orthogonal to about tol, and mixing eigenvectors of (nearly) equal eigenvalues leaves the
+// transform as it is, while the other pairs then converge quadratically.  Measured against the
+// FP64 oracle at C1's observation settings: 4.3e-4 of the largest increment without the
+// cleanup at 256^2 x 16, 9.8e-6 with it (3.0 -> 3.4 mean sweeps); at 512^2 x 64, 6.2e-4 and
+// 2.8e-5 (2.4 -> 3.3 mean sweeps).
 constexpr float kWideTurn = 0.1f;
 // the wide analysis walks taller tiles: fewer cold starts, and its many waves hide
 // the longer CTAs (512^2, M = 64: 58.7 ms at 4 x 8, 59.3 at 4 x 4, 62.8 at 4 x 2;
@@ -336,6 +339,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
         //    into qv at the start of every sweep.
         int sweeps = 0;
         bool converged = false;
+        bool cleanup = false;  // this sweep turns no nearly degenerate pair (see kWideTurn)
         const float tol2 = A.tol * A.tol, stop2 = A.stop * A.stop;  // the tests below compare squares
         float sc = 1.f;
         for (int sw = 0; sw < A.max_sweeps; sw++) {
@@ -346,7 +350,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
 #pragma unroll
             for (int l = 0; l < MP; l += 2) { a0 = fmaf(qv[l], qv[l], a0); a1 = fmaf(qv[l + 1], qv[l + 1], a1); }
             float a = a0 + a1;
-            bool rot = false;
+            bool rot = false, wide = false;
             float worst = 0.f;  // largest g^2 / (a b) of the sweep
 #pragma unroll 1
             for (int rr = 1; rr < MP; rr++) {
@@ -363,31 +367,43 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
                 const float alo = low ? a : b, ahi = low ? b : a;
                 // |g| > tol sqrt(alo ahi), on squares
                 const float p2 = alo * ahi, g2 = g * g;
-                const bool doit = g2 > tol2 * p2;
-                if (doit) {
+                bool apply = false;
+                if (g2 > tol2 * p2) {
                     // any exact rotation converges; cs^2 + sn^2 = 1 keeps the columns' span
-                    worst = fmaxf(worst, __fdividef(g2, p2));
                     // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = d / e, multiplied through by |e|:
                     // one reciprocal on the critical path instead of two
                     const float d = ahi - alo, e = 2.f * g;
                     const float t = __fdividef(copysignf(fabsf(e), d * e), fabsf(d) + sqrt_approx(fmaf(d, d, e * e)));
-                    // a wide turn of a (nearly) degenerate pair remixes what the sweep's other
-                    // rotations removed, so this sweep cannot rely on quadratic convergence
-                    if (fabsf(t) > kWideTurn) worst = fmaxf(worst, stop2);
-                    const float cs = rsqrtf(fmaf(t, t, 1.f));
-                    // low: cs a - sn b; high: sn a + cs b (sn = cs t), with the scales
-                    const float rho = (low ? -t : t) * __fdividef(sp, sc);
+                    const bool wt = fabsf(t) > kWideTurn;  // both lanes of the pair agree
+                    apply = !(cleanup && wt);
+                    if (apply) {
+                        worst = fmaxf(worst, __fdividef(g2, p2));
+                        wide |= wt;
+                        const float cs = rsqrtf(fmaf(t, t, 1.f));
+                        // low: cs a - sn b; high: sn a + cs b (sn = cs t), with the scales
+                        const float rho = (low ? -t : t) * __fdividef(sp, sc);
 #pragma unroll
-                    for (int l = 0; l < MP; l++) qv[l] = fmaf(rho, pq[l], qv[l]);
-                    sc *= cs;
-                    a = low ? a - t * g : a + t * g;
+                        for (int l = 0; l < MP; l++) qv[l] = fmaf(rho, pq[l], qv[l]);
+                        sc *= cs;
+                        a = low ? a - t * g : a + t * g;
+                    }
                 }
-                rot |= doit;
+                rot |= apply;
             }
             // group max of the sweep's relative off-diagonal
 #pragma unroll
             for (int o = MP / 2; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
-            const bool done = !rot || worst < stop2;
+            // the quadratic stop; after a sweep with a wide turn, one cleanup sweep first
+            const bool quad = (__ballot_sync(0xffffffffu, rot) & gmask) == 0u || worst < stop2;
+            const bool any_wide = (__ballot_sync(0xffffffffu, wide) & gmask) != 0u;
+            bool done;
+            if (cleanup) {
+                done = quad;
+                cleanup = false;
+            } else {
+                done = quad && !any_wide;
+                cleanup = quad && any_wide;
+            }
             const unsigned ballot = __ballot_sync(0xffffffffu, !done && active);
             if (!converged) {
                 sweeps = sw + 1;
@@ -853,8 +869,10 @@ __global__ void __launch_bounds__(kWideThreads, TC ? 4 : 5) analysis_wide_kernel
             const int hoff = (r >> 1) * kHS + 16 * (r & 1);  // rows [16 r, 16 r + 16) of a home slot
             float xa[16], xb[16];
             float sa = 1.f, sb = 1.f, na = 0.f, nb = 0.f;
+            bool cleanup = false;  // this sweep turns no nearly degenerate pair (see kWideTurn)
             for (int sw = 0; sw < A.max_sweeps; sw++) {
-                bool big = false;  // some rotated pair's relative off-diagonal reached sqrt(tol)
+                bool big = false;   // some rotated pair's relative off-diagonal reached sqrt(tol)
+                bool wide = false;  // some rotation turned wider than atan(kWideTurn)
                 for (int L = 0; L < 6; L++) {
                     const int H = 32 >> L;
                     const int b = s >> (5 - L), i = s & (H - 1);
@@ -891,12 +909,18 @@ __global__ void __launch_bounds__(kWideThreads, TC ? 4 : 5) analysis_wide_kernel
                         const float alo = alow ? na : nb, ahi = alow ? nb : na;
                         // |g| > tol sqrt(alo ahi), on squares
                         const float p2 = alo * ahi, g2 = g * g;
-                        if (g2 > tol2 * p2) {
+                        float tt = 0.f;
+                        bool turn = g2 > tol2 * p2;
+                        if (turn) {
                             // tt = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = d / e, times |e|
                             const float d = ahi - alo, e = 2.f * g;
-                            const float tt = __fdividef(copysignf(fabsf(e), d * e), fabsf(d) + sqrt_approx(fmaf(d, d, e * e)));
-                            // a wide turn of a (nearly) degenerate pair also rules out the quadratic stop
-                            big |= g2 >= stop2 * p2 || fabsf(tt) > kWideTurn;
+                            tt = __fdividef(copysignf(fabsf(e), d * e), fabsf(d) + sqrt_approx(fmaf(d, d, e * e)));
+                            const bool wt = fabsf(tt) > kWideTurn;  // the quad agrees
+                            turn = !(cleanup && wt);
+                            wide |= turn && wt;
+                        }
+                        if (turn) {
+                            big |= g2 >= stop2 * p2;
                             const float cs = rsqrtf(fmaf(tt, tt, 1.f));
                             // low column: cs (lo - tt hi); high column: cs (hi + tt lo), with the scales
                             const float slo = alow ? sa : sb, shi = alow ? sb : sa;
@@ -948,9 +972,21 @@ __global__ void __launch_bounds__(kWideThreads, TC ? 4 : 5) analysis_wide_kernel
                     __syncthreads();
                 }
                 sweeps = sw + 1;
-                if (!__syncthreads_or(big ? 1 : 0)) {
-                    converged = true;
-                    break;
+                // the quadratic stop; after a sweep with a wide turn, one cleanup sweep first
+                const bool any_big = __syncthreads_or(big ? 1 : 0) != 0;
+                const bool any_wide = __syncthreads_or(wide ? 1 : 0) != 0;
+                if (cleanup) {
+                    cleanup = false;
+                    if (!any_big) {
+                        converged = true;
+                        break;
+                    }
+                } else if (!any_big) {
+                    if (!any_wide) {
+                        converged = true;
+                        break;
+                    }
+                    cleanup = true;
                 }
             }
         }
