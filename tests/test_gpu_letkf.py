@@ -82,8 +82,10 @@ def test_analysis_matches_oracle(nx, M, p, L, beta):
 WORKLOAD_TOL = 1e-4
 
 
-@pytest.mark.parametrize("nx,M,rows", [(256, 16, (0, 16)), (512, 64, (0, 8))])
+@pytest.mark.parametrize("nx,M,rows", [(256, 16, (0, 16)), (512, 64, (0, 8)), (1024, 64, (1020, 1024))])
 def test_workload_analysis_matches_oracle(nx, M, rows):
+    """(1024^2 x 64 is the largest DA configuration: its last rows, whose windows wrap
+    around the periodic edge.)"""
     cfg = lbl.config_default("DA_LETKF", nx, M, da_xyprune=4, letkf_rloc_len=1, letkf_covinf=1.1, obs_error_u=0.1,
                              obs_error_rho=0.01, daprune=1, iiter=20, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP,
                              ic_amp=1.0, ens_init=lbl.ENS_PERTURBED, ens_perturb=0.1)
