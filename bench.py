@@ -81,6 +81,7 @@ WORKLOADS = {
                     "trained on 4096 8x-box-filtered 2048^2 snapshots; nature run plain Smagorinsky"),
 }
 CLOSURE = False  # the ensemble (and the CPU baselines) use the trained closure (workload C4)
+CLOSURE_REFRESH = 10  # the closure's network runs every this many steps (lbl_set_closure_refresh)
 WORKLOAD = WORKLOADS["C1"][2]
 
 
@@ -750,9 +751,11 @@ def closure_params():
 
 def with_closure(obj):
     """Switch an engine ensemble or an oracle to the trained closure when the workload
-    asks for it."""
+    asks for it (the engine with its refresh interval; the oracle evaluates every step)."""
     if CLOSURE:
         obj.set_closure(*closure_params())
+        if CLOSURE_REFRESH > 1 and hasattr(obj, "set_closure_refresh"):
+            obj.set_closure_refresh(CLOSURE_REFRESH)
     return obj
 
 
@@ -808,12 +811,18 @@ def main():
                     help="time the stream-collide alone at these grids and exit")
     ap.add_argument("--closure", action="store_true",
                     help="with --lbm: the learned-closure stream-collide (trained parameters of the package)")
+    ap.add_argument("--closure-refresh", type=int, default=10,
+                    help="C4: run the closure's network every this many steps, holding each cell's multiplier between "
+                         "(1: every step)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global NX, M, WORKLOAD, STORAGE, CLOSURE, GRAM
+    global NX, M, WORKLOAD, STORAGE, CLOSURE, GRAM, CLOSURE_REFRESH
     NX, M, WORKLOAD = WORKLOADS.get(args.workload, WORKLOADS["C1"])
     CLOSURE = args.workload == "C4"
+    CLOSURE_REFRESH = args.closure_refresh
+    if CLOSURE and CLOSURE_REFRESH > 1:
+        WORKLOAD += f"; the network runs every {CLOSURE_REFRESH} steps, each cell's multiplier held between"
     STORAGE = 1 if args.storage == "f16" else 0
     GRAM = {"f32": 0, "bf16": 1, "tf32x3": 2}[args.gram]
     if GRAM == 1:

@@ -303,6 +303,13 @@ int lbl_h5_write_dataset(const char* path, uint64_t d0, uint64_t d1, uint64_t d2
  * lbl_autotune chose and returns to the heuristic's for the kernel now in use. */
 int lbl_set_closure(lbl_ctx* ctx, const float* params, double nu_ref, double dx_ref);
 
+/* Evaluate the closure's network every `steps` stream-collide steps (1, the default:
+ * every step).  The network runs on steps 0, steps, 2 steps, ... of every forecast
+ * chunk and stores each cell's multiplier m; the steps between keep m and apply it to
+ * the current |S| (nu_t = m (cs dx)^2 |S|), at the cost of the plain stream-collide.
+ * Needs nx <= 1024 for steps > 1.  No counterpart in the reference. */
+int lbl_set_closure_refresh(lbl_ctx* ctx, int steps);
+
 /* Training data from the code's own runs: a run of the fine configuration (mode set
  * to NATURE; every member a seeded random-phase IC) is spun up for `spinup` steps,
  * then every `spacing` steps, n_snapshots times, each member's (u, v, uu, uv, vv) is

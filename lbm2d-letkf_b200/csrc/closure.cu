@@ -474,6 +474,37 @@ int lbl_set_closure(lbl_ctx* ctx, const float* params, double nu_ref, double dx_
     return LBL_OK;
 }
 
+int lbl_set_closure_refresh(lbl_ctx* ctx, int steps) {
+    if (!ctx) return LBL_ERR_ARG;
+    if (steps < 1 || steps > 1000) {
+        ctx->err = "the closure refresh interval must lie in [1, 1000] steps";
+        return LBL_ERR_ARG;
+    }
+    if (steps > 1 && ctx->P.nx > 1024) {
+        ctx->err = "holding the closure multiplier between evaluations needs nx <= 1024";
+        return LBL_ERR_UNSUPPORTED;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return LBL_ERR_CUDA;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess || cudaStreamSynchronize(ctx->side) != cudaSuccess)
+        return LBL_ERR_CUDA;
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);  // captured with the old schedule
+    ctx->graphs.clear();
+    if (steps > 1 && !ctx->d_mclos) {
+        const cudaError_t e = cudaMalloc(&ctx->d_mclos, sizeof(float) * size_t(ctx->P.M) * ctx->P.nxy);
+        if (e != cudaSuccess) {
+            ctx->err = std::string("cudaMalloc(closure multipliers): ") + cudaGetErrorString(e);
+            cudaGetLastError();
+            return e == cudaErrorMemoryAllocation ? LBL_ERR_NOMEM : LBL_ERR_CUDA;
+        }
+    }
+    if (steps == 1 && ctx->d_mclos) {
+        cudaFree(ctx->d_mclos);
+        ctx->d_mclos = nullptr;
+    }
+    ctx->closure_every = steps;
+    return LBL_OK;
+}
+
 int lbl_closure_infer(const float* params, const float* features, size_t n, int path, int device, float* out) {
     if (!params || !features || !out || n == 0 || (path != 0 && path != 1)) return LBL_ERR_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return LBL_ERR_CUDA;

@@ -270,7 +270,7 @@ void enqueue_steps(lbl_ctx* ctx, int n, int cur, cudaStream_t s, bool force_done
         const int src = (cur + k) & 1, dst = src ^ 1;
         const bool mac = k >= n - 2;
         launch_lbm_step(ctx, src, dst, ctx->d_force + size_t(k) * 2 * ctx->P.nxy,
-                        mac ? ctx->mac[dst] : nullptr, s, /*pdl=*/k > 0);
+                        mac ? ctx->mac[dst] : nullptr, s, /*pdl=*/k > 0, k);
     }
 }
 
@@ -633,6 +633,7 @@ void destroy_impl(lbl_ctx* ctx) {
     cudaFree(ctx->d_wdense); cudaFree(ctx->d_Q);
     cudaFree(ctx->d_stats); cudaFree(ctx->d_red); cudaFree(ctx->d_tmp); cudaFree(ctx->d_err); cudaFree(ctx->d_dump);
     cudaFree(ctx->d_closure);
+    cudaFree(ctx->d_mclos);
     for (int b = 0; b < 2; b++) {
         if (ctx->h_yo[b]) cudaFreeHost(ctx->h_yo[b]);
         if (ctx->h_sched[b]) cudaFreeHost(ctx->h_sched[b]);

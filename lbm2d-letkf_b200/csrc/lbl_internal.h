@@ -149,6 +149,8 @@ struct lbl_ctx {
 
     // learned closure (closure.h): fragment-ordered BF16 parameters, feature scales
     uint32_t* d_closure = nullptr;       // [kPackWords]
+    int closure_every = 1;               // lbl_set_closure_refresh: the network runs every this many steps
+    float* d_mclos = nullptr;            // [M][ny][nx] the cells' multipliers between evaluations (closure_every > 1)
     bool closure = false;
     lbl::ClosureScales closure_sc{};
 
@@ -172,8 +174,9 @@ void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s)
 // one step from population buffer src to dst (FP32 or FP16 storage)
 // pdl: the previous launch on s is the previous step; the launch may then overlap its
 // tail (programmatic dependent launch; the kernel waits for that grid's completion)
+// step: the step's index in its forecast chunk (it picks the closure's evaluate-or-hold variant)
 void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s,
-                     bool pdl = false);
+                     bool pdl = false, int step = 0);
 // strip height of the stream-collide for this grid, ensemble and kernel variant
 // (occupancy heuristic); call outside stream capture
 int lbm_strip_rows(const lbl_ctx* c);

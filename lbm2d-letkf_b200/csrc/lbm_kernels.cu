@@ -202,12 +202,26 @@ __device__ __forceinline__ float les_omega(float ue, float uw, float ve, float v
 // scales the Smagorinsky eddy viscosity: nu_t = m cs^2 dx^2 |S|.
 __device__ __forceinline__ float closure_omega(float ue, float uw, float ve, float vw, float un, float us, float vn,
                                                float vs, const Phys& P, const ClosureScales& csc,
-                                               const uint32_t* pack, uint32_t* stage) {
+                                               const uint32_t* pack, uint32_t* stage, float& m) {
     const float ux = (ue - uw) * P.inv_two_dx, uy = (un - us) * P.inv_two_dx;
     const float vx = (ve - vw) * P.inv_two_dx, vy = (vn - vs) * P.inv_two_dx;
     float feat[kMlpIn];
     const float smag = closure_features_fast(ux, uy, vx, vy, csc, feat);
-    const float m = mlp_forward_warp(pack, stage, feat);
+    m = mlp_forward_warp(pack, stage, feat);
+    const float nus = m * float(P.les_k * double(smag));
+    const float tau = float(fma(double(P.nu + nus), P.tau_k, 0.5));
+    return __frcp_rn(tau);
+}
+// The closure between two evaluations of the network (lbl_set_closure_refresh): the
+// cell's multiplier m from the last evaluation, |S| of this step, the same |S| and
+// relaxation arithmetic as closure_omega.
+__device__ __forceinline__ float closure_omega_held(float ue, float uw, float ve, float vw, float un, float us,
+                                                    float vn, float vs, const Phys& P, float m) {
+    const float ux = (ue - uw) * P.inv_two_dx, uy = (un - us) * P.inv_two_dx;
+    const float vx = (ve - vw) * P.inv_two_dx, vy = (vn - vs) * P.inv_two_dx;
+    const float s11 = ux, s22 = vy, s12 = 0.5f * (uy + vx);
+    const float ss = fmaf(s11, s11, fmaf(2.f * s12, s12, s22 * s22));
+    const float smag = closure_sqrt(2.f * ss);
     const float nus = m * float(P.les_k * double(smag));
     const float tau = float(fma(double(P.nu + nus), P.tau_k, 0.5));
     return __frcp_rn(tau);
@@ -462,10 +476,14 @@ __global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __res
 // ---------------------------------------------------------------------------
 // (256 threads: the plain kernel is held to 4 CTAs per SM, 64 registers, the closure variant
 // to 2, 128 registers)
-template <bool WRITE_MAC, int MAXT, int NX, typename T, bool CL = false, bool CLU = false>
+// CL: the learned closure evaluates its network in every cell (and stores the cell's
+// multiplier in mclos when given); CLH: the closure between evaluations, with the
+// multipliers held in mclos.
+template <bool WRITE_MAC, int MAXT, int NX, typename T, bool CL = false, bool CLU = false, bool CLH = false>
 __global__ void __launch_bounds__(MAXT, MAXT == 256 ? (CL ? 2 : 4) : 1)
     lbm_step_kernel(const T* __restrict__ fin, T* __restrict__ fout, const float* __restrict__ force,
-                    float* __restrict__ mac, Phys P, int TY, const uint32_t* __restrict__ cpack, ClosureScales csc) {
+                    float* __restrict__ mac, Phys P, int TY, const uint32_t* __restrict__ cpack, ClosureScales csc,
+                    float* __restrict__ mclos) {
     // CLU: rows wider than one CTA.  The cluster's CTAs (blockIdx.z = chunk) each take
     // blockDim.x columns of the same strip and read the (u, v) of the neighbour
     // columns across a chunk edge from the neighbour CTA's ring (distributed shared
@@ -558,11 +576,17 @@ __global__ void __launch_bounds__(MAXT, MAXT == 256 ? (CL ? 2 : 4) : 1)
             __syncthreads();
         }
         float omega;
-        if constexpr (CL)
+        if constexpr (CL) {
+            float mm;
             omega = closure_omega(ap[lxp], am[lxm], ap[W + lxp], am[W + lxm], ub, uc, vb, vc, P, csc, s_pack,
-                                  s_stage);
-        else
+                                  s_stage, mm);
+            if (mclos) mclos[size_t(m) * nxy + ij + x] = mm;
+        } else if constexpr (CLH) {
+            omega = closure_omega_held(ap[lxp], am[lxm], ap[W + lxp], am[W + lxm], ub, uc, vb, vc, P,
+                                       __ldg(mclos + size_t(m) * nxy + ij + x));
+        } else {
             omega = les_omega(ap[lxp], am[lxm], ap[W + lxp], am[W + lxm], ub, uc, vb, vc, P);
+        }
         collide(fa, ra, ua, va, omega, Fx[ij], Fy[ij], P);
 #pragma unroll
         for (int q = 0; q < kQ; q++) Store<T>::st(fo + q * nxy + ij, fa[q], w_q(q));
@@ -1088,10 +1112,11 @@ void launch_direct_t(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout,
     const size_t sm = sizeof(float) * 6 * P.nx;
     if (mac_out)
         launch_step(lbm_step_kernel<true, MAXT, NX, T>, grid, P.nx, sm, s, pdl, fin, fout, force, mac_out, P, ty,
-                    static_cast<const uint32_t*>(nullptr), ClosureScales{});
+                    static_cast<const uint32_t*>(nullptr), ClosureScales{}, static_cast<float*>(nullptr));
     else
         launch_step(lbm_step_kernel<false, MAXT, NX, T>, grid, P.nx, sm, s, pdl, fin, fout, force,
-                    static_cast<float*>(nullptr), P, ty, static_cast<const uint32_t*>(nullptr), ClosureScales{});
+                    static_cast<float*>(nullptr), P, ty, static_cast<const uint32_t*>(nullptr), ClosureScales{},
+                    static_cast<float*>(nullptr));
 }
 
 // rows wider than 1024 columns: clusters of cluster_chunks(nx) CTAs per strip
@@ -1116,10 +1141,10 @@ void launch_cluster_t(const lbl_ctx* c, int strips, int ty, const T* fin, T* fou
     const ClosureScales sc = CL ? c->closure_sc : ClosureScales{};
     if (mac_out)
         cudaLaunchKernelEx(&lc, lbm_step_kernel<true, 1024, NX, T, CL, true>, fin, fout, force, mac_out, P, ty, pk,
-                           sc);
+                           sc, static_cast<float*>(nullptr));
     else
         cudaLaunchKernelEx(&lc, lbm_step_kernel<false, 1024, NX, T, CL, true>, fin, fout, force,
-                           static_cast<float*>(nullptr), P, ty, pk, sc);
+                           static_cast<float*>(nullptr), P, ty, pk, sc, static_cast<float*>(nullptr));
 }
 template <bool CL>
 void launch_cluster(const lbl_ctx* c, int strips, int ty, int src, int dst, const float* force, float* mac_out,
@@ -1137,24 +1162,35 @@ void launch_cluster(const lbl_ctx* c, int strips, int ty, int src, int dst, cons
 // learned-closure variant (nx % 32 == 0 and nx <= 1024, checked by lbl_set_closure)
 template <int MAXT, int NX, typename T>
 void launch_closure_t(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout, const float* force,
-                      float* mac_out, cudaStream_t s, bool pdl) {
+                      float* mac_out, cudaStream_t s, bool pdl, bool held) {
     const Phys& P = c->P;
-    const size_t sm = closure_step_smem(P.nx);
     const uint32_t* pk = c->d_closure;
+    float* mc = c->d_mclos;  // null when the network runs every step
+    if (held) {  // the plain kernel's cost: the multipliers of the last evaluation
+        const size_t sm = sizeof(float) * 6 * P.nx;
+        if (mac_out)
+            launch_step(lbm_step_kernel<true, MAXT, NX, T, false, false, true>, grid, P.nx, sm, s, pdl, fin, fout,
+                        force, mac_out, P, ty, pk, c->closure_sc, mc);
+        else
+            launch_step(lbm_step_kernel<false, MAXT, NX, T, false, false, true>, grid, P.nx, sm, s, pdl, fin, fout,
+                        force, static_cast<float*>(nullptr), P, ty, pk, c->closure_sc, mc);
+        return;
+    }
+    const size_t sm = closure_step_smem(P.nx);
     if (mac_out)
         launch_step(lbm_step_kernel<true, MAXT, NX, T, true>, grid, P.nx, sm, s, pdl, fin, fout, force, mac_out, P,
-                    ty, pk, c->closure_sc);
+                    ty, pk, c->closure_sc, mc);
     else
         launch_step(lbm_step_kernel<false, MAXT, NX, T, true>, grid, P.nx, sm, s, pdl, fin, fout, force,
-                    static_cast<float*>(nullptr), P, ty, pk, c->closure_sc);
+                    static_cast<float*>(nullptr), P, ty, pk, c->closure_sc, mc);
 }
 template <int MAXT, int NX>
 void launch_closure(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
-                    cudaStream_t s, bool pdl) {
+                    cudaStream_t s, bool pdl, bool held) {
     if (c->f16)
-        launch_closure_t<MAXT, NX, __half>(c, grid, ty, c->h[src], c->h[dst], force, mac_out, s, pdl);
+        launch_closure_t<MAXT, NX, __half>(c, grid, ty, c->h[src], c->h[dst], force, mac_out, s, pdl, held);
     else
-        launch_closure_t<MAXT, NX, float>(c, grid, ty, c->f[src], c->f[dst], force, mac_out, s, pdl);
+        launch_closure_t<MAXT, NX, float>(c, grid, ty, c->f[src], c->f[dst], force, mac_out, s, pdl, held);
 }
 
 template <int MAXT, int NX>
@@ -1174,7 +1210,7 @@ int lbm_tma_prepare(int nx) {
 }
 
 void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, float* mac_out, cudaStream_t s,
-                     bool pdl) {
+                     bool pdl, int step) {
     const Phys& P = c->P;
     const int sq = (P.nx == P.ny) ? P.nx : 0;
 
@@ -1197,9 +1233,11 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
         return;
     }
     if (c->closure) {
-        if (sq == 256) launch_closure<256, 256>(c, grid, ty, src, dst, force, mac_out, s, pdl);
-        else if (P.nx <= 256) launch_closure<256, 0>(c, grid, ty, src, dst, force, mac_out, s, pdl);
-        else launch_closure<1024, 0>(c, grid, ty, src, dst, force, mac_out, s, pdl);
+        // the network runs on steps 0, k, 2k, ... of a chunk and the multipliers are held between
+        const bool held = c->d_mclos && c->closure_every > 1 && step % c->closure_every != 0;
+        if (sq == 256) launch_closure<256, 256>(c, grid, ty, src, dst, force, mac_out, s, pdl, held);
+        else if (P.nx <= 256) launch_closure<256, 0>(c, grid, ty, src, dst, force, mac_out, s, pdl, held);
+        else launch_closure<1024, 0>(c, grid, ty, src, dst, force, mac_out, s, pdl, held);
         return;
     }
     switch (sq) {

@@ -52,7 +52,7 @@ EXPORTS = (
     "lbl_letkf_analysis_noalloc", "lbl_bindiff", "lbl_ensemble_stat", "lbl_energy_spectrum",
     "lbl_set_io_prefix", "lbl_h5_write_dataset", "lbl_autotune", "lbl_set_closure", "lbl_closure_generate",
     "lbl_closure_grad", "lbl_closure_train", "lbl_closure_infer", "lbl_batch_create", "lbl_batch_last_error",
-    "lbl_batch_cycle_async", "lbl_batch_sync", "lbl_batch_destroy", "lbl_inject",
+    "lbl_batch_cycle_async", "lbl_batch_sync", "lbl_batch_destroy", "lbl_inject", "lbl_set_closure_refresh",
 )
 INJECT_NONE, INJECT_TMA_STALL = 0, 1
 CLOSURE_PARAMS, CLOSURE_FEATURES = 1313, 6
@@ -159,6 +159,7 @@ def load_library() -> ctypes.CDLL:
         "lbl_set_io_prefix": (I, [P, ctypes.c_char_p]),
         "lbl_autotune": (I, [P, IP, D]),
         "lbl_inject": (I, [P, I, I]),
+        "lbl_set_closure_refresh": (I, [P, I]),
         "lbl_h5_write_dataset": (I, [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, P, I]),
     }
     for name, (res, args) in sig.items():
@@ -352,6 +353,11 @@ class Ensemble:
         ty, ms = ctypes.c_int(), ctypes.c_double()
         self._check(self.lib.lbl_autotune(self._h, ctypes.byref(ty), ctypes.byref(ms)), "lbl_autotune")
         return ty.value, ms.value
+
+    def set_closure_refresh(self, steps: int):
+        """Run the closure's network every `steps` steps and hold each cell's multiplier
+        between (lbl_set_closure_refresh); 1 = every step."""
+        self._check(self.lib.lbl_set_closure_refresh(self._h, int(steps)), "lbl_set_closure_refresh")
 
     def inject(self, what: int, value: int = 0):
         """Fault injection for failure-path tests (lbl_inject): INJECT_TMA_STALL makes the

@@ -163,7 +163,7 @@ def spectrum_error(e_run, e_ref, kmax: int) -> float:
 
 
 def evaluate(params=None, meta=None, filter: int = 8, spinup: int = 20000, cycles: int = 100, members: int = 16,
-             spectrum_every: int = 5, seed: int = 0, device: int = 0, log=print):
+             spectrum_every: int = 5, seed: int = 0, device: int = 0, log=print, refresh: int = 1):
     """The closure against plain Smagorinsky in the coarse configuration, with the
     box-filtered fine run as the truth (an imperfect-model experiment: neither coarse
     model represents the truth exactly).
@@ -175,7 +175,8 @@ def evaluate(params=None, meta=None, filter: int = 8, spinup: int = 20000, cycle
       filtered truth is recorded;
     * spectrum: two free coarse runs from the filtered truth; their energy spectra
       and the filtered truth's, averaged over the run, and the mean |log10| error.
-    Returns the report dict."""
+    refresh: the network runs every `refresh` steps and each cell's multiplier is held
+    between (lbl_set_closure_refresh).  Returns the report dict."""
     if params is None:
         params, meta = load_params()
     coarse = coarse_config(n_ens=members)
@@ -207,6 +208,8 @@ def evaluate(params=None, meta=None, filter: int = 8, spinup: int = 20000, cycle
         if w is not None:
             e.set_closure(w, meta["nu_ref"], meta["dx_ref"])
             f1.set_closure(w, meta["nu_ref"], meta["dx_ref"])
+            e.set_closure_refresh(refresh)
+            f1.set_closure_refresh(refresh)
         for m in range(members):
             e.set_f(m, feq_populations(rt, ut + coarse.ens_perturb * dvel[m][0], vt + coarse.ens_perturb * dvel[m][1], c))
         f1.set_f(0, feq_populations(rt, ut, vt, c))
@@ -241,6 +244,7 @@ def evaluate(params=None, meta=None, filter: int = 8, spinup: int = 20000, cycle
     kq, kh = coarse.nx // 4, coarse.nx // 2 - 1
     rep = {
         "cycles": cycles, "members": members, "fine_grid": fine.nx, "filter": filter, "spinup_fine_steps": spinup,
+        "closure_refresh_steps": refresh,
         "dt_ratio": ratio, "wall_s": wall,
         "rmse_mean_second_half": {n: float(np.mean(v[half:])) for n, v in rmse.items()},
         "rmse_final": {n: float(v[-1]) for n, v in rmse.items()},
@@ -259,7 +263,8 @@ def evaluate(params=None, meta=None, filter: int = 8, spinup: int = 20000, cycle
 
 def _cli_eval(a):
     w, meta = load_params(a.params)
-    rep = evaluate(w, meta, filter=meta.get("filter", 8), spinup=a.spinup, cycles=a.cycles, members=a.members)
+    rep = evaluate(w, meta, filter=meta.get("filter", 8), spinup=a.spinup, cycles=a.cycles, members=a.members,
+                   refresh=a.refresh)
     if a.out:
         with open(a.out, "w") as f:
             json.dump(rep, f, indent=1)
@@ -291,6 +296,8 @@ def main():
     e.add_argument("--spinup", type=int, default=20000)
     e.add_argument("--cycles", type=int, default=100)
     e.add_argument("--members", type=int, default=16)
+    e.add_argument("--refresh", type=int, default=1,
+                   help="run the network every this many steps and hold the multipliers between")
     e.add_argument("--out", default=None, help="write the full report (series, spectra) as JSON")
     a = ap.parse_args()
     if a.cmd == "train":

@@ -180,3 +180,46 @@ def test_training_lowers_the_loss_below_smagorinsky():
     mse_smag = float(np.mean((1.0 - tgt[te]) ** 2))
     mse_const = float(np.var(tgt[te]))
     assert mse_mlp < mse_smag and mse_mlp < mse_const, (mse_mlp, mse_smag, mse_const)
+
+
+def test_held_multiplier_equals_evaluation_for_a_constant_network():
+    """lbl_set_closure_refresh: between two evaluations of the network each cell keeps its
+    multiplier.  A network whose output does not depend on its inputs (every weight zero,
+    m = softplus(b3)) gives the same multiplier either way, so a run that evaluates it
+    every 5 steps must equal, bit for bit, a run that evaluates it every step: the held
+    path recomputes |S| exactly as the evaluating path does."""
+    w = np.zeros(lbl.CLOSURE_PARAMS, np.float32)
+    w[-1] = 0.7  # b3
+    out = []
+    for k in (1, 5):
+        e = lbl.Ensemble(lbl.config_default("NATURE", 64, 2, cs=0.1, tau=0.51))
+        e.init(0)
+        e.set_closure(w)
+        e.set_closure_refresh(k)
+        e.update(0, 23)
+        out.append([e.get_f(m) for m in range(2)])
+        e.close()
+    for m in range(2):
+        np.testing.assert_array_equal(out[0][m], out[1][m])
+
+
+def test_held_multiplier_follows_the_network():
+    """With the trained network, holding the multipliers for 10 steps stays close to
+    evaluating every step (populations within 1e-4 relative after 100 steps; they differ,
+    since m changes from step to step)."""
+    from lbl import closure
+    w, meta = closure.load_params()
+    out = []
+    for k in (1, 10):
+        e = lbl.Ensemble(lbl.config_default("NATURE", 256, 2, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP, ic_amp=1.0))
+        e.init(0)
+        e.set_closure(w, meta["nu_ref"], meta["dx_ref"])
+        e.set_closure_refresh(k)
+        e.update(0, 100)
+        out.append(np.stack([e.get_f(m) for m in range(2)]).astype(np.float64))
+        e.close()
+    rel = np.max(np.abs(out[1] - out[0]) / np.abs(out[0]))
+    print(f"refresh 10 against 1 after 100 steps: {rel:.2e}")
+    assert np.all(np.isfinite(out[1])) and 0 < rel < 1e-4
+    with pytest.raises(lbl.LblError):
+        lbl.Ensemble(lbl.config_default("NATURE", 64, 1)).set_closure_refresh(0)
