@@ -399,6 +399,8 @@ def side_leg(lbl, name, device, flush_l2, K=10, W=3):
     saved = (NX, M, CLOSURE, WORKLOAD)
     NX, M, WORKLOAD = WORKLOADS[name]
     CLOSURE = name == "C4"
+    if CLOSURE and CLOSURE_REFRESH > 1:
+        WORKLOAD += f"; the network runs every {CLOSURE_REFRESH} steps, each cell's multiplier held between"
     T = STEPS_PER_CYCLE
     try:
         obs, _ = make_observations(lbl, 1)

@@ -130,6 +130,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(const float* __r
     float* sW = sD + kpad;                                    // [p*p][kpad] weights
     uint64_t* bar = reinterpret_cast<uint64_t*>(sW + G.p * G.p * kpad);
     uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 1);
+    int* s_fail = reinterpret_cast<int*>(s_taddr + 1);  // the poller's verdict, for the whole CTA
 
     const int tid = threadIdx.x, warp = tid >> 5;
     const int bi = blockIdx.x % G.nsx, bj = blockIdx.x / G.nsx;
@@ -198,8 +199,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(const float* __r
     const int ntiles = G.p * G.p / PPT;
     const int nch = kpad >> 2, c_lo = half * (nch >> 1), c_hi = c_lo + (nch >> 1);
     uint32_t phase = 0;
-    bool ok = true;
-    for (int t = 0; t < ntiles; t++) {
+    bool failed = false;  // uniform: a commit that never arrived stops the CTA's MMAs
+    for (int t = 0; t < ntiles && !failed; t++) {
         const int pat = t * PPT + s;
         const float* w = sW + pat * kpad;
         for (int c4 = c_lo; c4 < c_hi; c4++) {
@@ -231,12 +232,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(const float* __r
         }
         // one thread polls the barrier; the others sleep at the CTA barrier meanwhile
         if (tid == 0) {
-            ok = ok && mbar_wait_bounded(bar, phase);
+            *s_fail = mbar_wait_bounded(bar, phase) ? 0 : 1;
             tc_before();
         }
         __syncthreads();
         phase ^= 1;
         tc_after();
+        if (*s_fail) {  // leave the tile unread; the MMAs may still be in flight
+            failed = true;
+            break;
+        }
         // row r of D: this thread's lane (warp w reads lanes 32w..32w+31): the Gram row in
         // columns [0, MP), c_k in column MP
         const int pi = pat % G.p, pj = pat / G.p;
@@ -263,7 +268,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) gram_tc_kernel(const float* __r
         __syncthreads();  // the next tile rewrites A and the accumulator
         tc_after();
     }
-    if (!ok && tid == 0) atomicCAS(err, 0, 4);  // code 4: the Gram's MMA wait gave up
+    if (failed) {
+        // code 4: the Gram's MMA wait gave up.  Wait once more (bounded) for the commit before
+        // the accumulator is released; its rows of Q are not written.
+        if (tid == 0) {
+            atomicCAS(err, 0, 4);
+            mbar_wait_bounded(bar, phase ^ 1);
+        }
+        __syncthreads();
+    }
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(NCOL));
 }
 
@@ -273,7 +286,7 @@ size_t gram_tc_smem_mp(int kpad, int p) {
     // inside its operand (rows < 128 or MP, K steps < kpad/8), and would under either reading
     // of the two strides: (kpad/8 - 1) 256 + 15 x 128 + 32 kpad + 127 < 128 kpad x 4.
     return size_t(2) * kTcRows * kpad * 4 + size_t(2) * (MP + 16) * kpad * 4 + size_t(kpad) * MP * 4 + size_t(kpad) * 4 +
-           size_t(p) * p * kpad * 4 + 16;
+           size_t(p) * p * kpad * 4 + 32;
 }
 
 }  // namespace
