@@ -87,6 +87,7 @@ WORKLOAD = WORKLOADS["C1"][2]
 
 STORAGE = 0  # lbl_config.storage of the ensemble (the nature run stays FP32)
 GRAM = 0     # lbl_config.gram of the ensemble: 0 FP32, 1 BF16 tensor cores (32 < M <= 64)
+LBM_VARIANT = 0  # lbl_config.lbm_variant of the ensemble and the nature run (0: the library's choice)
 
 
 def workload_config(lib, mode="DA_LETKF", n_ens=None):
@@ -96,7 +97,7 @@ def workload_config(lib, mode="DA_LETKF", n_ens=None):
         mode, NX, M if n_ens is None else n_ens, da_xyprune=P_OBS, letkf_rloc_len=1, letkf_covinf=1.1, obs_error_u=0.1,
         obs_error_rho=0.01, iiter=20, daprune=5, cs=0.1, tau=0.51, ic_kind=lib.IC_K4EXP, ic_amp=1.0,
         ens_init=lib.ENS_PERTURBED, ens_perturb=0.1, storage=STORAGE if mode != "NATURE" else 0,
-        gram=GRAM if mode == "DA_LETKF" else 0)
+        gram=GRAM if mode == "DA_LETKF" else 0, lbm_variant=LBM_VARIANT)
 
 
 def measured_peak():
@@ -107,15 +108,21 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(nx=None, m=None, closure=None):
-    """DRAM bytes per stream-collide launch from the committed ncu summary, if any."""
-    if STORAGE:
-        return None
+def stream_collide_kernel(ens):
+    """The stream-collide kernel the context runs and its launch shape."""
+    shape = ens.launch_shape()
+    if CLOSURE:
+        return "lbm_step_kernel_closure", shape
+    return ("lbm_step_vec_kernel" if shape["columns_per_thread"] > 1 else "lbm_step_kernel"), shape
+
+
+def ncu_traffic(kernel, nx=None, m=None, storage=None):
+    """DRAM bytes per stream-collide launch from the committed ncu summary
+    profiles/<kernel>[_f16]_<nx>x<nx>_M<m>.md, if there is one."""
     nx = NX if nx is None else nx
     m = M if m is None else m
-    closure = CLOSURE if closure is None else closure
-    name = "lbm_step_kernel_closure" if closure else "lbm_step_kernel"
-    path = os.path.join(ROOT, "profiles", f"{name}_{nx}x{nx}_M{m}.md")
+    storage = STORAGE if storage is None else storage
+    path = os.path.join(ROOT, "profiles", f"{kernel}{'_f16' if storage else ''}_{nx}x{nx}_M{m}.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -343,7 +350,8 @@ def run_engine(args, dist, rank, world, device):
     bytes_per_launch = (36.0 if STORAGE else 72.0) * M * NX * NX
     achieved = bytes_per_launch / (ms_step * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = ncu_traffic()
+    kernel, shape = stream_collide_kernel(ens)
+    traffic = ncu_traffic(kernel)
     ens.profile_step(20)
     ms_isolated = ens.profile_step(200)
 
@@ -359,7 +367,7 @@ def run_engine(args, dist, rank, world, device):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "forecast_rmse_uv_last": rmse[-1] if rmse else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "lbm_step_kernel", "ms_per_launch": ms_step,
+                     "traffic": traffic, "kernel": kernel, "shape": shape, "ms_per_launch": ms_step,
                      "algorithmic_bytes_per_launch": bytes_per_launch, "peak_kind": peak_kind,
                      "timed": "forecast phase of the timed cycles (in-graph events), 100 launches per cycle",
                      "ms_per_launch_back_to_back": ms_isolated,
@@ -434,9 +442,10 @@ def side_leg(lbl, name, device, flush_l2, K=10, W=3):
             bpl = 72.0 * M * NX * NX
             achieved = bpl / (ms_step * 1e-3) / 1e9
             peak, peak_kind = measured_peak()
+            kernel, shape = stream_collide_kernel(ens)
             out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                               "frac": achieved / peak, "traffic": ncu_traffic(NX, M, False),
-                               "kernel": "lbm_step_kernel", "grid": f"{NX}x{NX}", "members": M,
+                               "frac": achieved / peak, "traffic": ncu_traffic(kernel, NX, M, 0),
+                               "kernel": kernel, "shape": shape, "grid": f"{NX}x{NX}", "members": M,
                                "ms_per_launch": ms_step, "algorithmic_bytes_per_launch": bpl, "peak_kind": peak_kind,
                                "timed": "forecast phase of the C2 cycles (in-graph events), 100 launches per cycle",
                                "regime": "HBM-bound: two 604 MB population buffers, far larger than the 126 MB L2"}
@@ -768,7 +777,8 @@ def lbm_sweep(args):
     import lbl
     for spec in args.lbm.split(","):
         nx, m = (int(v) for v in spec.lower().split("x"))
-        e = lbl.Ensemble(lbl.config_default("NATURE", nx, m, storage=STORAGE))
+        e = lbl.Ensemble(lbl.config_default("NATURE", nx, m, storage=STORAGE, lbm_variant=LBM_VARIANT))
+        tuned = e.autotune()[0] if args.autotune else None  # between creation and init
         e.init(0)
         if args.closure:
             e.set_closure(*closure_params())
@@ -780,11 +790,11 @@ def lbm_sweep(args):
         gbs = bytes_launch / (ms * 1e-3) / 1e9
         print(json.dumps({"lbm_stream_collide": {
             "nx": nx, "ny": nx, "members": m, "storage": "f16 deviations" if STORAGE else "f32",
-            "closure": "mlp" if args.closure else "smagorinsky",
+            "closure": "mlp" if args.closure else "smagorinsky", "lbm_variant": args.lbm_variant,
             "launches": args.steps, "ms_per_launch": ms,
             "glups": m * nx * nx / (ms * 1e-3) / 1e9, "algorithmic_bytes_per_launch": bytes_launch,
             "population_buffer_mb": bytes_launch / 2 / 1e6, "achieved_gbs": gbs, "peak_gbs": peak,
-            "frac": gbs / peak, "peak_kind": peak_kind}}), flush=True)
+            "frac": gbs / peak, "peak_kind": peak_kind, "autotuned": tuned is not None, "shape": e.launch_shape()}}), flush=True)
         e.close()
 
 
@@ -813,13 +823,18 @@ def main():
                     help="time the stream-collide alone at these grids and exit")
     ap.add_argument("--closure", action="store_true",
                     help="with --lbm: the learned-closure stream-collide (trained parameters of the package)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="with --lbm: time at the strip height lbl_autotune picks instead of the heuristic's")
+    ap.add_argument("--lbm-variant", choices=["auto", "direct", "tma", "vec", "vec2"], default="auto",
+                    help="stream-collide kernel: the library's choice, one column per thread, TMA-fed rows, or "
+                         "4 (vec, 128-bit) / 2 (vec2, 64-bit) columns per thread")
     ap.add_argument("--closure-refresh", type=int, default=10,
                     help="C4: run the closure's network every this many steps, holding each cell's multiplier between "
                          "(1: every step)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global NX, M, WORKLOAD, STORAGE, CLOSURE, GRAM, CLOSURE_REFRESH
+    global NX, M, WORKLOAD, STORAGE, CLOSURE, GRAM, CLOSURE_REFRESH, LBM_VARIANT
     NX, M, WORKLOAD = WORKLOADS.get(args.workload, WORKLOADS["C1"])
     CLOSURE = args.workload == "C4"
     CLOSURE_REFRESH = args.closure_refresh
@@ -827,6 +842,7 @@ def main():
         WORKLOAD += f"; the network runs every {CLOSURE_REFRESH} steps, each cell's multiplier held between"
     STORAGE = 1 if args.storage == "f16" else 0
     GRAM = {"f32": 0, "bf16": 1, "tf32x3": 2}[args.gram]
+    LBM_VARIANT = {"auto": 0, "direct": 1, "tma": 2, "vec": 3, "vec2": 4}[args.lbm_variant]
     if GRAM == 1:
         WORKLOAD += "; Gram on BF16 tensor cores with FP32 sums"
     elif GRAM == 2:

@@ -52,9 +52,14 @@ extern "C" {
 #define LBL_ERR_TIMEOUT   -10   /* a bounded wait inside a kernel gave up      */
 
 /* stream-collide kernel variants (lbl_config.lbm_variant) */
-#define LBL_LBM_AUTO   0    /* the direct-load kernel (measured faster on B200)  */
-#define LBL_LBM_DIRECT 1    /* per-thread global loads                           */
+#define LBL_LBM_AUTO   0    /* direct loads, 1 or 2 columns per thread by storage and
+                               width (the fastest measured on B200); lbl_autotune
+                               may pick 1, 2 or 4                                */
+#define LBL_LBM_DIRECT 1    /* per-thread global loads, 1 column per thread       */
 #define LBL_LBM_TMA    2    /* rows streamed into shared memory by the TMA unit  */
+#define LBL_LBM_VEC    3    /* 4 columns per thread: 128-bit loads and stores of
+                               FP32 rows (64-bit for FP16 deviations), nx <= 1024 */
+#define LBL_LBM_VEC2   4    /* 2 columns per thread: 64-bit (FP16: 32-bit)        */
 
 /* population storage (lbl_config.storage) */
 #define LBL_GRAM_F32  0  /* Gram dY^T R^-1 dY in FP32 (the reference's arithmetic)                       */
@@ -265,11 +270,24 @@ int lbl_letkf_analysis_noalloc(const lbl_config* cfg, const float* f_in, float* 
 int lbl_inject(lbl_ctx* ctx, int what, int value);
 
 /* Tile autotuning for this context's grid and ensemble size: times the fused
- * stream-collide on the rest state for candidate strip heights (rows per CTA) and
- * keeps the fastest for every later step.  Call between lbl_create and lbl_init (it
+ * stream-collide on the rest state for candidate strip heights (rows per CTA), and for
+ * the vector-load kernel both forms of its march, and keeps the fastest for every
+ * later step.  Call between lbl_create and lbl_init (it
  * overwrites the populations).  *strip_rows / *ms_per_launch (optional) receive
  * the choice and its time.  No counterpart in the reference. */
 int lbl_autotune(lbl_ctx* ctx, int* strip_rows, double* ms_per_launch);
+
+/* The stream-collide launch shape the context runs: columns per thread (1, or 2 / 4 for
+ * the vector-load kernel), whether its march prefetches the row after next (1 for the
+ * one-column kernels), and the strip height (rows per CTA).  lbl_autotune may change
+ * the last two.  No GPU work. */
+int lbl_stream_collide_shape(const lbl_ctx* ctx, int* columns_per_thread, int* prefetch, int* strip_rows);
+
+/* Set that shape, e.g. one an earlier lbl_autotune logged: prefetch 0 or 1 (0 only for
+ * the vector-load kernel), strip_rows in [1, ny], or 0 for the heuristic's.  Waits for
+ * the context's work and drops its captured graphs; results do not depend on the
+ * shape (every shape computes each cell in the same arithmetic). */
+int lbl_set_stream_collide_shape(lbl_ctx* ctx, int prefetch, int strip_rows);
 
 /* Directory prefix (config::prefix, "io" by default, config.h:287) under which the
  * LETKF matrix dumps go when cfg.write_mat is set: <prefix>/letkf/mat/ens<r>/

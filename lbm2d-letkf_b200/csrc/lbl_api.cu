@@ -192,7 +192,10 @@ int validate(const lbl_config& c, std::string& err) {
         err = "write_mat needs ny divisible by n_ens (the reference's batch per rank is whole rows)";
         return LBL_ERR_ARG;
     }
-    if (c.lbm_variant < LBL_LBM_AUTO || c.lbm_variant > LBL_LBM_TMA) { err = "unknown lbm_variant"; return LBL_ERR_ARG; }
+    if (c.lbm_variant < LBL_LBM_AUTO || c.lbm_variant > LBL_LBM_VEC2) { err = "unknown lbm_variant"; return LBL_ERR_ARG; }
+    if ((c.lbm_variant == LBL_LBM_VEC || c.lbm_variant == LBL_LBM_VEC2) && c.nx > 1024) {
+        err = "the vector-load stream-collide serves nx <= 1024"; return LBL_ERR_UNSUPPORTED;
+    }
     if (c.mode == LBL_MODE_DA_LETKF && !analysis_supported(c.n_ens)) {
         err = "DA_LETKF supports 2 <= n_ens <= 64 in this build"; return LBL_ERR_UNSUPPORTED;
     }
@@ -608,6 +611,16 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     }
     if (cfg->lbm_variant == LBL_LBM_TMA && !ctx->use_tma)
         return fail(ctx, LBL_ERR_UNSUPPORTED, "TMA stream-collide unavailable for this grid (nx <= 512) or driver");
+    if (cfg->lbm_variant == LBL_LBM_VEC) ctx->vec = 4;
+    if (cfg->lbm_variant == LBL_LBM_VEC2) ctx->vec = 2;
+    // measured on B200 (back-to-back launches): the 2-column march gains from the
+    // prefetched row up to 256 columns, the 4-column one (215 against 168 registers)
+    // loses; FP16 deviations pay only with vector loads (512^2 x 64: 164 against
+    // 218 us), FP32 at 512^2 x 64 stays fastest one column per thread (215 against
+    // 228 us), and at 256^2 x 16 two columns gain (12.9 against 14.4 us)
+    ctx->vec_auto = cfg->lbm_variant == LBL_LBM_AUTO && cfg->nx <= 1024;
+    if (ctx->vec_auto) ctx->vec = (ctx->f16 || cfg->nx <= 256) ? 2 : 0;
+    ctx->vec_pf = ctx->vec == 2 ? cfg->nx <= 256 : ctx->vec == 0;  // (the one-column kernels always prefetch)
     ctx->ty_default = lbm_strip_rows(ctx);
     for (auto& e : ctx->ev) LBL_CK(cudaEventCreate(&e));
     for (auto& e : ctx->user_ev) LBL_CK(cudaEventCreate(&e));
@@ -1319,8 +1332,7 @@ int lbl_autotune(lbl_ctx* ctx, int* strip_rows_out, double* ms_per_launch) {
     launch_rest_state(ctx, ctx->stream);
     LBL_CK(cudaGetLastError());
     const float* force = ctx->d_force;
-    const int heuristic = lbm_strip_rows(ctx);
-    int best = heuristic;
+    int best = 0;
     double best_ms = 1e30;
     // each candidate: the best of three samples of at least ~2 ms of back-to-back launches
     auto sample = [&](int reps, double* ms_out) -> int {
@@ -1334,24 +1346,73 @@ int lbl_autotune(lbl_ctx* ctx, int* strip_rows_out, double* ms_per_launch) {
         *ms_out = double(ms) / reps;
         return LBL_OK;
     };
-    for (int ty : {heuristic, 2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16, 20, 24, 32, 40, 48, 64}) {
-        if (ty > ctx->P.ny) continue;
-        ctx->ty_tuned = ty;
-        double one = 0;
-        LBL_TRY(sample(2, &one));  // warm-up and a first estimate
-        const int reps = int(std::min(200.0, std::max(4.0, 2.0 / std::max(one, 1e-4))));
-        double t = 1e30;
-        for (int k = 0; k < 3; k++) {
-            double m = 0;
-            LBL_TRY(sample(reps, &m));
-            t = std::min(t, m);
-        }
-        if (t < best_ms * 0.99) { best_ms = t; best = ty; }
+    // the vector-load kernel also has two march forms (with and without the prefetched
+    // row), and an LBL_LBM_AUTO context may take 1, 2 or 4 columns per thread; the
+    // heuristic's own choice comes first, so a tie keeps it
+    struct Form { int vec; bool pf; };
+    std::vector<Form> forms{{ctx->vec, ctx->vec_pf}};
+    Form best_form = forms[0];
+    if (!ctx->closure && (ctx->vec || ctx->vec_auto)) {
+        const std::vector<int> widths = ctx->vec_auto ? std::vector<int>{0, 2, 4} : std::vector<int>{ctx->vec};
+        for (int w : widths)
+            for (bool pf : {true, false})
+                if ((w || pf) && !(w == ctx->vec && pf == ctx->vec_pf)) forms.push_back({w, pf});
     }
+    for (const Form& fm : forms) {
+        ctx->vec = fm.vec;
+        ctx->vec_pf = fm.pf;
+        ctx->ty_tuned = 0;
+        const int heuristic = lbm_strip_rows(ctx);
+        if (best == 0) best = heuristic;
+        for (int ty : {heuristic, 2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16, 20, 24, 32, 40, 48, 64}) {
+            if (ty > ctx->P.ny) continue;
+            ctx->ty_tuned = ty;
+            double one = 0;
+            LBL_TRY(sample(2, &one));  // warm-up and a first estimate
+            const int reps = int(std::min(200.0, std::max(4.0, 2.0 / std::max(one, 1e-4))));
+            double t = 1e30;
+            for (int k = 0; k < 3; k++) {
+                double m = 0;
+                LBL_TRY(sample(reps, &m));
+                t = std::min(t, m);
+            }
+            if (t < best_ms * 0.99) { best_ms = t; best = ty; best_form = fm; }
+        }
+    }
+    ctx->vec = best_form.vec;
+    ctx->vec_pf = best_form.pf;
     ctx->ty_tuned = best;
     LBL_TRY(check_timeout(ctx));
     if (strip_rows_out) *strip_rows_out = best;
     if (ms_per_launch) *ms_per_launch = best_ms;
+    return LBL_OK;
+}
+
+int lbl_stream_collide_shape(const lbl_ctx* ctx, int* columns_per_thread, int* prefetch, int* strip_rows) {
+    if (!ctx) return LBL_ERR_ARG;
+    const bool vec = ctx->vec && !ctx->closure && !ctx->use_tma;
+    if (columns_per_thread) *columns_per_thread = vec ? ctx->vec : 1;
+    if (prefetch) *prefetch = vec ? int(ctx->vec_pf) : 1;
+    if (strip_rows) *strip_rows = ctx->ty_tuned > 0 ? ctx->ty_tuned : ctx->ty_default;
+    return LBL_OK;
+}
+
+int lbl_set_stream_collide_shape(lbl_ctx* ctx, int prefetch, int strip_rows) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    const bool vec = ctx->vec && !ctx->closure && !ctx->use_tma;
+    if (prefetch != 0 && prefetch != 1) return fail(ctx, LBL_ERR_ARG, "prefetch must be 0 or 1");
+    if (!vec && prefetch == 0)
+        return fail(ctx, LBL_ERR_UNSUPPORTED, "only the vector-load stream-collide has a march without prefetch");
+    if (strip_rows < 0 || strip_rows > ctx->P.ny) return fail(ctx, LBL_ERR_ARG, "strip_rows must lie in [0, ny]");
+    // graphs captured with the old shape are rebuilt on demand
+    LBL_CK(cudaStreamSynchronize(ctx->stream));
+    LBL_CK(cudaStreamSynchronize(ctx->side));
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
+    ctx->graphs.clear();
+    if (vec) ctx->vec_pf = prefetch == 1;
+    ctx->ty_tuned = strip_rows;
+    ctx->ty_default = lbm_strip_rows(ctx);
     return LBL_OK;
 }
 

@@ -133,6 +133,9 @@ struct lbl_ctx {
     // TMA descriptors of the two population buffers (input side of a step)
     CUtensorMap tmap[2];
     bool use_tma = false;
+    int vec = 0;                         // columns per thread of the vector-load stream-collide (0: one)
+    bool vec_pf = false;                 // its march prefetches the row after next
+    bool vec_auto = false;               // LBL_LBM_AUTO: lbl_autotune may change the columns per thread
     int ty_tuned = 0;                    // stream-collide strip height chosen by lbl_autotune (0: heuristic)
     int ty_default = 0;                  // the heuristic's strip height for the kernel that runs
     int* d_err = nullptr;                // bounded-wait timeout flag of the TMA kernel

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "lbl_internal.h"
 
@@ -611,6 +612,233 @@ __global__ void __launch_bounds__(MAXT, MAXT == 256 ? (CL ? 2 : 4) : 1)
 }
 
 // ---------------------------------------------------------------------------
+// Vector-load stream-collide: lbm_step_kernel's column march with each thread owning
+// VW consecutive columns x0 .. x0+VW-1.  Every population row of the pull is one
+// VW-wide load (VW = 4: 128 bits) of the thread's own columns; a direction with
+// ex = +1 pulls from x-1, so its VW values shift up by one column in registers and
+// the column x0-1 comes in as one scalar load (ex = -1 mirrors that with x0+VW).
+// The analysis populations, the macros and the forcing move as VW-wide loads and
+// stores too.  The x+-1 stencil of the Smagorinsky term is in registers except at
+// the thread's two edge columns, whose (u, v) come through a 3-row shared ring that
+// holds one float4 per thread, (u, v) of its first and of its last column.  The
+// arithmetic of a cell is lbm_step_kernel's (macros_v, les_omega, collide), so the
+// two kernels agree bit for bit.  Row offsets of rows j-2 .. j+1 and the strip
+// halos are handled as in lbm_step_kernel.
+// ---------------------------------------------------------------------------
+template <typename T, int VW>
+struct VecIO;
+template <>
+struct VecIO<float, 2> {
+    static __device__ __forceinline__ void ld(const float* p, float (&o)[2], float) {
+        const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+    }
+    static __device__ __forceinline__ void st(float* p, const float (&o)[2], float) {
+        *reinterpret_cast<float2*>(p) = make_float2(o[0], o[1]);
+    }
+};
+template <>
+struct VecIO<float, 4> {
+    static __device__ __forceinline__ void ld(const float* p, float (&o)[4], float) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+        o[2] = t.z;
+        o[3] = t.w;
+    }
+    static __device__ __forceinline__ void st(float* p, const float (&o)[4], float) {
+        *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+    }
+};
+// FP16 deviations: the values Store<__half> gives, VW at a time (32 or 64 bits)
+template <int VW>
+struct VecIO<__half, VW> {
+    static_assert(VW == 2 || VW == 4, "2 or 4 columns per thread");
+    using Word = typename std::conditional<VW == 2, unsigned, uint2>::type;
+    static __device__ __forceinline__ void ld(const __half* p, float (&o)[VW], float w) {
+        const Word t = __ldg(reinterpret_cast<const Word*>(p));
+        const __half2* h = reinterpret_cast<const __half2*>(&t);
+#pragma unroll
+        for (int k = 0; k < VW / 2; k++) {
+            const float2 d = __half22float2(h[k]);
+            o[2 * k] = w + d.x;
+            o[2 * k + 1] = w + d.y;
+        }
+    }
+    static __device__ __forceinline__ void st(__half* p, const float (&o)[VW], float w) {
+        Word t;
+        __half2* h = reinterpret_cast<__half2*>(&t);
+#pragma unroll
+        for (int k = 0; k < VW / 2; k++) h[k] = __halves2half2(__float2half_rn(o[2 * k] - w), __float2half_rn(o[2 * k + 1] - w));
+        *reinterpret_cast<Word*>(p) = t;
+    }
+};
+
+template <bool WRITE_MAC, int NX, int VW, bool PF, typename T>
+__global__ void __launch_bounds__(NX ? NX / VW : 1024 / VW)
+    lbm_step_vec_kernel(const T* __restrict__ fin, T* __restrict__ fout, const float* __restrict__ force,
+                        float* __restrict__ mac, Phys P, int TY) {
+    extern __shared__ float4 s_edge[];  // [3][nt]: (u, v) of the first and of the last column
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" :::);
+    const int nx = NX ? NX : P.nx, ny = NX ? NX : P.ny, nxy = NX ? NX * NX : P.nxy;
+    const int nt = nx / VW;  // threads of a row
+    const int t = threadIdx.x;
+    const int x0 = t * VW;
+    const int xl = x0 == 0 ? nx - 1 : x0 - 1;    // column x0-1, periodic
+    const int xr = x0 + VW == nx ? 0 : x0 + VW;  // column x0+VW, periodic
+    const int tm = t == 0 ? nt - 1 : t - 1, tp = t == nt - 1 ? 0 : t + 1;
+    const int m = blockIdx.y;
+    const int j0 = blockIdx.x * TY;
+    const int j1 = min(j0 + TY, ny);
+    const T* __restrict__ fm = fin + size_t(m) * kQ * nxy;
+    T* __restrict__ fo = fout + size_t(m) * kQ * nxy;
+
+    auto wrap_row = [&](int r) { return (r < 0 ? r + ny : (r >= ny ? r - ny : r)) * nx; };
+    int o_m = wrap_row(j0 - 2), o_0 = wrap_row(j0 - 1), o_p = wrap_row(j0);
+    auto advance = [&]() {
+        o_m = o_0;
+        o_0 = o_p;
+        o_p = (o_p + nx == nxy) ? 0 : o_p + nx;
+    };
+    // pull streaming of the thread's VW columns: fc[q][k] = f[(x0+k-ex, j-ey)] (lbm.cu:82-87)
+    auto pull = [&](float (&fc)[kQ][VW]) {
+#pragma unroll
+        for (int q = 0; q < kQ; q++) {
+            const int row = ey_q(q) == -1 ? o_p : (ey_q(q) == 0 ? o_0 : o_m);
+            const T* b = fm + q * nxy + row;
+            float w[VW];
+            VecIO<T, VW>::ld(b + x0, w, w_q(q));
+            if (ex_q(q) == 0) {
+#pragma unroll
+                for (int k = 0; k < VW; k++) fc[q][k] = w[k];
+            } else if (ex_q(q) == 1) {
+                fc[q][0] = Store<T>::ld(b + xl, w_q(q));
+#pragma unroll
+                for (int k = 1; k < VW; k++) fc[q][k] = w[k - 1];
+            } else {
+#pragma unroll
+                for (int k = 0; k < VW - 1; k++) fc[q][k] = w[k + 1];
+                fc[q][VW - 1] = Store<T>::ld(b + xr, w_q(q));
+            }
+        }
+    };
+    auto macros_row = [&](const float (&fc)[kQ][VW], float (&r)[VW], float (&u)[VW], float (&v)[VW]) {
+#pragma unroll
+        for (int k = 0; k < VW; k++) {
+            float g[kQ];
+#pragma unroll
+            for (int q = 0; q < kQ; q++) g[q] = fc[q][k];
+            macros_v(g, r[k], u[k], v[k], P.c);
+        }
+    };
+    // finalise row A: Smagorinsky from the ring (A's edge neighbours) and the rows above
+    // (B) and below (C), collide, store
+    int ij = j0 * nx + x0;
+    auto finalise = [&](float (&fa)[kQ][VW], const float (&ra)[VW], const float (&ua)[VW], const float (&va)[VW],
+                        const float (&ub)[VW], const float (&vb)[VW], const float (&uc)[VW], const float (&vc)[VW],
+                        const float4* sa) {
+        const float4 em = sa[tm], ep = sa[tp];  // the neighbours' edge columns of row A
+        float fx[VW], fy[VW];
+        VecIO<float, VW>::ld(force + ij, fx, 0.f);
+        VecIO<float, VW>::ld(force + nxy + ij, fy, 0.f);
+#pragma unroll
+        for (int k = 0; k < VW; k++) {
+            const float ue = k < VW - 1 ? ua[k + 1] : ep.x, ve = k < VW - 1 ? va[k + 1] : ep.y;
+            const float uw = k > 0 ? ua[k - 1] : em.z, vw = k > 0 ? va[k - 1] : em.w;
+            const float omega = les_omega(ue, uw, ve, vw, ub[k], uc[k], vb[k], vc[k], P);
+            float g[kQ];
+#pragma unroll
+            for (int q = 0; q < kQ; q++) g[q] = fa[q][k];
+            collide(g, ra[k], ua[k], va[k], omega, fx[k], fy[k], P);
+#pragma unroll
+            for (int q = 0; q < kQ; q++) fa[q][k] = g[q];
+        }
+#pragma unroll
+        for (int q = 0; q < kQ; q++) VecIO<T, VW>::st(fo + q * nxy + ij, fa[q], w_q(q));
+        if (WRITE_MAC) {
+            float* mm = mac + size_t(m) * 3 * nxy + ij;
+            VecIO<float, VW>::st(mm, ra, 0.f);
+            VecIO<float, VW>::st(mm + nxy, ua, 0.f);
+            VecIO<float, VW>::st(mm + 2 * nxy, va, 0.f);
+        }
+        ij += nx;
+    };
+    auto edges = [&](const float (&uu)[VW], const float (&vv)[VW]) {
+        return make_float4(uu[0], vv[0], uu[VW - 1], vv[VW - 1]);
+    };
+    if constexpr (PF) {
+        // three row slots rotate roles (A = row being finalised, B = next row, C = the
+        // row after, prefetched); the march is unrolled by three so that the rotation is
+        // a renaming of registers.  Slot k's edges also live in s_edge[k]; uc, vc hold
+        // the row below A.
+        float f[3][kQ][VW], r[3][VW], u[3][VW], v[3][VW];
+        {  // halo row below the strip: only its u,v are needed
+            pull(f[2]);
+            float rr[VW];
+            macros_row(f[2], rr, u[2], v[2]);
+        }
+        advance();
+        pull(f[0]);  // row j0
+        macros_row(f[0], r[0], u[0], v[0]);
+        s_edge[t] = edges(u[0], v[0]);
+        advance();
+        pull(f[1]);  // row j0+1
+        auto row = [&](float (&fa)[kQ][VW], float (&fb)[kQ][VW], float (&fc)[kQ][VW], float (&ra)[VW],
+                       float (&ua)[VW], float (&va)[VW], float (&rb)[VW], float (&ub)[VW], float (&vb)[VW],
+                       const float (&uc)[VW], const float (&vc)[VW], const float4* sa, float4* sb, int jc) {
+            advance();
+            if (jc + 2 <= j1) pull(fc);  // prefetch the row after next
+            macros_row(fb, rb, ub, vb);
+            sb[t] = edges(ub, vb);
+            __syncthreads();
+            finalise(fa, ra, ua, va, ub, vb, uc, vc, sa);
+        };
+        const float4* s0 = s_edge;
+        float4* s1 = s_edge + nt;
+        float4* s2 = s_edge + 2 * nt;
+        for (int jc = j0; jc < j1; jc += 3) {
+            row(f[0], f[1], f[2], r[0], u[0], v[0], r[1], u[1], v[1], u[2], v[2], s0, s1, jc);
+            if (jc + 1 < j1) row(f[1], f[2], f[0], r[1], u[1], v[1], r[2], u[2], v[2], u[0], v[0], s1, s2, jc + 1);
+            if (jc + 2 < j1) row(f[2], f[0], f[1], r[2], u[2], v[2], r[0], u[0], v[0], u[1], v[1], s2, s_edge, jc + 2);
+        }
+    } else {
+        // two population slots (A, B), no prefetch: row B is pulled in the step that
+        // needs its macros.  The march is unrolled by two; the (u, v) of the row below A
+        // is a copy, and the ring slot of each row is an index (rows rotate over three).
+        float f[2][kQ][VW], r[2][VW], u[2][VW], v[2][VW], uc[VW], vc[VW];
+        pull(f[1]);  // halo row below the strip: only its u,v are needed
+        macros_row(f[1], r[1], uc, vc);
+        advance();
+        pull(f[0]);  // row j0
+        macros_row(f[0], r[0], u[0], v[0]);
+        s_edge[t] = edges(u[0], v[0]);
+        int sa = 0;  // ring slot of row A
+        auto row = [&](float (&fa)[kQ][VW], float (&fb)[kQ][VW], float (&ra)[VW], float (&ua)[VW],
+                       float (&va)[VW], float (&rb)[VW], float (&ub)[VW], float (&vb)[VW]) {
+            advance();
+            pull(fb);  // row A+1: a strip row or the halo row above
+            macros_row(fb, rb, ub, vb);
+            const int sb = sa == 2 ? 0 : sa + 1;
+            s_edge[sb * nt + t] = edges(ub, vb);
+            __syncthreads();
+            finalise(fa, ra, ua, va, ub, vb, uc, vc, s_edge + sa * nt);
+#pragma unroll
+            for (int k = 0; k < VW; k++) {
+                uc[k] = ua[k];
+                vc[k] = va[k];
+            }
+            sa = sb;
+        };
+        for (int jc = j0; jc < j1; jc += 2) {
+            row(f[0], f[1], r[0], u[0], v[0], r[1], u[1], v[1]);
+            if (jc + 1 < j1) row(f[1], f[0], r[1], u[1], v[1], r[0], u[0], v[0]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Batched persistent stream-collide: one launch steps every experiment of a batch
 // (own grid, members, buffers, forcing and strip height).  The work items are
 // (experiment, member, strip, 128-column chunk); a grid sized to the GPU's resident
@@ -975,8 +1203,27 @@ StepKernel direct_kernel(const lbl_ctx* c) {
             return {(const void*)lbm_step_kernel<false, 1024, 0, T>, P.nx, sm};
     }
 }
+template <int VW, bool PF, typename T>
+StepKernel vec_kernel_w(const lbl_ctx* c) {
+    const Phys& P = c->P;
+    const int sq = (P.nx == P.ny) ? P.nx : 0;
+    const void* fn = sq == 64     ? (const void*)lbm_step_vec_kernel<false, 64, VW, PF, T>
+                     : sq == 128  ? (const void*)lbm_step_vec_kernel<false, 128, VW, PF, T>
+                     : sq == 256  ? (const void*)lbm_step_vec_kernel<false, 256, VW, PF, T>
+                     : sq == 512  ? (const void*)lbm_step_vec_kernel<false, 512, VW, PF, T>
+                     : sq == 1024 ? (const void*)lbm_step_vec_kernel<false, 1024, VW, PF, T>
+                                  : (const void*)lbm_step_vec_kernel<false, 0, VW, PF, T>;
+    return {fn, P.nx / VW, sizeof(float4) * 3 * (P.nx / VW)};
+}
+template <typename T>
+StepKernel vec_kernel_t(const lbl_ctx* c) {
+    if (c->vec == 2) return c->vec_pf ? vec_kernel_w<2, true, T>(c) : vec_kernel_w<2, false, T>(c);
+    return c->vec_pf ? vec_kernel_w<4, true, T>(c) : vec_kernel_w<4, false, T>(c);
+}
+StepKernel vec_kernel(const lbl_ctx* c) { return c->f16 ? vec_kernel_t<__half>(c) : vec_kernel_t<float>(c); }
 StepKernel step_kernel(const lbl_ctx* c) {
     const Phys& P = c->P;
+    if (c->vec && !c->closure) return vec_kernel(c);
     if (c->use_tma) {
         const int sq = (P.nx == P.ny) ? P.nx : 0;
         const void* fn = sq == 64    ? (const void*)lbm_step_tma_kernel<false, 64>
@@ -1193,6 +1440,51 @@ void launch_closure(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const
         launch_closure_t<MAXT, NX, float>(c, grid, ty, c->f[src], c->f[dst], force, mac_out, s, pdl, held);
 }
 
+// vector-load stream-collide (FP32 storage, nx a multiple of 32 up to 1024)
+template <int NX, int VW, bool PF, typename T>
+void launch_vec_s(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout, const float* force, float* mac_out,
+                  cudaStream_t s, bool pdl) {
+    const int nt = c->P.nx / VW;
+    const size_t sm = sizeof(float4) * 3 * nt;
+    if (mac_out)
+        launch_step(lbm_step_vec_kernel<true, NX, VW, PF, T>, grid, nt, sm, s, pdl, fin, fout, force, mac_out, c->P,
+                    ty);
+    else
+        launch_step(lbm_step_vec_kernel<false, NX, VW, PF, T>, grid, nt, sm, s, pdl, fin, fout, force,
+                    static_cast<float*>(nullptr), c->P, ty);
+}
+template <int NX, int VW, bool PF>
+void launch_vec_t(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
+                  cudaStream_t s, bool pdl) {
+    if (c->f16)
+        launch_vec_s<NX, VW, PF, __half>(c, grid, ty, c->h[src], c->h[dst], force, mac_out, s, pdl);
+    else
+        launch_vec_s<NX, VW, PF, float>(c, grid, ty, c->f[src], c->f[dst], force, mac_out, s, pdl);
+}
+template <int VW, bool PF>
+void launch_vec_w(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
+                  cudaStream_t s, bool pdl) {
+    const int sq = (c->P.nx == c->P.ny) ? c->P.nx : 0;
+    switch (sq) {
+        case 64: launch_vec_t<64, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        case 128: launch_vec_t<128, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        case 256: launch_vec_t<256, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        case 512: launch_vec_t<512, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        case 1024: launch_vec_t<1024, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        default: launch_vec_t<0, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl);
+    }
+}
+void launch_vec(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
+                cudaStream_t s, bool pdl) {
+    if (c->vec == 2) {
+        if (c->vec_pf) launch_vec_w<2, true>(c, grid, ty, src, dst, force, mac_out, s, pdl);
+        else launch_vec_w<2, false>(c, grid, ty, src, dst, force, mac_out, s, pdl);
+    } else {
+        if (c->vec_pf) launch_vec_w<4, true>(c, grid, ty, src, dst, force, mac_out, s, pdl);
+        else launch_vec_w<4, false>(c, grid, ty, src, dst, force, mac_out, s, pdl);
+    }
+}
+
 template <int MAXT, int NX>
 void launch_direct(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
                    cudaStream_t s, bool pdl) {
@@ -1238,6 +1530,10 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
         if (sq == 256) launch_closure<256, 256>(c, grid, ty, src, dst, force, mac_out, s, pdl, held);
         else if (P.nx <= 256) launch_closure<256, 0>(c, grid, ty, src, dst, force, mac_out, s, pdl, held);
         else launch_closure<1024, 0>(c, grid, ty, src, dst, force, mac_out, s, pdl, held);
+        return;
+    }
+    if (c->vec) {
+        launch_vec(c, grid, ty, src, dst, force, mac_out, s, pdl);
         return;
     }
     switch (sq) {

@@ -37,7 +37,7 @@ ERRORS = {
     -5: "LBL_ERR_NAN", -6: "LBL_ERR_STATE", -7: "LBL_ERR_NOMEM", -8: "LBL_ERR_UNSUPPORTED",
     -9: "LBL_ERR_NOCONV", -10: "LBL_ERR_TIMEOUT",
 }
-LBM_AUTO, LBM_DIRECT, LBM_TMA = 0, 1, 2
+LBM_AUTO, LBM_DIRECT, LBM_TMA, LBM_VEC, LBM_VEC2 = 0, 1, 2, 3, 4
 STORAGE_F32, STORAGE_F16 = 0, 1
 GRAM_F32, GRAM_BF16, GRAM_TF32X3 = 0, 1, 2
 
@@ -50,7 +50,7 @@ EXPORTS = (
     "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_timer_csv", "lbl_timer_clear",
     "lbl_timer_transit", "lbl_profile_step", "lbl_get_cycle_phases", "lbl_event_record", "lbl_event_elapsed",
     "lbl_letkf_analysis_noalloc", "lbl_bindiff", "lbl_ensemble_stat", "lbl_energy_spectrum",
-    "lbl_set_io_prefix", "lbl_h5_write_dataset", "lbl_autotune", "lbl_set_closure", "lbl_closure_generate",
+    "lbl_set_io_prefix", "lbl_h5_write_dataset", "lbl_autotune", "lbl_stream_collide_shape", "lbl_set_stream_collide_shape", "lbl_set_closure", "lbl_closure_generate",
     "lbl_closure_grad", "lbl_closure_train", "lbl_closure_infer", "lbl_batch_create", "lbl_batch_last_error",
     "lbl_batch_cycle_async", "lbl_batch_sync", "lbl_batch_destroy", "lbl_inject", "lbl_set_closure_refresh",
 )
@@ -158,6 +158,8 @@ def load_library() -> ctypes.CDLL:
         "lbl_energy_spectrum": (I, [F, F, I, I, D]),
         "lbl_set_io_prefix": (I, [P, ctypes.c_char_p]),
         "lbl_autotune": (I, [P, IP, D]),
+        "lbl_stream_collide_shape": (I, [P, IP, IP, IP]),
+        "lbl_set_stream_collide_shape": (I, [P, I, I]),
         "lbl_inject": (I, [P, I, I]),
         "lbl_set_closure_refresh": (I, [P, I]),
         "lbl_h5_write_dataset": (I, [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, P, I]),
@@ -353,6 +355,19 @@ class Ensemble:
         ty, ms = ctypes.c_int(), ctypes.c_double()
         self._check(self.lib.lbl_autotune(self._h, ctypes.byref(ty), ctypes.byref(ms)), "lbl_autotune")
         return ty.value, ms.value
+
+    def launch_shape(self) -> dict:
+        """The stream-collide launch shape (lbl_stream_collide_shape)."""
+        c, p, ty = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.lbl_stream_collide_shape(self._h, ctypes.byref(c), ctypes.byref(p), ctypes.byref(ty)),
+                    "lbl_stream_collide_shape")
+        return {"columns_per_thread": c.value, "prefetch": bool(p.value), "strip_rows": ty.value}
+
+    def set_launch_shape(self, prefetch: bool = True, strip_rows: int = 0):
+        """Set the stream-collide launch shape (lbl_set_stream_collide_shape); strip_rows 0
+        takes the heuristic's."""
+        self._check(self.lib.lbl_set_stream_collide_shape(self._h, int(bool(prefetch)), int(strip_rows)),
+                    "lbl_set_stream_collide_shape")
 
     def set_closure_refresh(self, steps: int):
         """Run the closure's network every `steps` steps and hold each cell's multiplier

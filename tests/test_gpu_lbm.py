@@ -207,6 +207,49 @@ def test_stream_collide_variants_agree(nx):
     np.testing.assert_allclose(out[lbl.LBM_TMA][2], ud, rtol=0, atol=1e-4 * np.max(np.abs(ud)))
 
 
+@pytest.mark.parametrize("nx,ny,members,variant,storage", [
+    (64, 64, 3, "LBM_VEC", 0), (64, 64, 3, "LBM_VEC2", 0), (128, 128, 2, "LBM_VEC", 0), (256, 256, 2, "LBM_VEC", 0),
+    (256, 256, 2, "LBM_VEC2", 0), (96, 40, 2, "LBM_VEC", 0), (32, 8, 2, "LBM_VEC", 0), (512, 512, 1, "LBM_VEC", 0),
+    (1024, 64, 1, "LBM_VEC2", 0), (256, 256, 2, "LBM_VEC2", 1), (512, 512, 1, "LBM_VEC", 1), (96, 40, 2, "LBM_VEC2", 1),
+    (64, 64, 3, "LBM_VEC", 1)])
+def test_vector_stream_collide_is_bit_identical(nx, ny, members, variant, storage):
+    """The vector-load stream-collide (4 or 2 columns per thread) does each cell's
+    arithmetic in the same explicitly rounded sequence as the one-column kernel, so
+    populations and macros agree bit for bit, in FP32 and in FP16 deviation storage,
+    with and without the prefetched row and whatever the strip height.  The sizes
+    cover every compiled grid width and the run-time one (96 x 40, 1024 x 64, and
+    32 x 8, where one thread holds a quarter of the row)."""
+    out = {}
+    cfg = dict(ny=ny, storage=storage)
+    e = lbl.Ensemble(lbl.config_default("NATURE", nx, members, lbm_variant=lbl.LBM_DIRECT, **cfg))
+    e.init(0)
+    e.update(0, 25)
+    ref = [e.get_f(m) for m in range(members)] + [a for m in range(members) for a in e.get_fields(m)[:3]]
+    e.close()
+    for prefetch, strip in ((True, 0), (False, 0), (True, 5), (False, 3)):
+        e = lbl.Ensemble(lbl.config_default("NATURE", nx, members, lbm_variant=getattr(lbl, variant), **cfg))
+        e.set_launch_shape(prefetch, strip)
+        shape = e.launch_shape()
+        assert shape["columns_per_thread"] == (4 if variant == "LBM_VEC" else 2) and shape["prefetch"] == prefetch
+        e.init(0)
+        e.update(0, 25)
+        out = [e.get_f(m) for m in range(members)] + [a for m in range(members) for a in e.get_fields(m)[:3]]
+        e.close()
+        for a, b in zip(ref, out):
+            np.testing.assert_array_equal(a, b)
+
+
+def test_vector_stream_collide_rejects_what_it_does_not_serve():
+    with pytest.raises(lbl.LblError, match="nx <= 1024"):
+        lbl.Ensemble(lbl.config_default("NATURE", 2048, 1, lbm_variant=lbl.LBM_VEC))
+    e = lbl.Ensemble(lbl.config_default("NATURE", 64, 1, lbm_variant=lbl.LBM_DIRECT))
+    with pytest.raises(lbl.LblError, match="without prefetch"):
+        e.set_launch_shape(False, 0)
+    with pytest.raises(lbl.LblError, match="strip_rows"):
+        e.set_launch_shape(True, 65)
+    e.close()
+
+
 @pytest.mark.parametrize("fixture,physics", [("ref_longrun_id0.npz", {}),
                                              ("ref_longrun_c0_id0.npz", dict(cs=0.1, tau=0.51))])
 def test_long_run_statistics_match_reference(fixture, physics):
