@@ -718,7 +718,8 @@ def run_batch(args):
         e.init(0)
         e.cycle_async(0, None, None, None, T)
         e.cycle_async(T, *obs[0], T)  # observations resident from here on
-        exps.append({"nx": nx, "M": m, "ens": e, "strip_rows": ty, "ms_per_lbm_launch_tuned": ms_tuned})
+        exps.append({"nx": nx, "M": m, "ens": e, "strip_rows": ty, "ms_per_lbm_launch_tuned": ms_tuned,
+                     "shape": e.launch_shape()})
     for c in range(W):
         for x in exps:
             x["ens"].cycle_async((c + 2) * T, None, None, None, T)
@@ -744,7 +745,7 @@ def run_batch(args):
                        ", obs every 4th point, GC radius 4 cells, inflation 1.1, 100 LBM steps + 1 analysis per cycle",
                        "concurrency": "one context, stream and per-cycle CUDA graph per experiment"},
             "glups": lu / (ms / 1e3) / 1e9,
-            "experiments": [{"nx": x["nx"], "M": x["M"], "strip_rows": x["strip_rows"],
+            "experiments": [{"nx": x["nx"], "M": x["M"], "strip_rows": x["strip_rows"], "shape": x["shape"],
                              "ms_per_lbm_launch_tuned": x["ms_per_lbm_launch_tuned"],
                              "ms_per_cycle_in_batch": spans[i] / K} for i, x in enumerate(exps)]}
     for x in exps:
