@@ -471,6 +471,7 @@ int lbl_set_closure(lbl_ctx* ctx, const float* params, double nu_ref, double dx_
     ctx->closure_sc.dx_ref = dx_ref > 0 ? float(dx_ref) : float(ctx->cfg.h_ref / 255.0);
     ctx->closure = true;
     ctx->ty_default = lbm_strip_rows(ctx);
+    ctx->ty_held = ctx->closure_every > 1 ? lbm_strip_rows_held(ctx) : 0;
     return LBL_OK;
 }
 
@@ -502,6 +503,7 @@ int lbl_set_closure_refresh(lbl_ctx* ctx, int steps) {
         ctx->d_mclos = nullptr;
     }
     ctx->closure_every = steps;
+    ctx->ty_held = steps > 1 ? lbm_strip_rows_held(ctx) : 0;
     return LBL_OK;
 }
 

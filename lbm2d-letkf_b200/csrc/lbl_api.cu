@@ -1413,6 +1413,7 @@ int lbl_set_stream_collide_shape(lbl_ctx* ctx, int prefetch, int strip_rows) {
     if (vec) ctx->vec_pf = prefetch == 1;
     ctx->ty_tuned = strip_rows;
     ctx->ty_default = lbm_strip_rows(ctx);
+    if (ctx->closure && ctx->closure_every > 1) ctx->ty_held = lbm_strip_rows_held(ctx);
     return LBL_OK;
 }
 

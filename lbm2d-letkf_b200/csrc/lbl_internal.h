@@ -136,6 +136,7 @@ struct lbl_ctx {
     int vec = 0;                         // columns per thread of the vector-load stream-collide (0: one)
     bool vec_pf = false;                 // its march prefetches the row after next
     bool vec_auto = false;               // LBL_LBM_AUTO: lbl_autotune may change the columns per thread
+    int ty_held = 0;                     // strip height of the closure's held-multiplier steps (0: ty's)
     int ty_tuned = 0;                    // stream-collide strip height chosen by lbl_autotune (0: heuristic)
     int ty_default = 0;                  // the heuristic's strip height for the kernel that runs
     int* d_err = nullptr;                // bounded-wait timeout flag of the TMA kernel
@@ -183,6 +184,7 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
 // strip height of the stream-collide for this grid, ensemble and kernel variant
 // (occupancy heuristic); call outside stream capture
 int lbm_strip_rows(const lbl_ctx* c);
+int lbm_strip_rows_held(const lbl_ctx* c);  // for the closure's held-multiplier steps
 // fill both population buffers with the rest state (rho = rho_ref, u = v = 0)
 void launch_rest_state(const lbl_ctx* c, cudaStream_t s);
 // FP16 deviation storage <-> FP32 populations, all members

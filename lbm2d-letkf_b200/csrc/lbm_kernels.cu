@@ -200,32 +200,44 @@ __device__ __forceinline__ float les_omega(float ue, float uw, float ve, float v
 
 // Learned closure: the same central differences as les_omega_v give the features,
 // the warp's tensor cores evaluate the MLP for its 32 cells, and the multiplier m
-// scales the Smagorinsky eddy viscosity: nu_t = m cs^2 dx^2 |S|.
+// scales the Smagorinsky eddy viscosity: nu_t = m cs^2 dx^2 |S|.  The strain, |S| and
+// the relaxation time are explicitly rounded operations shared by the evaluating and
+// the held form, so that every kernel running them (one column or two per thread)
+// rounds alike, whatever contractions the compiler would choose.
+struct ClosureStrain {
+    float ux, uy, vx, vy;
+};
+__device__ __forceinline__ ClosureStrain closure_strain(float ue, float uw, float ve, float vw, float un, float us,
+                                                        float vn, float vs, const Phys& P) {
+    return {__fmul_rn(__fsub_rn(ue, uw), P.inv_two_dx), __fmul_rn(__fsub_rn(un, us), P.inv_two_dx),
+            __fmul_rn(__fsub_rn(ve, vw), P.inv_two_dx), __fmul_rn(__fsub_rn(vn, vs), P.inv_two_dx)};
+}
+// |S| = sqrt(2 S:S)
+__device__ __forceinline__ float closure_smag(const ClosureStrain& g) {
+    const float s12 = __fmul_rn(0.5f, __fadd_rn(g.uy, g.vx));
+    const float ss = __fmaf_rn(g.ux, g.ux, __fmaf_rn(__fmul_rn(2.f, s12), s12, __fmul_rn(g.vy, g.vy)));
+    return closure_sqrt(__fmul_rn(2.f, ss));
+}
+// omega = 1/tau, tau = 0.5 + 3 (nu + m nu_smag) / c^2 / dt
+__device__ __forceinline__ float closure_relax(float m, float smag, const Phys& P) {
+    const float nus = __fmul_rn(m, float(P.les_k * double(smag)));
+    const float tau = float(fma(double(__fadd_rn(P.nu, nus)), P.tau_k, 0.5));
+    return __frcp_rn(tau);
+}
 __device__ __forceinline__ float closure_omega(float ue, float uw, float ve, float vw, float un, float us, float vn,
                                                float vs, const Phys& P, const ClosureScales& csc,
                                                const uint32_t* pack, uint32_t* stage, float& m) {
-    const float ux = (ue - uw) * P.inv_two_dx, uy = (un - us) * P.inv_two_dx;
-    const float vx = (ve - vw) * P.inv_two_dx, vy = (vn - vs) * P.inv_two_dx;
+    const ClosureStrain g = closure_strain(ue, uw, ve, vw, un, us, vn, vs, P);
     float feat[kMlpIn];
-    const float smag = closure_features_fast(ux, uy, vx, vy, csc, feat);
+    closure_features_fast(g.ux, g.uy, g.vx, g.vy, csc, feat);
     m = mlp_forward_warp(pack, stage, feat);
-    const float nus = m * float(P.les_k * double(smag));
-    const float tau = float(fma(double(P.nu + nus), P.tau_k, 0.5));
-    return __frcp_rn(tau);
+    return closure_relax(m, closure_smag(g), P);
 }
 // The closure between two evaluations of the network (lbl_set_closure_refresh): the
-// cell's multiplier m from the last evaluation, |S| of this step, the same |S| and
-// relaxation arithmetic as closure_omega.
+// cell's multiplier m from the last evaluation, |S| of this step.
 __device__ __forceinline__ float closure_omega_held(float ue, float uw, float ve, float vw, float un, float us,
                                                     float vn, float vs, const Phys& P, float m) {
-    const float ux = (ue - uw) * P.inv_two_dx, uy = (un - us) * P.inv_two_dx;
-    const float vx = (ve - vw) * P.inv_two_dx, vy = (vn - vs) * P.inv_two_dx;
-    const float s11 = ux, s22 = vy, s12 = 0.5f * (uy + vx);
-    const float ss = fmaf(s11, s11, fmaf(2.f * s12, s12, s22 * s22));
-    const float smag = closure_sqrt(2.f * ss);
-    const float nus = m * float(P.les_k * double(smag));
-    const float tau = float(fma(double(P.nu + nus), P.tau_k, 0.5));
-    return __frcp_rn(tau);
+    return closure_relax(m, closure_smag(closure_strain(ue, uw, ve, vw, un, us, vn, vs, P)), P);
 }
 
 // ---------------------------------------------------------------------------
@@ -675,10 +687,12 @@ struct VecIO<__half, VW> {
     }
 };
 
-template <bool WRITE_MAC, int NX, int VW, bool PF, typename T>
+// CLH: the learned closure between two evaluations of its network, each cell's
+// multiplier read from mclos (lbm_step_kernel's CLH form, cell for cell)
+template <bool WRITE_MAC, int NX, int VW, bool PF, typename T, bool CLH = false>
 __global__ void __launch_bounds__(NX ? NX / VW : 1024 / VW)
     lbm_step_vec_kernel(const T* __restrict__ fin, T* __restrict__ fout, const float* __restrict__ force,
-                        float* __restrict__ mac, Phys P, int TY) {
+                        float* __restrict__ mac, Phys P, int TY, const float* __restrict__ mclos) {
     extern __shared__ float4 s_edge[];  // [3][nt]: (u, v) of the first and of the last column
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" :::);
@@ -740,14 +754,19 @@ __global__ void __launch_bounds__(NX ? NX / VW : 1024 / VW)
                         const float (&ub)[VW], const float (&vb)[VW], const float (&uc)[VW], const float (&vc)[VW],
                         const float4* sa) {
         const float4 em = sa[tm], ep = sa[tp];  // the neighbours' edge columns of row A
-        float fx[VW], fy[VW];
+        float fx[VW], fy[VW], mh[VW];
         VecIO<float, VW>::ld(force + ij, fx, 0.f);
         VecIO<float, VW>::ld(force + nxy + ij, fy, 0.f);
+        if constexpr (CLH) VecIO<float, VW>::ld(mclos + size_t(m) * nxy + ij, mh, 0.f);
 #pragma unroll
         for (int k = 0; k < VW; k++) {
             const float ue = k < VW - 1 ? ua[k + 1] : ep.x, ve = k < VW - 1 ? va[k + 1] : ep.y;
             const float uw = k > 0 ? ua[k - 1] : em.z, vw = k > 0 ? va[k - 1] : em.w;
-            const float omega = les_omega(ue, uw, ve, vw, ub[k], uc[k], vb[k], vc[k], P);
+            float omega;
+            if constexpr (CLH)
+                omega = closure_omega_held(ue, uw, ve, vw, ub[k], uc[k], vb[k], vc[k], P, mh[k]);
+            else
+                omega = les_omega(ue, uw, ve, vw, ub[k], uc[k], vb[k], vc[k], P);
             float g[kQ];
 #pragma unroll
             for (int q = 0; q < kQ; q++) g[q] = fa[q][k];
@@ -1236,13 +1255,31 @@ StepKernel step_kernel(const lbl_ctx* c) {
     return c->f16 ? direct_kernel<__half>(c) : direct_kernel<float>(c);
 }
 
+// The closure's held-multiplier steps run the two-column vector-load kernel when the
+// context's plain steps do (with the prefetched row, grids up to 256 columns wide), else
+// lbm_step_kernel's CLH form.
+bool held_vec(const lbl_ctx* c) { return c->vec == 2 && c->vec_pf && c->P.nx <= 256; }
+template <typename T>
+StepKernel held_kernel_t(const lbl_ctx* c) {
+    const Phys& P = c->P;
+    const int sq = (P.nx == P.ny) ? P.nx : 0;
+    if (held_vec(c))
+        return {sq == 256 ? (const void*)lbm_step_vec_kernel<false, 256, 2, true, T, true>
+                          : (const void*)lbm_step_vec_kernel<false, 0, 2, true, T, true>,
+                P.nx / 2, sizeof(float4) * 3 * (P.nx / 2)};
+    const size_t sm = sizeof(float) * 6 * P.nx;
+    if (sq == 256) return {(const void*)lbm_step_kernel<false, 256, 256, T, false, false, true>, P.nx, sm};
+    if (P.nx <= 256) return {(const void*)lbm_step_kernel<false, 256, 0, T, false, false, true>, P.nx, sm};
+    return {(const void*)lbm_step_kernel<false, 1024, 0, T, false, false, true>, P.nx, sm};
+}
+StepKernel held_kernel(const lbl_ctx* c) { return c->f16 ? held_kernel_t<__half>(c) : held_kernel_t<float>(c); }
+
 // Strip height: fill the GPU's resident CTA slots with as few waves as possible,
 // counting the two halo rows each strip pulls.  Queried outside stream capture (at
 // context creation and when the closure is switched), for the kernel that runs: an
 // occupancy query inside a capture may fail and must not decide the launch shape.
-int strip_rows(const lbl_ctx* c) {
+int strip_rows_for(const lbl_ctx* c, const StepKernel& k) {
     const Phys& P = c->P;
-    const StepKernel k = step_kernel(c);
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1261,6 +1298,7 @@ int strip_rows(const lbl_ctx* c) {
     }
     return best;
 }
+int strip_rows(const lbl_ctx* c) { return strip_rows_for(c, step_kernel(c)); }
 
 }  // namespace
 
@@ -1413,7 +1451,32 @@ void launch_closure_t(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout
     const Phys& P = c->P;
     const uint32_t* pk = c->d_closure;
     float* mc = c->d_mclos;  // null when the network runs every step
+    if (held && held_vec(c)) {  // the multipliers of the last evaluation, two columns per thread
+        const int nt = P.nx / 2;
+        const int tyh = c->ty_held > 0 ? c->ty_held : ty;
+        const dim3 gh((P.ny + tyh - 1) / tyh, P.M);
+        const size_t sm = sizeof(float4) * 3 * nt;
+        if (NX == 256) {
+            if (mac_out)
+                launch_step(lbm_step_vec_kernel<true, 256, 2, true, T, true>, gh, nt, sm, s, pdl, fin, fout, force,
+                            mac_out, P, tyh, static_cast<const float*>(mc));
+            else
+                launch_step(lbm_step_vec_kernel<false, 256, 2, true, T, true>, gh, nt, sm, s, pdl, fin, fout, force,
+                            static_cast<float*>(nullptr), P, tyh, static_cast<const float*>(mc));
+        } else {
+            if (mac_out)
+                launch_step(lbm_step_vec_kernel<true, 0, 2, true, T, true>, gh, nt, sm, s, pdl, fin, fout, force,
+                            mac_out, P, tyh, static_cast<const float*>(mc));
+            else
+                launch_step(lbm_step_vec_kernel<false, 0, 2, true, T, true>, gh, nt, sm, s, pdl, fin, fout, force,
+                            static_cast<float*>(nullptr), P, tyh, static_cast<const float*>(mc));
+        }
+        return;
+    }
     if (held) {  // the plain kernel's cost: the multipliers of the last evaluation
+        const int tyh = c->ty_held > 0 ? c->ty_held : ty;
+        grid = dim3((P.ny + tyh - 1) / tyh, P.M);
+        ty = tyh;
         const size_t sm = sizeof(float) * 6 * P.nx;
         if (mac_out)
             launch_step(lbm_step_kernel<true, MAXT, NX, T, false, false, true>, grid, P.nx, sm, s, pdl, fin, fout,
@@ -1448,10 +1511,10 @@ void launch_vec_s(const lbl_ctx* c, dim3 grid, int ty, const T* fin, T* fout, co
     const size_t sm = sizeof(float4) * 3 * nt;
     if (mac_out)
         launch_step(lbm_step_vec_kernel<true, NX, VW, PF, T>, grid, nt, sm, s, pdl, fin, fout, force, mac_out, c->P,
-                    ty);
+                    ty, static_cast<const float*>(nullptr));
     else
         launch_step(lbm_step_vec_kernel<false, NX, VW, PF, T>, grid, nt, sm, s, pdl, fin, fout, force,
-                    static_cast<float*>(nullptr), c->P, ty);
+                    static_cast<float*>(nullptr), c->P, ty, static_cast<const float*>(nullptr));
 }
 template <int NX, int VW, bool PF>
 void launch_vec_t(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
@@ -1549,6 +1612,7 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
 }
 
 int lbm_strip_rows(const lbl_ctx* c) { return strip_rows(c); }
+int lbm_strip_rows_held(const lbl_ctx* c) { return strip_rows_for(c, held_kernel(c)); }
 
 void launch_batch_step(const BatchExp* exps, int n_exp, int total, int step, int* counter, int grid, bool mac,
                        bool pdl, cudaStream_t s) {

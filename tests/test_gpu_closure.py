@@ -203,6 +203,27 @@ def test_held_multiplier_equals_evaluation_for_a_constant_network():
         np.testing.assert_array_equal(out[0][m], out[1][m])
 
 
+@pytest.mark.parametrize("storage", [0, 1])
+def test_held_steps_vector_kernel_is_bit_identical(storage):
+    """The held-multiplier steps run the two-column vector-load kernel when the context's
+    plain steps do (LBL_LBM_AUTO at 256 columns) and lbm_step_kernel's CLH form under
+    LBL_LBM_DIRECT: same populations bit for bit, FP32 and FP16 storage."""
+    from lbl import closure
+    w, meta = closure.load_params()
+    out = {}
+    for v in (lbl.LBM_DIRECT, lbl.LBM_AUTO):
+        e = lbl.Ensemble(lbl.config_default("NATURE", 256, 2, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP, ic_amp=1.0,
+                                            lbm_variant=v, storage=storage))
+        e.init(0)
+        e.set_closure(w, meta["nu_ref"], meta["dx_ref"])
+        e.set_closure_refresh(10)
+        e.update(0, 47)
+        out[v] = [e.get_f(m) for m in range(2)] + [a for m in range(2) for a in e.get_fields(m)[:3]]
+        e.close()
+    for a, b in zip(out[lbl.LBM_DIRECT], out[lbl.LBM_AUTO]):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_held_multiplier_follows_the_network():
     """With the trained network, holding the multipliers for 10 steps stays close to
     evaluating every step (populations within 1e-4 relative after 100 steps; they differ,
