@@ -214,6 +214,18 @@ int lbl_get_diagnostics(lbl_ctx* ctx, int member, double* energy, double* enstro
 /* RMSE of the ensemble-mean (u,v) against host truth fields (FP64). */
 int lbl_rmse_uv(lbl_ctx* ctx, const float* u_true, const float* v_true, double* rmse);
 
+/* lbl_rmse_uv without waiting: enqueues the upload of the true fields, the FP64
+ * reduction and the copy of the RMSE into *rmse on the context's stream and returns.
+ * u_true, v_true and rmse must stay valid (and the fields unchanged) until the stream
+ * has passed this point (lbl_sync, an lbl_event_elapsed on a later event, or the next
+ * blocking call); in pinned host memory the copies are asynchronous. */
+int lbl_rmse_uv_async(lbl_ctx* ctx, const float* u_true, const float* v_true, double* rmse);
+
+/* The context's CUDA stream (a cudaStream_t), for ordering a caller's own device work
+ * with the context's: work the caller enqueues on it runs between the context's calls
+ * in submission order.  Valid until lbl_destroy. */
+void* lbl_get_stream(lbl_ctx* ctx);
+
 /* Profiling: n back-to-back launches of the fused stream-collide kernel on the
  * context's stream, timed with CUDA events; *ms_per_launch = average per launch.
  * The state advances by n steps with the last computed force field. */

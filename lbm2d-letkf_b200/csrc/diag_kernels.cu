@@ -125,4 +125,10 @@ void launch_rmse(const lbl_ctx* c, const float* mac, const float* ut, const floa
     rmse_kernel<<<(c->P.nxy + 255) / 256, 256, 0, s>>>(mac, c->P.nxy, c->P.M, ut, vt, red);
 }
 
+// red[1] = sqrt(red[0] / nxy), the RMSE the host would form (IEEE division and square root)
+__global__ void rmse_finish_kernel(double* red, int nxy) { red[1] = sqrt(red[0] / double(nxy)); }
+void launch_rmse_finish(const lbl_ctx* c, double* red, cudaStream_t s) {
+    rmse_finish_kernel<<<1, 1, 0, s>>>(red, c->P.nxy);
+}
+
 }  // namespace lbl

@@ -1305,6 +1305,21 @@ int lbl_rmse_uv(lbl_ctx* ctx, const float* u_true, const float* v_true, double* 
     return LBL_OK;
 }
 
+int lbl_rmse_uv_async(lbl_ctx* ctx, const float* u_true, const float* v_true, double* rmse) {
+    if (!ctx || !u_true || !v_true || !rmse) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    const size_t nxy = size_t(ctx->P.nxy);
+    LBL_CK(cudaMemcpyAsync(ctx->d_tmp, u_true, sizeof(float) * nxy, cudaMemcpyHostToDevice, ctx->stream));
+    LBL_CK(cudaMemcpyAsync(ctx->d_tmp + nxy, v_true, sizeof(float) * nxy, cudaMemcpyHostToDevice, ctx->stream));
+    launch_rmse(ctx, ctx->mac[ctx->cur], ctx->d_tmp, ctx->d_tmp + nxy, ctx->d_red, ctx->stream);
+    launch_rmse_finish(ctx, ctx->d_red, ctx->stream);
+    LBL_CK(cudaGetLastError());
+    LBL_CK(cudaMemcpyAsync(rmse, ctx->d_red + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    return LBL_OK;
+}
+
+void* lbl_get_stream(lbl_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
 int lbl_profile_step(lbl_ctx* ctx, int n, double* ms_per_launch) {
     if (!ctx || n < 1 || !ms_per_launch) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));

@@ -277,6 +277,7 @@ void launch_diag(const lbl_ctx* c, const float* mac, int member, double* red, cu
 void launch_output_fields(const lbl_ctx* c, const float* mac, float* vor, float* stats, int* nan, cudaStream_t s);
 void launch_rmse(const lbl_ctx* c, const float* mac, const float* ut, const float* vt, double* red,
                  cudaStream_t s);
+void launch_rmse_finish(const lbl_ctx* c, double* red, cudaStream_t s);
 
 // ---- host helpers (host_io.cpp) ----
 std::string to_string_aligned(int t, int digits);

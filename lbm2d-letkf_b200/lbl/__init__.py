@@ -47,7 +47,7 @@ EXPORTS = (
     "lbl_update", "lbl_update_async", "lbl_assimilate", "lbl_assimilate_async", "lbl_assimilate_files",
     "lbl_cycle_async", "lbl_sync", "lbl_output", "lbl_output_async", "lbl_get_f", "lbl_set_f", "lbl_get_fields",
     "lbl_get_ens_stats", "lbl_get_force", "lbl_get_force_state", "lbl_get_observed",
-    "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_timer_csv", "lbl_timer_clear",
+    "lbl_get_letkf_stats", "lbl_get_diagnostics", "lbl_rmse_uv", "lbl_rmse_uv_async", "lbl_get_stream", "lbl_timer_csv", "lbl_timer_clear",
     "lbl_timer_transit", "lbl_profile_step", "lbl_get_cycle_phases", "lbl_event_record", "lbl_event_elapsed",
     "lbl_letkf_analysis_noalloc", "lbl_bindiff", "lbl_ensemble_stat", "lbl_energy_spectrum",
     "lbl_set_io_prefix", "lbl_h5_write_dataset", "lbl_autotune", "lbl_stream_collide_shape", "lbl_set_stream_collide_shape", "lbl_set_closure", "lbl_closure_generate",
@@ -134,6 +134,8 @@ def load_library() -> ctypes.CDLL:
         "lbl_get_letkf_stats": (I, [P, IP, IP, IP, IP]),
         "lbl_get_diagnostics": (I, [P, I, D, D, D]),
         "lbl_rmse_uv": (I, [P, F, F, D]),
+        "lbl_rmse_uv_async": (I, [P, F, F, D]),
+        "lbl_get_stream": (P, [P]),
         "lbl_set_closure": (I, [P, F, ctypes.c_double, ctypes.c_double]),
         "lbl_closure_generate": (I, [CP, I, I, I, I, I, F, F, U, ctypes.POINTER(U), ctypes.c_char_p, U]),
         "lbl_closure_grad": (I, [F, F, F, U, I, F, F]),
@@ -335,6 +337,25 @@ class Ensemble:
         r = ctypes.c_double()
         self._check(self.lib.lbl_rmse_uv(self._h, _fp(ut), _fp(vt), ctypes.byref(r)), "lbl_rmse_uv")
         return r.value
+
+    def rmse_uv_async(self, u_true: np.ndarray, v_true: np.ndarray, out: np.ndarray, index: int = 0):
+        """lbl_rmse_uv_async: enqueue the RMSE of the ensemble mean (u, v) against the true
+        fields; out[index] (a float64 array, pinned for an asynchronous copy) holds it once
+        the context's stream has passed this point (sync(), or event_elapsed on a later
+        event).  u_true and v_true must be contiguous float32 arrays of nx*ny values that
+        stay alive and unchanged until then."""
+        for a in (u_true, v_true):
+            if a.dtype != np.float32 or not a.flags["C_CONTIGUOUS"] or a.size != self.nxy:
+                raise ValueError("rmse_uv_async needs contiguous float32 arrays of nx*ny values")
+        if out.dtype != np.float64 or not 0 <= index < out.size:
+            raise ValueError("out must be a float64 array with a slot at index")
+        ptr = ctypes.cast(out.ctypes.data + 8 * index, ctypes.POINTER(ctypes.c_double))
+        self._check(self.lib.lbl_rmse_uv_async(self._h, _fp(u_true), _fp(v_true), ptr), "lbl_rmse_uv_async")
+
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer (lbl_get_stream), e.g. for
+        torch.cuda.ExternalStream."""
+        return int(self.lib.lbl_get_stream(self._h) or 0)
 
     def timer_csv(self, which: int = TIMER_MAIN) -> str:
         n = self.lib.lbl_timer_csv(self._h, which, None, 0)

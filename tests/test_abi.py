@@ -17,7 +17,7 @@ HEADER = os.path.join(ROOT, "include", "lbl.h")
 
 def declared_functions():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?(?:int|char\s*\*|const char\*)\s*\**\s*(lbl_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?(?:int|void|char\s*\*|const char\*)\s*\**\s*(lbl_\w+)\s*\(", text, re.M)))
 
 
 def test_header_declares_the_exported_set():

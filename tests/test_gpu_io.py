@@ -150,3 +150,40 @@ def test_driver_observe_then_letkf(tmp_path):
     for k in range(4):
         assert os.path.exists(f"{pre}/calc/ens{k:04d}/vor_step0000000020.dat")
     assert os.path.exists(f"{pre}/calc/ens_vor_std_step0000000020.dat")
+
+
+def test_async_rmse_equals_the_blocking_one():
+    """lbl_rmse_uv_async enqueues what lbl_rmse_uv does and leaves the value in the
+    caller's (pinned) double; it equals the blocking form (to the rounding of an FP64
+    sum accumulated in no fixed order) after the stream has passed it.  lbl_get_stream hands out the
+    context's stream, on which a caller's own work runs in submission order."""
+    torch = pytest.importorskip("torch")
+    e = lbl.Ensemble(lbl.config_default("NATURE", 128, 3))
+    e.init(0)
+    rng = np.random.default_rng(5)
+    truth = [tuple(torch.from_numpy(rng.standard_normal((128, 128)).astype(np.float32) * 0.01).pin_memory().numpy()
+                   for _ in range(2)) for _ in range(3)]
+    out = torch.zeros(3, dtype=torch.float64).pin_memory().numpy()
+    ref = []
+    for k in range(3):
+        e.update(k * 5, 5)
+        ref.append(e.rmse_uv(*truth[k]))
+    e2 = lbl.Ensemble(lbl.config_default("NATURE", 128, 3))
+    e2.init(0)
+    for k in range(3):
+        e2.update(k * 5, 5)
+        e2.rmse_uv_async(*truth[k], out, k)
+    e2.sync()
+    # the FP64 sum is accumulated with atomics, in no fixed order: equal to rounding
+    np.testing.assert_allclose(out, np.array(ref), rtol=1e-12, atol=0)
+    s = e2.stream()
+    assert s != 0
+    buf = torch.zeros(1 << 20, device="cuda:0")
+    with torch.cuda.stream(torch.cuda.ExternalStream(s, device="cuda:0")):
+        buf.fill_(2.0)
+    e2.sync()
+    assert float(buf.sum()) == 2.0 * (1 << 20)
+    with pytest.raises(ValueError):
+        e2.rmse_uv_async(truth[0][0].astype(np.float64), truth[0][1], out, 0)
+    e.close()
+    e2.close()
