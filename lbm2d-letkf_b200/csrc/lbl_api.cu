@@ -1396,6 +1396,7 @@ int lbl_autotune(lbl_ctx* ctx, int* strip_rows_out, double* ms_per_launch) {
     }
     ctx->vec = best_form.vec;
     ctx->vec_pf = best_form.pf;
+    ctx->ty_default = lbm_strip_rows(ctx);  // the heuristic's height for the kept form
     ctx->ty_tuned = best;
     LBL_TRY(check_timeout(ctx));
     if (strip_rows_out) *strip_rows_out = best;

@@ -626,7 +626,8 @@ __global__ void __launch_bounds__(MAXT, MAXT == 256 ? (CL ? 2 : 4) : 1)
 // ---------------------------------------------------------------------------
 // Vector-load stream-collide: lbm_step_kernel's column march with each thread owning
 // VW consecutive columns x0 .. x0+VW-1.  Every population row of the pull is one
-// VW-wide load (VW = 4: 128 bits) of the thread's own columns; a direction with
+// VW-wide load of the thread's own columns (FP32 rows: 64 bits at VW = 2, 128 bits
+// at VW = 4; FP16 deviations: 32 or 64 bits, widened as Store<__half> does); a direction with
 // ex = +1 pulls from x-1, so its VW values shift up by one column in registers and
 // the column x0-1 comes in as one scalar load (ex = -1 mirrors that with x0+VW).
 // The analysis populations, the macros and the forcing move as VW-wide loads and
