@@ -947,7 +947,12 @@ __global__ void __launch_bounds__(kWideThreads, TC ? 4 : 5) analysis_wide_kernel
                                     sSc[cb] = sb;
                                 }
                             }
-                            __syncthreads();
+                            // from level 2 on a block's H <= 8 quads are one warp, and only
+                            // they touch its columns until the level ends
+                            if (L >= 2)
+                                __syncwarp();
+                            else
+                                __syncthreads();
                             cb = 2 * H * b + H + ((i + j + 1) & (H - 1));
                             wide_load16(xb, sA + 2 * cb * kHS + hoff);
                             nb = sN[cb];
