@@ -1,6 +1,6 @@
 // ref_letkf_glue.cu -- ORACLE TOOLING (test infrastructure only).
 //
-// The glue half of the reference-side LETKF checker (ref_letkf_harness.cu holds the
+// The glue half of the reference-side LETKF checker (ref_letkf_solver.cu holds the
 // solver half and describes the whole).  This translation unit includes the
 // reference's src/config.h and src/lbm.h unmodified, compiled where they lie with the
 // reference's nvcc flags and -D knobs (oracle/Makefile), and restates letkf.cu's glue
@@ -128,6 +128,9 @@ namespace glue {
 int n_obs_total() { return n_obs; }
 int n_obs_side() { return n_obs_x; }
 float inflation() { return beta; }
+int xyprune() { return ::xyprune; }
+float obs_error_u() { return config::obs_error_u; }
+float obs_error_rho() { return config::obs_error_rho; }
 void pack_xk(const float* f, float* xk, int nxy) {
     k_pack_xk<<<dim3((unsigned(nxy) + 255) / 256, config::Q), 256>>>(f, xk, nxy);
 }
