@@ -239,6 +239,27 @@ def test_vector_stream_collide_is_bit_identical(nx, ny, members, variant, storag
             np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("nx,members,storage", [(128, 4, 0), (256, 2, 1)])
+def test_autotuned_shape_is_reported_and_bit_identical(nx, members, storage):
+    """lbl_autotune on an LBL_LBM_AUTO context picks the columns per thread (1, 2 or 4),
+    the march form and the strip height; lbl_stream_collide_shape reports the pick, and
+    the run equals the one-column kernel's bit for bit."""
+    ref = lbl.Ensemble(lbl.config_default("NATURE", nx, members, lbm_variant=lbl.LBM_DIRECT, storage=storage))
+    ref.init(0)
+    ref.update(0, 30)
+    e = lbl.Ensemble(lbl.config_default("NATURE", nx, members, storage=storage))
+    ty, ms = e.autotune()
+    shape = e.launch_shape()
+    assert shape["columns_per_thread"] in (1, 2, 4) and shape["strip_rows"] == ty and ms > 0
+    assert shape["prefetch"] or shape["columns_per_thread"] > 1
+    e.init(0)
+    e.update(0, 30)
+    for m in range(members):
+        np.testing.assert_array_equal(e.get_f(m), ref.get_f(m))
+    e.close()
+    ref.close()
+
+
 def test_vector_stream_collide_rejects_what_it_does_not_serve():
     with pytest.raises(lbl.LblError, match="nx <= 1024"):
         lbl.Ensemble(lbl.config_default("NATURE", 2048, 1, lbm_variant=lbl.LBM_VEC))
