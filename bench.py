@@ -535,6 +535,29 @@ def reference_build_line(args):
                     "so its cycles/s is below this bound"}
 
 
+def reference_osse_cycle(cycles=5, warmup=2, exe=None):
+    """The reference's own whole DA cycle on this GPU (oracle/_ref/ref_osse_p4r1 time ...):
+    its update() for the M members in turn, then its LETKF call sequence (letkf.cu glue,
+    letkf_solver.h's cuBLAS / cuSOLVER calls, ranks in turn) with C1's DA settings, as one
+    process; wall time of `cycles` cycles after `warmup`.  Returns its cycles/s, or
+    {"unavailable": why}."""
+    exe = exe or os.path.join(ROOT, "oracle", "_ref", "ref_osse_p4r1")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_osse_p4r1 not built (it needs the reference sources at build time)"}
+    try:
+        out = subprocess.run([exe, "time", str(M), str(cycles), str(STEPS_PER_CYCLE), str(warmup)],
+                             capture_output=True, text=True, timeout=900, check=True).stdout
+        sec = float(next(l for l in out.splitlines() if l.startswith("ref_osse_time")).split()[4])
+    except Exception as e:  # no GPU, or the run failed
+        return {"unavailable": f"ref_osse_p4r1 did not run: {type(e).__name__}"}
+    return {"cycles_per_s": cycles / sec, "ms_per_cycle": 1e3 * sec / cycles, "cycles": cycles, "warmup": warmup,
+            "kind": "the reference's src/lbm.cu + src/data.cu (unmodified) for the 16 members x 100 steps, then its "
+                    "LETKF call sequence (oracle/ref_letkf_solver.cu: letkf.cu glue, letkf_solver.h cuBLAS/cuSOLVER "
+                    "calls, syevjBatched) with DA_XYPRUNE 4, LETKF_RLOC_LEN 1, covinf 1.1, obs errors 0.1 / 0.01, "
+                    "256x256; one process, members and ranks in turn (the reference spreads them over 16 MPI "
+                    "processes); its compiled default physics (the cost does not depend on it)"}
+
+
 def analysis_roofline(stats, ms_phase):
     """The LETKF analysis against the FP32 SIMT peak: algorithmic flops per grid point
     (Gram 2 n_obs M^2, transform 2*9*M^2 + 4 M^3, Jacobi 18 M M(M-1)/2 per sweep at the
@@ -606,6 +629,7 @@ def run_reference(args, rank, world):
     if NX == 256 and not CLOSURE:
         rb = reference_build_line(args)
         line["reference_build"] = rb
+        line["reference_build_cycle"] = reference_osse_cycle()
         if "cycles_per_s_upper_bound" in rb:
             line["reference_build_bound_cycles_per_s"] = rb["cycles_per_s_upper_bound"]
             line["reference_build_bound_kind"] = (

@@ -89,6 +89,7 @@ struct Mat {
         CK(cudaMemset(p, 0, sizeof(real) * size()));
     }
     void free() { cudaFree(p); p = nullptr; }
+    void zero() { CK(cudaMemset(p, 0, sizeof(real) * size())); }
 };
 
 // ---- elementwise kernels of cu_matrix.hpp, same expressions ---------------------
@@ -190,28 +191,44 @@ struct Eigen {
         CKS(cusolverDnXsyevjSetSortEig(params, 0));
     }
     ~Eigen() {
+        cudaFree(work);
+        cudaFree(info);
         cusolverDnDestroySyevjInfo(params);
         cusolverDnDestroy(h);
+    }
+    // work space and info buffer, grown on demand and kept, as the reference's
+    // workspace_.reallocate / info_.reallocate keep theirs
+    real* work = nullptr;
+    int* info = nullptr;
+    size_t work_cap = 0, info_cap = 0;
+    void reserve(size_t lwork, size_t ninfo) {
+        if (lwork > work_cap) {
+            cudaFree(work);
+            CK(cudaMalloc(&work, sizeof(real) * lwork));
+            work_cap = lwork;
+        }
+        if (ninfo > info_cap) {
+            cudaFree(info);
+            CK(cudaMalloc(&info, sizeof(int) * ninfo));
+            info_cap = ninfo;
+        }
     }
     // V holds Q on entry; returns 0 (batched) or 1 (per-matrix stand-in for n > 32)
     int solve(Mat& V, Mat& d) {
         const int n = V.rows, nb = V.batch;
-        int* info = nullptr;
-        CK(cudaMalloc(&info, sizeof(int) * nb));
         int lwork = 0;
-        real* work = nullptr;
         int evd = 0;
         if (n <= 32) {
             CKS(cusolverDnSsyevjBatched_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, V.p, n, d.p,
                                                    &lwork, params, nb));
-            CK(cudaMalloc(&work, sizeof(real) * size_t(lwork)));
+            reserve(size_t(lwork), size_t(nb));
             CKS(cusolverDnSsyevjBatched(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, V.p, n, d.p, work,
                                         lwork, info, params, nb));
         } else {
             evd = 1;
             CKS(cusolverDnSsyevj_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, V.p, n, d.p,
                                             &lwork, params));
-            CK(cudaMalloc(&work, sizeof(real) * size_t(lwork)));
+            reserve(size_t(lwork), size_t(nb));
             for (int b = 0; b < nb; b++)
                 CKS(cusolverDnSsyevj(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, V.p + V.stride() * b, n,
                                      d.p + d.stride() * b, work, lwork, info + b, params));
@@ -221,8 +238,6 @@ struct Eigen {
         CK(cudaMemcpy(h_info.data(), info, sizeof(int) * nb, cudaMemcpyDeviceToHost));
         for (int b = 0; b < nb; b++)
             if (h_info[b] != 0) std::fprintf(stderr, "warning: syevj info[%d] = %d\n", b, h_info[b]);
-        cudaFree(work);
-        cudaFree(info);
         return evd;
     }
 };
@@ -251,6 +266,51 @@ __global__ void k_lambda(const real* d, real* lam, int n_ens, int i_batch0, int 
 }
 
 
+namespace {
+// The solver's matrices, allocated once for a (grid, members) shape and kept, as the
+// reference's init_geo (letkf_solver.h:78-109) allocates them once per rank; every rank
+// below starts from zeroed matrices, as a fresh init_geo would give it.
+struct Workspace {
+    int nx = 0, ny = 0, M = 0;
+    std::vector<real*> xk, yk;
+    Mat X, Y, yo, xbar, ybar, dX, dY, dyo, rR, Q, V, d, D, tmp_ee, tmp_oe, tmp_o, tmp_e, P, w, W, Xsol;
+    Blas* blas = nullptr;
+    Eigen* eigen = nullptr;
+    std::vector<Mat*> mats() {
+        return {&X, &Y, &yo, &xbar, &ybar, &dX, &dY, &dyo, &rR, &Q, &V, &d, &D, &tmp_ee, &tmp_oe, &tmp_o, &tmp_e, &P,
+                &w, &W, &Xsol};
+    }
+    void ensure(int nx_, int ny_, int M_) {
+        if (nx_ == nx && ny_ == ny && M_ == M) return;
+        for (real* p : xk) cudaFree(p);
+        for (real* p : yk) cudaFree(p);
+        for (Mat* m : mats())
+            if (m->p) m->free();
+        nx = nx_; ny = ny_; M = M_;
+        const size_t nxy = size_t(nx) * ny;
+        const int n_obs = glue::n_obs_total();
+        const int n_batch = int(nxy / M);
+        xk.assign(M, nullptr);
+        yk.assign(M, nullptr);
+        for (int k = 0; k < M; k++) {
+            CK(cudaMalloc(&xk[k], sizeof(real) * n_stt * nxy));
+            CK(cudaMalloc(&yk[k], sizeof(real) * n_obs * nxy));
+        }
+        X.init(n_stt, M, n_batch); Y.init(n_obs, M, n_batch); yo.init(n_obs, 1, n_batch);
+        xbar.init(n_stt, 1, n_batch); ybar.init(n_obs, 1, n_batch); dyo.init(n_obs, 1, n_batch);
+        dX.init(n_stt, M, n_batch); dY.init(n_obs, M, n_batch);
+        rR.init(n_obs, n_obs, n_batch);
+        Q.init(M, M, n_batch); V.init(M, M, n_batch); d.init(M, 1, n_batch); D.init(M, M, n_batch);
+        tmp_ee.init(M, M, n_batch); tmp_oe.init(n_obs, M, n_batch); tmp_o.init(n_obs, 1, n_batch);
+        tmp_e.init(M, 1, n_batch); P.init(M, M, n_batch); w.init(M, 1, n_batch); W.init(M, M, n_batch);
+        Xsol.init(n_stt, M, n_batch);
+        if (!blas) blas = new Blas();
+        if (!eigen) eigen = new Eigen();
+    }
+};
+Workspace ws;  // the drivers are single-threaded
+}  // namespace
+
 namespace refletkf {
 
 int analyse(const std::vector<const float*>& f_in, const std::vector<float*>& f_out, const float* ro_d,
@@ -264,11 +324,9 @@ int analyse(const std::vector<const float*>& f_in, const std::vector<float*>& f_
         std::exit(1);
     }
     // members' packed state and observation ensemble (the reference's xk, yk per rank)
-    std::vector<real*> xk(M), yk(M);
-    for (int k = 0; k < M; k++) {
-        CK(cudaMalloc(&xk[k], sizeof(real) * n_stt * nxy));
-        CK(cudaMalloc(&yk[k], sizeof(real) * n_obs * nxy));
-    }
+    ws.ensure(nx, ny, M);
+    std::vector<real*>& xk = ws.xk;
+    std::vector<real*>& yk = ws.yk;
     const real *ro = ro_d, *uo = uo_d, *vo = vo_d;
     // every member packs its xk and yk over the whole grid (letkf.cu:133-187)
     for (int k = 0; k < M; k++) {
@@ -277,25 +335,21 @@ int analyse(const std::vector<const float*>& f_in, const std::vector<float*>& f_
         CK(cudaDeviceSynchronize());
     }
 
-    Blas blas;
-    Eigen eigen;
+    Blas& blas = *ws.blas;
+    Eigen& eigen = *ws.eigen;
     int evd = 0;
     const int n_batch = int(nxy / M);
     for (int rank = 0; rank < M; rank++) {
         const int i_batch0 = n_batch * rank;
         const int r_j0 = i_batch0 / nx, r_j1 = (i_batch0 + n_batch) / nx;
         if (r_j1 <= j0 || r_j0 >= j1) continue;
-        // init_geo (letkf_solver.h:80-109)
-        Mat X, Y, yo, xbar, ybar, dX, dY, dyo, rR, Q, V, d, D, tmp_ee, tmp_oe, tmp_o, tmp_e, P, w, W, Xsol;
-        X.init(n_stt, M, n_batch); Y.init(n_obs, M, n_batch); yo.init(n_obs, 1, n_batch);
-        xbar.init(n_stt, 1, n_batch); ybar.init(n_obs, 1, n_batch); dyo.init(n_obs, 1, n_batch);
-        dX.init(n_stt, M, n_batch); dY.init(n_obs, M, n_batch);
-        rR.init(n_obs, n_obs, n_batch);
+        // init_geo (letkf_solver.h:80-109): the kept matrices, zeroed
+        for (Mat* m : ws.mats()) m->zero();
+        Mat &X = ws.X, &Y = ws.Y, &yo = ws.yo, &xbar = ws.xbar, &ybar = ws.ybar, &dX = ws.dX, &dY = ws.dY,
+            &dyo = ws.dyo, &rR = ws.rR, &Q = ws.Q, &V = ws.V, &d = ws.d, &D = ws.D, &tmp_ee = ws.tmp_ee,
+            &tmp_oe = ws.tmp_oe, &tmp_o = ws.tmp_o, &tmp_e = ws.tmp_e, &P = ws.P, &w = ws.w, &W = ws.W,
+            &Xsol = ws.Xsol;
         set_identity(rR, 1);
-        Q.init(M, M, n_batch); V.init(M, M, n_batch); d.init(M, 1, n_batch); D.init(M, M, n_batch);
-        tmp_ee.init(M, M, n_batch); tmp_oe.init(n_obs, M, n_batch); tmp_o.init(n_obs, 1, n_batch);
-        tmp_e.init(M, 1, n_batch); P.init(M, M, n_batch); w.init(M, 1, n_batch); W.init(M, M, n_batch);
-        Xsol.init(n_stt, M, n_batch);
         // set_rR (init_letkf) and the inputs of this rank
         glue::set_rR(rR.p, rR.rows, rR.stride(), nx, i_batch0, n_batch);
         CK(cudaDeviceSynchronize());
@@ -340,13 +394,6 @@ int analyse(const std::vector<const float*>& f_in, const std::vector<float*>& f_
         for (int k = 0; k < M; k++) k_scatter<<<n_batch, 32>>>(Xsol.p, f_out[k], M, k, i_batch0, n_batch, int(nxy));
         if (lam) k_lambda<<<n_batch, (M + 31) / 32 * 32>>>(d.p, lam, M, i_batch0, n_batch);
         CK(cudaDeviceSynchronize());
-        for (Mat* m : {&X, &Y, &yo, &xbar, &ybar, &dX, &dY, &dyo, &rR, &Q, &V, &d, &D, &tmp_ee, &tmp_oe, &tmp_o,
-                       &tmp_e, &P, &w, &W, &Xsol})
-            m->free();
-    }
-    for (int k = 0; k < M; k++) {
-        cudaFree(xk[k]);
-        cudaFree(yk[k]);
     }
     return evd;
 }

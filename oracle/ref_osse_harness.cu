@@ -29,11 +29,25 @@
 // the analysis populations (rf, uf, vf of lbm.h:72-109).
 //
 // usage: ref_osse <M> <cycles> <steps> <seed> <out.bin>
+//        ref_osse time <M> <cycles> <steps> <warmup_cycles>
+//
+// The `time` form measures the cycle of the reference's code on this GPU, as one
+// process: the M members each advanced `steps` steps by update() in turn, then the
+// analysis (ranks in turn) with one fixed set of observations made from the nature run
+// once beforehand, the refresh and the swap; no file output, no RMSE.  After
+// `warmup_cycles` untimed cycles it prints
+//   ref_osse_time <M> <cycles> <steps> <seconds>
+// for `cycles` cycles, CLOCK_MONOTONIC around them with a device synchronisation at
+// both ends.  The reference itself runs one MPI rank per member, the members'
+// forecasts in separate processes sharing the GPU and the ranks' analyses side by
+// side; this measures the same device work issued from one process.
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <memory>
 #include <random>
+#include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -85,7 +99,77 @@ static double rmse(const std::vector<double>& mu, const std::vector<double>& mv,
     return std::sqrt(s / double(ut.size()));
 }
 
+static int time_cycles(int argc, char** argv) {
+    if (argc != 6) {
+        std::fprintf(stderr, "usage: %s time <M> <cycles> <steps> <warmup_cycles>\n", argv[0]);
+        return 1;
+    }
+    const int M = std::atoi(argv[2]), cycles = std::atoi(argv[3]), steps = std::atoi(argv[4]);
+    const int warmup = std::atoi(argv[5]);
+    const int nx = config::nx, ny = config::ny, nxy = nx * ny;
+    const int p = glue::xyprune();
+    if (M < 2 || M > 64 || ny % M || cycles < 1 || steps < 1 || warmup < 0) {
+        std::fprintf(stderr, "bad arguments\n");
+        return 1;
+    }
+    std::vector<std::unique_ptr<data>> mem;
+    for (int k = 0; k < M; k++) mem.emplace_back(new data(334 + k));
+    // one set of observations of the nature run after `steps` steps
+    std::vector<real> hr(nxy), hu(nxy), hv(nxy), hro(nxy), huo(nxy), hvo(nxy);
+    {
+        auto nature = data(0);
+        for (int t = 0; t < steps; t++) update(nature, t);
+        CK(cudaDeviceSynchronize());
+        CK(cudaMemcpy(hr.data(), nature.d().r.data(), sizeof(real) * nxy, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hu.data(), nature.d().u.data(), sizeof(real) * nxy, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hv.data(), nature.d().v.data(), sizeof(real) * nxy, cudaMemcpyDeviceToHost));
+    }
+    std::mt19937 gen(1);
+    std::normal_distribution<float> nd(0.f, 1.f);
+    for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+            const int ij = i + nx * j;
+            const bool site = i % p == 0 && j % p == 0;
+            hro[ij] = site ? hr[ij] + glue::obs_error_rho() * nd(gen) : NAN;
+            huo[ij] = site ? hu[ij] + glue::obs_error_u() * nd(gen) : NAN;
+            hvo[ij] = site ? hv[ij] + glue::obs_error_u() * nd(gen) : NAN;
+        }
+    real *ro, *uo, *vo;
+    CK(cudaMalloc(&ro, sizeof(real) * nxy));
+    CK(cudaMalloc(&uo, sizeof(real) * nxy));
+    CK(cudaMalloc(&vo, sizeof(real) * nxy));
+    CK(cudaMemcpy(ro, hro.data(), sizeof(real) * nxy, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(uo, huo.data(), sizeof(real) * nxy, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(vo, hvo.data(), sizeof(real) * nxy, cudaMemcpyHostToDevice));
+    const int blocks = (nxy + 255) / 256;
+    std::vector<const float*> fin(M);
+    std::vector<float*> fout(M);
+    int t = 0;
+    auto cycle = [&]() {
+        for (int s = 0; s < steps; s++, t++)
+            for (auto& d : mem) update(*d, t);
+        for (int k = 0; k < M; k++) {
+            fin[k] = mem[k]->d().f.data();
+            fout[k] = mem[k]->dn().f.data();
+        }
+        refletkf::analyse(fin, fout, ro, uo, vo, nx, ny, 0, ny, nullptr);
+        for (auto& d : mem) {
+            k_refresh_ru<<<blocks, 256>>>(d->dn().f.data(), d->dn().r.data(), d->dn().u.data(), nxy);
+            d->swap();
+        }
+    };
+    for (int c = 0; c < warmup; c++) cycle();
+    CK(cudaDeviceSynchronize());
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int c = 0; c < cycles; c++) cycle();
+    CK(cudaDeviceSynchronize());
+    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::printf("ref_osse_time %d %d %d %.6f\n", M, cycles, steps, sec);
+    return 0;
+}
+
 int main(int argc, char** argv) {
+    if (argc >= 2 && std::string(argv[1]) == "time") return time_cycles(argc, argv);
     if (argc != 6) {
         std::fprintf(stderr, "usage: %s <M> <cycles> <steps> <seed> <out.bin>\n", argv[0]);
         return 1;
