@@ -30,19 +30,18 @@ One bench "step" = one DA cycle = the LETKF analysis + 100 LBM steps.
             buffers, so the stream-collide launches inside its cycles are
             HBM-bound) and C4 (C1 with the learned closure)
 
-`--impl reference` times the reference's path on the host cores.  The reference
-has no CPU implementation (its only backend is CUDA + MPI + cuBLAS/cuSOLVER), so
-its arm is the FP64 OpenMP restatement of the reference's path in oracle/,
-configured by the oracle's own restatement of config.h (the product library is
-never loaded in that arm).  One step of that arm is exactly 1/M of a cycle's
-work (one member's 100 LBM steps + the analysis of ny/M rows), so the K steps'
-wall time is what the line reports.  Where the reference's own LBM build
-(oracle/_ref/ref_lbm: its src/lbm.cu and src/data.cu compiled unmodified) is
-present and a GPU is visible, the line also carries `reference_build`: that
-build's forecast run as M processes sharing the GPU, one per member as the
-reference's one-MPI-rank-per-member runs do, and the cycles/s bound it implies
-(`reference_build_bound_cycles_per_s`; forecast only: the reference's LETKF
-needs MPI and HDF5 and is not built, so its real cycle is slower still).
+`--impl reference` is the reference arm.  At the C1 shape it runs the reference's
+own code on this GPU (oracle/_ref/ref_osse_p4r1, built from the reference's sources
+here): one step is one whole DA cycle, its LBM (src/lbm.cu, src/data.cu, unmodified)
+for the 16 members x 100 steps and its LETKF call sequence (letkf.cu glue and
+letkf_solver.h's cuBLAS / cuSOLVER calls, restated because those two files need MPI
+and HDF5), as one process.  The reference has no CPU implementation; the FP64 OpenMP
+restatement of its path in oracle/ on the host cores is the line's cpu_baseline
+(configured by the oracle's own restatement of config.h: the product library is
+never loaded in that arm), and the value where the reference's build cannot serve the
+workload.  The line also carries `reference_build`: the reference's forecast alone run
+as M processes sharing the GPU, one per member as its one-MPI-rank-per-member runs
+do, and the cycles/s bound it implies (`reference_build_bound_cycles_per_s`).
 
 Multi-GPU: replicas only (one independent experiment per GPU, no collective on
 the data path); `value` is the cycles of all ranks / the slowest rank's time.
@@ -577,13 +576,16 @@ def analysis_roofline(stats, ms_phase):
 
 
 def run_reference(args, rank, world):
-    """The reference's path on the host cores: the FP64 OpenMP restatement (oracle/),
-    configured by the oracle's own copy of config.h (no product library is loaded).
-
-    One step is exactly 1/M of a DA cycle's work: 100 LBM steps of one member (each
-    member's forecast costs the same) plus the LETKF analysis of ny/M of the grid rows
-    of the whole M-member ensemble, the row slice moving on each step, so that M steps
-    make one whole cycle.  value = (K/M) cycles over the K timed steps' wall time."""
+    """The reference arm.  At the C1 shape (256^2, 16 members, plain Smagorinsky) it is
+    the reference's own code on this GPU (oracle/_ref/ref_osse_p4r1, built from the
+    reference's sources here): one step is one whole DA cycle, its LBM for the 16
+    members x 100 steps and its LETKF call sequence; `steps` cycles timed after `warmup`.
+    The reference has no CPU implementation; the FP64 OpenMP restatement of the path
+    (oracle/) on the host cores is the cpu_baseline, timed on one cycle's work: one
+    sample step is 100 LBM steps of one member plus the analysis of ny/M rows of the
+    whole ensemble, the row slice moving, so M sample steps are one cycle.  Where the
+    reference's build cannot serve the workload the port is the value.  No product
+    library is loaded in this process."""
     import oracle
     if rank != 0:
         return None
@@ -609,36 +611,43 @@ def run_reference(args, rank, world):
         da.assimilate_rows(ro, uo, vo, j0, j0 + rows)
         return time.perf_counter() - t0
 
-    for k in range(args.warmup):
-        one(k)
-    sec = [one(args.warmup + k) for k in range(args.steps)]
-    total = sum(sec)
-    value = (args.steps / M) / total
+    gpu_ref = NX == 256 and M == 16 and not CLOSURE
+    port_steps = M if gpu_ref else args.steps  # one whole cycle beside the GPU reference
+    one(0)
+    sec = [one(1 + k) for k in range(port_steps)]
+    port_value = (port_steps / M) / sum(sec)
     fc.close()
     da.close()
-    sample = (f"one step = 1/{M} of a cycle: {T} LBM steps of 1 of the {M} members + the LETKF analysis of "
-              f"{rows} of the {NX} rows (moving slice; {M} steps = one whole cycle)")
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "backend": "FP64 OpenMP CPU restatement of the reference path "
-                                                        "(the reference has no CPU implementation)",
-                       "step": sample},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+    sample = (f"{port_steps} steps of 1/{M} of a cycle: {T} LBM steps of 1 of the {M} members + the LETKF analysis "
+              f"of {rows} of the {NX} rows (moving slice; {M} steps = one whole cycle)")
+    cpu = {"value": port_value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample,
+           "backend": "FP64 OpenMP CPU restatement of the reference path (the reference has no CPU implementation)"}
+    ref = reference_osse_cycle(cycles=args.steps, warmup=args.warmup) if gpu_ref else {
+        "unavailable": "the reference's build serves 256x256, 16 members, plain Smagorinsky"}
+    if "cycles_per_s" in ref:
+        value, ms_step, steps, dtype = ref["cycles_per_s"], ref["ms_per_cycle"], args.steps, "f32"
+        backend = ("the reference's own code on this GPU (oracle/_ref/ref_osse_p4r1): " + ref["kind"])
+        step = "one step = one whole DA cycle (100 LBM steps of the 16 members + one LETKF analysis)"
+    else:
+        value, ms_step, steps, dtype = port_value, 1e3 * sum(sec) / port_steps, port_steps, "f64"
+        backend, step = cpu["backend"], sample
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "backend": backend, "step": step},
+            "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if NX == 256 and not CLOSURE:
+    if gpu_ref:
+        line["reference_build_cycle"] = ref
         rb = reference_build_line(args)
         line["reference_build"] = rb
-        line["reference_build_cycle"] = reference_osse_cycle()
         if "cycles_per_s_upper_bound" in rb:
             line["reference_build_bound_cycles_per_s"] = rb["cycles_per_s_upper_bound"]
             line["reference_build_bound_kind"] = (
                 "forecast-only upper bound on the reference build's DA cycles/s on this GPU: its own LBM "
-                "(src/lbm.cu + src/data.cu, unmodified) for the 16 members x 100 steps; its analysis would only "
-                "add time. Engine cycles/s divided by this number is a lower bound on the speed-up")
+                "(src/lbm.cu + src/data.cu, unmodified) for the 16 members x 100 steps as 16 processes or one")
     else:
-        line["reference_build"] = {"unavailable": "the reference build runs its compiled 256x256 "
-                                                  "plain-Smagorinsky default only"}
+        line["reference_build"] = {"unavailable": ref["unavailable"]}
     return line
 
 
