@@ -1669,27 +1669,55 @@ void launch_macros(const lbl_ctx* c, int buf, float* mac, cudaStream_t s) {
         macros_kernel<float><<<grid, 256, 0, s>>>(c->f[buf], mac, c->P);
 }
 
-// FP16 deviation storage <-> FP32 populations, element-wise over [M][9][ny][nx]
-__global__ void expand_kernel(const __half* __restrict__ h, float* __restrict__ f, size_t n, int nxy) {
-    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x) * blockDim.x) {
-        const int q = int((e / nxy) % kQ);
-        f[e] = w_q_rt(q) + __half2float(h[e]);
+// FP16 deviation storage <-> FP32 populations over [M][9][ny][nx]: one grid row per
+// population plane (q = plane mod 9, so no division per element), eight values per
+// thread and iteration (16-byte FP16 and 2 x 16-byte FP32 accesses; nxy is a multiple
+// of 256)
+__global__ void expand_kernel(const __half* __restrict__ h, float* __restrict__ f, int nxy) {
+    const size_t plane = blockIdx.y;
+    const float w = w_q_rt(int(plane % kQ));
+    const uint4* hp = reinterpret_cast<const uint4*>(h + plane * nxy);
+    float4* fp = reinterpret_cast<float4*>(f + plane * nxy);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nxy / 8; e += gridDim.x * blockDim.x) {
+        const uint4 v = __ldg(hp + e);
+        const __half2* h2 = reinterpret_cast<const __half2*>(&v);
+        float o[8];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float2 d = __half22float2(h2[k]);
+            o[2 * k] = w + d.x;
+            o[2 * k + 1] = w + d.y;
+        }
+        fp[2 * e] = make_float4(o[0], o[1], o[2], o[3]);
+        fp[2 * e + 1] = make_float4(o[4], o[5], o[6], o[7]);
     }
 }
-__global__ void compress_kernel(const float* __restrict__ f, __half* __restrict__ h, size_t n, int nxy) {
-    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x) * blockDim.x) {
-        const int q = int((e / nxy) % kQ);
-        h[e] = __float2half_rn(f[e] - w_q_rt(q));
+__global__ void compress_kernel(const float* __restrict__ f, __half* __restrict__ h, int nxy) {
+    const size_t plane = blockIdx.y;
+    const float w = w_q_rt(int(plane % kQ));
+    const float4* fp = reinterpret_cast<const float4*>(f + plane * nxy);
+    uint4* hp = reinterpret_cast<uint4*>(h + plane * nxy);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nxy / 8; e += gridDim.x * blockDim.x) {
+        const float4 a = __ldg(fp + 2 * e), b = __ldg(fp + 2 * e + 1);
+        uint4 v;
+        __half2* h2 = reinterpret_cast<__half2*>(&v);
+        h2[0] = __halves2half2(__float2half_rn(a.x - w), __float2half_rn(a.y - w));
+        h2[1] = __halves2half2(__float2half_rn(a.z - w), __float2half_rn(a.w - w));
+        h2[2] = __halves2half2(__float2half_rn(b.x - w), __float2half_rn(b.y - w));
+        h2[3] = __halves2half2(__float2half_rn(b.z - w), __float2half_rn(b.w - w));
+        hp[e] = v;
     }
 }
 
 void launch_expand(const lbl_ctx* c, const __half* h, float* f, cudaStream_t s) {
-    const size_t n = size_t(c->P.M) * kQ * c->P.nxy;
-    expand_kernel<<<4 * 148, 256, 0, s>>>(h, f, n, c->P.nxy);
+    const int nxy = c->P.nxy;
+    dim3 grid(std::max(1, std::min(64, nxy / 8 / 256)), c->P.M * kQ);
+    expand_kernel<<<grid, 256, 0, s>>>(h, f, nxy);
 }
 void launch_compress(const lbl_ctx* c, const float* f, __half* h, cudaStream_t s) {
-    const size_t n = size_t(c->P.M) * kQ * c->P.nxy;
-    compress_kernel<<<4 * 148, 256, 0, s>>>(f, h, n, c->P.nxy);
+    const int nxy = c->P.nxy;
+    dim3 grid(std::max(1, std::min(64, nxy / 8 / 256)), c->P.M * kQ);
+    compress_kernel<<<grid, 256, 0, s>>>(f, h, nxy);
 }
 
 }  // namespace lbl
