@@ -1,4 +1,4 @@
-"""The host side of bench.py's reference-build timing (`reference_build` of the
+"""The host side of bench.py's reference-build timing (`reference_build` and the cycle rate of the
 `--impl reference` line), on the CPU: a stand-in executable that speaks the `time`
 protocol of oracle/ref_lbm_harness.cu (create the ready file, wait for the go file,
 print `ref_lbm_time <id> <nsteps> <t0_ns> <t1_ns>`) replaces the reference build, so
@@ -73,3 +73,33 @@ def test_analysis_roofline_counts_the_survey_flops():
         assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
     finally:
         bench.NX, bench.M = nx, m
+
+
+FAKE_OSSE = """#!{py}
+import sys
+_, mode, m, cycles, steps, warmup = sys.argv
+assert mode == "time"
+print("ensemble 0: initial velocity with random_seed = 0")
+print("ref_osse_time", m, cycles, steps, {sec})
+sys.exit({rc})
+"""
+
+
+def _fake_osse(tmp_path, sec=0.5, rc=0):
+    path = tmp_path / "fake_ref_osse"
+    path.write_text(FAKE_OSSE.format(py=sys.executable, sec=sec, rc=rc))
+    path.chmod(path.stat().st_mode | stat.S_IXUSR)
+    return str(path)
+
+
+def test_reference_cycle_rate_is_parsed(tmp_path):
+    """reference_osse_cycle (the reference arm's value at C1): the `time` protocol of
+    oracle/ref_osse_harness.cu, `ref_osse_time <M> <cycles> <steps> <seconds>`."""
+    r = bench.reference_osse_cycle(cycles=5, warmup=2, exe=_fake_osse(tmp_path, sec=0.55))
+    assert r["cycles_per_s"] == pytest.approx(5 / 0.55) and r["ms_per_cycle"] == pytest.approx(110.0)
+    assert r["cycles"] == 5 and r["warmup"] == 2
+
+
+def test_reference_cycle_failures_are_reported(tmp_path):
+    assert "unavailable" in bench.reference_osse_cycle(exe=_fake_osse(tmp_path, rc=2))
+    assert "unavailable" in bench.reference_osse_cycle(exe=str(tmp_path / "nothing_here"))
