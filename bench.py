@@ -80,7 +80,7 @@ WORKLOADS = {
                     "trained on 4096 8x-box-filtered 2048^2 snapshots; nature run plain Smagorinsky"),
 }
 CLOSURE = False  # the ensemble (and the CPU baselines) use the trained closure (workload C4)
-CLOSURE_REFRESH = 10  # the closure's network runs every this many steps (lbl_set_closure_refresh)
+CLOSURE_REFRESH = 20  # the closure's network runs every this many steps (lbl_set_closure_refresh)
 WORKLOAD = WORKLOADS["C1"][2]
 
 
@@ -869,7 +869,7 @@ def main():
     ap.add_argument("--lbm-variant", choices=["auto", "direct", "tma", "vec", "vec2"], default="auto",
                     help="stream-collide kernel: the library's choice, one column per thread, TMA-fed rows, or "
                          "4 (vec, 128-bit) / 2 (vec2, 64-bit) columns per thread")
-    ap.add_argument("--closure-refresh", type=int, default=10,
+    ap.add_argument("--closure-refresh", type=int, default=20,
                     help="C4: run the closure's network every this many steps, holding each cell's multiplier between "
                          "(1: every step)")
     args = ap.parse_args()
