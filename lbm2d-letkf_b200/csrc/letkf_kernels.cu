@@ -148,13 +148,13 @@ constexpr int kCW = 4, kCH = 2;  // chain tile (points in x, points in y)
 // cleanup sweep in which such turns are skipped: the nearly degenerate pairs are already
 // orthogonal to about tol, and mixing eigenvectors of (nearly) equal eigenvalues leaves the
 // transform as it is, while the other pairs then converge quadratically.  Measured against the
-// FP64 oracle at C1's observation settings: 4.3e-4 of the largest increment without the
+// FP64 oracle with observation errors 0.1 (u, v) and 0.01 (rho): 4.3e-4 of the largest increment without the
 // cleanup at 256^2 x 16, 9.8e-6 with it (3.0 -> 3.4 mean sweeps); at 512^2 x 64, 6.2e-4 and
 // 2.8e-5 (2.4 -> 3.3 mean sweeps).
 constexpr float kWideTurn = 0.1f;
 // the wide analysis walks taller tiles: fewer cold starts, and its many waves hide
 // the longer CTAs (512^2, M = 64: 58.7 ms at 4 x 8, 59.3 at 4 x 4, 62.8 at 4 x 2;
-// C1's kernel is fastest at 4 x 2)
+// 16 members' kernel is fastest at 4 x 2 on 256^2)
 constexpr int kWCW = 4, kWCH = 8;
 
 // DUMP = true recomputes the tiles that cover the rows of D and, instead of writing
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
             float a = a0 + a1;
             bool rot = false, wide = false;
             float worst = 0.f;  // largest g^2 / (a b) of the sweep
-// three rounds per loop body: the C1 analysis phase 0.637 against 0.643 ms (one round:
+// three rounds per loop body: the 256^2 x 16 analysis phase 0.637 against 0.643 ms (one round:
             // run-time loop control; all fifteen: 0.720 ms, the body no longer fits the instruction cache)
 #pragma unroll 3
             for (int rr = 1; rr < MP; rr++) {
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(128) analysis_kernel(const float* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// The local analysis for 32 < M <= 64 (the C2 ensembles; the reference runs them
+// The local analysis for 32 < M <= 64 (the 64-member ensembles; the reference runs them
 // through EigenG-Batched).  One CTA of 128 threads walks one kWCW x kWCH tile of points;
 // thread t owns rows [32h, 32h + 32) (h = t & 1) of member column k = t >> 1 for the
 // Gram, the warm start and the transform; the two halves of a column combine their

@@ -6,9 +6,9 @@ The reference side is oracle/_ref/ref_osse_p4r1 (oracle/ref_osse_harness.cu): th
 nature run and 16 members as reference `data` objects advanced by the reference's
 update() (src/lbm.cu, src/data.cu compiled unmodified), every 100 steps the members
 analysed by the reference's LETKF call sequence (letkf.cu glue, letkf_solver.h's cuBLAS /
-cuSOLVER calls) with C1's DA settings (DA_XYPRUNE 4, LETKF_RLOC_LEN 1, LETKF_COVINF 1.1,
-OBS_ERROR_U 0.1, OBS_ERROR_RHO 0.01), observations of the nature run's macros at every
-4th point plus seeded noise.  It writes each cycle's observations and true (u, v).
+cuSOLVER calls) with the 256^2 x 16 workload's DA settings (DA_XYPRUNE 4,
+LETKF_RLOC_LEN 1, LETKF_COVINF 1.1, OBS_ERROR_U 0.1, OBS_ERROR_RHO 0.01), observations
+of the nature run's macros at every 4th point plus seeded noise.  It writes each cycle's observations and true (u, v).
 
 The engine side replays them through the C ABI: the same configuration (the reference's
 default physics, 256^2, 16 members with the reference's member initial conditions),

@@ -23,7 +23,7 @@ import oracle
 # LETKF_RLOC_LEN, OBS_ERROR_U, OBS_ERROR_RHO, initial-condition kind and amplitude,
 # oracle steps, noise seed, stored rows
 CASES = {
-    # C1's localisation and observation errors (sigma_u 0.1, sigma_rho 0.01), the
+    # the 256^2 x 16 workload's localisation and observation errors (sigma_u 0.1, sigma_rho 0.01), the
     # bench's initial spectrum (rms 1.0 physical)
     "p4r1_m16": dict(harness="p4r1", M=16, nx=64, p=4, L=1, su=0.1, sr=0.01, ic="k4exp", amp=1.0, steps=10,
                      seed=11, rows=(0, 1, 2, 3, 33, 63)),

@@ -93,7 +93,7 @@ def _fake_osse(tmp_path, sec=0.5, rc=0):
 
 
 def test_reference_cycle_rate_is_parsed(tmp_path):
-    """reference_osse_cycle (the reference arm's value at C1): the `time` protocol of
+    """reference_osse_cycle (the reference arm's value at 256^2 x 16): the `time` protocol of
     oracle/ref_osse_harness.cu, `ref_osse_time <M> <cycles> <steps> <seconds>`."""
     r = bench.reference_osse_cycle(cycles=5, warmup=2, exe=_fake_osse(tmp_path, sec=0.55))
     assert r["cycles_per_s"] == pytest.approx(5 / 0.55) and r["ms_per_cycle"] == pytest.approx(110.0)

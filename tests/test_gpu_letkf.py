@@ -42,7 +42,7 @@ CASES = [  # nx, M, p, L, beta
     (128, 16, 4, 2, 1.2),
     (256, 16, 4, 1, 1.1),
     (96, 12, 4, 1, 1.1),
-    (64, 64, 4, 1, 1.1),   # 32 < M <= 64: the 64-thread analysis kernel (C2's ensemble size)
+    (64, 64, 4, 1, 1.1),   # 32 < M <= 64: the 64-thread analysis kernel (the 512^2 workload's ensemble size)
     (64, 48, 4, 1, 1.1),
     (64, 40, 2, 0, 1.05),
     (64, 33, 4, 1, 1.1),   # 31 zero padding columns in the quad-owned Jacobi
@@ -76,7 +76,7 @@ def test_analysis_matches_oracle(nx, M, p, L, beta):
 
 
 # The bench workloads at their own observation errors (sigma_u 0.1, sigma_rho 0.01):
-# C1 (256^2 x 16) and C2's exact shape (512^2 x 64, the wide analysis kernel), analysed
+# 256^2 x 16 and 512^2 x 64 (the wide analysis kernel), the benchmark workloads' shapes, analysed
 # on a band of rows by the FP64 oracle.  Measured: 1.0e-5 and 2.8e-5 of the largest
 # increment (the reference's own FP32 cuBLAS/cuSOLVER path sits 3e-6..2.5e-5 from FP64).
 WORKLOAD_TOL = 1e-4

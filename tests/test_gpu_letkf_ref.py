@@ -2,7 +2,7 @@
 
 tests/golden/ref_letkf_<case>.npz hold the analysis that the reference's letkf.cu glue
 and letkf_solver.h cuBLAS / cuSOLVER sequence (oracle/_ref/ref_letkf_*) computed for
-inputs regenerated here bit for bit (tests/letkf_ref_cases.py): C1's localisation and
+inputs regenerated here bit for bit (tests/letkf_ref_cases.py): the 256^2 x 16 workload's localisation and
 observation errors at M = 16 and 32, the pointwise p = 1 analysis, and p = 4 without
 LETKF_RLOC_LEN at small observation errors.  Both sides work in FP32 (the engine: FP32
 Gram and its own Jacobi; the reference: cuBLAS and syevjBatched at tolerance 1e-6).

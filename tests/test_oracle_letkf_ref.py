@@ -53,6 +53,6 @@ def test_oracle_matches_reference_solver(case):
     sums = lc.checksums(inc)
     ref_sums = z["inc_sums"]
     cerr = np.abs(sums - ref_sums) / np.maximum(np.abs(ref_sums), 1e-300)
-    # the plain sum can cancel to near zero; judge it against the sum of |increments| instead
+    # the plain sum can cancel to near zero; compare it with the sum of |increments| instead
     cerr[0] = abs(sums[0] - ref_sums[0]) / float(np.sum(np.abs(inc)))
     assert np.all(cerr < CHECKSUM_TOL), f"{case}: checksum errors {cerr}"

@@ -1,6 +1,6 @@
 """The whole DA_LETKF experiment against the reference's own code
 (tests/golden/ref_osse_p4r1.npz, made by tests/golden/make_osse_ref.py on a B200):
-100 cycles of 100 steps, 256^2, 16 members, C1's DA settings, run by the reference's
+100 cycles of 100 steps, 256^2, 16 members, the 256^2 x 16 workload's DA settings, run by the reference's
 LBM and LETKF call sequence (oracle/ref_osse_harness.cu) and by the engine through the
 C ABI on the reference's observations.  The requirement is analysis RMSE within 2 % of
 the reference's; the recorded agreement is about 1e-5 on the mean and 6e-5 per cycle.
