@@ -87,6 +87,7 @@ WORKLOAD = WORKLOADS["C1"][2]
 STORAGE = 0  # lbl_config.storage of the ensemble (the nature run stays FP32)
 GRAM = 0     # lbl_config.gram of the ensemble: 0 FP32, 1 BF16 tensor cores (32 < M <= 64)
 LBM_VARIANT = 0  # lbl_config.lbm_variant of the ensemble and the nature run (0: the library's choice)
+PREFETCH = None  # the stream-collide's march form (lbl_set_stream_collide_shape), None: the library's choice
 
 
 def workload_config(lib, mode="DA_LETKF", n_ens=None):
@@ -261,7 +262,7 @@ def run_engine(args, dist, rank, world, device):
     import oracle
     K, W = args.steps, args.warmup
     obs, truth = make_observations(lbl, W + K + 1)
-    ens = with_closure(lbl.Ensemble(workload_config(lbl), device=device))
+    ens = with_closure(with_shape(lbl.Ensemble(workload_config(lbl), device=device)))
     ens.init(0)
     T = STEPS_PER_CYCLE
     # first cycle has no analysis (t = 0): bring the ensemble to t = 100
@@ -320,7 +321,7 @@ def run_engine(args, dist, rank, world, device):
     stats = ens.letkf_stats()
 
     # ---- e2e: host observations in, RMSE out, every cycle -----------------------------
-    e2e_ens = with_closure(lbl.Ensemble(workload_config(lbl), device=device))
+    e2e_ens = with_closure(with_shape(lbl.Ensemble(workload_config(lbl), device=device)))
     e2e_ens.init(0)
     e2e_ens.cycle_async(0, None, None, None, T)
     for c in range(W):
@@ -801,6 +802,13 @@ def closure_params():
         return z["params"].astype(np.float32), meta["nu_ref"], meta["dx_ref"]
 
 
+def with_shape(ens):
+    """Apply --prefetch (the stream-collide's march form) to an engine context."""
+    if PREFETCH is not None:
+        ens.set_launch_shape(PREFETCH, 0)
+    return ens
+
+
 def with_closure(obj):
     """Switch an engine ensemble or an oracle to the trained closure when the workload
     asks for it (the engine with its refresh interval; the oracle evaluates every step)."""
@@ -820,6 +828,8 @@ def lbm_sweep(args):
         nx, m = (int(v) for v in spec.lower().split("x"))
         e = lbl.Ensemble(lbl.config_default("NATURE", nx, m, storage=STORAGE, lbm_variant=LBM_VARIANT))
         tuned = e.autotune()[0] if args.autotune else None  # between creation and init
+        if PREFETCH is not None:
+            e.set_launch_shape(PREFETCH, 0)
         e.init(0)
         if args.closure:
             e.set_closure(*closure_params())
@@ -866,6 +876,9 @@ def main():
                     help="with --lbm: the learned-closure stream-collide (trained parameters of the package)")
     ap.add_argument("--autotune", action="store_true",
                     help="with --lbm: time at the strip height lbl_autotune picks instead of the heuristic's")
+    ap.add_argument("--prefetch", type=int, default=None, choices=[0, 1],
+                    help="the stream-collide's march (lbl_set_stream_collide_shape): 0 pulls each row when "
+                         "needed, 1 holds the row after next in registers; default: the library's choice")
     ap.add_argument("--lbm-variant", choices=["auto", "direct", "tma", "vec", "vec2"], default="auto",
                     help="stream-collide kernel: the library's choice, one column per thread, TMA-fed rows, or "
                          "4 (vec, 128-bit) / 2 (vec2, 64-bit) columns per thread")
@@ -875,7 +888,7 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global NX, M, WORKLOAD, STORAGE, CLOSURE, GRAM, CLOSURE_REFRESH, LBM_VARIANT
+    global NX, M, WORKLOAD, STORAGE, CLOSURE, GRAM, CLOSURE_REFRESH, LBM_VARIANT, PREFETCH
     NX, M, WORKLOAD = WORKLOADS.get(args.workload, WORKLOADS["C1"])
     CLOSURE = args.workload == "C4"
     CLOSURE_REFRESH = args.closure_refresh
@@ -884,6 +897,7 @@ def main():
     STORAGE = 1 if args.storage == "f16" else 0
     GRAM = {"f32": 0, "bf16": 1, "tf32x3": 2}[args.gram]
     LBM_VARIANT = {"auto": 0, "direct": 1, "tma": 2, "vec": 3, "vec2": 4}[args.lbm_variant]
+    PREFETCH = args.prefetch
     if GRAM == 1:
         WORKLOAD += "; Gram on BF16 tensor cores with FP32 sums"
     elif GRAM == 2:
