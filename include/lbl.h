@@ -301,6 +301,47 @@ int lbl_stream_collide_shape(const lbl_ctx* ctx, int* columns_per_thread, int* p
  * shape (every shape computes each cell in the same arithmetic). */
 int lbl_set_stream_collide_shape(lbl_ctx* ctx, int prefetch, int strip_rows);
 
+/* ---- y-slab split of one experiment over ranks --------------------------------------
+ * Replaces the reference's member-sharded MPI layout, whose analysis transposes the ensemble
+ * all-to-all every cycle (util/letkf_solver.h:135-215, 374-394; letkf.cu:191, 273, 315).
+ * Every rank holds all M members of the rows [row0, row0 + own) of a grid of ny_global
+ * rows, plus `halo` rows on each side: create the context with cfg.ny = own + 2 * halo
+ * (the rest of cfg as for the whole grid), then call lbl_slab_set before lbl_init.  The
+ * constants (dx = h_ref / (ny_global - 1), the forcing's coordinates) and the initial
+ * condition then are the whole grid's, and local row r is global row
+ * (row0 - halo + r) mod ny_global.  Every kernel runs over the slab as if it were periodic;
+ * after k steps the outer 2k rows on each side are stale and the neighbours' packed rows
+ * replace them:
+ *   - step at most halo / 2 steps with lbl_update_async, then exchange 2k rows;
+ *   - after lbl_assimilate_async exchange all `halo` rows (the analysis of the halo rows
+ *     reads past the slab).
+ * The observation fields given to lbl_assimilate are the slab's own nx * cfg.ny rows,
+ * halos included.  Own rows then equal the whole-grid run bit for bit.  Conditions:
+ * halo >= 2 and own >= halo; DA_LETKF also needs halo >= the window reach
+ * (2 * LETKF_RLOC_LEN * DA_XYPRUNE rows, 2 * DA_XYPRUNE without LETKF_RLOC_LEN), and
+ * halo and row0 multiples of lcm(8, DA_XYPRUNE).  Modes NATURE and DA_LETKF; no learned
+ * closure, matrix dumps, files (output, lbl_assimilate_files), cycle graph
+ * (lbl_cycle_async), diagnostics or batch.  lbl_rmse_uv covers the own rows; its truth
+ * fields are the slab's nx * cfg.ny values. */
+int lbl_slab_set(lbl_ctx* ctx, int ny_global, int row0, int halo);
+
+/* Bytes of one packed halo buffer of `rows` rows: M * 9 * rows * nx elements of the
+ * storage type (4 bytes, or 2 with LBL_STORAGE_F16).  No GPU work. */
+int lbl_slab_halo_bytes(const lbl_ctx* ctx, int rows, size_t* bytes);
+
+/* Pack, on the context's stream (lbl_get_stream), the rows the neighbours need after the
+ * last call: to_prev (for the slab above, rows [row0 - rows, ...)) gets local rows
+ * [2 halo - rows, 2 halo), to_next (for the slab below) local rows
+ * [cfg.ny - 2 halo, cfg.ny - 2 halo + rows); both [member][q][rows][nx].  rows in
+ * [1, halo]; device buffers of lbl_slab_halo_bytes, 16-byte aligned.  The transfer is
+ * the caller's (NCCL send / receive, or a copy between contexts on one GPU). */
+int lbl_slab_pack(lbl_ctx* ctx, int rows, void* to_prev, void* to_next);
+
+/* Unpack, on the context's stream, the neighbours' packed rows: from_prev (the slab
+ * above's to_next) into local rows [0, rows), from_next (the slab below's to_prev) into
+ * [cfg.ny - rows, cfg.ny).  A single slab (ny_global = own) is its own neighbour. */
+int lbl_slab_unpack(lbl_ctx* ctx, int rows, const void* from_prev, const void* from_next);
+
 /* Directory prefix (config::prefix, "io" by default, config.h:287) under which the
  * LETKF matrix dumps go when cfg.write_mat is set: <prefix>/letkf/mat/ens<r>/
  * <label>.float_<rows>_<cols>_<batch>.<t>.h5 (letkf.cu:276-306, cu_matrix.hpp:97-117),

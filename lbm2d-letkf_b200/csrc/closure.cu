@@ -436,6 +436,10 @@ int lbl_set_closure(lbl_ctx* ctx, const float* params, double nu_ref, double dx_
     if (!ctx) return LBL_ERR_ARG;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return LBL_ERR_CUDA;
     if (params) {
+        if (ctx->slab_ny) {
+            ctx->err = "a y-slab runs the Smagorinsky closure only";
+            return LBL_ERR_UNSUPPORTED;
+        }
         if (ctx->P.nx % 32 != 0) {  // whole warps of cells
             ctx->err = "the learned closure needs nx a multiple of 32";
             return LBL_ERR_UNSUPPORTED;

@@ -49,11 +49,12 @@ __global__ void diag_kernel(const float* __restrict__ mac, int nx, int ny, int m
     block_add(r, red + 2);
 }
 
+// over the cells [ij0, ij0 + n) of each plane (the whole grid, or a y-slab's own rows)
 __global__ void rmse_kernel(const float* __restrict__ mac, int nxy, int M, const float* __restrict__ ut,
-                            const float* __restrict__ vt, double* __restrict__ red) {
-    const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+                            const float* __restrict__ vt, double* __restrict__ red, int ij0, int n) {
+    const int ij = ij0 + blockIdx.x * blockDim.x + threadIdx.x;
     double s = 0;
-    if (ij < nxy) {
+    if (ij < ij0 + n) {
         const double du = field(mac, nxy, 0, M, 1, ij) - double(ut[ij]);
         const double dv = field(mac, nxy, 0, M, 2, ij) - double(vt[ij]);
         s = du * du + dv * dv;
@@ -120,15 +121,25 @@ void launch_diag(const lbl_ctx* c, const float* mac, int member, double* red, cu
     diag_kernel<<<(c->P.nxy + 255) / 256, 256, 0, s>>>(mac, c->P.nx, c->P.ny, m0, m1, double(c->P.dx), red);
 }
 
-void launch_rmse(const lbl_ctx* c, const float* mac, const float* ut, const float* vt, double* red, cudaStream_t s) {
-    cudaMemsetAsync(red, 0, sizeof(double), s);
-    rmse_kernel<<<(c->P.nxy + 255) / 256, 256, 0, s>>>(mac, c->P.nxy, c->P.M, ut, vt, red);
+// the cells the RMSE covers: the whole grid, or a y-slab's own rows (not its halos)
+void rmse_cells(const lbl_ctx* c, int* ij0, int* n) {
+    *ij0 = c->slab_ny ? c->slab_halo * c->P.nx : 0;
+    *n = c->slab_ny ? (c->P.ny - 2 * c->slab_halo) * c->P.nx : c->P.nxy;
 }
 
-// red[1] = sqrt(red[0] / nxy), the RMSE the host would form (IEEE division and square root)
-__global__ void rmse_finish_kernel(double* red, int nxy) { red[1] = sqrt(red[0] / double(nxy)); }
+void launch_rmse(const lbl_ctx* c, const float* mac, const float* ut, const float* vt, double* red, cudaStream_t s) {
+    int ij0, n;
+    rmse_cells(c, &ij0, &n);
+    cudaMemsetAsync(red, 0, sizeof(double), s);
+    rmse_kernel<<<(n + 255) / 256, 256, 0, s>>>(mac, c->P.nxy, c->P.M, ut, vt, red, ij0, n);
+}
+
+// red[1] = sqrt(red[0] / n), the RMSE the host would form (IEEE division and square root)
+__global__ void rmse_finish_kernel(double* red, int n) { red[1] = sqrt(red[0] / double(n)); }
 void launch_rmse_finish(const lbl_ctx* c, double* red, cudaStream_t s) {
-    rmse_finish_kernel<<<1, 1, 0, s>>>(red, c->P.nxy);
+    int ij0, n;
+    rmse_cells(c, &ij0, &n);
+    rmse_finish_kernel<<<1, 1, 0, s>>>(red, n);
 }
 
 }  // namespace lbl

@@ -23,6 +23,12 @@ namespace {
 
 int wait_output(lbl_ctx* ctx);
 
+// what a y-slab context (lbl_slab_set) does not do
+constexpr const char* kSlabCycle =
+    "a y-slab exchanges halos between its steps: lbl_update_async, lbl_assimilate_async and lbl_slab_pack / "
+    "lbl_slab_unpack replace the cycle graph";
+constexpr const char* kSlabWhole = "a y-slab reads and writes no files and has no whole-grid diagnostics";
+
 // a failed allocation is LBL_ERR_NOMEM; it is not sticky, so the runtime's last-error
 // slot is cleared for the calls that follow
 #define LBL_CK(call)                                                                            \
@@ -88,13 +94,17 @@ int set_device(lbl_ctx* ctx) {
 // ---------------------------------------------------------------------------
 // configuration
 // ---------------------------------------------------------------------------
-Phys derive_phys(const lbl_config& cfg) {
+// The physical constants come from the grid of ny_global rows (dx = h_ref / (ny_global - 1), the forcing's
+// 1/ny); the array shape from cfg.ny.  The two differ only for a y-slab, whose cfg.ny is its own rows plus halos.
+Phys derive_phys(const lbl_config& cfg, int ny_global = 0, int row0_local = 0) {
+    const int nyg = ny_global > 0 ? ny_global : cfg.ny;
     Phys P{};
     P.nx = cfg.nx; P.ny = cfg.ny; P.M = cfg.n_ens; P.nxy = cfg.nx * cfg.ny;
+    P.y0g = row0_local; P.nyg = nyg;
     // the reference's constexpr `real` arithmetic: h_ref is rounded to float first
     // (config.h:158), then divided in float (config.h:250-251)
     P.c = float(cfg.u_ref) / float(cfg.cfl);                       // config.h:248 (constexpr real)
-    P.dx = float(cfg.h_ref) / float(cfg.ny - 1);                   // config.h:250
+    P.dx = float(cfg.h_ref) / float(nyg - 1);                      // config.h:250
     P.dt = P.dx / P.c;                                             // config.h:251
     double nu = cfg.nu;
     if (cfg.tau > 0) nu = (cfg.tau - 0.5) * double(P.c) * double(P.c) * double(P.dt) / 3.0;
@@ -107,7 +117,7 @@ Phys derive_phys(const lbl_config& cfg) {
     P.c_d = P.c; P.dt_d = P.dt;
     P.tau_k = 3.0 / P.c_d / P.c_d / P.dt_d;
     P.inv_nx = 1.0f / float(cfg.nx);
-    P.inv_ny = 1.0f / float(cfg.ny);
+    P.inv_ny = 1.0f / float(nyg);
     P.inv_c = 1.0f / P.c;
     P.inv_c2 = 1.0f / (P.c * P.c);
     P.inv_cs2 = 1.0f / P.cs2;
@@ -373,10 +383,11 @@ bool da_due(const lbl_ctx* ctx, int t) { return ((t / ctx->cfg.iiter) % ctx->cfg
 // the reference's DATA_ASSIMILATION run modes (config.h:32-53)
 bool is_da_mode(int mode) { return mode == LBL_MODE_DA_LETKF || mode == LBL_MODE_DA_NUDGING; }
 
-// initial velocity of one ensemble id on the device, rescaled on the host (FP32)
+// initial velocity of one ensemble id on the device, rescaled on the host (FP32).  A y-slab
+// computes and rescales the whole grid's field, then keeps its own rows and halos.
 int ic_member(lbl_ctx* ctx, int seed, std::vector<float>& u, std::vector<float>& v) {
     const lbl_config& cfg = ctx->cfg;
-    const int nx = cfg.nx, ny = cfg.ny, nk = nx / 2;
+    const int nx = cfg.nx, ny = ctx->slab_ny ? ctx->slab_ny : cfg.ny, nk = nx / 2;
     std::mt19937 eng(seed);                                      // data.cu:43-45
     std::uniform_real_distribution<float> dist(-1, 1);
     std::vector<double> kx, ky, pp, th;
@@ -430,6 +441,16 @@ int ic_member(lbl_ctx* ctx, int seed, std::vector<float>& u, std::vector<float>&
         for (size_t ij = 0; ij < nxy; ij++) e += double(u[ij]) * u[ij] + double(v[ij]) * v[ij];
         const float s = float(cfg.ic_amp / std::sqrt(e / double(nxy) + 1e-300));
         for (size_t ij = 0; ij < nxy; ij++) { u[ij] *= s; v[ij] *= s; }
+    }
+    if (ctx->slab_ny) {
+        std::vector<float> us(size_t(ctx->P.nxy)), vs(size_t(ctx->P.nxy));
+        for (int j = 0; j < ctx->P.ny; j++) {
+            const size_t g = size_t((j + ctx->P.y0g) % ny) * nx, l = size_t(j) * nx;
+            std::copy(u.begin() + g, u.begin() + g + nx, us.begin() + l);
+            std::copy(v.begin() + g, v.begin() + g + nx, vs.begin() + l);
+        }
+        u.swap(us);
+        v.swap(vs);
     }
     return LBL_OK;
 }
@@ -1061,6 +1082,7 @@ int lbl_assimilate_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, 
 
 int lbl_assimilate_files(lbl_ctx* ctx, int t, const char* io_prefix) {
     if (!ctx || !io_prefix) return LBL_ERR_ARG;
+    if (ctx->slab_ny) return fail(ctx, LBL_ERR_UNSUPPORTED, kSlabWhole);
     LBL_TRY(wait_output(ctx));  // an OBSERVE output of this context may still be writing the files
     if (!is_da_mode(ctx->cfg.mode)) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate needs mode DA_LETKF or DA_NUDGING");
     if (ctx->cfg.da_dummy) return LBL_OK;                           // DA_DUMMY (main.cu:94)
@@ -1085,6 +1107,7 @@ int lbl_cycle_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
     if (!ctx) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
     if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_cycle_async before lbl_init");
+    if (ctx->slab_ny) return fail(ctx, LBL_ERR_UNSUPPORTED, kSlabCycle);
     if (n_fc < 0) return fail(ctx, LBL_ERR_ARG, "n_fc < 0");
     if (n_fc > ctx->force_cap) {
         // more steps than one graph's forcing buffer: the cycle graph takes the first
@@ -1115,6 +1138,7 @@ int lbl_cycle_async(lbl_ctx* ctx, int t, const float* ro, const float* uo, const
 int lbl_output_async(lbl_ctx* ctx, int t, const char* io_prefix) {
     if (!ctx || !io_prefix) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
+    if (ctx->slab_ny) return fail(ctx, LBL_ERR_UNSUPPORTED, kSlabWhole);
     const lbl_config& cfg = ctx->cfg;
     if (t % (cfg.iiter * cfg.ioprune) != 0) return LBL_OK;          // io.cu:23
     LBL_TRY(wait_output(ctx));                                       // the staging is free again
@@ -1278,6 +1302,7 @@ int lbl_get_letkf_stats(lbl_ctx* ctx, int* max_sweeps, int* n_noconv, int* nan_f
 int lbl_get_diagnostics(lbl_ctx* ctx, int member, double* energy, double* enstrophy, double* mass) {
     if (!ctx || member < -1 || member >= ctx->P.M) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
+    if (ctx->slab_ny) return fail(ctx, LBL_ERR_UNSUPPORTED, kSlabWhole);
     launch_diag(ctx, ctx->mac[ctx->cur], member, ctx->d_red, ctx->stream);
     LBL_CK(cudaGetLastError());
     double h[3];
@@ -1301,7 +1326,9 @@ int lbl_rmse_uv(lbl_ctx* ctx, const float* u_true, const float* v_true, double* 
     double h = 0;
     LBL_CK(cudaMemcpyAsync(&h, ctx->d_red, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     LBL_CK(cudaStreamSynchronize(ctx->stream));
-    *rmse = std::sqrt(h / double(nxy));
+    int ij0, n;
+    rmse_cells(ctx, &ij0, &n);
+    *rmse = std::sqrt(h / double(n));
     return LBL_OK;
 }
 
@@ -1431,6 +1458,82 @@ int lbl_set_stream_collide_shape(lbl_ctx* ctx, int prefetch, int strip_rows) {
     ctx->ty_default = lbm_strip_rows(ctx);
     if (ctx->closure && ctx->closure_every > 1) ctx->ty_held = lbm_strip_rows_held(ctx);
     return LBL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// y-slab split of one experiment (slab.cu has the halo kernel).  The context was created with
+// cfg.ny = own rows + 2 halo; the constants come from the global grid; the forcing and the
+// initial condition use global rows.  Every kernel then runs unchanged over the slab as if it
+// were periodic: the rows the wrap corrupts are the outer ones, which the neighbours refresh.
+// ---------------------------------------------------------------------------
+int lbl_slab_set(lbl_ctx* ctx, int ny_global, int row0, int halo) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    if (ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_slab_set after lbl_init");
+    const lbl_config& cfg = ctx->cfg;
+    if (cfg.mode != LBL_MODE_NATURE && cfg.mode != LBL_MODE_DA_LETKF)
+        return fail(ctx, LBL_ERR_UNSUPPORTED, "a y-slab runs NATURE or DA_LETKF (OBSERVE draws its noise over the "
+                                              "whole grid, nudging is not split)");
+    if (cfg.write_mat) return fail(ctx, LBL_ERR_UNSUPPORTED, "a y-slab writes no LETKF matrices");
+    if (ctx->closure) return fail(ctx, LBL_ERR_UNSUPPORTED, "a y-slab runs the Smagorinsky closure only");
+    const int own = cfg.ny - 2 * halo;
+    if (halo < 2) return fail(ctx, LBL_ERR_ARG, "the halo must hold at least 2 rows (the stream-collide reaches j +- 2)");
+    if (own < halo) return fail(ctx, LBL_ERR_ARG, "a y-slab must own at least `halo` rows (cfg.ny >= 3 halo)");
+    if (ny_global < own || 2 * halo > ny_global || row0 < 0 || row0 >= ny_global)
+        return fail(ctx, LBL_ERR_ARG, "need own rows <= ny_global, 2 halo <= ny_global and 0 <= row0 < ny_global");
+    if (cfg.mode == LBL_MODE_DA_LETKF) {
+        // the analysis of an own row reads observation sites up to nl * p rows away; sites and the
+        // analysis tiles (2 or 8 rows) must fall on the whole grid's
+        const int reach = ctx->G.nl * ctx->G.p, p = ctx->G.p;
+        int align = 8;
+        while (align % p) align += 8;
+        if (halo < reach) return fail(ctx, LBL_ERR_ARG, "the halo must cover the analysis window (nl * p rows)");
+        if (halo % align || row0 % align || ny_global % p)
+            return fail(ctx, LBL_ERR_ARG, "halo and row0 must be multiples of lcm(8, DA_XYPRUNE) and DA_XYPRUNE "
+                                          "must divide ny_global");
+    }
+    ctx->slab_ny = ny_global;
+    ctx->slab_row0 = row0;
+    ctx->slab_halo = halo;
+    ctx->P = derive_phys(cfg, ny_global, ((row0 - halo) % ny_global + ny_global) % ny_global);
+    for (auto& g : ctx->graphs) cudaGraphExecDestroy(g.second);
+    ctx->graphs.clear();
+    return LBL_OK;
+}
+
+int lbl_slab_halo_bytes(const lbl_ctx* ctx, int rows, size_t* bytes) {
+    if (!ctx || !bytes || rows < 0) return LBL_ERR_ARG;
+    *bytes = size_t(ctx->P.M) * kQ * size_t(rows) * ctx->P.nx * (ctx->f16 ? sizeof(__half) : sizeof(float));
+    return LBL_OK;
+}
+
+namespace {
+int slab_halo(lbl_ctx* ctx, int rows, void* prev, void* next, bool unpack) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    if (!ctx->slab_ny) return fail(ctx, LBL_ERR_STATE, "not a y-slab context (lbl_slab_set)");
+    if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "halo exchange before lbl_init");
+    if (rows < 1 || rows > ctx->slab_halo) return fail(ctx, LBL_ERR_ARG, "rows must lie in [1, halo]");
+    if (!prev || !next || (reinterpret_cast<uintptr_t>(prev) | reinterpret_cast<uintptr_t>(next)) % 16)
+        return fail(ctx, LBL_ERR_ARG, "the halo buffers must be 16-byte aligned device memory");
+    const int h = ctx->slab_halo, ny = ctx->P.ny;
+    // sent: rows [2h - rows, 2h) go to the previous slab, [ny - 2h, ny - 2h + rows) to the next;
+    // received: the previous slab's into [0, rows), the next's into [ny - rows, ny)
+    const int a_prev = unpack ? 0 : 2 * h - rows, a_next = unpack ? ny - rows : ny - 2 * h;
+    void* f = ctx->f16 ? static_cast<void*>(ctx->h[ctx->cur]) : static_cast<void*>(ctx->f[ctx->cur]);
+    launch_slab_halo(f, ctx->f16 ? sizeof(__half) : sizeof(float), ctx->P.nx, ny, ctx->P.M * kQ, rows, a_prev,
+                     a_next, prev, next, unpack, ctx->stream);
+    LBL_CK(cudaGetLastError());
+    return LBL_OK;
+}
+}  // namespace
+
+int lbl_slab_pack(lbl_ctx* ctx, int rows, void* to_prev, void* to_next) {
+    return slab_halo(ctx, rows, to_prev, to_next, false);
+}
+
+int lbl_slab_unpack(lbl_ctx* ctx, int rows, const void* from_prev, const void* from_next) {
+    return slab_halo(ctx, rows, const_cast<void*>(from_prev), const_cast<void*>(from_next), true);
 }
 
 int lbl_set_io_prefix(lbl_ctx* ctx, const char* io_prefix) {
@@ -1579,9 +1682,10 @@ int lbl_batch_create(lbl_ctx* const* ctxs, int n, int strip_rows, lbl_batch** ou
     for (lbl_ctx* c : v) {
         if (!c || !c->initialised) { rc = LBL_ERR_STATE; b->err = "every context must exist and be initialised"; break; }
         if (c->device != v[0]->device) { rc = LBL_ERR_ARG; b->err = "the contexts of a batch share one device"; break; }
-        if (c->f16 || c->use_tma || c->closure || c->P.nx % kBatchW != 0) {
+        if (c->f16 || c->use_tma || c->closure || c->slab_ny || c->P.nx % kBatchW != 0) {
             rc = LBL_ERR_UNSUPPORTED;
-            b->err = "batched steps need FP32 storage, the direct stream-collide, no closure and nx a multiple of 128";
+            b->err = "batched steps need FP32 storage, the direct stream-collide, no closure, whole grids and nx a "
+                     "multiple of 128";
             break;
         }
     }

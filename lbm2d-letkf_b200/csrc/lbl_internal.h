@@ -39,7 +39,8 @@ struct Phys {
     double les_k;            // cs*cs*dx*dx evaluated in double like lbm.cu:59-60
     double tau_k;            // 3/c/c/dt chain, applied as ((3*nu)/c)/c)/dt in double
     double c_d, dt_d;        // c, dt widened to double for the tau chain
-    float inv_nx, inv_ny;    // 1/nx, 1/ny for the forcing coordinates
+    float inv_nx, inv_ny;    // 1/nx, 1/ny of the global grid for the forcing coordinates
+    int y0g, nyg;            // global row of local row 0 and the global row count (a y-slab; else 0, ny)
     // reciprocals of the constant divisors, rounded to float on the host: under
     // -use_fast_math, x / constant rounds exactly like x * (1/constant)
     float inv_c, inv_c2, inv_cs2, inv_two_dx;
@@ -158,6 +159,10 @@ struct lbl_ctx {
     bool closure = false;
     lbl::ClosureScales closure_sc{};
 
+    // y-slab split (lbl_slab_set): this context holds the global rows [slab_row0, slab_row0 + ny - 2 slab_halo)
+    // of a grid of slab_ny rows, plus slab_halo rows on each side; slab_ny = 0 for a whole grid
+    int slab_ny = 0, slab_row0 = 0, slab_halo = 0;
+
     // CUDA graphs keyed by (kind, n, parity)
     std::map<long long, cudaGraphExec_t> graphs;
 
@@ -175,6 +180,10 @@ namespace lbl {
 void launch_ic_velocity(const double* modes /*[4][n]*/, int n_modes, int nx, int ny,
                         float* u, float* v, cudaStream_t s);
 void launch_force_chunk(const lbl_ctx* c, int nsteps, int slot0, cudaStream_t s);
+// y-slab halos (slab.cu): rows [a_prev, a_prev + rows) and [a_next, a_next + rows) of every (member, q)
+// plane of the populations `f` (elem bytes each) to / from two packed buffers [plane][rows][nx]
+void launch_slab_halo(void* f, size_t elem, int nx, int ny, int planes, int rows, int a_prev, int a_next,
+                      void* buf_prev, void* buf_next, bool unpack, cudaStream_t s);
 // one step from population buffer src to dst (FP32 or FP16 storage)
 // pdl: the previous launch on s is the previous step; the launch may then overlap its
 // tail (programmatic dependent launch; the kernel waits for that grid's completion)
@@ -278,6 +287,7 @@ void launch_output_fields(const lbl_ctx* c, const float* mac, float* vor, float*
 void launch_rmse(const lbl_ctx* c, const float* mac, const float* ut, const float* vt, double* red,
                  cudaStream_t s);
 void launch_rmse_finish(const lbl_ctx* c, double* red, cudaStream_t s);
+void rmse_cells(const lbl_ctx* c, int* ij0, int* n);  // the cells an RMSE covers
 
 // ---- host helpers (host_io.cpp) ----
 std::string to_string_aligned(int t, int digits);

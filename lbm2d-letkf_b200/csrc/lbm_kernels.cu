@@ -265,6 +265,9 @@ __global__ void ic_velocity_kernel(const double* __restrict__ modes, int n, int 
     v[i + nx * j] = vtmp;
 }
 
+// the global row of local row j: the row itself for a whole grid, shifted and wrapped for a y-slab
+__device__ __forceinline__ int global_row(int j, const Phys& P) { return (j + P.y0g) % P.nyg; }
+
 // ---------------------------------------------------------------------------
 // Watanabe-97 forcing for `nsteps` consecutive steps (data.cu:317-348).  The
 // field does not depend on the member, so it is computed once per step for the
@@ -284,10 +287,10 @@ __global__ void force_chunk_kernel(const float* __restrict__ pool, const int* __
     __syncthreads();
     const int ij = blockIdx.x * blockDim.x + threadIdx.x;
     if (ij >= P.nxy) return;
-    const int nx = P.nx, ny = P.ny;
-    const int i = ij % nx, j = ij / nx;
+    const int nx = P.nx;
+    const int i = ij % nx, j = global_row(ij / nx, P);
     const float x = float(i - nx / 2) * P.inv_nx;
-    const float y = float(j - ny / 2) * P.inv_ny;
+    const float y = float(j - P.nyg / 2) * P.inv_ny;
     const float* force_kx = s_mode;
     const float* force_ky = s_mode + n;
     const float* force_rand = s_mode + 2 * n;
@@ -442,10 +445,10 @@ __global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __res
     __syncthreads();
     const int ij = blockIdx.x * blockDim.x + threadIdx.x;
     if (ij >= P.nxy) return;
-    const int nx = P.nx, ny = P.ny;
-    const int i = ij % nx, j = ij / nx;
+    const int nx = P.nx;
+    const int i = ij % nx, j = global_row(ij / nx, P);
     const float x = float(i - nx / 2) * P.inv_nx;
-    const float y = float(j - ny / 2) * P.inv_ny;
+    const float y = float(j - P.nyg / 2) * P.inv_ny;
     float sn[kRegModes], cn[kRegModes];
 #pragma unroll
     for (int k = 0; k < kRegModes; k++) {

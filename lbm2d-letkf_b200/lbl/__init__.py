@@ -53,6 +53,7 @@ EXPORTS = (
     "lbl_set_io_prefix", "lbl_h5_write_dataset", "lbl_autotune", "lbl_stream_collide_shape", "lbl_set_stream_collide_shape", "lbl_set_closure", "lbl_closure_generate",
     "lbl_closure_grad", "lbl_closure_train", "lbl_closure_infer", "lbl_batch_create", "lbl_batch_last_error",
     "lbl_batch_cycle_async", "lbl_batch_sync", "lbl_batch_destroy", "lbl_inject", "lbl_set_closure_refresh",
+    "lbl_slab_set", "lbl_slab_halo_bytes", "lbl_slab_pack", "lbl_slab_unpack",
 )
 INJECT_NONE, INJECT_TMA_STALL = 0, 1
 CLOSURE_PARAMS, CLOSURE_FEATURES = 1313, 6
@@ -164,6 +165,10 @@ def load_library() -> ctypes.CDLL:
         "lbl_set_stream_collide_shape": (I, [P, I, I]),
         "lbl_inject": (I, [P, I, I]),
         "lbl_set_closure_refresh": (I, [P, I]),
+        "lbl_slab_set": (I, [P, I, I, I]),
+        "lbl_slab_halo_bytes": (I, [P, I, ctypes.POINTER(U)]),
+        "lbl_slab_pack": (I, [P, I, P, P]),
+        "lbl_slab_unpack": (I, [P, I, P, P]),
         "lbl_h5_write_dataset": (I, [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, P, I]),
     }
     for name, (res, args) in sig.items():
@@ -389,6 +394,30 @@ class Ensemble:
         takes the heuristic's."""
         self._check(self.lib.lbl_set_stream_collide_shape(self._h, int(bool(prefetch)), int(strip_rows)),
                     "lbl_set_stream_collide_shape")
+
+    # -- y-slab split (lbl_slab_set; the exchange between ranks is lbl.slab's) ----------
+    def slab_set(self, ny_global: int, row0: int, halo: int):
+        """Make this context the rows [row0, row0 + ny - 2 halo) of a grid of ny_global rows,
+        with `halo` rows on each side (lbl_slab_set; between construction and init)."""
+        self._check(self.lib.lbl_slab_set(self._h, int(ny_global), int(row0), int(halo)), "lbl_slab_set")
+
+    def slab_halo_bytes(self, rows: int) -> int:
+        """Bytes of one packed halo buffer of `rows` rows (lbl_slab_halo_bytes)."""
+        n = ctypes.c_size_t()
+        self._check(self.lib.lbl_slab_halo_bytes(self._h, int(rows), ctypes.byref(n)), "lbl_slab_halo_bytes")
+        return n.value
+
+    def slab_pack(self, rows: int, to_prev: int, to_next: int):
+        """Pack the rows the neighbours need into two device buffers (addresses), on the
+        context's stream (lbl_slab_pack)."""
+        self._check(self.lib.lbl_slab_pack(self._h, int(rows), ctypes.c_void_p(to_prev), ctypes.c_void_p(to_next)),
+                    "lbl_slab_pack")
+
+    def slab_unpack(self, rows: int, from_prev: int, from_next: int):
+        """Unpack the neighbours' packed rows into the halos, on the context's stream
+        (lbl_slab_unpack)."""
+        self._check(self.lib.lbl_slab_unpack(self._h, int(rows), ctypes.c_void_p(from_prev),
+                                             ctypes.c_void_p(from_next)), "lbl_slab_unpack")
 
     def set_closure_refresh(self, steps: int):
         """Run the closure's network every `steps` steps and hold each cell's multiplier
