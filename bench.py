@@ -43,8 +43,11 @@ workload.  The line also carries `reference_build`: the reference's forecast alo
 as M processes sharing the GPU, one per member as its one-MPI-rank-per-member runs
 do, and the cycles/s bound it implies (`reference_build_bound_cycles_per_s`).
 
-Multi-GPU: replicas only (one independent experiment per GPU, no collective on
+Multi-GPU: by default replicas (one independent experiment per GPU, no collective on
 the data path); `value` is the cycles of all ranks / the slowest rank's time.
+`--shard slab` instead splits the workload's one experiment into y-bands, one per GPU
+(lbl.slab: all members of a band of rows per GPU, halo rows exchanged by NCCL send /
+receive); its value is that one experiment's cycles/s ("scaling": "strong").
 """
 import argparse
 import json
@@ -401,6 +404,85 @@ def run_engine(args, dist, rank, world, device):
         line["gpu_launches"] += c2["gpu_launches"] + c4["gpu_launches"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(oracle, obs[0])
+    return line
+
+
+def run_slab(args, dist, rank, world, device):
+    """The workload's ONE experiment split into y-bands, one band per GPU (lbl.slab): every rank
+    holds all members of ~NX/world rows plus 8 halo rows on each side, exchanges 8 rows with each
+    neighbour (NCCL send / receive on the engine's stream) every 4 steps and after each analysis,
+    and analyses its own rows.  The experiment is the same at every N ("scaling": "strong"); its
+    cycles/s is the one experiment's, timed per cycle with CUDA events on each rank's engine
+    stream, max over ranks.  One GPU is its own neighbour (the split's whole cost, no transfer)."""
+    import lbl
+    import torch
+    from lbl import slab
+    K, W = args.steps, args.warmup
+    T = STEPS_PER_CYCLE
+    obs, truth = make_observations(lbl, W + 2 * K + 1)
+    group = dist.group.WORLD if dist is not None else None
+    exp = slab.SlabExperiment(workload_config(lbl), world=world, group=group, device=device)
+    band = exp.local[0].ens
+    exp.init(0)
+    exp.update(0, T)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")
+    stream = torch.cuda.ExternalStream(band.stream(), device=f"cuda:{device}")
+
+    def flush_l2():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+
+    clk = ClockSampler(device).__enter__()
+    for c in range(W):
+        exp.assimilate((c + 1) * T, *obs[c])
+        exp.update((c + 1) * T, T)
+    exp.sync()
+    torch.cuda.synchronize(device)
+    barrier(dist)
+
+    def timed(c0, with_rmse):
+        ms, rmse = 0.0, []
+        for c in range(c0, c0 + K):
+            flush_l2()
+            band.event_record(0)
+            exp.assimilate((c + 1) * T, *obs[c])
+            exp.update((c + 1) * T, T)
+            if with_rmse:
+                rmse.append(exp.rmse_uv(*truth[c + 1]))
+            band.event_record(1)
+            ms += band.event_elapsed(0, 1)
+        exp.sync()
+        torch.cuda.synchronize(device)
+        barrier(dist)
+        return reduce_max(dist, ms, device), rmse
+
+    ms, _ = timed(W, False)
+    ms_e2e, rmse = timed(W + K, True)
+    clk.__exit__(None, None, None)
+    halo = exp.halo
+    k = halo // 2
+    chunks = -(-T // k)
+    nsites = (NX // P_OBS) ** 2
+    line = {
+        "metric": METRIC, "value": K / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f16 storage, f32 compute" if STORAGE else "f32",
+        "data": "synthetic (seeded nature run + Gaussian observation noise)",
+        "config": {"workload": WORKLOAD + f"; ONE experiment split in {world} y-bands",
+                   "parallelism": f"y-slab x{world}", "bands": [list(b) for b in exp.bands], "halo_rows": halo,
+                   "exchange": (f"{2 * k} rows per neighbour every {k} steps and {halo} after each analysis, "
+                                + ("NCCL send / receive" if world > 1 else "the band is its own neighbour")),
+                   "l2": "flushed (256 MB write on the engine's stream) between timed cycles, outside the timed "
+                         "intervals",
+                   "observations": "whole-grid host fields every cycle, each band uploads its rows"},
+        "e2e": {"value": K / (ms_e2e / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": 3 * nsites * 4 // world + 2 * NX * NX * 4 // world,
+                "d2h_bytes_per_step": 8, "forecast_rmse_uv_last": rmse[-1] if rmse else None},
+        "gpu_launches": K * (chunks * (1 + k + 2) + 5),
+        "letkf": exp.letkf_stats(),
+        "clocks": clk.summary(),
+    }
+    exp.close()
     return line
 
 
@@ -876,6 +958,9 @@ def main():
                     help="with --lbm: the learned-closure stream-collide (trained parameters of the package)")
     ap.add_argument("--autotune", action="store_true",
                     help="with --lbm: time at the strip height lbl_autotune picks instead of the heuristic's")
+    ap.add_argument("--shard", choices=["replicas", "slab"], default="replicas",
+                    help="N GPUs: independent experiments (replicas, the default) or the workload's one experiment "
+                         "split in y-bands, one per GPU (slab; C1 / C2 shapes)")
     ap.add_argument("--prefetch", type=int, default=None, choices=[0, 1],
                     help="the stream-collide's march (lbl_set_stream_collide_shape): 0 pulls each row when "
                          "needed, 1 holds the row after next in registers; default: the library's choice")
@@ -923,7 +1008,7 @@ def main():
         return
     dist, rank, world, device = init_dist()
     try:
-        line = run_engine(args, dist, rank, world, device)
+        line = (run_slab if args.shard == "slab" else run_engine)(args, dist, rank, world, device)
         if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
     finally:
