@@ -160,3 +160,26 @@ def test_slab_conditions_are_checked():
     with pytest.raises(lbl.LblError, match="Smagorinsky"):
         e.set_closure(np.zeros(lbl.CLOSURE_PARAMS, np.float32), 1e-4, 0.1)
     e.close()
+
+
+def test_c1_workload_in_two_bands_equals_the_whole_grid():
+    """The 256^2 x 16 DA workload's own settings (Cs 0.1, tau 0.51: nu from the global dt; the
+    k^4 exp initial condition rescaled by the whole grid's energy; members = the nature IC plus
+    10 % perturbations) through one forecast and one analysis in two bands."""
+    cfg = lbl.config_default("DA_LETKF", 256, 16, da_xyprune=4, letkf_rloc_len=1, letkf_covinf=1.1, obs_error_u=0.1,
+                             obs_error_rho=0.01, iiter=20, daprune=5, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP,
+                             ic_amp=1.0, ens_init=lbl.ENS_PERTURBED, ens_perturb=0.1)
+    ro, uo, vo, ut, vt = _observations(256, 100)
+    whole = _whole(cfg)
+    with slab.SlabExperiment(cfg, world=2) as exp:
+        exp.init(0)
+        _assert_own_rows_equal(whole, exp, "initial condition")
+        whole.update(0, 100)
+        exp.update(0, 100)
+        whole.assimilate(100, ro, uo, vo)
+        exp.assimilate(100, ro, uo, vo)
+        exp.sync()
+        assert whole.letkf_stats()["max_sweeps"] > 0
+        _assert_own_rows_equal(whole, exp, "one cycle")
+        assert exp.rmse_uv(ut, vt) == pytest.approx(whole.rmse_uv(ut, vt), rel=1e-12)
+    whole.close()
