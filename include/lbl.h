@@ -214,8 +214,9 @@ int lbl_get_diagnostics(lbl_ctx* ctx, int member, double* energy, double* enstro
 /* RMSE of the ensemble-mean (u,v) against host truth fields (FP64). */
 int lbl_rmse_uv(lbl_ctx* ctx, const float* u_true, const float* v_true, double* rmse);
 
-/* lbl_rmse_uv without waiting: enqueues the upload of the true fields, the FP64
- * reduction and the copy of the RMSE into *rmse on the context's stream and returns.
+/* lbl_rmse_uv without waiting: enqueues the upload of the true fields (on the context's
+ * second stream, so that it overlaps the work already queued, such as a cycle's forecast),
+ * the FP64 reduction and the copy of the RMSE into *rmse on the context's stream, and returns.
  * u_true, v_true and rmse must stay valid (and the fields unchanged) until the stream
  * has passed this point (lbl_sync, an lbl_event_elapsed on a later event, or the next
  * blocking call); in pinned host memory the copies are asynchronous. */

@@ -1332,15 +1332,22 @@ int lbl_rmse_uv(lbl_ctx* ctx, const float* u_true, const float* v_true, double* 
     return LBL_OK;
 }
 
+// The true fields go up on the side stream, beside the work the engine stream still has
+// queued (a cycle's forecast): ev[14] marks that the previous RMSE has read d_tmp, ev[13]
+// that this one's fields have arrived.
 int lbl_rmse_uv_async(lbl_ctx* ctx, const float* u_true, const float* v_true, double* rmse) {
     if (!ctx || !u_true || !v_true || !rmse) return LBL_ERR_ARG;
     LBL_TRY(set_device(ctx));
     const size_t nxy = size_t(ctx->P.nxy);
-    LBL_CK(cudaMemcpyAsync(ctx->d_tmp, u_true, sizeof(float) * nxy, cudaMemcpyHostToDevice, ctx->stream));
-    LBL_CK(cudaMemcpyAsync(ctx->d_tmp + nxy, v_true, sizeof(float) * nxy, cudaMemcpyHostToDevice, ctx->stream));
+    LBL_CK(cudaStreamWaitEvent(ctx->side, ctx->ev[14], 0));
+    LBL_CK(cudaMemcpyAsync(ctx->d_tmp, u_true, sizeof(float) * nxy, cudaMemcpyHostToDevice, ctx->side));
+    LBL_CK(cudaMemcpyAsync(ctx->d_tmp + nxy, v_true, sizeof(float) * nxy, cudaMemcpyHostToDevice, ctx->side));
+    LBL_CK(cudaEventRecord(ctx->ev[13], ctx->side));
+    LBL_CK(cudaStreamWaitEvent(ctx->stream, ctx->ev[13], 0));
     launch_rmse(ctx, ctx->mac[ctx->cur], ctx->d_tmp, ctx->d_tmp + nxy, ctx->d_red, ctx->stream);
     launch_rmse_finish(ctx, ctx->d_red, ctx->stream);
     LBL_CK(cudaGetLastError());
+    LBL_CK(cudaEventRecord(ctx->ev[14], ctx->stream));
     LBL_CK(cudaMemcpyAsync(rmse, ctx->d_red + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     return LBL_OK;
 }

@@ -169,7 +169,8 @@ struct lbl_ctx {
     // timers
     lbl::TimerMap timers[2];
     cudaEvent_t ev[16] = {};             // 0-3 stage timing, 4-5 sched staging, 6-7 obs staging, 8-9 profile,
-                                         // 10-12 phase events recorded inside the graphs
+                                         // 10-12 phase events recorded inside the graphs, 13-14 the
+                                         // asynchronous RMSE's true fields (arrived / read)
     cudaEvent_t user_ev[8] = {};         // lbl_event_record slots
     bool have_events = false;
 };
