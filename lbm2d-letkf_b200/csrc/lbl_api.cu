@@ -638,10 +638,13 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     // prefetched row up to 256 columns, the 4-column one (215 against 168 registers)
     // loses; FP16 deviations pay only with vector loads (512^2 x 64: 164 against
     // 218 us), FP32 at 512^2 x 64 stays fastest one column per thread (215 against
-    // 228 us), and at 256^2 x 16 two columns gain (12.9 against 14.4 us)
+    // 228 us), and at 256^2 x 16 two columns gain (12.9 against 14.4 us).  On a grid that
+    // is not square (a y-slab's band) the prefetching 2-column march holds 128 registers
+    // against 94 without prefetch, and loses: 256 x 272 x 16, 16.4 against 14.5 us
     ctx->vec_auto = cfg->lbm_variant == LBL_LBM_AUTO && cfg->nx <= 1024;
     if (ctx->vec_auto) ctx->vec = (ctx->f16 || cfg->nx <= 256) ? 2 : 0;
-    ctx->vec_pf = ctx->vec == 2 ? cfg->nx <= 256 : ctx->vec == 0;  // (the one-column kernels always prefetch)
+    ctx->vec_pf = ctx->vec == 2 ? cfg->nx <= 256 && cfg->nx == cfg->ny
+                                : ctx->vec == 0;  // (the one-column kernels always prefetch)
     ctx->ty_default = lbm_strip_rows(ctx);
     for (auto& e : ctx->ev) LBL_CK(cudaEventCreate(&e));
     for (auto& e : ctx->user_ev) LBL_CK(cudaEventCreate(&e));

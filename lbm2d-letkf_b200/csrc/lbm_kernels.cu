@@ -489,7 +489,8 @@ __global__ void __launch_bounds__(256) force_chunk_reg_kernel(const float* __res
 // friction) straight from registers.  Rows j0-1 and j1 are pulled as halo so that
 // the whole step is one pass over f: 72 B/cell of compulsory traffic in FP32.
 // NX > 0 fixes the (square) grid at compile time so that plane and row offsets are
-// immediates; NX = 0 reads nx, ny from P.
+// immediates; NX < 0 fixes only nx = -NX (a y-slab's band: ny and the plane stride from
+// P); NX = 0 reads nx, ny from P.
 // ---------------------------------------------------------------------------
 // (256 threads: the plain kernel is held to 4 CTAs per SM, 64 registers, the closure variant
 // to 2, 128 registers)
@@ -512,7 +513,7 @@ __global__ void __launch_bounds__(MAXT, MAXT == 256 ? (CL ? 2 : 4) : 1)
     // frees, so the launch gap between steps overlaps this grid's tail.
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" :::);
-    const int nx = NX ? NX : P.nx, ny = NX ? NX : P.ny, nxy = NX ? NX * NX : P.nxy;
+    const int nx = NX ? (NX < 0 ? -NX : NX) : P.nx, ny = NX > 0 ? NX : P.ny, nxy = NX > 0 ? NX * NX : P.nxy;
     const int W = CLU ? int(blockDim.x) : nx;  // columns of this CTA
     const int xl = threadIdx.x;
     const int x = CLU ? int(blockIdx.z) * W + xl : xl;
@@ -695,13 +696,13 @@ struct VecIO<__half, VW> {
 // CLH: the learned closure between two evaluations of its network, each cell's
 // multiplier read from mclos (lbm_step_kernel's CLH form, cell for cell)
 template <bool WRITE_MAC, int NX, int VW, bool PF, typename T, bool CLH = false>
-__global__ void __launch_bounds__(NX ? NX / VW : 1024 / VW)
+__global__ void __launch_bounds__(NX ? (NX < 0 ? -NX : NX) / VW : 1024 / VW)
     lbm_step_vec_kernel(const T* __restrict__ fin, T* __restrict__ fout, const float* __restrict__ force,
                         float* __restrict__ mac, Phys P, int TY, const float* __restrict__ mclos) {
     extern __shared__ float4 s_edge[];  // [3][nt]: (u, v) of the first and of the last column
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" :::);
-    const int nx = NX ? NX : P.nx, ny = NX ? NX : P.ny, nxy = NX ? NX * NX : P.nxy;
+    const int nx = NX ? (NX < 0 ? -NX : NX) : P.nx, ny = NX > 0 ? NX : P.ny, nxy = NX > 0 ? NX * NX : P.nxy;
     const int nt = nx / VW;  // threads of a row
     const int t = threadIdx.x;
     const int x0 = t * VW;
@@ -1189,6 +1190,13 @@ __global__ void macros_kernel(const T* __restrict__ f, float* __restrict__ mac, 
     mm[2 * P.nxy + ij] = v;
 }
 
+// The compile-time shape of the plain stream-collide: nx for the square grids it is built
+// for, -nx for a y-slab's band of 256 or 512 columns (nx fixed, rows from P), else 0.
+int shape_key(const Phys& P) {
+    if (P.nx == P.ny) return (P.nx == 64 || P.nx == 128 || P.nx == 256 || P.nx == 512 || P.nx == 1024) ? P.nx : 0;
+    return (P.nx == 256 || P.nx == 512) ? -P.nx : 0;
+}
+
 // The kernel launch_lbm_step runs for a context (its WRITE_MAC = false form), with its
 // block size and dynamic shared memory, for the occupancy query of the strip height.
 struct StepKernel {
@@ -1216,7 +1224,9 @@ StepKernel direct_kernel(const lbl_ctx* c) {
         return {(const void*)lbm_step_kernel<false, 1024, 0, T, true>, P.nx, sm};
     }
     const size_t sm = sizeof(float) * 6 * P.nx;
-    switch (sq) {
+    switch (shape_key(P)) {
+        case -256: return {(const void*)lbm_step_kernel<false, 256, -256, T>, P.nx, sm};
+        case -512: return {(const void*)lbm_step_kernel<false, 1024, -512, T>, P.nx, sm};
         case 64: return {(const void*)lbm_step_kernel<false, 256, 64, T>, P.nx, sm};
         case 128: return {(const void*)lbm_step_kernel<false, 256, 128, T>, P.nx, sm};
         case 256: return {(const void*)lbm_step_kernel<false, 256, 256, T>, P.nx, sm};
@@ -1230,8 +1240,10 @@ StepKernel direct_kernel(const lbl_ctx* c) {
 template <int VW, bool PF, typename T>
 StepKernel vec_kernel_w(const lbl_ctx* c) {
     const Phys& P = c->P;
-    const int sq = (P.nx == P.ny) ? P.nx : 0;
-    const void* fn = sq == 64     ? (const void*)lbm_step_vec_kernel<false, 64, VW, PF, T>
+    const int sq = shape_key(P);
+    const void* fn = sq == -256   ? (const void*)lbm_step_vec_kernel<false, -256, VW, PF, T>
+                     : sq == -512 ? (const void*)lbm_step_vec_kernel<false, -512, VW, PF, T>
+                     : sq == 64   ? (const void*)lbm_step_vec_kernel<false, 64, VW, PF, T>
                      : sq == 128  ? (const void*)lbm_step_vec_kernel<false, 128, VW, PF, T>
                      : sq == 256  ? (const void*)lbm_step_vec_kernel<false, 256, VW, PF, T>
                      : sq == 512  ? (const void*)lbm_step_vec_kernel<false, 512, VW, PF, T>
@@ -1532,8 +1544,9 @@ void launch_vec_t(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const f
 template <int VW, bool PF>
 void launch_vec_w(const lbl_ctx* c, dim3 grid, int ty, int src, int dst, const float* force, float* mac_out,
                   cudaStream_t s, bool pdl) {
-    const int sq = (c->P.nx == c->P.ny) ? c->P.nx : 0;
-    switch (sq) {
+    switch (shape_key(c->P)) {
+        case -256: launch_vec_t<-256, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        case -512: launch_vec_t<-512, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
         case 64: launch_vec_t<64, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
         case 128: launch_vec_t<128, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
         case 256: launch_vec_t<256, VW, PF>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
@@ -1604,7 +1617,9 @@ void launch_lbm_step(const lbl_ctx* c, int src, int dst, const float* force, flo
         launch_vec(c, grid, ty, src, dst, force, mac_out, s, pdl);
         return;
     }
-    switch (sq) {
+    switch (shape_key(P)) {
+        case -256: launch_direct<256, -256>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
+        case -512: launch_direct<1024, -512>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
         case 64: launch_direct<256, 64>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
         case 128: launch_direct<256, 128>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;
         case 256: launch_direct<256, 256>(c, grid, ty, src, dst, force, mac_out, s, pdl); break;

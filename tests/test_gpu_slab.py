@@ -64,11 +64,13 @@ def test_pack_and_unpack_move_the_planned_rows():
 
 
 @pytest.mark.parametrize("storage", [lbl.STORAGE_F32, lbl.STORAGE_F16])
-@pytest.mark.parametrize("world,halo,bands", [
-    (1, 2, None), (2, 2, None), (3, 2, [(0, 40), (40, 40), (80, 48)]), (4, 8, None), (2, 6, [(0, 72), (72, 56)]),
+@pytest.mark.parametrize("nx,world,halo,bands", [
+    (128, 1, 2, None), (128, 2, 2, None), (128, 3, 2, [(0, 40), (40, 40), (80, 48)]), (128, 4, 8, None),
+    (128, 2, 6, [(0, 72), (72, 56)]),
+    (256, 2, 8, None), (512, 2, 8, None),  # the bands' kernels specialised on 256 and 512 columns
 ])
-def test_forecast_bands_equal_the_whole_grid(storage, world, halo, bands):
-    cfg = lbl.config_default("NATURE", 128, 4, storage=storage)
+def test_forecast_bands_equal_the_whole_grid(storage, nx, world, halo, bands):
+    cfg = lbl.config_default("NATURE", nx, 4, storage=storage)
     whole = _whole(cfg)
     with slab.SlabExperiment(cfg, world=world, halo=halo, bands=bands) as exp:
         exp.init(0)
