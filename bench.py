@@ -461,7 +461,8 @@ def run_slab(args, dist, rank, world, device):
     clk.__exit__(None, None, None)
     halo = exp.halo
     k = halo // 2
-    chunks = -(-T // k)
+    segments = -(-T // exp.segment)  # forcing launches per cycle (lbl_slab_forecast_begin)
+    chunks = sum(-(-min(exp.segment, T - i) // k) for i in range(0, T, exp.segment))
     nsites = (NX // P_OBS) ** 2
     line = {
         "metric": METRIC, "value": K / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
@@ -478,7 +479,9 @@ def run_slab(args, dist, rank, world, device):
         "e2e": {"value": K / (ms_e2e / 1e3), "unit": UNIT,
                 "h2d_bytes_per_step": 3 * nsites * 4 // world + 2 * NX * NX * 4 // world,
                 "d2h_bytes_per_step": 8, "forecast_rmse_uv_last": rmse[-1] if rmse else None},
-        "gpu_launches": K * (chunks * (1 + k + 2) + 5),
+        # per cycle: forcing, the steps, a pack and an unpack per chunk, then the observation
+        # operator, the analysis and the analysis' pack and unpack
+        "gpu_launches": K * (segments + T + 2 * chunks + 4),
         "letkf": exp.letkf_stats(),
         "clocks": clk.summary(),
     }

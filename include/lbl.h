@@ -313,7 +313,8 @@ int lbl_set_stream_collide_shape(lbl_ctx* ctx, int prefetch, int strip_rows);
  * (row0 - halo + r) mod ny_global.  Every kernel runs over the slab as if it were periodic;
  * after k steps the outer 2k rows on each side are stale and the neighbours' packed rows
  * replace them:
- *   - step at most halo / 2 steps with lbl_update_async, then exchange 2k rows;
+ *   - step at most halo / 2 steps (lbl_slab_forecast_chunk, or lbl_update_async), then
+ *     exchange 2k rows;
  *   - after lbl_assimilate_async exchange all `halo` rows (the analysis of the halo rows
  *     reads past the slab).
  * The observation fields given to lbl_assimilate are the slab's own nx * cfg.ny rows,
@@ -325,6 +326,19 @@ int lbl_set_stream_collide_shape(lbl_ctx* ctx, int prefetch, int strip_rows);
  * (lbl_cycle_async), diagnostics or batch.  lbl_rmse_uv covers the own rows; its truth
  * fields are the slab's nx * cfg.ny values. */
 int lbl_slab_set(lbl_ctx* ctx, int ny_global, int row0, int halo);
+
+/* A band's forecast in chunks, with the halo exchange between them.  lbl_slab_forecast_begin
+ * computes the forcing of the next nsteps steps in one launch (nsteps in
+ * [1, lbl_slab_forecast_steps], the steps the forcing buffer holds: every band of an experiment
+ * must begin the same nsteps, so take the smallest over the bands).  Each
+ * lbl_slab_forecast_chunk then advances k of those steps (k in [1, halo / 2]), on the
+ * context's stream; rho, u, v are written on the last two steps of the begun forecast only, as
+ * one lbl_update call writes them.  After each chunk the caller exchanges 2k rows.  Until the
+ * last chunk, lbl_update and lbl_assimilate return LBL_ERR_STATE.  Replaces a loop of
+ * lbl_update_async calls of k steps, which computes the forcing and writes the macros per call. */
+int lbl_slab_forecast_steps(const lbl_ctx* ctx, int* max_steps);
+int lbl_slab_forecast_begin(lbl_ctx* ctx, int t0, int nsteps);
+int lbl_slab_forecast_chunk(lbl_ctx* ctx, int k);
 
 /* Bytes of one packed halo buffer of `rows` rows: M * 9 * rows * nx elements of the
  * storage type (4 bytes, or 2 with LBL_STORAGE_F16).  No GPU work. */

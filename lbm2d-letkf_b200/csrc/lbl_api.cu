@@ -23,6 +23,9 @@ namespace {
 
 int wait_output(lbl_ctx* ctx);
 
+// a chunked forecast (lbl_slab_forecast_begin) owns the forcing buffer until its last chunk
+constexpr const char* kSlabBegun = "a chunked forecast (lbl_slab_forecast_begin) has steps left";
+
 // what a y-slab context (lbl_slab_set) does not do
 constexpr const char* kSlabCycle =
     "a y-slab exchanges halos between its steps: lbl_update_async, lbl_assimilate_async and lbl_slab_pack / "
@@ -756,6 +759,7 @@ int init_impl(lbl_ctx* ctx, int ens_offset) {
 
 int update_impl(lbl_ctx* ctx, int nsteps, bool sync) {
     if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_update before lbl_init");
+    if (ctx->fc_off < ctx->fc_total) return fail(ctx, LBL_ERR_STATE, kSlabBegun);
     if (nsteps < 0) return fail(ctx, LBL_ERR_ARG, "nsteps < 0");
     int left = nsteps;
     while (left > 0) {
@@ -829,6 +833,7 @@ int nudging_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const fl
 int assimilate_impl(lbl_ctx* ctx, int t, const float* ro, const float* uo, const float* vo, bool sync) {
     if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate before lbl_init");
     if (!is_da_mode(ctx->cfg.mode)) return fail(ctx, LBL_ERR_STATE, "lbl_assimilate needs mode DA_LETKF or DA_NUDGING");
+    if (ctx->fc_off < ctx->fc_total) return fail(ctx, LBL_ERR_STATE, kSlabBegun);
     if (ctx->cfg.da_dummy) return LBL_OK;                           // DA_DUMMY: no assimilation (main.cu:94)
     if (ctx->cfg.mode == LBL_MODE_DA_NUDGING) return nudging_impl(ctx, t, ro, uo, vo, sync);
     TimerMap& tm = ctx->timers[LBL_TIMER_LETKF];
@@ -1537,6 +1542,51 @@ int slab_halo(lbl_ctx* ctx, int rows, void* prev, void* next, bool unpack) {
     return LBL_OK;
 }
 }  // namespace
+
+int lbl_slab_forecast_steps(const lbl_ctx* ctx, int* max_steps) {
+    if (!ctx || !max_steps) return LBL_ERR_ARG;
+    *max_steps = ctx->force_cap;
+    return LBL_OK;
+}
+
+int lbl_slab_forecast_begin(lbl_ctx* ctx, int t0, int nsteps) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    (void)t0;
+    if (!ctx->slab_ny) return fail(ctx, LBL_ERR_STATE, "not a y-slab context (lbl_slab_set)");
+    if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_slab_forecast_begin before lbl_init");
+    if (ctx->fc_off < ctx->fc_total) return fail(ctx, LBL_ERR_STATE, kSlabBegun);
+    if (nsteps < 1 || nsteps > ctx->force_cap)
+        return fail(ctx, LBL_ERR_ARG, "nsteps must lie in [1, lbl_slab_forecast_steps]");
+    // the forcing of every step at once, as the whole-grid cycle graph computes it
+    LBL_TRY(schedule_force(ctx, nsteps));
+    launch_force_chunk(ctx, nsteps, 0, ctx->stream);
+    LBL_CK(cudaGetLastError());
+    ctx->fc_total = nsteps;
+    ctx->fc_off = 0;
+    return LBL_OK;
+}
+
+int lbl_slab_forecast_chunk(lbl_ctx* ctx, int k) {
+    if (!ctx) return LBL_ERR_ARG;
+    LBL_TRY(set_device(ctx));
+    if (ctx->fc_off >= ctx->fc_total)
+        return fail(ctx, LBL_ERR_STATE, "no chunked forecast has steps left (lbl_slab_forecast_begin)");
+    if (k < 1 || k > ctx->slab_halo / 2 || k > ctx->fc_total - ctx->fc_off)
+        return fail(ctx, LBL_ERR_ARG, "k must lie in [1, min(halo / 2, steps left)]");
+    const size_t plane2 = size_t(2) * ctx->P.nxy;
+    for (int s = 0; s < k; s++) {
+        const int g = ctx->fc_off + s, src = ctx->cur, dst = src ^ 1;
+        // rho, u, v are written on the forecast's last two steps only, as by one lbl_update call
+        float* mac = g >= ctx->fc_total - 2 ? ctx->mac[dst] : nullptr;
+        launch_lbm_step(ctx, src, dst, ctx->d_force + size_t(g) * plane2, mac, ctx->stream, /*pdl=*/s > 0, g);
+        ctx->cur = dst;
+    }
+    LBL_CK(cudaGetLastError());
+    ctx->fc_off += k;
+    ctx->last_force_slot = ctx->fc_off - 1;
+    return LBL_OK;
+}
 
 int lbl_slab_pack(lbl_ctx* ctx, int rows, void* to_prev, void* to_next) {
     return slab_halo(ctx, rows, to_prev, to_next, false);

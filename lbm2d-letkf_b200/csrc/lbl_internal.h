@@ -162,6 +162,7 @@ struct lbl_ctx {
     // y-slab split (lbl_slab_set): this context holds the global rows [slab_row0, slab_row0 + ny - 2 slab_halo)
     // of a grid of slab_ny rows, plus slab_halo rows on each side; slab_ny = 0 for a whole grid
     int slab_ny = 0, slab_row0 = 0, slab_halo = 0;
+    int fc_total = 0, fc_off = 0;        // chunked forecast (lbl_slab_forecast_begin): steps begun, steps done
 
     // CUDA graphs keyed by (kind, n, parity)
     std::map<long long, cudaGraphExec_t> graphs;

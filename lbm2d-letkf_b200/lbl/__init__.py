@@ -53,7 +53,8 @@ EXPORTS = (
     "lbl_set_io_prefix", "lbl_h5_write_dataset", "lbl_autotune", "lbl_stream_collide_shape", "lbl_set_stream_collide_shape", "lbl_set_closure", "lbl_closure_generate",
     "lbl_closure_grad", "lbl_closure_train", "lbl_closure_infer", "lbl_batch_create", "lbl_batch_last_error",
     "lbl_batch_cycle_async", "lbl_batch_sync", "lbl_batch_destroy", "lbl_inject", "lbl_set_closure_refresh",
-    "lbl_slab_set", "lbl_slab_halo_bytes", "lbl_slab_pack", "lbl_slab_unpack",
+    "lbl_slab_set", "lbl_slab_halo_bytes", "lbl_slab_pack", "lbl_slab_unpack", "lbl_slab_forecast_steps",
+    "lbl_slab_forecast_begin", "lbl_slab_forecast_chunk",
 )
 INJECT_NONE, INJECT_TMA_STALL = 0, 1
 CLOSURE_PARAMS, CLOSURE_FEATURES = 1313, 6
@@ -169,6 +170,9 @@ def load_library() -> ctypes.CDLL:
         "lbl_slab_halo_bytes": (I, [P, I, ctypes.POINTER(U)]),
         "lbl_slab_pack": (I, [P, I, P, P]),
         "lbl_slab_unpack": (I, [P, I, P, P]),
+        "lbl_slab_forecast_steps": (I, [P, ctypes.POINTER(I)]),
+        "lbl_slab_forecast_begin": (I, [P, I, I]),
+        "lbl_slab_forecast_chunk": (I, [P, I]),
         "lbl_h5_write_dataset": (I, [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, P, I]),
     }
     for name, (res, args) in sig.items():
@@ -400,6 +404,20 @@ class Ensemble:
         """Make this context the rows [row0, row0 + ny - 2 halo) of a grid of ny_global rows,
         with `halo` rows on each side (lbl_slab_set; between construction and init)."""
         self._check(self.lib.lbl_slab_set(self._h, int(ny_global), int(row0), int(halo)), "lbl_slab_set")
+
+    def slab_forecast_steps(self) -> int:
+        """The most steps one chunked forecast can begin (lbl_slab_forecast_steps)."""
+        n = ctypes.c_int()
+        self._check(self.lib.lbl_slab_forecast_steps(self._h, ctypes.byref(n)), "lbl_slab_forecast_steps")
+        return n.value
+
+    def slab_forecast_begin(self, t0: int, nsteps: int):
+        """Compute the forcing of the next nsteps steps at once (lbl_slab_forecast_begin)."""
+        self._check(self.lib.lbl_slab_forecast_begin(self._h, int(t0), int(nsteps)), "lbl_slab_forecast_begin")
+
+    def slab_forecast_chunk(self, k: int):
+        """Advance k begun steps on the context's stream (lbl_slab_forecast_chunk)."""
+        self._check(self.lib.lbl_slab_forecast_chunk(self._h, int(k)), "lbl_slab_forecast_chunk")
 
     def slab_halo_bytes(self, rows: int) -> int:
         """Bytes of one packed halo buffer of `rows` rows (lbl_slab_halo_bytes)."""

@@ -155,6 +155,16 @@ class SlabExperiment:
         except Exception:
             self.close()
             raise
+        # every band begins forecasts of the same length: the fewest steps any band's forcing buffer holds
+        seg = min(b.ens.slab_forecast_steps() for b in self.local)
+        if group is not None and world > 1:
+            import torch
+            import torch.distributed as dist
+            dev = f"cuda:{device}" if dist.get_backend(group) == "nccl" else "cpu"
+            t = torch.tensor([seg], dtype=torch.int64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MIN, group=group)
+            seg = int(t.item())
+        self.segment = seg
 
     # -- set-up --------------------------------------------------------------------
     def init(self, ens_offset: int = 0):
@@ -202,16 +212,23 @@ class SlabExperiment:
 
     # -- the cycle ------------------------------------------------------------------
     def update(self, t0: int, nsteps: int):
-        """nsteps steps from t0, exchanging after every halo / 2 of them."""
+        """nsteps steps from t0: the forcing of up to `segment` steps at once
+        (lbl_slab_forecast_begin), then chunks of halo / 2 steps with an exchange after each."""
         k_max = max(1, self.halo // 2)
         t, left = t0, nsteps
         while left > 0:
-            k = min(k_max, left)
+            n = min(left, self.segment)
             for b in self.local:
-                b.ens.update(t, k, sync=False)
-            self.exchange(2 * k)
-            t += k
-            left -= k
+                b.ens.slab_forecast_begin(t, n)
+            done = 0
+            while done < n:
+                k = min(k_max, n - done)
+                for b in self.local:
+                    b.ens.slab_forecast_chunk(k)
+                self.exchange(2 * k)
+                done += k
+            t += n
+            left -= n
 
     def local_fields(self, b: _Band, *fields):
         """Slices of whole-grid (ny, nx) fields holding band b's rows, halos included."""

@@ -161,6 +161,24 @@ def test_slab_conditions_are_checked():
         e.output(0, "/nonexistent")
     with pytest.raises(lbl.LblError, match="Smagorinsky"):
         e.set_closure(np.zeros(lbl.CLOSURE_PARAMS, np.float32), 1e-4, 0.1)
+    # the chunked forecast: begun steps only, at most halo / 2 per chunk, nothing else until done
+    with pytest.raises(lbl.LblError, match="no chunked forecast"):
+        e.slab_forecast_chunk(2)
+    with pytest.raises(lbl.LblError, match=r"\[1, lbl_slab_forecast_steps\]"):
+        e.slab_forecast_begin(0, e.slab_forecast_steps() + 1)
+    e.slab_forecast_begin(0, 6)
+    with pytest.raises(lbl.LblError, match="has steps left"):
+        e.update(0, 1)
+    with pytest.raises(lbl.LblError, match="has steps left"):
+        e.slab_forecast_begin(0, 6)
+    with pytest.raises(lbl.LblError, match=r"halo / 2"):
+        e.slab_forecast_chunk(5)
+    e.slab_forecast_chunk(4)
+    with pytest.raises(lbl.LblError, match=r"steps left\)"):
+        e.slab_forecast_chunk(3)
+    e.slab_forecast_chunk(2)
+    e.update(6, 1)
+    e.sync()
     e.close()
 
 
