@@ -253,15 +253,17 @@ void compact_obs(const lbl_ctx* ctx, const float* ro, const float* uo, const flo
 }
 
 // schedule the forcing of `n` consecutive calls and upload the offsets through
-// one of two pinned staging buffers (an event guards each buffer's reuse)
-int schedule_force(lbl_ctx* ctx, int n) {
+// one of two pinned staging buffers (an event guards each buffer's reuse), on `st`
+// (the context's stream by default)
+int schedule_force(lbl_ctx* ctx, int n, cudaStream_t st = nullptr) {
+    if (!st) st = ctx->stream;
     const int b = ctx->sched_buf;
     ctx->sched_buf ^= 1;
     LBL_CK(cudaEventSynchronize(ctx->ev[4 + b]));
     int* h = ctx->h_sched[b];
     for (int s = 0; s < n; s++) LBL_TRY(force_call(ctx, &h[s]));
-    LBL_CK(cudaMemcpyAsync(ctx->d_sched, h, sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream));
-    LBL_CK(cudaEventRecord(ctx->ev[4 + b], ctx->stream));
+    LBL_CK(cudaMemcpyAsync(ctx->d_sched, h, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    LBL_CK(cudaEventRecord(ctx->ev[4 + b], st));
     return LBL_OK;
 }
 
@@ -746,6 +748,7 @@ int init_impl(lbl_ctx* ctx, int ens_offset) {
         }
     }
     // forcing: cursor starts "outdated", two update_forces calls at init (data.cu:236, :158)
+    ctx->fc_free_recorded = false;
     ctx->i_rand_outdated = ctx->n_rand_buf;
     ctx->rand_block = -1;
     LBL_TRY(schedule_force(ctx, 2));
@@ -761,6 +764,7 @@ int update_impl(lbl_ctx* ctx, int nsteps, bool sync) {
     if (!ctx->initialised) return fail(ctx, LBL_ERR_STATE, "lbl_update before lbl_init");
     if (ctx->fc_off < ctx->fc_total) return fail(ctx, LBL_ERR_STATE, kSlabBegun);
     if (nsteps < 0) return fail(ctx, LBL_ERR_ARG, "nsteps < 0");
+    ctx->fc_free_recorded = false;  // these steps read the forcing slots on the context's stream
     int left = nsteps;
     while (left > 0) {
         // each chunk writes macros on its last two steps, so whatever the chunking,
@@ -1558,10 +1562,20 @@ int lbl_slab_forecast_begin(lbl_ctx* ctx, int t0, int nsteps) {
     if (ctx->fc_off < ctx->fc_total) return fail(ctx, LBL_ERR_STATE, kSlabBegun);
     if (nsteps < 1 || nsteps > ctx->force_cap)
         return fail(ctx, LBL_ERR_ARG, "nsteps must lie in [1, lbl_slab_forecast_steps]");
-    // the forcing of every step at once, as the whole-grid cycle graph computes it
-    LBL_TRY(schedule_force(ctx, nsteps));
-    launch_force_chunk(ctx, nsteps, 0, ctx->stream);
+    // The forcing of every step at once, as the whole-grid cycle graph computes it.  After a
+    // chunked forecast it runs on the side stream, beside whatever the context's stream still
+    // runs (the analysis), once the last step that read the slots is done (ev[15]); the first
+    // chunk waits for it (ev[16]).
+    const bool side = ctx->fc_free_recorded;
+    cudaStream_t fs = side ? ctx->side : ctx->stream;
+    if (side) LBL_CK(cudaStreamWaitEvent(ctx->side, ctx->ev[15], 0));
+    LBL_TRY(schedule_force(ctx, nsteps, fs));
+    launch_force_chunk(ctx, nsteps, 0, fs);
     LBL_CK(cudaGetLastError());
+    if (side) {
+        LBL_CK(cudaEventRecord(ctx->ev[16], ctx->side));
+        LBL_CK(cudaStreamWaitEvent(ctx->stream, ctx->ev[16], 0));
+    }
     ctx->fc_total = nsteps;
     ctx->fc_off = 0;
     return LBL_OK;
@@ -1585,6 +1599,10 @@ int lbl_slab_forecast_chunk(lbl_ctx* ctx, int k) {
     LBL_CK(cudaGetLastError());
     ctx->fc_off += k;
     ctx->last_force_slot = ctx->fc_off - 1;
+    if (ctx->fc_off == ctx->fc_total) {  // the forcing slots are free once this step is done
+        LBL_CK(cudaEventRecord(ctx->ev[15], ctx->stream));
+        ctx->fc_free_recorded = true;
+    }
     return LBL_OK;
 }
 

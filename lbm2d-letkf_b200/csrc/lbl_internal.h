@@ -163,15 +163,17 @@ struct lbl_ctx {
     // of a grid of slab_ny rows, plus slab_halo rows on each side; slab_ny = 0 for a whole grid
     int slab_ny = 0, slab_row0 = 0, slab_halo = 0;
     int fc_total = 0, fc_off = 0;        // chunked forecast (lbl_slab_forecast_begin): steps begun, steps done
+    bool fc_free_recorded = false;       // ev[15] follows the last reader of the forcing slots
 
     // CUDA graphs keyed by (kind, n, parity)
     std::map<long long, cudaGraphExec_t> graphs;
 
     // timers
     lbl::TimerMap timers[2];
-    cudaEvent_t ev[16] = {};             // 0-3 stage timing, 4-5 sched staging, 6-7 obs staging, 8-9 profile,
+    cudaEvent_t ev[17] = {};             // 0-3 stage timing, 4-5 sched staging, 6-7 obs staging, 8-9 profile,
                                          // 10-12 phase events recorded inside the graphs, 13-14 the
-                                         // asynchronous RMSE's true fields (arrived / read)
+                                         // asynchronous RMSE's true fields (arrived / read), 15-16 a chunked
+                                         // forecast's forcing slots (free after its last step / filled)
     cudaEvent_t user_ev[8] = {};         // lbl_event_record slots
     bool have_events = false;
 };
