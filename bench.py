@@ -23,7 +23,8 @@ One bench "step" = one DA cycle = the LETKF analysis + 100 LBM steps.
             / the average launch time from CUDA events (lbl_profile_step)
   cpu_baseline  the FP64 OpenMP oracle on this host's cores, bounded sample
   analysis_roofline  the LETKF analysis phase against the nominal FP32 SIMT peak
-            (algorithmic flops of the survey's per-point formulas)
+            (algorithmic flops per grid point: Gram 2 n_obs M^2, transform
+            2*9*M^2 + 4 M^3, Jacobi 18 M M(M-1)/2 per sweep)
 
   roofline_hbm, c2_cycles_per_s, c4_cycles_per_s  (default C1 line on one GPU)
             two side legs timed the same way: C2 (512^2 x 64, 604 MB population

@@ -59,7 +59,7 @@ def test_a_missing_build_is_reported(tmp_path):
     assert "unavailable" in r
 
 
-def test_analysis_roofline_counts_the_survey_flops():
+def test_analysis_roofline_counts_the_per_point_flops():
     """analysis_roofline: Gram 2 n_obs M^2 + transform 2*9*M^2 + 4 M^3 + Jacobi 18 M M(M-1)/2
     per sweep, per grid point, over the phase time, against 148 x 128 x 2 x 1.965 GHz."""
     nx, m = bench.NX, bench.M
