@@ -12,6 +12,8 @@ the only traffic is a halo of rows between neighbouring bands:
   rank sends 2k rows to each neighbour (one packed buffer of all members and directions per
   neighbour), and after an analysis all `halo` rows (the analysis of halo rows reads past the
   band);
+* a forecast computes its forcing once (lbl_slab_forecast_begin) and advances in chunks of
+  halo / 2 steps (lbl_slab_forecast_chunk), the exchange between chunks;
 * the own rows then equal the single-context run bit for bit.
 
 `ring_exchange` moves the packed buffers with torch.distributed point-to-point operations
@@ -130,7 +132,10 @@ class SlabExperiment:
     initialised torch.distributed process group, NCCL for GPUs) this process holds its own
     rank's band on `device`; without it the experiment's `world` bands all live in this
     process on `device` and exchange by reading each other's buffers.  halo: rows kept on each
-    side (default_halo(cfg) if None); every band must own at least `halo` rows.
+    side (default_halo(cfg) if None); every band must own at least `halo` rows.  With a group,
+    construction, update, assimilate and rmse_uv are collective: every rank calls them in the
+    same order (the bands agree on the forecast segment length by an all-reduce at
+    construction, and exchange halos in every update and assimilate).
     """
 
     def __init__(self, cfg, world: int = 1, group=None, halo: Optional[int] = None, device: int = 0,

@@ -182,24 +182,28 @@ def test_slab_conditions_are_checked():
     e.close()
 
 
-def test_c1_workload_in_two_bands_equals_the_whole_grid():
+@pytest.mark.parametrize("world", [2, 4])
+def test_c1_workload_in_bands_equals_the_whole_grid(world):
     """The 256^2 x 16 DA workload's own settings (Cs 0.1, tau 0.51: nu from the global dt; the
     k^4 exp initial condition rescaled by the whole grid's energy; members = the nature IC plus
-    10 % perturbations) through one forecast and one analysis in two bands."""
+    10 % perturbations) through three whole cycles (100 steps, then an analysis) in 2 and 4
+    bands: bit for bit, and the same RMSE."""
     cfg = lbl.config_default("DA_LETKF", 256, 16, da_xyprune=4, letkf_rloc_len=1, letkf_covinf=1.1, obs_error_u=0.1,
                              obs_error_rho=0.01, iiter=20, daprune=5, cs=0.1, tau=0.51, ic_kind=lbl.IC_K4EXP,
                              ic_amp=1.0, ens_init=lbl.ENS_PERTURBED, ens_perturb=0.1)
-    ro, uo, vo, ut, vt = _observations(256, 100)
+    obs = [_observations(256, 100 * c) for c in (1, 2, 3)]
     whole = _whole(cfg)
-    with slab.SlabExperiment(cfg, world=2) as exp:
+    with slab.SlabExperiment(cfg, world=world) as exp:
         exp.init(0)
         _assert_own_rows_equal(whole, exp, "initial condition")
-        whole.update(0, 100)
-        exp.update(0, 100)
-        whole.assimilate(100, ro, uo, vo)
-        exp.assimilate(100, ro, uo, vo)
-        exp.sync()
-        assert whole.letkf_stats()["max_sweeps"] > 0
-        _assert_own_rows_equal(whole, exp, "one cycle")
-        assert exp.rmse_uv(ut, vt) == pytest.approx(whole.rmse_uv(ut, vt), rel=1e-12)
+        for c, (ro, uo, vo, ut, vt) in enumerate(obs):
+            t = 100 * c
+            whole.update(t, 100)
+            exp.update(t, 100)
+            whole.assimilate(t + 100, ro, uo, vo)
+            exp.assimilate(t + 100, ro, uo, vo)
+            exp.sync()
+            assert whole.letkf_stats()["max_sweeps"] > 0
+            _assert_own_rows_equal(whole, exp, f"cycle {c + 1}")
+            assert exp.rmse_uv(ut, vt) == pytest.approx(whole.rmse_uv(ut, vt), rel=1e-12)
     whole.close()
