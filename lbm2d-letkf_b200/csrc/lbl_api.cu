@@ -355,7 +355,7 @@ int launch_graph(lbl_ctx* ctx, int kind, int n) {
                                                cudaGetErrorString(le != cudaSuccess ? le : ee));
         }
         cudaGraphExec_t ge;
-        const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+        const cudaError_t ie = cudaGraphInstantiate(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(g);
         if (ie != cudaSuccess) return fail(ctx, LBL_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
         it = ctx->graphs.emplace(key, ge).first;
@@ -549,8 +549,13 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     ctx->P = derive_phys(*cfg);
     ctx->G = derive_geo(*cfg);
     LBL_TRY(set_device(ctx));
-    LBL_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-    LBL_CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    // the engine's stream at the device's highest priority, the side stream (the forcing beside
+    // the analysis) at its lowest: with node priorities kept in the graphs, the forcing fills the
+    // SMs the analysis leaves idle instead of competing with it
+    int prio_low = 0, prio_high = 0;
+    LBL_CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    LBL_CK(cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_high));
+    LBL_CK(cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, prio_low));
     LBL_CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
     LBL_CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
     const size_t nxy = size_t(ctx->P.nxy), M = size_t(ctx->P.M);
@@ -1897,7 +1902,7 @@ int batch_launch(lbl_batch* b, int t, const float* const* rho_o, const float* co
                                                    cudaGetErrorString(le != cudaSuccess ? le : ee));
         }
         cudaGraphExec_t ge;
-        const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+        const cudaError_t ie = cudaGraphInstantiate(&ge, g, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(g);
         if (ie != cudaSuccess) return batch_fail(b, LBL_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ie));
         it = b->graphs.emplace(key, ge).first;
