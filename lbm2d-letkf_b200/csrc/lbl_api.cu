@@ -337,7 +337,10 @@ int launch_graph(lbl_ctx* ctx, int kind, int n) {
             cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0);
             launch_force_chunk(ctx, n, 0, ctx->side);
             cudaEventRecord(ctx->join_ev, ctx->side);
-            cur = enqueue_analysis(ctx, cur, ctx->stream);
+            cudaStreamWaitEvent(ctx->hi, ctx->fork_ev, 0);
+            cur = enqueue_analysis(ctx, cur, ctx->hi);
+            cudaEventRecord(ctx->hi_ev, ctx->hi);
+            cudaStreamWaitEvent(ctx->stream, ctx->hi_ev, 0);
             cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0);
             cudaEventRecordWithFlags(ctx->ev[11], ctx->stream, cudaEventRecordExternal);
             enqueue_steps(ctx, n, cur, ctx->stream, true);
@@ -549,15 +552,19 @@ int create_impl(const lbl_config* cfg, int device, lbl_ctx* ctx) {
     ctx->P = derive_phys(*cfg);
     ctx->G = derive_geo(*cfg);
     LBL_TRY(set_device(ctx));
-    // the engine's stream at the device's highest priority, the side stream (the forcing beside
-    // the analysis) at its lowest: with node priorities kept in the graphs, the forcing fills the
-    // SMs the analysis leaves idle instead of competing with it
+    // The engine's and the side stream at the default priority; the cycle graph's analysis
+    // branch is captured on a stream at the device's highest priority and keeps it (node
+    // priorities), so the forcing beside it fills the SMs the analysis leaves idle instead of
+    // competing with it.  Only the analysis is raised: steps and forcing of contexts that
+    // share the GPU keep competing on equal terms.
     int prio_low = 0, prio_high = 0;
     LBL_CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
-    LBL_CK(cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_high));
-    LBL_CK(cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, prio_low));
+    LBL_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    LBL_CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    LBL_CK(cudaStreamCreateWithPriority(&ctx->hi, cudaStreamNonBlocking, prio_high));
     LBL_CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
     LBL_CK(cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming));
+    LBL_CK(cudaEventCreateWithFlags(&ctx->hi_ev, cudaEventDisableTiming));
     const size_t nxy = size_t(ctx->P.nxy), M = size_t(ctx->P.M);
     ctx->f16 = cfg->storage == LBL_STORAGE_F16;
     for (int b = 0; b < 2; b++) {
@@ -695,6 +702,8 @@ void destroy_impl(lbl_ctx* ctx) {
     if (ctx->out_ev) cudaEventDestroy(ctx->out_ev);
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
+    if (ctx->hi_ev) cudaEventDestroy(ctx->hi_ev);
+    if (ctx->hi) cudaStreamDestroy(ctx->hi);
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
 }

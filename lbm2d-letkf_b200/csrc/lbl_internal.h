@@ -76,7 +76,8 @@ struct lbl_ctx {
     std::string err;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;         // forcing branch of the cycle graph
-    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    cudaStream_t hi = nullptr;           // analysis branch of the cycle graph, at the highest priority
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr, hi_ev = nullptr;
 
     // ensemble state, double buffered like data::d()/dn() (data.h:45-64)
     float* f[2] = {nullptr, nullptr};    // [M][9][ny][nx] FP32 populations (LBL_STORAGE_F32)
